@@ -1,0 +1,371 @@
+"""Coarse-pass diff2 benchmark (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision bf16x3|tf32x3|tf32|fp32] [--config c2]
+
+Workload: the production coarse shape (128^3 blob reference, padding 2, coarse
+image 64 = 2112 half-plane pixels of which 1641 lie inside radius 32,
+HEALPix order 2 x 24 psi = 4608 orientations, 113 translations within radius
+6 px, 256 particles with per-particle CTF at SNR 0.05), synthetic and seeded.
+One step = one pass of the hot path over the 256-particle batch: projection
+of all orientations, phase-shift generation, norms, cross-term contraction,
+FP64 combine, diff2[p][o][t] store and per-particle min/argmin.
+Metric: diff2 evaluations per second (P*O*T per step), whole job.
+
+Multi-GPU: the path shards by particle with no exchange (replicas only); each
+rank scores its own 256 particles and rank 0 reports units of all ranks over
+the slowest rank's device time.
+
+--impl reference times the reference's CPU path.  The reference project has no
+CPU implementation of the coarse kernel, so this arm runs the C restatement of
+cuda_kernel_diff2_coarse (oracle/diff2_oracle.c, FP32, all host threads) on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "t2-relion-kernel_b200")
+METRIC = "diff2 evals/s (coarse pass)"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def load_package():
+    if "relion_b200" in sys.modules:
+        return sys.modules["relion_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "relion_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["relion_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_synth():
+    load_package()
+    import importlib
+    return importlib.import_module("relion_b200.synth")
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    c = [x.strip() for x in line.split(",")]
+                    if len(c) < 9:
+                        continue
+                    try:
+                        sm.append(float(c[1]))
+                        smax = float(c[2])
+                    except ValueError:
+                        continue
+                    for n, v in zip(names, c[5:9]):
+                        if v.lower() == "active":
+                            reasons.add(n)
+            os.unlink(self.path)
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (oracle FP32 port), bounded sample
+# ---------------------------------------------------------------------------
+def cpu_sample(pr, budget_s: float, max_particles: int | None = None) -> dict:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the checker's C restatement; measured here as the CPU baseline only
+    nthreads = os.cpu_count() or 1
+    op = oracle.projector_for(pr)
+    t0 = time.perf_counter()
+    done = 0
+    evals = 0
+    while True:
+        p = done % pr.P
+        oracle.diff2_coarse_f32(op, pr.eulers, pr.trans_x, pr.trans_y, pr.fimg_re[p], pr.fimg_im[p],
+                                pr.corr[p], nthreads=nthreads)
+        done += 1
+        evals += pr.O * pr.T
+        el = time.perf_counter() - t0
+        if el >= budget_s or (max_particles is not None and done >= max_particles):
+            break
+    return {"value": evals / el, "unit": "diff2 evals/s", "cores": nthreads, "kind": "port",
+            "sample": f"{done} particle(s) x {pr.O} orientations x {pr.T} translations of the same "
+                      f"workload, FP32 C restatement of cuda_kernel_diff2_coarse, {nthreads} threads, "
+                      f"{el:.1f} s"}
+
+
+# ---------------------------------------------------------------------------
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "tf32x3", "tf32", "fp32"])
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(n_gpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return rank, world, local, pg
+
+
+def reference_arm(args):
+    rank, world, local, _ = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0, None
+    if rank != 0:
+        return 0
+    synth = load_synth()
+    pr = synth.make_problem(args.config, seed=20251203)
+    per_step_particles = 2
+    # warm-up steps (untimed), then K timed steps, each a bounded sample
+    for _ in range(args.warmup):
+        cpu_sample(pr, 0.0, max_particles=1)
+    t0 = time.perf_counter()
+    evals = 0
+    for k in range(args.steps):
+        s = cpu_sample(pr, 0.0, max_particles=per_step_particles)
+        evals += per_step_particles * pr.O * pr.T
+    el = time.perf_counter() - t0
+    v = evals / el
+    cores = os.cpu_count() or 1
+    line = {"metric": METRIC, "value": v, "unit": "diff2 evals/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"{args.config}: {pr.P} particles x {pr.O} orientations x {pr.T} translations, "
+                                   f"image {pr.img_size} ({pr.N_img} px); each step = {per_step_particles} "
+                                   f"particles (bounded CPU sample)", "particles_per_step": per_step_particles},
+            "cpu_baseline": {"value": v, "unit": "diff2 evals/s", "cores": cores, "kind": "port",
+                             "sample": s["sample"]},
+            "e2e": {"value": v, "unit": "diff2 evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+PREC = {"fp32": 0, "tf32": 1, "tf32x3": 2, "bf16x3": 3}
+
+
+def ours_arm(args):
+    import torch
+    rank, world, local, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    pkg = load_package()
+    synth = load_synth()
+    pr = synth.make_problem(args.config, seed=20251203 + rank)
+    prec = PREC[args.precision]
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    P, O, T, N = pr.P, pr.O, pr.T, pr.N_img
+    x, y = synth.pixel_coords(pr.imgX, pr.imgY, view.maxR)
+    K_c = int(((x.astype(float) ** 2 + y.astype(float) ** 2) * view.padding_factor ** 2 <= view.maxR2_padded).sum())
+
+    eul = torch.as_tensor(pr.eulers.reshape(-1), device=dev)
+    tx = torch.as_tensor(pr.trans_x, device=dev)
+    ty = torch.as_tensor(pr.trans_y, device=dev)
+    re = torch.as_tensor(pr.fimg_re, device=dev)
+    im = torch.as_tensor(pr.fimg_im, device=dev)
+    corr = torch.as_tensor(pr.corr, device=dev)
+    out = torch.empty(P * O * T, device=dev, dtype=torch.float32)
+    mn = torch.empty(P, device=dev, dtype=torch.float64)
+    am = torch.empty(P, device=dev, dtype=torch.int64)
+    flush = torch.empty(2 * L2_BYTES // 4, device=dev, dtype=torch.float32)
+    batch = pkg.make_batch(eul, tx, ty, re, im, corr, out, O=O, T=T, P=P, N_img=N, out_min=mn, out_argmin=am)
+    wsb = pkg.batch_workspace_bytes(view, batch, prec)
+    ws = torch.empty(max(wsb, 16), device=dev, dtype=torch.uint8)
+
+    def step():
+        pkg.diff2_coarse_batch(view, batch, prec, ws, stream)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- timed region: K steps, L2 flushed before each, events per step ----
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = pkg.launch_count()
+    for k in range(args.steps):
+        flush.zero_()
+        evs[k][0].record(stream)
+        step()
+        evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    l1 = pkg.launch_count()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    evals_step = P * O * T
+    value = world * evals_step * args.steps / (total_ms / 1e3)
+
+    # ---- dominant kernel timing (events on the launching stream) ----
+    kern = pkg.kernel_breakdown(view, batch, prec, ws, stream, reps=3) if hasattr(pkg, "kernel_breakdown") else {}
+
+    # ---- end to end through the public API with host buffers ----
+    h_re = torch.empty_like(re, device="cpu").pin_memory()
+    h_im = torch.empty_like(im, device="cpu").pin_memory()
+    h_corr = torch.empty_like(corr, device="cpu").pin_memory()
+    h_re.copy_(torch.as_tensor(pr.fimg_re))
+    h_im.copy_(torch.as_tensor(pr.fimg_im))
+    h_corr.copy_(torch.as_tensor(pr.corr))
+    h_mn = torch.empty(P, dtype=torch.float64).pin_memory()
+    h_am = torch.empty(P, dtype=torch.int64).pin_memory()
+    e2e_steps = max(3, min(args.steps, 10))
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        re.copy_(h_re, non_blocking=True)
+        im.copy_(h_im, non_blocking=True)
+        corr.copy_(h_corr, non_blocking=True)
+        step()
+        h_mn.copy_(mn, non_blocking=True)
+        h_am.copy_(am, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_val = world * evals_step * e2e_steps / (e2e_ms / 1e3)
+    h2d = 3 * P * N * 4
+    d2h = P * (8 + 8)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(pr, args.cpu_budget)
+
+    peaks, peak_src = measured_peaks()
+    roof = None
+    flops_per_launch = evals_step * 4.0 * K_c
+    if kern.get("dominant_ms"):
+        if prec == 0:
+            # FP32 CUDA-core kernel: no driver-measured FP32 peak exists; report
+            # against the nominal FP32 rate (148 SMs x 128 lanes x 2 x max clock)
+            smax = (clk.get("sm_max_mhz") or 1965.0) * 1e6
+            peak = 148 * 128 * 2 * smax / 1e12
+            roof = {"bound": "fp32-cuda-core", "achieved": flops_per_launch / (kern["dominant_ms"] / 1e3) / 1e12,
+                    "peak": peak, "unit": "TFLOP/s", "peak_source": "nominal FP32 at max SM clock"}
+        else:
+            peak = float(peaks.get("bf16_tflops_sustained", 1400.0))
+            if prec in (1, 2):
+                peak = peak / 2.0  # TF32 tensor rate is half the BF16 rate
+            roof = {"bound": "tensor", "achieved": flops_per_launch / (kern["dominant_ms"] / 1e3) / 1e12,
+                    "peak": peak, "unit": "TFLOP/s",
+                    "peak_source": f"{peak_src} bf16_tflops_sustained" + (" / 2 (tf32 rate)" if prec in (1, 2) else "")}
+        roof["frac"] = roof["achieved"] / roof["peak"]
+        roof["traffic"] = kern.get("traffic")
+        roof["kernel"] = kern.get("dominant")
+        roof["algorithmic"] = f"{evals_step} evals x 4*K_c ({K_c}) flops = {flops_per_launch:.4g} flop per launch"
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "diff2 evals/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": {"fp32": "f32", "tf32": "tf32", "tf32x3": "tf32x3", "bf16x3": "bf16x3"}[args.precision],
+                "data": "synthetic (seeded blob reference, HEALPix grid, CTF, Gaussian noise)",
+                "config": {"workload": f"{args.config}: {P} particles x {O} orientations x {T} translations, "
+                                       f"image {pr.img_size} ({N} px, {K_c} in radius)",
+                           "precision": args.precision, "particles": P, "orientations": O, "translations": T,
+                           "pixels_in_radius": K_c, "l2": "flushed (256 MB write) before every timed step",
+                           "parallelism": f"replicas x{world}"},
+                "roofline": roof, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_val, "unit": "diff2 evals/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h,
+                        "note": "H2D of images+corr from pinned memory, batch call, D2H of per-particle min/argmin"},
+                "clocks": clk, "gpu_launches": int(l1 - l0), "kernels": kern.get("per_kernel_ms")}
+        print(json.dumps(line), flush=True)
+    proj.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return ours_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

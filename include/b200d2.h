@@ -1,0 +1,196 @@
+/*
+ * b200d2.h -- C ABI of the B200 coarse-pass diff2 library (libb200d2.so).
+ *
+ * RELION's coarse expectation step scores every particle image against every
+ * projected reference orientation at every trial translation:
+ *
+ *   diff2[p][o][t] = sum_px  corr_p(px)/2 * | proj_o(px) - shift_t(img_p)(px) |^2
+ *
+ * This header is the drop-in boundary that replaces the reference harness's
+ * C++ entry points (Edgarrrrrr/T2-RELION-kernel; file:line given per entry).
+ * All pointers named d_* are device pointers; h_* are host pointers.  Every
+ * call returns a b200d2_status (0 = success) instead of raising SIGSEGV as the
+ * reference's HANDLE_ERROR does (src/common.h:20-36).  Calls taking a stream
+ * are asynchronous on that stream and do no host synchronisation.
+ */
+#ifndef B200D2_H_
+#define B200D2_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum b200d2_status {
+  B200D2_OK = 0,
+  B200D2_ERR_INVALID = 1,     /* bad argument / shape */
+  B200D2_ERR_UNSUPPORTED = 2, /* configuration outside the supported path */
+  B200D2_ERR_CUDA = 3,        /* CUDA runtime error */
+  B200D2_ERR_OOM = 4,         /* device allocation failed */
+  B200D2_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+  B200D2_ERR_NO_DEVICE = 6    /* no usable sm_100 device */
+} b200d2_status;
+
+/* How the projector volume is interpolated. */
+enum {
+  /* cudaArray + cudaFilterModeLinear texture, clamp, unnormalised
+   * coordinates: the reference's default (src/acc_projector_impl.h:40-107). */
+  B200D2_INTERP_TEXTURE = 0,
+  /* linear device arrays + software trilinear with exact FP32 weights: the
+   * reference's PROJECTOR_NO_TEXTURES path (src/acc_projector_impl.h:109-116,
+   * src/cuda_device_utils.cuh:73-108). */
+  B200D2_INTERP_LINEAR = 1
+};
+
+/* Precision of the cross term in the tensor-core path. */
+enum {
+  B200D2_PREC_FP32 = 0,    /* plain FP32 CUDA-core kernel (the drop-in) */
+  B200D2_PREC_TF32 = 1,    /* one TF32 product, FP32 accumulation in TMEM */
+  B200D2_PREC_TF32X3 = 2,  /* hi*hi + hi*lo + lo*hi TF32 split */
+  B200D2_PREC_BF16X3 = 3,  /* hi*hi + hi*lo + lo*hi BF16 split */
+  B200D2_PREC_FP64 = 4     /* FP64 CUDA-core kernel (GPU oracle) */
+};
+
+/*
+ * Kernel-side projector view, passed by value to kernels.  Mirrors
+ * AccProjectorKernel (src/acc_projectorkernel_impl.h:15-60): same field names
+ * and meaning, plus the texture handles and the linear arrays.
+ */
+typedef struct b200d2_view {
+  int mdlX, mdlXY, mdlZ;
+  int imgX, imgY, imgZ;
+  int mdlInitY, mdlInitZ;
+  int maxR, maxR2, maxR2_padded;
+  float padding_factor;
+  unsigned long long tex_re; /* cudaTextureObject_t, 0 if absent */
+  unsigned long long tex_im;
+  const float* lin_re; /* device [mdlZ][mdlY][mdlX], NULL if absent */
+  const float* lin_im;
+  int interp; /* B200D2_INTERP_* used by kernels taking this view */
+} b200d2_view;
+
+typedef struct b200d2_projector b200d2_projector; /* opaque, owns device memory */
+
+/* ------------------------------------------------------------------------
+ * Projector (replaces AccProjector::setMdlDim + initMdl,
+ * src/acc_projector_impl.h:10-216, and constructFromFile :300-356)
+ * ---------------------------------------------------------------------- */
+
+/* Upload a padded Hermitian-half Fourier volume [mdlZ][mdlY][mdlX] (x fastest)
+ * from host memory.  use_texture: 1 = texture objects only, 0 = linear arrays
+ * only, 2 = both.  Only 3D references (mdlZ > 1) are supported. */
+int b200d2_projector_create(int mdlX, int mdlY, int mdlZ, int mdlInitY,
+                            int mdlInitZ, int mdlMaxR, float padding_factor,
+                            const float* h_real, const float* h_imag,
+                            int use_texture, b200d2_projector** out);
+
+/* Load the reference harness's projector_proc_*.dat format
+ * (src/acc_projector_impl.h:300-356). */
+int b200d2_projector_load_dat(const char* path, int use_texture,
+                              b200d2_projector** out);
+
+/* Free all device memory of the projector (AccProjector::clear). */
+int b200d2_projector_destroy(b200d2_projector* p);
+
+/* Model geometry: dims[0..5] = mdlX, mdlY, mdlZ, mdlInitY, mdlInitZ, mdlMaxR. */
+int b200d2_projector_dims(const b200d2_projector* p, int* dims, float* pf);
+
+/* AccProjectorKernel::makeKernel (src/acc_projectorkernel_impl.h:410-433):
+ * maxR = min(mdlMaxR, imgMaxR), maxR2 = maxR^2,
+ * maxR2_padded = int(maxR^2 * pf * pf).  interp selects the projection path
+ * (the projector must hold the matching representation). */
+int b200d2_projector_view(const b200d2_projector* p, int imgX, int imgY,
+                          int imgZ, int imgMaxR, int interp, b200d2_view* out);
+
+/* ------------------------------------------------------------------------
+ * Single-particle drop-in (replaces runDiff2KernelCoarse,
+ * src/acc_helper_functions_impl.h:15-499, non-CC 3D-reference 2D-image branch)
+ *
+ * d_diff2s[o*T + t] += diff2(o, t), accumulating onto the caller's buffer
+ * exactly as the reference does (src/diff2.cuh:533-536).  d_eulers holds 9
+ * floats per orientation (row-major 3x3); image arrays hold N_img half-plane
+ * pixels in pixel_index2coor order.  corr must be >= 0.
+ * precision: B200D2_PREC_FP32 (FP32 CUDA cores).
+ * ---------------------------------------------------------------------- */
+int b200d2_diff2_coarse(const b200d2_view* view, const float* d_trans_x,
+                        const float* d_trans_y, const float* d_corr,
+                        const float* d_real, const float* d_imag,
+                        const float* d_eulers, float* d_diff2s, size_t O,
+                        size_t T, size_t N_img, void* stream, int precision);
+
+/* FP64 variant (replaces runDiff2KernelCoarseDouble,
+ * src/acc_helper_functions_impl.h:503-854): double arithmetic for the phase
+ * shift, the differences and the sum; projections are the same FP32
+ * interpolated samples.  filter_img zeroes image pixels outside the radius as
+ * the reference's filter_img flag does (src/diff2.cuh:339-345). */
+int b200d2_diff2_coarse_f64(const b200d2_view* view, const float* d_trans_x,
+                            const float* d_trans_y, const float* d_corr,
+                            const float* d_real, const float* d_imag,
+                            const float* d_eulers, double* d_diff2s, size_t O,
+                            size_t T, size_t N_img, int filter_img,
+                            void* stream);
+
+/* ------------------------------------------------------------------------
+ * Batched coarse pass (north-star layout diff2[p][o][t]).  The reference
+ * launches one runDiff2KernelCoarse per particle (src/main.cu:483-503); this
+ * call scores P particles that share the orientation and translation sets in
+ * one pass.  Image p lives at d_real/d_imag/d_corr + p * img_stride.
+ * ---------------------------------------------------------------------- */
+typedef struct b200d2_batch {
+  const float* d_eulers; /* [O][9] */
+  int O;
+  const float* d_trans_x; /* [T] phase slopes (RELION: -2*pi*shift/ori_size) */
+  const float* d_trans_y;
+  int T;
+  int P;
+  int N_img;
+  const float* d_real; /* [P][img_stride] CTF-folded image (RELION Fimg) */
+  const float* d_imag;
+  const float* d_corr; /* [P][img_stride] Minvsigma2 * CTF^2 (>= 0) */
+  long long img_stride;
+  float* d_diff2;      /* [P][O][T] */
+  int accumulate;      /* 1: d_diff2 += diff2 (drop-in), 0: d_diff2 = diff2 */
+  double* d_min;       /* optional [P]: per-particle minimum diff2 */
+  long long* d_argmin; /* optional [P]: o*T + t of that minimum (lowest index on ties) */
+} b200d2_batch;
+
+/* Bytes of device scratch the batch needs for `precision` (0 for the
+ * CUDA-core paths). */
+size_t b200d2_diff2_coarse_batch_workspace(const b200d2_view* view,
+                                           const b200d2_batch* batch,
+                                           int precision);
+
+/* Run the batch.  precision: B200D2_PREC_FP32 (CUDA cores) or one of the
+ * tensor-core forms.  d_workspace must hold the bytes reported above. */
+int b200d2_diff2_coarse_batch(const b200d2_view* view, const b200d2_batch* batch,
+                              int precision, void* d_workspace,
+                              size_t workspace_bytes, void* stream);
+
+/* Per-particle minimum and its index over d_diff2[p][0 .. n) (FP64 min,
+ * lowest index on ties).  Used by the CUDA-core path; fused into the
+ * tensor-core epilogue. */
+int b200d2_minloc(const float* d_diff2, long long n, int P, double* d_min,
+                  long long* d_argmin, void* stream);
+
+/* Run a single stage of the batch pipeline, so that a caller can time one
+ * kernel with events on its stream.  Stages are numbered in pipeline order
+ * from 0; b200d2_stage_name returns NULL past the last stage of `precision`.
+ * Running every stage in order is equivalent to b200d2_diff2_coarse_batch
+ * with accumulate = 1. */
+int b200d2_diff2_coarse_batch_stage(const b200d2_view* view,
+                                    const b200d2_batch* batch, int precision,
+                                    int stage, void* d_workspace,
+                                    size_t workspace_bytes, void* stream);
+const char* b200d2_stage_name(int precision, int stage);
+
+/* Number of kernels this library has launched in the process so far (all
+ * entry points, all devices).  Lets a caller count launches in a region. */
+unsigned long long b200d2_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200D2_H_ */

@@ -1,0 +1,194 @@
+"""ctypes front end of the C oracle (oracle/diff2_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py as the checker.  The product library never
+imports this module.
+
+Also exposes, when present, the reference project's own CUDA kernels compiled
+into oracle/_ref/libref_diff2.so (see oracle/ref_shim.cu) for GPU-side
+parity tests.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libref_diff2.so")
+
+INTERP_EXACT = 0
+INTERP_TEX_ROUND = 1
+INTERP_TEX_TRUNC = 2
+
+
+class OrcProjector(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("mdlX", "mdlY", "mdlZ", "mdlInitY", "mdlInitZ", "mdlMaxR")] + [
+        ("padding_factor", C.c_float)] + [
+        (n, C.c_int) for n in ("imgX", "imgY", "imgZ", "maxR", "maxR2", "maxR2_padded")] + [
+        ("re", C.c_void_p), ("im", C.c_void_p)]
+
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE, os.path.join(HERE, "liboracle.so")], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        L.orc_projector_init.argtypes = [C.POINTER(OrcProjector)] + [C.c_int] * 6 + [C.c_float, P, P] + [C.c_int] * 4
+        L.orc_project_pixels.argtypes = [C.POINTER(OrcProjector), P, C.c_long, P, P, C.c_long, C.c_int, P, P, C.c_int]
+        L.orc_diff2_coarse_f64.argtypes = [C.POINTER(OrcProjector), P, C.c_long, P, P, C.c_long, P, P, P,
+                                           C.c_long, C.c_int, P, C.c_int]
+        L.orc_diff2_coarse_f32.argtypes = [C.POINTER(OrcProjector), P, C.c_long, P, P, C.c_long, P, P, P,
+                                           C.c_long, P, C.c_int]
+        L.orc_filter_image.argtypes = [C.POINTER(OrcProjector), P, P, P, C.c_long, P, P, P, P]
+        L.orc_filter_image.restype = C.c_long
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Projector:
+    """Oracle-side projector: keeps the volume arrays alive for the C struct."""
+
+    def __init__(self, pv, imgX: int, imgY: int, imgMaxR: int, imgZ: int = 1):
+        self.re = np.ascontiguousarray(pv.re, dtype=np.float32)
+        self.im = np.ascontiguousarray(pv.im, dtype=np.float32)
+        self.s = OrcProjector()
+        lib().orc_projector_init(C.byref(self.s), pv.mdlX, pv.mdlY, pv.mdlZ, pv.mdlInitY, pv.mdlInitZ,
+                                 pv.mdlMaxR, pv.padding_factor, _p(self.re), _p(self.im),
+                                 imgX, imgY, imgZ, imgMaxR)
+
+    @property
+    def maxR(self) -> int:
+        return self.s.maxR
+
+    @property
+    def maxR2_padded(self) -> int:
+        return self.s.maxR2_padded
+
+
+def projector_for(prob) -> Projector:
+    return Projector(prob.projector, prob.imgX, prob.imgY, prob.imgMaxR)
+
+
+def project_pixels(proj: Projector, eulers: np.ndarray, px: np.ndarray, py: np.ndarray,
+                   mode: int = INTERP_TEX_ROUND, nthreads: int = 0):
+    eulers = np.ascontiguousarray(eulers, np.float32)
+    px = np.ascontiguousarray(px, np.int32)
+    py = np.ascontiguousarray(py, np.int32)
+    O, K = eulers.shape[0], px.size
+    re = np.zeros((O, K), np.float64)
+    im = np.zeros((O, K), np.float64)
+    lib().orc_project_pixels(C.byref(proj.s), _p(eulers), O, _p(px), _p(py), K, mode, _p(re), _p(im), nthreads)
+    return re, im
+
+
+def diff2_coarse_f64(proj: Projector, eulers, trans_x, trans_y, fre, fim, corr,
+                     mode: int = INTERP_TEX_ROUND, diff2_init=None, nthreads: int = 0) -> np.ndarray:
+    """FP64 restatement of cuda_kernel_diff2_coarse for one particle -> [O, T]."""
+    eulers = np.ascontiguousarray(eulers, np.float32)
+    tx = np.ascontiguousarray(trans_x, np.float32)
+    ty = np.ascontiguousarray(trans_y, np.float32)
+    fre = np.ascontiguousarray(fre, np.float32)
+    fim = np.ascontiguousarray(fim, np.float32)
+    corr = np.ascontiguousarray(corr, np.float32)
+    O, T, N = eulers.shape[0], tx.size, fre.size
+    out = np.zeros((O, T), np.float64) if diff2_init is None else np.array(diff2_init, np.float64).reshape(O, T)
+    lib().orc_diff2_coarse_f64(C.byref(proj.s), _p(eulers), O, _p(tx), _p(ty), T, _p(fre), _p(fim), _p(corr),
+                               N, mode, _p(out), nthreads)
+    return out
+
+
+def diff2_coarse_f32(proj: Projector, eulers, trans_x, trans_y, fre, fim, corr,
+                     diff2_init=None, nthreads: int = 0) -> np.ndarray:
+    """FP32 port of cuda_kernel_diff2_coarse (the CPU baseline) -> [O, T] float32."""
+    eulers = np.ascontiguousarray(eulers, np.float32)
+    tx = np.ascontiguousarray(trans_x, np.float32)
+    ty = np.ascontiguousarray(trans_y, np.float32)
+    fre = np.ascontiguousarray(fre, np.float32)
+    fim = np.ascontiguousarray(fim, np.float32)
+    corr = np.ascontiguousarray(corr, np.float32)
+    O, T, N = eulers.shape[0], tx.size, fre.size
+    out = np.zeros((O, T), np.float32) if diff2_init is None else np.array(diff2_init, np.float32).reshape(O, T)
+    lib().orc_diff2_coarse_f32(C.byref(proj.s), _p(eulers), O, _p(tx), _p(ty), T, _p(fre), _p(fim), _p(corr),
+                               N, _p(out), nthreads)
+    return out
+
+
+def filter_image(proj: Projector, fre, fim, corr):
+    """FilterCoarseParamImage restatement -> (re, im, corr, coor_xy, n_inside)."""
+    N = fre.size
+    fre = np.ascontiguousarray(fre, np.float32)
+    fim = np.ascontiguousarray(fim, np.float32)
+    corr = np.ascontiguousarray(corr, np.float32)
+    ore, oim, oc = np.zeros(N, np.float32), np.zeros(N, np.float32), np.zeros(N, np.float32)
+    oxy = np.zeros(2 * N, np.float32)
+    n = lib().orc_filter_image(C.byref(proj.s), _p(fre), _p(fim), _p(corr), N, _p(ore), _p(oim), _p(oc), _p(oxy))
+    return ore, oim, oc, oxy, int(n)
+
+
+# --------------------------------------------------------------------------
+# error statistics (restatement of ErrorComparator / check_array_equal,
+# reference src/check.cuh:11-148: |ref| <= 1e-12 skipped for relative error)
+# --------------------------------------------------------------------------
+def error_stats(test: np.ndarray, ref: np.ndarray) -> dict:
+    a = np.asarray(test, np.float64).ravel()
+    b = np.asarray(ref, np.float64).ravel()
+    ae = np.abs(a - b)
+    m = np.abs(b) > 1e-12
+    re = ae[m] / np.abs(b[m])
+    return dict(count=int(a.size), count_rel=int(m.sum()),
+                sum_abs=float(ae.sum()), max_abs=float(ae.max(initial=0.0)),
+                avg_abs=float(ae.mean()) if a.size else 0.0,
+                sum_rel=float(re.sum()), max_rel=float(re.max(initial=0.0)),
+                avg_rel=float(re.mean()) if re.size else 0.0)
+
+
+def weights_from_diff2(d: np.ndarray) -> tuple[float, np.ndarray]:
+    """Per-particle minimum and normalised exp(-(diff2 - min)) weights in FP64."""
+    d = np.asarray(d, np.float64).ravel()
+    mn = float(d.min())
+    w = np.exp(-(d - mn))
+    return mn, w / w.sum()
+
+
+# --------------------------------------------------------------------------
+# the reference project's own kernels (GPU), compiled into oracle/_ref
+# --------------------------------------------------------------------------
+_ref = None
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_PATH)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        L = C.CDLL(REF_PATH)
+        P = C.c_void_p
+        L.refshim_projector_create.argtypes = [C.c_int] * 6 + [C.c_float, P, P]
+        L.refshim_projector_create.restype = P
+        L.refshim_projector_destroy.argtypes = [P]
+        L.refshim_diff2_coarse.argtypes = [P] + [C.c_int] * 4 + [P] * 7 + [C.c_long] * 3 + [P]
+        L.refshim_diff2_coarse_double.argtypes = [P] + [C.c_int] * 4 + [P] * 7 + [C.c_long] * 3 + [C.c_int, P]
+        L.refshim_variant_workspace_bytes.argtypes = [C.c_int] * 6
+        L.refshim_variant_workspace_bytes.restype = C.c_size_t
+        L.refshim_variant_run.argtypes = [C.c_int, P] + [C.c_int] * 4 + [P] * 9 + [C.c_int] * 5 + [P]
+        _ref = L
+    return _ref

@@ -1,0 +1,158 @@
+// ref_shim.cu -- C entry points around the reference project's own CUDA code.
+//
+// TEST INFRASTRUCTURE ONLY.  This translation unit is compiled by
+// oracle/Makefile against the reference sources where they lie
+// (Edgarrrrrr/T2-RELION-kernel, src/*.cuh / src/*.h) into oracle/_ref/.  It
+// contains no reference code itself: it includes the reference headers and
+// exposes their entry points with plain C signatures so that the parity tests
+// can run the reference kernels on the same device buffers as this
+// repository's kernels.  Nothing in the product links or loads it.
+//
+// Wrapped entry points (reference file:line):
+//   AccProjector::setMdlDim / initMdl         src/acc_projector_impl.h:10-216
+//   AccProjectorKernel::makeKernel            src/acc_projectorkernel_impl.h:410-433
+//   runDiff2KernelCoarse                      src/acc_helper_functions_impl.h:15-499
+//   runDiff2KernelCoarseDouble                src/acc_helper_functions_impl.h:503-854
+//   CoarseMatrixKernel*::run (5 variants)     src/coarse_splitImg_*.cuh
+#include <cuda_runtime.h>
+
+// standard headers the reference headers expect to be included first
+#include <algorithm>
+#include <cstdint>
+#include <fstream>
+#include <iostream>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "acc_helper_functions_impl.h"
+#include "acc_projector.h"
+#include "acc_projector_impl.h"
+#include "acc_projectorkernel_impl.h"
+#include "coarse_kernel.cuh"
+#include "diff2.cuh"
+
+namespace {
+struct RefProjector {
+  AccProjector proj;
+  int mdlX, mdlY, mdlZ;
+};
+
+AccProjectorKernel make_view(RefProjector* p, int imgX, int imgY, int imgZ,
+                             int imgMaxR) {
+  return AccProjectorKernel::makeKernel(p->proj, imgX, imgY, imgZ, imgMaxR);
+}
+}  // namespace
+
+extern "C" {
+
+int refshim_abi_version(void) { return 2; }
+
+void* refshim_projector_create(int mdlX, int mdlY, int mdlZ, int initY,
+                               int initZ, int maxR, float pf, const float* re,
+                               const float* im) {
+  RefProjector* p = new RefProjector();
+  p->mdlX = mdlX;
+  p->mdlY = mdlY;
+  p->mdlZ = mdlZ;
+  p->proj.setMdlDim(mdlX, mdlY, mdlZ, initY, initZ, maxR, pf);
+  p->proj.initMdl(const_cast<float*>(re), const_cast<float*>(im));
+  if (cudaDeviceSynchronize() != cudaSuccess) return nullptr;
+  return p;
+}
+
+void refshim_projector_destroy(void* h) {
+  delete reinterpret_cast<RefProjector*>(h);
+}
+
+int refshim_diff2_coarse(void* h, int imgX, int imgY, int imgZ, int imgMaxR,
+                         float* d_eulers, float* d_tx, float* d_ty,
+                         float* d_corr, float* d_re, float* d_im,
+                         float* d_diff2s, long O, long T, long N_img,
+                         void* stream) {
+  RefProjector* p = reinterpret_cast<RefProjector*>(h);
+  AccProjectorKernel k = make_view(p, imgX, imgY, imgZ, imgMaxR);
+  runDiff2KernelCoarse(k, d_tx, d_ty, nullptr, d_corr, d_re, d_im, d_eulers,
+                       d_diff2s, 1.f, (unsigned long)O, (unsigned long)T,
+                       (unsigned long)N_img, (cudaStream_t)stream, false,
+                       false);
+  return (int)cudaGetLastError();
+}
+
+int refshim_diff2_coarse_double(void* h, int imgX, int imgY, int imgZ,
+                                int imgMaxR, float* d_eulers, float* d_tx,
+                                float* d_ty, float* d_corr, float* d_re,
+                                float* d_im, double* d_diff2s, long O, long T,
+                                long N_img, int filter_img, void* stream) {
+  RefProjector* p = reinterpret_cast<RefProjector*>(h);
+  AccProjectorKernel k = make_view(p, imgX, imgY, imgZ, imgMaxR);
+  runDiff2KernelCoarseDouble(k, d_tx, d_ty, nullptr, d_corr, d_re, d_im,
+                             d_eulers, d_diff2s, 1.f, (unsigned long)O,
+                             (unsigned long)T, (unsigned long)N_img,
+                             (cudaStream_t)stream, false, false,
+                             filter_img != 0);
+  return (int)cudaGetLastError();
+}
+
+// variant: 0 cuda-core im2col, 1 tensor-core im2col, 2 + conflict removal,
+// 3 + texture-fetch masking (filtered image), 4 + cross-CTA translation reuse
+// (filtered image, workspace).  Constructor arguments follow the functors'
+// declared meaning (T, O, image_size, full_image_size, sm_num); the harness at
+// src/main.cu:399-411 passes sm_num into full_image_size for variants 0-2.
+size_t refshim_variant_workspace_bytes(int variant, int T, int O, int K_filtered,
+                                       int N_img, int sm_num) {
+  if (variant == 4) {
+    CoarseMatrixKernelIm2colSplitImgBCFProjOverlapTransDBNfuse<> k(
+        T, O, K_filtered, N_img, sm_num);
+    return k.get_workspace_size_bytes();
+  }
+  return 0;
+}
+
+int refshim_variant_run(int variant, void* h, int imgX, int imgY, int imgZ,
+                        int imgMaxR, float* d_eulers, float* d_tx, float* d_ty,
+                        float* d_re, float* d_im, float* d_corr,
+                        float* d_diff2s, float* d_coor_xy,
+                        unsigned int* d_workspace, int T, int O, int K_filtered,
+                        int N_img, int sm_num, void* stream) {
+  RefProjector* p = reinterpret_cast<RefProjector*>(h);
+  AccProjectorKernel k = make_view(p, imgX, imgY, imgZ, imgMaxR);
+  cudaStream_t s = (cudaStream_t)stream;
+  switch (variant) {
+    case 0: {
+      CoarseMatrixKernelCudaCoreIm2colSplitImgNfuse<> f(T, O, N_img, 0, sm_num);
+      f.run(d_eulers, d_tx, d_ty, d_re, d_im, k, d_corr, d_diff2s, d_diff2s, s);
+      break;
+    }
+    case 1: {
+      CoarseMatrixKernelIm2colSplitImgNfuse<> f(T, O, N_img, 0, sm_num);
+      f.run(d_eulers, d_tx, d_ty, d_re, d_im, k, d_corr, d_diff2s, d_diff2s, s);
+      break;
+    }
+    case 2: {
+      CoarseMatrixKernelIm2colSplitImgBCFNfuse<> f(T, O, N_img, 0, sm_num);
+      f.run(d_eulers, d_tx, d_ty, d_re, d_im, k, d_corr, d_diff2s, d_diff2s, s);
+      break;
+    }
+    case 3: {
+      CoarseMatrixKernelIm2colSplitImgBCFProjOverlapNfuse<> f(
+          T, O, K_filtered, N_img, sm_num);
+      f.run(d_eulers, d_tx, d_ty, d_re, d_im, k, d_corr, d_diff2s, d_diff2s, s,
+            d_coor_xy);
+      break;
+    }
+    case 4: {
+      CoarseMatrixKernelIm2colSplitImgBCFProjOverlapTransDBNfuse<> f(
+          T, O, K_filtered, N_img, sm_num);
+      f.run(d_eulers, d_tx, d_ty, d_re, d_im, k, d_corr, d_diff2s, d_diff2s, s,
+            d_coor_xy, d_workspace);
+      break;
+    }
+    default:
+      return -1;
+  }
+  return (int)cudaGetLastError();
+}
+
+}  // extern "C"

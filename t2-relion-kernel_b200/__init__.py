@@ -1,0 +1,275 @@
+"""Python mirror of the coarse-pass diff2 C ABI (include/b200d2.h).
+
+The compute path is libb200d2.so (hand-written CUDA for sm_100a); this module
+only binds it with ctypes and converts torch tensors to device pointers.  There
+is no CPU fallback: importing works without a GPU, but every compute call needs
+the library and a CUDA device and raises B200D2Error otherwise.
+
+Names follow the reference harness (Edgarrrrrr/T2-RELION-kernel):
+`Projector` is AccProjector (src/acc_projector.h), `Projector.view()` is
+AccProjectorKernel::makeKernel (src/acc_projectorkernel_impl.h:410),
+`run_diff2_kernel_coarse` is runDiff2KernelCoarse
+(src/acc_helper_functions_impl.h:15) and `run_diff2_kernel_coarse_double` is
+runDiff2KernelCoarseDouble (src/acc_helper_functions_impl.h:503).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libb200d2.so")
+
+INTERP_TEXTURE = 0
+INTERP_LINEAR = 1
+PREC_FP32 = 0
+PREC_TF32 = 1
+PREC_TF32X3 = 2
+PREC_BF16X3 = 3
+PREC_FP64 = 4
+
+_STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: "out of memory",
+           5: "device wait timed out", 6: "no device"}
+
+
+class B200D2Error(RuntimeError):
+    def __init__(self, code: int, where: str):
+        super().__init__(f"{where}: {_STATUS.get(code, 'status %d' % code)} ({code})")
+        self.code = code
+
+
+class View(C.Structure):
+    """b200d2_view: kernel-side projector view (mirrors AccProjectorKernel)."""
+
+    _fields_ = [(n, C.c_int) for n in ("mdlX", "mdlXY", "mdlZ", "imgX", "imgY", "imgZ", "mdlInitY",
+                                         "mdlInitZ", "maxR", "maxR2", "maxR2_padded")] + [
+        ("padding_factor", C.c_float), ("tex_re", C.c_ulonglong), ("tex_im", C.c_ulonglong),
+        ("lin_re", C.c_void_p), ("lin_im", C.c_void_p), ("interp", C.c_int)]
+
+
+class Batch(C.Structure):
+    """b200d2_batch: P particles sharing orientations and translations."""
+
+    _fields_ = [("d_eulers", C.c_void_p), ("O", C.c_int), ("d_trans_x", C.c_void_p), ("d_trans_y", C.c_void_p),
+                ("T", C.c_int), ("P", C.c_int), ("N_img", C.c_int), ("d_real", C.c_void_p),
+                ("d_imag", C.c_void_p), ("d_corr", C.c_void_p), ("img_stride", C.c_longlong),
+                ("d_diff2", C.c_void_p), ("accumulate", C.c_int), ("d_min", C.c_void_p),
+                ("d_argmin", C.c_void_p)]
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def lib():
+    """Load libb200d2.so (fails loudly if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise B200D2Error(6, f"libb200d2.so not built ({LIB_PATH}); run t2-relion-kernel_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def _declare(L):
+    P, I, F, Z = C.c_void_p, C.c_int, C.c_float, C.c_size_t
+    sig = {
+        "b200d2_projector_create": [I, I, I, I, I, I, F, P, P, I, C.POINTER(P)],
+        "b200d2_projector_load_dat": [C.c_char_p, I, C.POINTER(P)],
+        "b200d2_projector_destroy": [P],
+        "b200d2_projector_dims": [P, P, P],
+        "b200d2_projector_view": [P, I, I, I, I, I, C.POINTER(View)],
+        "b200d2_diff2_coarse": [C.POINTER(View), P, P, P, P, P, P, P, Z, Z, Z, P, I],
+        "b200d2_diff2_coarse_f64": [C.POINTER(View), P, P, P, P, P, P, P, Z, Z, Z, I, P],
+        "b200d2_diff2_coarse_batch": [C.POINTER(View), C.POINTER(Batch), I, P, Z, P],
+        "b200d2_minloc": [P, C.c_longlong, I, P, P, P],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    L.b200d2_diff2_coarse_batch_workspace.argtypes = [C.POINTER(View), C.POINTER(Batch), I]
+    L.b200d2_diff2_coarse_batch_workspace.restype = C.c_size_t
+    L.b200d2_diff2_coarse_batch_stage.argtypes = [C.POINTER(View), C.POINTER(Batch), I, I, P, Z, P]
+    L.b200d2_diff2_coarse_batch_stage.restype = C.c_int
+    L.b200d2_stage_name.argtypes = [I, I]
+    L.b200d2_stage_name.restype = C.c_char_p
+    L.b200d2_launch_count.argtypes = []
+    L.b200d2_launch_count.restype = C.c_ulonglong
+    # optional entry points declared by later modules of the library
+    for name, (args, res) in _EXTRA.items():
+        if hasattr(L, name):
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+
+
+_EXTRA: dict = {}
+
+
+def _check(code: int, where: str) -> None:
+    if code != 0:
+        raise B200D2Error(code, where)
+
+
+def _ptr(t) -> int:
+    """Device pointer of a torch CUDA tensor (or an int address)."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    if not t.is_cuda:
+        raise B200D2Error(1, "expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise B200D2Error(1, "expected a contiguous tensor")
+    return t.data_ptr()
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+class Projector:
+    """Resident padded Fourier volume (AccProjector).  use_texture: 1 texture,
+    0 linear arrays, 2 both."""
+
+    def __init__(self, pv=None, use_texture: int = 2, *, dat_path: str | None = None):
+        self._h = C.c_void_p()
+        if dat_path is not None:
+            _check(lib().b200d2_projector_load_dat(dat_path.encode(), use_texture, C.byref(self._h)),
+                   "projector_load_dat")
+        else:
+            re = np.ascontiguousarray(pv.re, np.float32)
+            im = np.ascontiguousarray(pv.im, np.float32)
+            _check(lib().b200d2_projector_create(pv.mdlX, pv.mdlY, pv.mdlZ, pv.mdlInitY, pv.mdlInitZ,
+                                                 pv.mdlMaxR, float(pv.padding_factor),
+                                                 re.ctypes.data_as(C.c_void_p), im.ctypes.data_as(C.c_void_p),
+                                                 use_texture, C.byref(self._h)), "projector_create")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def dims(self):
+        d = (C.c_int * 6)()
+        pf = C.c_float()
+        _check(lib().b200d2_projector_dims(self._h, d, C.byref(pf)), "projector_dims")
+        return tuple(d), pf.value
+
+    def view(self, imgX: int, imgY: int, imgMaxR: int, imgZ: int = 1, interp: int = INTERP_TEXTURE) -> View:
+        v = View()
+        _check(lib().b200d2_projector_view(self._h, imgX, imgY, imgZ, imgMaxR, interp, C.byref(v)),
+               "projector_view")
+        return v
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().b200d2_projector_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_diff2_kernel_coarse(view: View, trans_x, trans_y, corr, real, imag, eulers, diff2s,
+                            O: int, T: int, N_img: int, stream=None, precision: int = PREC_FP32):
+    """runDiff2KernelCoarse: diff2s[o*T+t] += diff2 (FP32 CUDA cores)."""
+    _check(lib().b200d2_diff2_coarse(C.byref(view), _ptr(trans_x), _ptr(trans_y), _ptr(corr), _ptr(real),
+                                     _ptr(imag), _ptr(eulers), _ptr(diff2s), O, T, N_img, _stream(stream),
+                                     precision), "diff2_coarse")
+
+
+def run_diff2_kernel_coarse_double(view: View, trans_x, trans_y, corr, real, imag, eulers, diff2s,
+                                   O: int, T: int, N_img: int, filter_img: bool = False, stream=None):
+    """runDiff2KernelCoarseDouble: diff2s (double) += FP64 diff2."""
+    _check(lib().b200d2_diff2_coarse_f64(C.byref(view), _ptr(trans_x), _ptr(trans_y), _ptr(corr), _ptr(real),
+                                         _ptr(imag), _ptr(eulers), _ptr(diff2s), O, T, N_img,
+                                         1 if filter_img else 0, _stream(stream)), "diff2_coarse_f64")
+
+
+def launch_count() -> int:
+    """Kernels launched by libb200d2 in this process so far."""
+    return int(lib().b200d2_launch_count())
+
+
+def make_batch(eulers, trans_x, trans_y, real, imag, corr, diff2, *, O: int, T: int, P: int, N_img: int,
+               img_stride: int | None = None, accumulate: bool = False, out_min=None, out_argmin=None) -> Batch:
+    b = Batch()
+    b.d_eulers, b.O = _ptr(eulers), O
+    b.d_trans_x, b.d_trans_y, b.T = _ptr(trans_x), _ptr(trans_y), T
+    b.P, b.N_img = P, N_img
+    b.d_real, b.d_imag, b.d_corr = _ptr(real), _ptr(imag), _ptr(corr)
+    b.img_stride = N_img if img_stride is None else img_stride
+    b.d_diff2 = _ptr(diff2)
+    b.accumulate = 1 if accumulate else 0
+    b.d_min = _ptr(out_min)
+    b.d_argmin = _ptr(out_argmin)
+    return b
+
+
+def batch_workspace_bytes(view: View, batch: Batch, precision: int) -> int:
+    return int(lib().b200d2_diff2_coarse_batch_workspace(C.byref(view), C.byref(batch), precision))
+
+
+def diff2_coarse_batch(view: View, batch: Batch, precision: int = PREC_BF16X3, workspace=None, stream=None):
+    """Score P particles against O orientations x T translations -> diff2[p][o][t]."""
+    ws = _ptr(workspace) if workspace is not None else None
+    nbytes = workspace.numel() * workspace.element_size() if workspace is not None and not isinstance(
+        workspace, int) else 0
+    _check(lib().b200d2_diff2_coarse_batch(C.byref(view), C.byref(batch), precision, ws, nbytes,
+                                           _stream(stream)), "diff2_coarse_batch")
+
+
+def minloc(diff2, n: int, P: int, out_min=None, out_argmin=None, stream=None):
+    _check(lib().b200d2_minloc(_ptr(diff2), n, P, _ptr(out_min), _ptr(out_argmin), _stream(stream)), "minloc")
+
+
+def stage_names(precision: int) -> list[str]:
+    out, i = [], 0
+    while True:
+        n = lib().b200d2_stage_name(precision, i)
+        if not n:
+            return out
+        out.append(n.decode())
+        i += 1
+
+
+def kernel_breakdown(view: View, batch: Batch, precision: int, workspace=None, stream=None, reps: int = 3) -> dict:
+    """Time each pipeline stage (one kernel each) with CUDA events on `stream`.
+
+    Runs every stage in order `reps` times (the outputs accumulate; callers
+    reset them afterwards if they need the values)."""
+    import torch
+    st = stream if stream is not None else torch.cuda.current_stream()
+    names = stage_names(precision)
+    ws = _ptr(workspace) if workspace is not None else None
+    nbytes = workspace.numel() * workspace.element_size() if workspace is not None else 0
+    acc = {n: 0.0 for n in names}
+    for _ in range(reps):
+        for i, n in enumerate(names):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            _check(lib().b200d2_diff2_coarse_batch_stage(C.byref(view), C.byref(batch), precision, i, ws, nbytes,
+                                                         _stream(st)), "batch_stage")
+            b.record(st)
+            b.synchronize()
+            acc[n] += a.elapsed_time(b)
+    per = {n: v / reps for n, v in acc.items()}
+    dom = max(per, key=per.get) if per else None
+    return {"per_kernel_ms": per, "dominant": dom, "dominant_ms": per.get(dom) if dom else None, "traffic": None}

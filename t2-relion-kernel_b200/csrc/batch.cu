@@ -1,0 +1,124 @@
+// batch.cu -- the batched coarse pass entry (b200d2_diff2_coarse_batch).
+//
+// Dispatches on precision: the CUDA-core direct kernels (FP32, FP64) or the
+// tensor-core pipeline (tc_pipeline.cu).  The reference has no batched call:
+// its harness loops runDiff2KernelCoarse over particles (src/main.cu:483-503).
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace b200d2 {
+int direct_batch(const b200d2_view& view, const float* eulers, const float* tx,
+                 const float* ty, const float* re, const float* im,
+                 const float* corr, long long img_stride, void* out,
+                 long long out_stride, int O, int T, int N_img, int P,
+                 bool fp64, int filter_img, cudaStream_t s);
+int minloc(const float* d, long long n, int P, double* mn, long long* arg, cudaStream_t s);
+size_t tc_workspace_bytes(const b200d2_view& view, const b200d2_batch& b, int precision);
+int tc_run(const b200d2_view& view, const b200d2_batch& b, int precision, void* ws,
+           size_t ws_bytes, cudaStream_t s);
+
+static int validate(const b200d2_view* v, const b200d2_batch* b) {
+  if (!v || !b) return B200D2_ERR_INVALID;
+  if (b->O < 0 || b->T < 0 || b->P < 0 || b->N_img < 0) return B200D2_ERR_INVALID;
+  if (b->O == 0 || b->T == 0 || b->P == 0) return B200D2_OK;
+  if (!b->d_eulers || !b->d_trans_x || !b->d_trans_y || !b->d_real || !b->d_imag ||
+      !b->d_corr || !b->d_diff2)
+    return B200D2_ERR_INVALID;
+  if (b->img_stride < b->N_img) return B200D2_ERR_INVALID;
+  if ((long long)v->imgX * v->imgY < b->N_img) return B200D2_ERR_INVALID;
+  if (v->mdlZ == 0) return B200D2_ERR_UNSUPPORTED;
+  if (v->interp == B200D2_INTERP_TEXTURE && (!v->tex_re || !v->tex_im)) return B200D2_ERR_INVALID;
+  if (v->interp == B200D2_INTERP_LINEAR && (!v->lin_re || !v->lin_im)) return B200D2_ERR_INVALID;
+  if (v->imgX > 32767 || v->imgY > 32767) return B200D2_ERR_UNSUPPORTED;
+  return B200D2_OK;
+}
+
+static unsigned long long g_launches = 0;
+void count_launch(unsigned n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
+
+}  // namespace b200d2
+
+extern "C" unsigned long long b200d2_launch_count(void) {
+  return __atomic_load_n(&b200d2::g_launches, __ATOMIC_RELAXED);
+}
+
+extern "C" size_t b200d2_diff2_coarse_batch_workspace(const b200d2_view* view,
+                                                      const b200d2_batch* batch,
+                                                      int precision) {
+  if (b200d2::validate(view, batch) != B200D2_OK) return 0;
+  if (precision == B200D2_PREC_FP32 || precision == B200D2_PREC_FP64) return 0;
+  return b200d2::tc_workspace_bytes(*view, *batch, precision);
+}
+
+extern "C" int b200d2_diff2_coarse_batch(const b200d2_view* view, const b200d2_batch* batch,
+                                         int precision, void* d_workspace,
+                                         size_t workspace_bytes, void* stream) {
+  int st = b200d2::validate(view, batch);
+  if (st != B200D2_OK) return st;
+  const b200d2_batch& b = *batch;
+  if (b.O == 0 || b.T == 0 || b.P == 0) return B200D2_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long per = (long long)b.O * b.T;
+  if (precision == B200D2_PREC_FP32) {
+    if (!b.accumulate)
+      B200D2_CUDA_TRY(cudaMemsetAsync(b.d_diff2, 0, sizeof(float) * per * b.P, s));
+    st = b200d2::direct_batch(*view, b.d_eulers, b.d_trans_x, b.d_trans_y, b.d_real, b.d_imag,
+                              b.d_corr, b.img_stride, b.d_diff2, per, b.O, b.T, b.N_img, b.P,
+                              false, 0, s);
+    if (st != B200D2_OK) return st;
+    if (b.d_min || b.d_argmin) st = b200d2::minloc(b.d_diff2, per, b.P, b.d_min, b.d_argmin, s);
+    return st;
+  }
+  if (precision == B200D2_PREC_TF32 || precision == B200D2_PREC_TF32X3 ||
+      precision == B200D2_PREC_BF16X3) {
+    const size_t need = b200d2::tc_workspace_bytes(*view, b, precision);
+    if (need > 0 && (!d_workspace || workspace_bytes < need)) return B200D2_ERR_INVALID;
+    return b200d2::tc_run(*view, b, precision, d_workspace, workspace_bytes, s);
+  }
+  return B200D2_ERR_UNSUPPORTED;
+}
+
+namespace b200d2 {
+const char* tc_stage_name(int precision, int stage);
+int tc_run_stage(const b200d2_view& view, const b200d2_batch& b, int precision, int stage,
+                 void* ws, size_t ws_bytes, cudaStream_t s);
+}  // namespace b200d2
+
+extern "C" const char* b200d2_stage_name(int precision, int stage) {
+  if (precision == B200D2_PREC_FP32) {
+    static const char* names[] = {"diff2_direct_kernel<float>", "minloc_kernel"};
+    return (stage >= 0 && stage < 2) ? names[stage] : nullptr;
+  }
+  if (precision == B200D2_PREC_TF32 || precision == B200D2_PREC_TF32X3 ||
+      precision == B200D2_PREC_BF16X3)
+    return b200d2::tc_stage_name(precision, stage);
+  return nullptr;
+}
+
+extern "C" int b200d2_diff2_coarse_batch_stage(const b200d2_view* view,
+                                               const b200d2_batch* batch, int precision,
+                                               int stage, void* d_workspace,
+                                               size_t workspace_bytes, void* stream) {
+  int st = b200d2::validate(view, batch);
+  if (st != B200D2_OK) return st;
+  const b200d2_batch& b = *batch;
+  if (b.O == 0 || b.T == 0 || b.P == 0) return B200D2_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long per = (long long)b.O * b.T;
+  if (precision == B200D2_PREC_FP32) {
+    if (stage == 0)
+      return b200d2::direct_batch(*view, b.d_eulers, b.d_trans_x, b.d_trans_y, b.d_real,
+                                  b.d_imag, b.d_corr, b.img_stride, b.d_diff2, per, b.O, b.T,
+                                  b.N_img, b.P, false, 0, s);
+    if (stage == 1) return b200d2::minloc(b.d_diff2, per, b.P, b.d_min, b.d_argmin, s);
+    return B200D2_ERR_INVALID;
+  }
+  if (precision == B200D2_PREC_TF32 || precision == B200D2_PREC_TF32X3 ||
+      precision == B200D2_PREC_BF16X3) {
+    const size_t need = b200d2::tc_workspace_bytes(*view, b, precision);
+    if (need > 0 && (!d_workspace || workspace_bytes < need)) return B200D2_ERR_INVALID;
+    return b200d2::tc_run_stage(*view, b, precision, stage, d_workspace, workspace_bytes, s);
+  }
+  return B200D2_ERR_UNSUPPORTED;
+}

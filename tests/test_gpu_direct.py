@@ -1,0 +1,139 @@
+"""GPU parity of the plain CUDA-core kernels (FP32 drop-in, FP64) against the
+reference's own kernels run on the same device buffers, and against the CPU
+oracle.  Tolerances: FP32 drop-in vs reference FP32 kernel <= 1e-5 relative
+(max over all diff2); FP64 kernels <= 1e-6."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from gpu_util import DeviceProblem, RefKernels, argmin_consistent, ours_f32, ours_f64
+
+pytestmark = pytest.mark.gpu
+TOL_FP32 = 1e-5
+
+
+@pytest.fixture(scope="module")
+def c1(pkg, synth, cuda, oracle):
+    pr = synth.make_problem("c1")
+    proj = pkg.Projector(pr.projector, use_texture=2)
+    ref = RefKernels(oracle, pr)
+    yield pr, proj, DeviceProblem(cuda, pr), ref
+    ref.close()
+    proj.close()
+
+
+@pytest.fixture(scope="module")
+def c2(pkg, synth, cuda, oracle):
+    pr = synth.make_problem("c2", P=3)
+    proj = pkg.Projector(pr.projector, use_texture=2)
+    ref = RefKernels(oracle, pr)
+    yield pr, proj, DeviceProblem(cuda, pr), ref
+    ref.close()
+    proj.close()
+
+
+def _check_case(pkg, oracle, case, particles):
+    pr, proj, dp, ref = case
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    worst = 0.0
+    for p in particles:
+        mine = ours_f32(pkg, view, dp, p)
+        theirs = ref.f32(dp, p)
+        theirs64 = ref.f64(dp, p)
+        s = oracle.error_stats(mine, theirs)
+        s64 = oracle.error_stats(mine, theirs64)
+        worst = max(worst, s["max_rel"], s64["max_rel"])
+        assert s["max_rel"] <= TOL_FP32, s
+        assert s64["max_rel"] <= TOL_FP32, s64
+        ok, gap = argmin_consistent(mine, theirs64, TOL_FP32)
+        assert ok, gap
+    return worst
+
+
+def test_fp32_dropin_matches_reference_c1(pkg, oracle, c1):
+    print("c1 worst rel", _check_case(pkg, oracle, c1, range(c1[0].P)))
+
+
+def test_fp32_dropin_matches_reference_c2(pkg, oracle, c2):
+    print("c2 worst rel", _check_case(pkg, oracle, c2, range(c2[0].P)))
+
+
+def test_fp64_matches_reference_double_kernel(pkg, oracle, c1):
+    pr, proj, dp, ref = c1
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    for p in range(2):
+        mine = ours_f64(pkg, view, dp, p)
+        theirs = ref.f64(dp, p)
+        s = oracle.error_stats(mine, theirs)
+        assert s["max_rel"] <= 1e-6, s
+        # filter_img semantics
+        mf = ours_f64(pkg, view, dp, p, filter_img=True)
+        tf = ref.f64(dp, p, filter_img=True)
+        assert oracle.error_stats(mf, tf)["max_rel"] <= 1e-6
+
+
+def test_fp64_matches_cpu_oracle_texture_emulation(pkg, oracle, c1):
+    pr, proj, dp, ref = c1
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    op = oracle.projector_for(pr)
+    for p in range(2):
+        mine = ours_f64(pkg, view, dp, p)
+        orc = oracle.diff2_coarse_f64(op, pr.eulers, pr.trans_x, pr.trans_y, pr.fimg_re[p], pr.fimg_im[p],
+                                      pr.corr[p], mode=oracle.INTERP_TEX_ROUND)
+        s = oracle.error_stats(mine, orc)
+        print("fp64 vs oracle(tex)", s["max_rel"], s["avg_rel"])
+        assert s["max_rel"] <= 1e-5, s
+
+
+def test_linear_interp_matches_oracle_exact(pkg, oracle, c1):
+    pr, proj, dp, ref = c1
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR, interp=pkg.INTERP_LINEAR)
+    op = oracle.projector_for(pr)
+    for p in range(2):
+        mine = ours_f32(pkg, view, dp, p)
+        orc = oracle.diff2_coarse_f64(op, pr.eulers, pr.trans_x, pr.trans_y, pr.fimg_re[p], pr.fimg_im[p],
+                                      pr.corr[p], mode=oracle.INTERP_EXACT)
+        s = oracle.error_stats(mine, orc)
+        assert s["max_rel"] <= TOL_FP32, s
+
+
+def test_dropin_accumulates_like_reference(pkg, oracle, c1):
+    pr, proj, dp, ref = c1
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    init = np.random.default_rng(1).uniform(0, 100, (pr.O, pr.T)).astype(np.float32)
+    mine = ours_f32(pkg, view, dp, 0, init=init)
+    theirs = ref.f32(dp, 0, init=init)
+    assert oracle.error_stats(mine, theirs)["max_rel"] <= TOL_FP32
+
+
+@pytest.mark.parametrize("o_lim,r2", [(37, 5), (1, 0), (200, 64), (577 - 1, 2)])
+def test_ragged_shapes(pkg, synth, oracle, cuda, o_lim, r2):
+    """Orientation counts that are not tile multiples, T = 1, T = 197 (> one
+    128-translation tile), against the reference kernel."""
+    pr = synth.make_problem("c1", P=1, orient_limit=o_lim)
+    sh = synth.translation_grid(r2)
+    import math
+    pr.shifts = sh
+    pr.trans_x = (-2 * math.pi * sh[:, 0] / pr.projector.ori_size).astype(np.float32)
+    pr.trans_y = (-2 * math.pi * sh[:, 1] / pr.projector.ori_size).astype(np.float32)
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    ref = RefKernels(oracle, pr)
+    dp = DeviceProblem(cuda, pr)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    mine = ours_f32(pkg, view, dp, 0)
+    theirs = ref.f32(dp, 0)
+    ref.close()
+    proj.close()
+    assert mine.shape == (o_lim, sh.shape[0])
+    assert oracle.error_stats(mine, theirs)["max_rel"] <= TOL_FP32
+
+
+def test_empty_problem_is_noop(pkg, cuda, c1):
+    pr, proj, dp, ref = c1
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    out = cuda.full((4,), 7.0, device="cuda")
+    pkg.run_diff2_kernel_coarse(view, dp.tx, dp.ty, dp.corr[0], dp.re[0], dp.im[0], dp.eulers, out, 0, pr.T,
+                                pr.N_img)
+    cuda.cuda.synchronize()
+    assert out.cpu().tolist() == [7.0] * 4

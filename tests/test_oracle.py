@@ -1,0 +1,141 @@
+"""CPU tests of the oracle (restatement of the reference's coarse diff2), the
+synthetic workload generator and the HEALPix grid.  No GPU needed."""
+from __future__ import annotations
+
+import glob
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_oracle_projector_view(oracle, synth):
+    pr = synth.make_problem("c1", P=1)
+    op = oracle.projector_for(pr)
+    # makeKernel: maxR = min(mdlMaxR=32, imgMaxR=16); maxR2_padded = int(16^2 * 2 * 2)
+    assert op.maxR == 16
+    assert op.maxR2_padded == 1024
+    assert pr.N_img == 544
+
+
+def test_filter_image_partition(oracle, synth):
+    """FilterCoarseParamImage: inside pixels first in index order, outside from the back."""
+    pr = synth.make_problem("c1", P=1)
+    op = oracle.projector_for(pr)
+    re, im, corr, xy, n = oracle.filter_image(op, pr.fimg_re[0], pr.fimg_im[0], pr.corr[0])
+    x, y = synth.pixel_coords(pr.imgX, pr.imgY, op.maxR)
+    inside = (x.astype(np.int64) ** 2 + y.astype(np.int64) ** 2) * 4 <= op.maxR2_padded
+    assert n == int(inside.sum()) == 414
+    np.testing.assert_array_equal(re[:n], pr.fimg_re[0][inside])
+    np.testing.assert_array_equal(re[n:][::-1], pr.fimg_re[0][~inside])
+    np.testing.assert_array_equal(xy[0:2 * n:2], x[inside].astype(np.float32))
+
+
+def test_oracle_f32_port_matches_f64(oracle, synth):
+    pr = synth.make_problem("c1", P=2)
+    op = oracle.projector_for(pr)
+    for p in range(2):
+        d64 = oracle.diff2_coarse_f64(op, pr.eulers, pr.trans_x, pr.trans_y, pr.fimg_re[p], pr.fimg_im[p], pr.corr[p])
+        d32 = oracle.diff2_coarse_f32(op, pr.eulers, pr.trans_x, pr.trans_y, pr.fimg_re[p], pr.fimg_im[p], pr.corr[p])
+        assert oracle.error_stats(d32, d64)["max_rel"] < 1e-5
+
+
+def test_oracle_accumulates_onto_initial_buffer(oracle, synth):
+    pr = synth.make_problem("g0", P=1)
+    op = oracle.projector_for(pr)
+    args = (op, pr.eulers, pr.trans_x, pr.trans_y, pr.fimg_re[0], pr.fimg_im[0], pr.corr[0])
+    init = np.arange(pr.O * pr.T, dtype=np.float64).reshape(pr.O, pr.T)
+    a = oracle.diff2_coarse_f64(*args)
+    b = oracle.diff2_coarse_f64(*args, diff2_init=init)
+    np.testing.assert_allclose(b - init, a, rtol=0, atol=1e-9)
+
+
+def test_texture_weights_differ_from_exact(oracle, synth):
+    """The 8-bit texture weights move diff2 by ~1e-5..1e-4 relative: the reason
+    the FP32 drop-in keeps the texture path (parity at 1e-5)."""
+    pr = synth.make_problem("c1", P=1)
+    op = oracle.projector_for(pr)
+    args = (op, pr.eulers, pr.trans_x, pr.trans_y, pr.fimg_re[0], pr.fimg_im[0], pr.corr[0])
+    tex = oracle.diff2_coarse_f64(*args, mode=oracle.INTERP_TEX_ROUND)
+    ex = oracle.diff2_coarse_f64(*args, mode=oracle.INTERP_EXACT)
+    r = oracle.error_stats(tex, ex)["max_rel"]
+    assert 1e-7 < r < 1e-3
+
+
+def test_high_snr_recovers_true_pose(oracle, synth):
+    pr = synth.make_problem("c1", P=3)
+    op = oracle.projector_for(pr)
+    # noiseless version of the particles: argmin must be the true pose
+    import math
+    x, y = synth.pixel_coords(pr.imgX, pr.imgY, op.maxR)
+    for p in range(3):
+        a = synth.project_exact(pr.projector, pr.eulers[pr.true_orient[p]], x, y, op.maxR)
+        sh = pr.shifts[pr.true_trans[p]]
+        ph = -2.0 * math.pi * (x * sh[0] + y * sh[1]) / pr.projector.ori_size
+        xim = a * np.exp(-1j * ph)
+        d = oracle.diff2_coarse_f64(op, pr.eulers, pr.trans_x, pr.trans_y, xim.real.astype(np.float32),
+                                    xim.imag.astype(np.float32), np.ones(pr.N_img, np.float32),
+                                    mode=oracle.INTERP_EXACT)
+        o, t = np.unravel_index(np.argmin(d), d.shape)
+        assert (o, t) == (pr.true_orient[p], pr.true_trans[p])
+
+
+def test_error_stats_restatement(oracle):
+    ref = np.array([1.0, 2.0, 0.0, 4.0])
+    test = np.array([1.1, 2.0, 1e-3, 3.0])
+    s = oracle.error_stats(test, ref)
+    assert s["count"] == 4 and s["count_rel"] == 3  # |ref| <= 1e-12 skipped
+    assert s["max_abs"] == pytest.approx(1.0)
+    assert s["max_rel"] == pytest.approx(0.25)
+
+
+def test_weights_normalised(oracle):
+    mn, w = oracle.weights_from_diff2(np.array([3.0, 1.0, 2.0]))
+    assert mn == 1.0 and w.sum() == pytest.approx(1.0) and np.argmax(w) == 1
+
+
+def test_healpix_grid(synth):
+    import importlib
+    hp = importlib.import_module("relion_b200.healpix")
+    for order in range(4):
+        th, ph = hp.pix2ang_ring(2 ** order)
+        assert th.size == 12 * 4 ** order
+        z = np.cos(th)
+        assert np.all(np.diff(z) <= 1e-12)  # RING order runs north to south
+        assert abs(z.sum()) < 1e-9  # equal-area: symmetric about the equator
+    eul, _ = hp.orientation_grid(1, 12)
+    assert eul.shape == (576, 9)
+    r = eul.reshape(-1, 3, 3).astype(np.float64)
+    np.testing.assert_allclose(r @ np.swapaxes(r, 1, 2), np.broadcast_to(np.eye(3), r.shape), atol=1e-6)
+    np.testing.assert_allclose(np.linalg.det(r), 1.0, atol=1e-5)
+
+
+def test_config_shapes(synth):
+    pr = synth.make_problem("c1")
+    assert (pr.P, pr.O, pr.T, pr.N_img) == (8, 576, 21, 544)
+    assert synth.translation_grid(36).shape[0] == 113
+    assert synth.translation_grid(16).shape[0] == 49
+    assert synth.translation_grid(4).shape[0] == 13
+    assert synth.translation_grid(64).shape[0] == 197
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "ref_*.npz"))))
+def test_oracle_against_reference_golden(oracle, path):
+    """Golden vectors written by the reference's own kernels (runDiff2KernelCoarse
+    and runDiff2KernelCoarseDouble, compiled from the reference sources and run
+    on a B200 by tests/golden/make_golden.py)."""
+    g = np.load(path)
+    from types import SimpleNamespace
+    pv = SimpleNamespace(re=g["vol_re"], im=g["vol_im"], **{k: int(g[k]) for k in
+                         ("mdlX", "mdlY", "mdlZ", "mdlInitY", "mdlInitZ", "mdlMaxR")},
+                         padding_factor=float(g["pf"]))
+    op = oracle.Projector(pv, int(g["imgX"]), int(g["imgY"]), int(g["imgMaxR"]))
+    for p in range(g["fimg_re"].shape[0]):
+        d = oracle.diff2_coarse_f64(op, g["eulers"], g["trans_x"], g["trans_y"], g["fimg_re"][p],
+                                    g["fimg_im"][p], g["corr"][p], mode=oracle.INTERP_TEX_ROUND)
+        s_d = oracle.error_stats(d, g["ref_f64"][p])
+        s_f = oracle.error_stats(d, g["ref_f32"][p])
+        assert s_d["max_rel"] < 2e-6, s_d
+        assert s_f["max_rel"] < 1e-5, s_f
