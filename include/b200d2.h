@@ -177,13 +177,19 @@ int b200d2_minloc(const float* d_diff2, long long n, int P, double* d_min,
 /* Run a single stage of the batch pipeline, so that a caller can time one
  * kernel with events on its stream.  Stages are numbered in pipeline order
  * from 0; b200d2_stage_name returns NULL past the last stage of `precision`.
- * Running every stage in order is equivalent to b200d2_diff2_coarse_batch
- * with accumulate = 1. */
+ * Running every stage in order is equivalent to b200d2_diff2_coarse_batch,
+ * except that the CUDA-core path then always accumulates. */
 int b200d2_diff2_coarse_batch_stage(const b200d2_view* view,
                                     const b200d2_batch* batch, int precision,
                                     int stage, void* d_workspace,
                                     size_t workspace_bytes, void* stream);
 const char* b200d2_stage_name(int precision, int stage);
+
+/* Status word of the last tensor-core batch run in this workspace: 0, or
+ * B200D2_ERR_TIMEOUT when a bounded device-side wait gave up (the outputs of
+ * that run are then incomplete).  Synchronises `stream`. */
+int b200d2_workspace_status(const void* d_workspace, void* stream,
+                            int* status);
 
 /* Number of kernels this library has launched in the process so far (all
  * entry points, all devices).  Lets a caller count launches in a region. */

@@ -425,3 +425,17 @@ long orc_filter_image(const orc_projector *p, const float *fre,
   }
   return ps;
 }
+
+/* Sample a [Z][Y][X] volume at texel coordinates (u, v, w) with the same
+ * interpolation routine the projections use (texture-unit emulation check). */
+void orc_tex_sample(const float *vol, int X, int Y, int Z, const float *uvw,
+                    long n, int mode, double *out) {
+  orc_projector p;
+  memset(&p, 0, sizeof(p));
+  p.mdlX = X;
+  p.mdlY = Y;
+  p.mdlZ = Z;
+  for (long i = 0; i < n; i++)
+    out[i] = orc_trilinear(vol, &p, uvw[3 * i], uvw[3 * i + 1], uvw[3 * i + 2],
+                           mode);
+}

@@ -192,3 +192,15 @@ def ref_lib():
         L.refshim_variant_run.argtypes = [C.c_int, P] + [C.c_int] * 4 + [P] * 9 + [C.c_int] * 5 + [P]
         _ref = L
     return _ref
+
+
+def tex_sample(vol: np.ndarray, uvw: np.ndarray, mode: int = INTERP_TEX_ROUND) -> np.ndarray:
+    """Emulated tex3D (linear filter, clamp, unnormalised) of vol [Z][Y][X] at uvw [n, 3]."""
+    L = lib()
+    L.orc_tex_sample.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_long, C.c_int, C.c_void_p]
+    vol = np.ascontiguousarray(vol, np.float32)
+    uvw = np.ascontiguousarray(uvw, np.float32)
+    out = np.zeros(uvw.shape[0], np.float64)
+    Z, Y, X = vol.shape
+    L.orc_tex_sample(_p(vol), X, Y, Z, _p(uvw), uvw.shape[0], mode, _p(out))
+    return out

@@ -101,6 +101,8 @@ def _declare(L):
     L.b200d2_diff2_coarse_batch_stage.restype = C.c_int
     L.b200d2_stage_name.argtypes = [I, I]
     L.b200d2_stage_name.restype = C.c_char_p
+    L.b200d2_workspace_status.argtypes = [P, P, C.POINTER(C.c_int)]
+    L.b200d2_workspace_status.restype = C.c_int
     L.b200d2_launch_count.argtypes = []
     L.b200d2_launch_count.restype = C.c_ulonglong
     # optional entry points declared by later modules of the library
@@ -273,3 +275,10 @@ def kernel_breakdown(view: View, batch: Batch, precision: int, workspace=None, s
     per = {n: v / reps for n, v in acc.items()}
     dom = max(per, key=per.get) if per else None
     return {"per_kernel_ms": per, "dominant": dom, "dominant_ms": per.get(dom) if dom else None, "traffic": None}
+
+
+def workspace_status(workspace, stream=None) -> int:
+    """0, or B200D2_ERR_TIMEOUT if a bounded device wait of the last tensor-core run gave up."""
+    st = C.c_int(-1)
+    _check(lib().b200d2_workspace_status(_ptr(workspace), _stream(stream), C.byref(st)), "workspace_status")
+    return st.value

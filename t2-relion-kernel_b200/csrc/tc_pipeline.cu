@@ -1,18 +1,777 @@
-// tc_pipeline.cu -- tensor-core coarse pass (placeholder until the tcgen05
-// kernels land).
+// tc_pipeline.cu -- tensor-core coarse pass for a batch of particles.
+//
+// diff2[p][o][t] = sum_px w|X|^2 + sum_px w|A_o|^2 - 2 Re sum_px (w S_t X_p) conj(A_o)
+//                =      normX[p] +       normA[p][o] - 2 cross[(p,t)][o]
+// with w = corr/2.  The cross term is a dense complex-as-real contraction:
+//   C[m = p*T + t][o] = sum_kk Aop[m][kk] * Bop[o][kk],   kk = 2*pixel + {re, im}
+// run on tcgen05 tensor cores with FP32 accumulation in TMEM.  Operands are
+// split into hi + lo parts (BF16 or TF32) and three products are accumulated
+// (hi*hi + hi*lo + lo*hi) to recover near-FP32 accuracy; the norms are
+// accumulated in FP64 and the final combination is FP64.
+//
+// Stages (one kernel each):
+//   0 pixel_list : in-radius pixel list (FilterCoarseParamImage, src/main.cu:88-151)
+//   1 phase      : per-translation separable phase tables e^{i x tx}, e^{i y ty}
+//   2 project    : B = projections of every orientation at every listed pixel
+//                  (project3Dmodel, src/acc_projectorkernel_impl.h:178-252), split
+//                  into hi/lo planes, plus |B|^2
+//   3 normx      : sum over all pixels of w|X|^2 per particle (FP64)
+//   4 norma      : normX[p] + sum_k w_p(k)|B_o(k)|^2 (FP64)
+//   5 gen_a      : A = w * X_p * e^{i(x tx + y ty)} for every (particle, translation)
+//                  row (translatePixel, src/cuda_device_utils.cuh:110-129), split
+//   6 gemm       : persistent tcgen05 contraction, TMA-fed, double-buffered TMEM
+//                  accumulators, fused FP64 combine + store + per-particle argmin
+//   7 finalize   : per-particle min / argmin from the packed keys
+#include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstring>
 
 #include "common.cuh"
+#include "tc_sm100.cuh"
 
 namespace b200d2 {
-size_t tc_workspace_bytes(const b200d2_view&, const b200d2_batch&, int) { return 0; }
-int tc_run(const b200d2_view&, const b200d2_batch&, int, void*, size_t, cudaStream_t) {
-  return B200D2_ERR_UNSUPPORTED;
+
+// ------------------------------------------------------------------ geometry
+struct TcGeom {
+  int P, O, T, N_img, K_c, Kpad, Mrows, Mpad, Opad, maxR, exw, eyw;
+  int elem, BK, terms;
+  size_t off_status, off_xy, off_idx, off_ex, off_ey, off_bhi, off_blo, off_q, off_normx, off_na,
+      off_ahi, off_alo, off_keys, total;
+};
+
+static inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Number of listed pixels and the largest |x| or |y| among them (the extent
+// of the phase tables).
+static int count_inside(const b200d2_view& v, int N_img, int* extent) {
+  int n = 0, r = 0;
+  for (int i = 0; i < N_img; ++i) {
+    int x = i % v.imgX, y = i / v.imgX;
+    if (y > v.maxR) y -= v.imgY;
+    if (pixel_maybe_inside(x, y, v.padding_factor, v.maxR2_padded)) {
+      ++n;
+      r = std::max(r, std::max(x < 0 ? -x : x, y < 0 ? -y : y));
+    }
+  }
+  if (extent) *extent = r;
+  return n;
 }
-}  // namespace b200d2
-namespace b200d2 {
-const char* tc_stage_name(int, int) { return nullptr; }
-int tc_run_stage(const b200d2_view&, const b200d2_batch&, int, int, void*, size_t, cudaStream_t) {
-  return B200D2_ERR_UNSUPPORTED;
+
+static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec) {
+  TcGeom g;
+  memset(&g, 0, sizeof(g));
+  g.P = b.P;
+  g.O = b.O;
+  g.T = b.T;
+  g.N_img = b.N_img;
+  int extent = 0;
+  g.K_c = count_inside(v, b.N_img, &extent);
+  g.elem = (prec == B200D2_PREC_BF16X3) ? 2 : 4;
+  g.BK = 128 / g.elem;
+  g.terms = (prec == B200D2_PREC_TF32) ? 1 : 3;
+  g.Kpad = (int)align_up((size_t)std::max(2 * g.K_c, 1), (size_t)g.BK);
+  g.Mrows = b.P * b.T;
+  g.Mpad = (int)align_up((size_t)g.Mrows, 128);
+  g.Opad = (int)align_up((size_t)b.O, 256);
+  g.maxR = extent;  // phase tables cover x in [0, extent], y in [-extent, extent]
+  g.exw = extent + 1;
+  g.eyw = 2 * extent + 1;
+  const int planes = g.terms == 3 ? 2 : 1;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = o;
+    o = align_up(o + bytes, 1024);
+    return at;
+  };
+  g.off_status = take(256);
+  g.off_xy = take(sizeof(int2) * (size_t)std::max(g.K_c, 1));
+  g.off_idx = take(sizeof(int) * (size_t)std::max(g.K_c, 1));
+  g.off_ex = take(sizeof(float2) * (size_t)g.T * g.exw);
+  g.off_ey = take(sizeof(float2) * (size_t)g.T * g.eyw);
+  g.off_bhi = take((size_t)g.Opad * g.Kpad * g.elem);
+  g.off_blo = planes == 2 ? take((size_t)g.Opad * g.Kpad * g.elem) : g.off_bhi;
+  g.off_q = take(sizeof(float) * (size_t)g.O * std::max(g.K_c, 1));
+  g.off_normx = take(sizeof(double) * (size_t)g.P);
+  g.off_na = take(sizeof(double) * (size_t)g.P * g.O);
+  g.off_ahi = take((size_t)g.Mpad * g.Kpad * g.elem);
+  g.off_alo = planes == 2 ? take((size_t)g.Mpad * g.Kpad * g.elem) : g.off_ahi;
+  g.off_keys = take(sizeof(unsigned long long) * (size_t)g.P);
+  g.total = o;
+  return g;
 }
+
+template <typename T>
+static inline T* ws_at(void* ws, size_t off) {
+  return reinterpret_cast<T*>(reinterpret_cast<uint8_t*>(ws) + off);
+}
+
+// ------------------------------------------------------------------ stage 0
+__global__ void __launch_bounds__(1024) tc_pixel_list_kernel(b200d2_view v, int N_img, int2* xy,
+                                                             int* idx, uint32_t* status,
+                                                             unsigned long long* keys, int P) {
+  __shared__ int s_cnt[32];
+  __shared__ int s_base;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    *status = 0;
+    s_base = 0;
+  }
+  for (int p = tid; p < P; p += blockDim.x) keys[p] = ~0ull;
+  __syncthreads();
+  for (int base = 0; base < N_img; base += 1024) {
+    const int i = base + tid;
+    int x = 0, y = 0;
+    bool in = false;
+    if (i < N_img) {
+      pixel_coor(i, v.imgX, v.imgY, v.maxR, x, y);
+      in = pixel_maybe_inside(x, y, v.padding_factor, v.maxR2_padded);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, in);
+    if (lane == 0) s_cnt[warp] = __popc(bal);
+    __syncthreads();
+    int off = 0, total = 0;
+    for (int w = 0; w < 32; ++w) {
+      const int c = s_cnt[w];
+      off += (w < warp) ? c : 0;
+      total += c;
+    }
+    if (in) {
+      const int slot = s_base + off + __popc(bal & ((1u << lane) - 1u));
+      xy[slot] = make_int2(x, y);
+      idx[slot] = i;
+    }
+    __syncthreads();
+    if (tid == 0) s_base += total;
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ stage 1
+__global__ void tc_phase_kernel(const float* __restrict__ tx, const float* __restrict__ ty, int T,
+                                int maxR, float2* ex, float2* ey) {
+  const int exw = maxR + 1, eyw = 2 * maxR + 1;
+  const int n1 = T * exw, n2 = T * eyw;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n1 + n2; i += gridDim.x * blockDim.x) {
+    double s, c;
+    if (i < n1) {
+      const int t = i / exw, x = i % exw;
+      sincos((double)x * (double)tx[t], &s, &c);
+      ex[i] = make_float2((float)c, (float)s);
+    } else {
+      const int j = i - n1, t = j / eyw, y = j % eyw - maxR;
+      sincos((double)y * (double)ty[t], &s, &c);
+      ey[j] = make_float2((float)c, (float)s);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ splits
+__device__ __forceinline__ float tf32_round(float v) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+  return __uint_as_float(r);
+}
+
+template <int PREC>
+__device__ __forceinline__ void store_split(void* hi, void* lo, size_t at, float re, float im) {
+  if constexpr (PREC == B200D2_PREC_BF16X3) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(re, im);
+    const float2 hf = __bfloat1622float2(h);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(re - hf.x, im - hf.y);
+    reinterpret_cast<__nv_bfloat162*>(hi)[at] = h;
+    reinterpret_cast<__nv_bfloat162*>(lo)[at] = l;
+  } else if constexpr (PREC == B200D2_PREC_TF32X3) {
+    const float hr = tf32_round(re), hm = tf32_round(im);
+    reinterpret_cast<float2*>(hi)[at] = make_float2(hr, hm);
+    reinterpret_cast<float2*>(lo)[at] = make_float2(tf32_round(re - hr), tf32_round(im - hm));
+  } else {
+    reinterpret_cast<float2*>(hi)[at] = make_float2(tf32_round(re), tf32_round(im));
+  }
+}
+
+// ------------------------------------------------------------------ stage 2
+template <int PREC>
+__global__ void __launch_bounds__(128) tc_project_kernel(b200d2_view v, const float* __restrict__ eulers,
+                                                         int O, const int2* __restrict__ xy, int K_c,
+                                                         int Kpad, void* bhi, void* blo, float* q) {
+  const int kp = blockIdx.x * blockDim.x + threadIdx.x;  // complex pixel slot
+  const int o = blockIdx.y;
+  if (kp >= Kpad / 2) return;
+  float2 b = make_float2(0.f, 0.f);
+  if (o < O && kp < K_c) {
+    float e[6];
+    const float* eo = eulers + (size_t)o * 9;
+    e[0] = eo[0];
+    e[1] = eo[1];
+    e[2] = eo[3];
+    e[3] = eo[4];
+    e[4] = eo[6];
+    e[5] = eo[7];
+    const int2 c = xy[kp];
+    b = project_pixel(v, (float)c.x, (float)c.y, e);
+    q[(size_t)o * K_c + kp] = __fmaf_rn(b.x, b.x, __fmul_rn(b.y, b.y));
+  }
+  store_split<PREC>(bhi, blo, (size_t)o * (Kpad / 2) + kp, b.x, b.y);
+}
+
+// ------------------------------------------------------------------ stage 3
+__global__ void __launch_bounds__(256) tc_normx_kernel(const float* __restrict__ re,
+                                                       const float* __restrict__ im,
+                                                       const float* __restrict__ corr,
+                                                       long long stride, int N_img, double* normx) {
+  const long long p = blockIdx.x;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < N_img; i += blockDim.x) {
+    const double r = re[p * stride + i], m = im[p * stride + i];
+    acc += (r * r + m * m) * ((double)corr[p * stride + i] / 2.0);
+  }
+  __shared__ double s[8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += s[w];
+    normx[p] = t;
+  }
+}
+
+// ------------------------------------------------------------------ stage 4
+// na[p][o] = normX[p] + sum_k w_p(k) |B_o(k)|^2, FP64 products and sums.
+// CTA tile: 32 particles x 64 orientations; thread tile 2 x 4.
+__global__ void __launch_bounds__(256) tc_norma_kernel(const float* __restrict__ corr, long long stride,
+                                                       const int* __restrict__ idx, int K_c,
+                                                       const float* __restrict__ q, int O, int P,
+                                                       const double* __restrict__ normx, double* na) {
+  __shared__ double sw[32][33];
+  __shared__ double sq[64][33];
+  const int tid = threadIdx.x, tp = tid >> 4, to = tid & 15;
+  const int p0 = blockIdx.y * 32, o0 = blockIdx.x * 64;
+  double acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+  for (int k0 = 0; k0 < K_c; k0 += 32) {
+    for (int e = tid; e < 32 * 32; e += 256) {
+      const int pp = e >> 5, k = e & 31;
+      double w = 0.0;
+      if (p0 + pp < P && k0 + k < K_c) w = (double)corr[(long long)(p0 + pp) * stride + idx[k0 + k]] / 2.0;
+      sw[pp][k] = w;
+    }
+    for (int e = tid; e < 64 * 32; e += 256) {
+      const int oo = e >> 5, k = e & 31;
+      sq[oo][k] = (o0 + oo < O && k0 + k < K_c) ? (double)q[(size_t)(o0 + oo) * K_c + k0 + k] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < 32; ++k) {
+      const double w0 = sw[2 * tp][k], w1 = sw[2 * tp + 1][k];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double qv = sq[to + 16 * j][k];
+        acc[0][j] = fma(w0, qv, acc[0][j]);
+        acc[1][j] = fma(w1, qv, acc[1][j]);
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int p = p0 + 2 * tp + i;
+    if (p >= P) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int o = o0 + to + 16 * j;
+      if (o < O) na[(size_t)p * O + o] = normx[p] + acc[i][j];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ stage 5
+// Row m = p*T + t of the translated, weighted image: a = (corr/2) X e^{i(x tx + y ty)}.
+template <int PREC>
+__global__ void __launch_bounds__(256) tc_gen_a_kernel(
+    const float* __restrict__ re, const float* __restrict__ im, const float* __restrict__ corr,
+    long long stride, const int2* __restrict__ xy, const int* __restrict__ idx, int K_c, int Kpad,
+    const float2* __restrict__ ex, const float2* __restrict__ ey, int T, int maxR, int Mrows,
+    void* ahi, void* alo) {
+  constexpr int ROWS = 32;
+  const int kp = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kp >= Kpad / 2) return;
+  const bool has = kp < K_c;
+  int x = 0, y = 0, pix = 0;
+  if (has) {
+    const int2 c = xy[kp];
+    x = c.x;
+    y = c.y;
+    pix = idx[kp];
+  }
+  const int exw = maxR + 1, eyw = 2 * maxR + 1;
+  const int m0 = blockIdx.y * ROWS;
+  int p = m0 / T;
+  int t = m0 - p * T;
+  int cur_p = -1;
+  float wr = 0.f, wi = 0.f;
+  for (int r = 0; r < ROWS; ++r) {
+    const int m = m0 + r;
+    float ar = 0.f, ai = 0.f;
+    if (has && m < Mrows) {
+      if (p != cur_p) {
+        const long long at = (long long)p * stride + pix;
+        const float w = corr[at] / 2;
+        wr = w * re[at];
+        wi = w * im[at];
+        cur_p = p;
+      }
+      const float2 fx = ex[t * exw + x];
+      const float2 fy = ey[t * eyw + y + maxR];
+      const float pr = __fmaf_rn(fx.x, fy.x, -__fmul_rn(fx.y, fy.y));
+      const float pi = __fmaf_rn(fx.x, fy.y, __fmul_rn(fx.y, fy.x));
+      ar = __fmaf_rn(wr, pr, -__fmul_rn(wi, pi));
+      ai = __fmaf_rn(wr, pi, __fmul_rn(wi, pr));
+    }
+    store_split<PREC>(ahi, alo, (size_t)m * (Kpad / 2) + kp, ar, ai);
+    if (++t == T) {
+      t = 0;
+      ++p;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ stage 6
+template <int PREC>
+struct GemmCfg {
+  static constexpr bool kTf32 = (PREC != B200D2_PREC_BF16X3);
+  static constexpr int kElem = kTf32 ? 4 : 2;
+  static constexpr int kBK = 128 / kElem;       // elements per 128-byte k-block row
+  static constexpr int kKStep = kTf32 ? 8 : 16;  // K of one tcgen05.mma
+  static constexpr int kTerms = (PREC == B200D2_PREC_TF32) ? 1 : 3;
+  static constexpr int kPlanes = kTerms == 3 ? 2 : 1;
+  static constexpr int kBM = 128, kBN = 256;
+  static constexpr int kATile = kBM * 128;
+  static constexpr int kBTile = kBN * 128;
+  static constexpr int kStageBytes = kPlanes * (kATile + kBTile);
+  static constexpr int kStages = kTerms == 3 ? 2 : 4;
+  static constexpr uint32_t kIdesc = sm100::idesc_f32acc(kTf32 ? 2u : 1u, kBM, kBN);
+  static constexpr int kBarBytes = 256;
+  static constexpr int kSmem = kStages * kStageBytes + kBarBytes + 1024;
+};
+
+struct GemmArgs {
+  int Mrows, Mtiles, Ntiles, O, T, KB, accumulate;
+  float* out;
+  const double* na;
+  unsigned long long* keys;
+  uint32_t* status;
+};
+
+__device__ __forceinline__ uint32_t ordered_bits(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__device__ __forceinline__ float from_ordered(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+constexpr uint64_t kWaitLimitNs = 4000000000ull;  // 4 s
+
+template <int PREC>
+__global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap mAhi,
+                                                         const __grid_constant__ CUtensorMap mAlo,
+                                                         const __grid_constant__ CUtensorMap mBhi,
+                                                         const __grid_constant__ CUtensorMap mBlo,
+                                                         const GemmArgs g) {
+  using C = GemmCfg<PREC>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::kStages * C::kStageBytes);
+  uint64_t* empty = full + C::kStages;
+  uint64_t* accf = empty + C::kStages;
+  uint64_t* acce = accf + 2;
+  uint64_t* drain = acce + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile uint32_t* s_abort = tmem_slot + 1;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C::kStages; ++s) {
+      sm100::mbar_init(&full[s], 1);
+      sm100::mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      sm100::mbar_init(&accf[b], 1);
+      sm100::mbar_init(&acce[b], 128);
+    }
+    sm100::mbar_init(drain, 1);
+    *s_abort = 0;
+    sm100::fence_barrier_init();
+    sm100::fence_proxy_async_smem();
+  }
+  if (warp == 0 && lane == 0) {
+    sm100::prefetch_tensormap(&mAhi);
+    sm100::prefetch_tensormap(&mBhi);
+    if (C::kPlanes == 2) {
+      sm100::prefetch_tensormap(&mAlo);
+      sm100::prefetch_tensormap(&mBlo);
+    }
+  }
+  if (warp == 1) {
+    sm100::tmem_alloc(tmem_slot, 512);
+    sm100::tmem_relinquish();
+  }
+  sm100::tc_fence_before();
+  __syncthreads();
+  sm100::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int num_tiles = g.Mtiles * g.Ntiles;
+
+  auto raise_abort = [&]() {
+    *s_abort = 1;
+    atomicExch(g.status, (uint32_t)B200D2_ERR_TIMEOUT);
+  };
+
+  if (warp == 0) {
+    // ------------------------------------------------ TMA producer
+    if (lane == 0) {
+      uint32_t gk = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+        const int m0 = (tile / g.Ntiles) * C::kBM, n0 = (tile % g.Ntiles) * C::kBN;
+        for (int kb = 0; kb < g.KB; ++kb, ++gk) {
+          const int s = gk % C::kStages;
+          const uint32_t u = gk / C::kStages;
+          if (u > 0 && !sm100::mbar_wait_bounded(&empty[s], (u - 1) & 1, s_abort, kWaitLimitNs)) {
+            raise_abort();
+            ok = false;
+            break;
+          }
+          sm100::mbar_arrive_expect_tx(&full[s], C::kStageBytes);
+          uint8_t* st = smem + s * C::kStageBytes;
+          const int kc = kb * C::kBK;
+          sm100::tma_load_2d(st, &mAhi, &full[s], kc, m0);
+          if (C::kPlanes == 2) sm100::tma_load_2d(st + C::kATile, &mAlo, &full[s], kc, m0);
+          uint8_t* sb = st + C::kPlanes * C::kATile;
+          sm100::tma_load_2d(sb, &mBhi, &full[s], kc, n0);
+          if (C::kPlanes == 2) sm100::tma_load_2d(sb + C::kBTile, &mBlo, &full[s], kc, n0);
+        }
+      }
+      // let the copies in flight land before the CTA can exit
+      const uint32_t issued = gk;
+      for (uint32_t j = (issued > (uint32_t)C::kStages ? issued - C::kStages : 0); j < issued; ++j)
+        sm100::mbar_wait_bounded(&full[j % C::kStages], (j / C::kStages) & 1, s_abort, kWaitLimitNs);
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      uint32_t gk = 0;
+      int i = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x, ++i) {
+        const int b = i & 1;
+        const uint32_t v = (uint32_t)(i >> 1);
+        if (v > 0 && !sm100::mbar_wait_bounded(&acce[b], (v - 1) & 1, s_abort, kWaitLimitNs)) {
+          raise_abort();
+          break;
+        }
+        sm100::tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(b * C::kBN);
+        for (int kb = 0; kb < g.KB; ++kb, ++gk) {
+          const int s = gk % C::kStages;
+          const uint32_t u = gk / C::kStages;
+          if (!sm100::mbar_wait_bounded(&full[s], u & 1, s_abort, kWaitLimitNs)) {
+            raise_abort();
+            ok = false;
+            break;
+          }
+          sm100::tc_fence_after();
+          const uint32_t st = sm100::smem_u32(smem + s * C::kStageBytes);
+          const uint32_t a_hi = st, a_lo = st + C::kATile;
+          const uint32_t b_hi = st + C::kPlanes * C::kATile, b_lo = b_hi + C::kBTile;
+#pragma unroll
+          for (int ks = 0; ks < C::kBK / C::kKStep; ++ks) {
+            const uint32_t koff = (uint32_t)(ks * C::kKStep * C::kElem);
+            const uint64_t dah = sm100::desc_k_sw128(a_hi + koff);
+            const uint64_t dbh = sm100::desc_k_sw128(b_hi + koff);
+            const uint32_t acc = (kb > 0 || ks > 0) ? 1u : 0u;
+            sm100::mma<C::kTf32>(d, dah, dbh, C::kIdesc, acc);
+            if (C::kTerms == 3) {
+              sm100::mma<C::kTf32>(d, dah, sm100::desc_k_sw128(b_lo + koff), C::kIdesc, 1u);
+              sm100::mma<C::kTf32>(d, sm100::desc_k_sw128(a_lo + koff), dbh, C::kIdesc, 1u);
+            }
+          }
+          sm100::mma_commit(&empty[s]);
+        }
+        if (ok) sm100::mma_commit(&accf[b]);
+      }
+      // every MMA issued by this thread has retired once `drain` fires
+      sm100::mma_commit(drain);
+      if (!sm100::mbar_wait_bounded(drain, 0, s_abort, kWaitLimitNs)) raise_abort();
+    }
+  } else {
+    // ------------------------------------------------ epilogue (warps 2..5)
+    const int qd = warp & 3;  // TMEM lane quadrant this warp may access
+    const int row = qd * 32 + lane;
+    int i = 0;
+    for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x, ++i) {
+      const int b = i & 1;
+      const uint32_t v = (uint32_t)(i >> 1);
+      int ok = 1;
+      if (lane == 0) ok = sm100::mbar_wait_bounded(&accf[b], v & 1, s_abort, kWaitLimitNs) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        if (lane == 0) raise_abort();
+        break;
+      }
+      sm100::tc_fence_after();
+      const int m0 = (tile / g.Ntiles) * C::kBM, n0 = (tile % g.Ntiles) * C::kBN;
+      const int m = m0 + row;
+      const bool vrow = m < g.Mrows;
+      const int p = vrow ? m / g.T : 0;
+      const int t = vrow ? m - p * g.T : 0;
+      const double* __restrict__ na_row = g.na + (size_t)p * g.O;
+      float* __restrict__ out_row = g.out + (size_t)p * g.O * g.T + t;
+      float best = __int_as_float(0x7f800000);
+      uint32_t best_idx = 0xffffffffu;
+#pragma unroll 1
+      for (int c = 0; c < C::kBN / 32; ++c) {
+        uint32_t r[32];
+        __syncwarp();
+        sm100::tmem_ld_32x32b_x32(tmem + (uint32_t)(b * C::kBN + c * 32) + ((uint32_t)(qd * 32) << 16), r);
+        sm100::tmem_ld_wait();
+        const int oc = n0 + c * 32;
+        if (vrow) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int o = oc + j;
+            if (o < g.O) {
+              const double dd = fma(-2.0, (double)__uint_as_float(r[j]), na_row[o]);
+              float f = (float)dd;
+              float* dst = out_row + (size_t)o * g.T;
+              if (g.accumulate) f += *dst;
+              *dst = f;
+              if (f < best) {
+                best = f;
+                best_idx = (uint32_t)(o * g.T + t);
+              }
+            }
+          }
+        }
+      }
+      sm100::tc_fence_before();
+      sm100::mbar_arrive(&acce[b]);
+      if (vrow && best_idx != 0xffffffffu) {
+        const unsigned long long key = ((unsigned long long)ordered_bits(best) << 32) | best_idx;
+        atomicMin(&g.keys[p], key);
+      }
+    }
+  }
+  __syncthreads();
+  if (warp == 1) {
+    sm100::tc_fence_after();
+    sm100::tmem_dealloc(tmem, 512);
+  }
+}
+
+// ------------------------------------------------------------------ stage 7
+__global__ void tc_finalize_kernel(const unsigned long long* keys, int P, double* mn, long long* arg) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const unsigned long long k = keys[p];
+  if (mn) mn[p] = (k == ~0ull) ? __longlong_as_double(0x7ff8000000000000LL) : (double)from_ordered((uint32_t)(k >> 32));
+  if (arg) arg[p] = (k == ~0ull) ? -1 : (long long)(k & 0xffffffffull);
+}
+
+// ------------------------------------------------------------------ host side
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+static int make_map(CUtensorMap* m, void* base, int elem, int cols, int rows, int box_rows) {
+  auto enc = get_encode();
+  if (!enc) return B200D2_ERR_CUDA;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)cols * elem};
+  const cuuint32_t box[2] = {(cuuint32_t)(128 / elem), (cuuint32_t)box_rows};
+  const cuuint32_t es[2] = {1, 1};
+  CUresult r = enc(m, elem == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                   base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? B200D2_OK : B200D2_ERR_CUDA;
+}
+
+static int num_sms() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+template <int PREC>
+static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeom& g, void* ws, int stage,
+                        cudaStream_t s) {
+  uint32_t* status = ws_at<uint32_t>(ws, g.off_status);
+  int2* xy = ws_at<int2>(ws, g.off_xy);
+  int* idx = ws_at<int>(ws, g.off_idx);
+  float2* ex = ws_at<float2>(ws, g.off_ex);
+  float2* ey = ws_at<float2>(ws, g.off_ey);
+  void* bhi = ws_at<void>(ws, g.off_bhi);
+  void* blo = ws_at<void>(ws, g.off_blo);
+  float* q = ws_at<float>(ws, g.off_q);
+  double* normx = ws_at<double>(ws, g.off_normx);
+  double* na = ws_at<double>(ws, g.off_na);
+  void* ahi = ws_at<void>(ws, g.off_ahi);
+  void* alo = ws_at<void>(ws, g.off_alo);
+  unsigned long long* keys = ws_at<unsigned long long>(ws, g.off_keys);
+  switch (stage) {
+    case 0:
+      tc_pixel_list_kernel<<<1, 1024, 0, s>>>(v, g.N_img, xy, idx, status, keys, g.P);
+      break;
+    case 1: {
+      const int n = g.T * (g.exw + g.eyw);
+      tc_phase_kernel<<<std::max(1, std::min((n + 255) / 256, 1024)), 256, 0, s>>>(
+          b.d_trans_x, b.d_trans_y, g.T, g.maxR, ex, ey);
+      break;
+    }
+    case 2: {
+      dim3 grid((g.Kpad / 2 + 127) / 128, g.Opad);
+      tc_project_kernel<PREC><<<grid, 128, 0, s>>>(v, b.d_eulers, g.O, xy, g.K_c, g.Kpad, bhi, blo, q);
+      break;
+    }
+    case 3:
+      tc_normx_kernel<<<g.P, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, g.N_img, normx);
+      break;
+    case 4: {
+      dim3 grid((g.O + 63) / 64, (g.P + 31) / 32);
+      tc_norma_kernel<<<grid, 256, 0, s>>>(b.d_corr, b.img_stride, idx, g.K_c, q, g.O, g.P, normx, na);
+      break;
+    }
+    case 5: {
+      dim3 grid((g.Kpad / 2 + 255) / 256, g.Mpad / 32);
+      tc_gen_a_kernel<PREC><<<grid, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, xy, idx, g.K_c,
+                                                 g.Kpad, ex, ey, g.T, g.maxR, g.Mrows, ahi, alo);
+      break;
+    }
+    case 6: {
+      using C = GemmCfg<PREC>;
+      CUtensorMap mAhi, mAlo, mBhi, mBlo;
+      int st = make_map(&mAhi, ahi, g.elem, g.Kpad, g.Mpad, C::kBM);
+      if (st == B200D2_OK) st = make_map(&mAlo, alo, g.elem, g.Kpad, g.Mpad, C::kBM);
+      if (st == B200D2_OK) st = make_map(&mBhi, bhi, g.elem, g.Kpad, g.Opad, C::kBN);
+      if (st == B200D2_OK) st = make_map(&mBlo, blo, g.elem, g.Kpad, g.Opad, C::kBN);
+      if (st != B200D2_OK) return st;
+      GemmArgs a;
+      a.Mrows = g.Mrows;
+      a.Mtiles = g.Mpad / C::kBM;
+      a.Ntiles = g.Opad / C::kBN;
+      a.O = g.O;
+      a.T = g.T;
+      a.KB = g.Kpad / C::kBK;
+      a.accumulate = b.accumulate;
+      a.out = b.d_diff2;
+      a.na = na;
+      a.keys = keys;
+      a.status = status;
+      static bool attr_set = false;
+      if (!attr_set) {
+        B200D2_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             C::kSmem));
+        attr_set = true;
+      }
+      const int tiles = a.Mtiles * a.Ntiles;
+      const int grid = std::max(1, std::min(tiles, num_sms()));
+      tc_gemm_kernel<PREC><<<grid, 192, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
+      break;
+    }
+    case 7:
+      tc_finalize_kernel<<<(g.P + 127) / 128, 128, 0, s>>>(keys, g.P, b.d_min, b.d_argmin);
+      break;
+    default:
+      return B200D2_ERR_INVALID;
+  }
+  count_launch();
+  return status_from_cuda(cudaGetLastError());
+}
+
+static int dispatch_stage(const b200d2_view& v, const b200d2_batch& b, int prec, const TcGeom& g, void* ws,
+                          int stage, cudaStream_t s) {
+  switch (prec) {
+    case B200D2_PREC_BF16X3: return launch_stage<B200D2_PREC_BF16X3>(v, b, g, ws, stage, s);
+    case B200D2_PREC_TF32X3: return launch_stage<B200D2_PREC_TF32X3>(v, b, g, ws, stage, s);
+    case B200D2_PREC_TF32: return launch_stage<B200D2_PREC_TF32>(v, b, g, ws, stage, s);
+    default: return B200D2_ERR_UNSUPPORTED;
+  }
+}
+
+static constexpr int kNumStages = 8;
+
+size_t tc_workspace_bytes(const b200d2_view& v, const b200d2_batch& b, int precision) {
+  return make_geom(v, b, precision).total;
+}
+
+const char* tc_stage_name(int precision, int stage) {
+  static const char* bf16[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_kernel<bf16x3>",
+                               "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<bf16x3>",
+                               "tc_gemm_kernel<bf16x3>", "tc_finalize_kernel"};
+  static const char* tf3[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_kernel<tf32x3>",
+                              "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<tf32x3>",
+                              "tc_gemm_kernel<tf32x3>", "tc_finalize_kernel"};
+  static const char* tf1[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_kernel<tf32>",
+                              "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<tf32>",
+                              "tc_gemm_kernel<tf32>", "tc_finalize_kernel"};
+  if (stage < 0 || stage >= kNumStages) return nullptr;
+  if (precision == B200D2_PREC_BF16X3) return bf16[stage];
+  if (precision == B200D2_PREC_TF32X3) return tf3[stage];
+  if (precision == B200D2_PREC_TF32) return tf1[stage];
+  return nullptr;
+}
+
+static int check_tc(const b200d2_view& v, const b200d2_batch& b) {
+  if (b.accumulate == 0) {
+    // fine: the epilogue overwrites
+  }
+  if ((long long)b.O * b.T >= 0xffffffffLL) return B200D2_ERR_UNSUPPORTED;  // argmin index is 32-bit
+  if (v.maxR > 4096) return B200D2_ERR_UNSUPPORTED;
+  return B200D2_OK;
+}
+
+int tc_run_stage(const b200d2_view& v, const b200d2_batch& b, int precision, int stage, void* ws,
+                 size_t ws_bytes, cudaStream_t s) {
+  int st = check_tc(v, b);
+  if (st != B200D2_OK) return st;
+  const TcGeom g = make_geom(v, b, precision);
+  if (ws_bytes < g.total) return B200D2_ERR_INVALID;
+  return dispatch_stage(v, b, precision, g, ws, stage, s);
+}
+
+int tc_run(const b200d2_view& v, const b200d2_batch& b, int precision, void* ws, size_t ws_bytes,
+           cudaStream_t s) {
+  int st = check_tc(v, b);
+  if (st != B200D2_OK) return st;
+  const TcGeom g = make_geom(v, b, precision);
+  if (ws_bytes < g.total) return B200D2_ERR_INVALID;
+  for (int i = 0; i < kNumStages && st == B200D2_OK; ++i) st = dispatch_stage(v, b, precision, g, ws, i, s);
+  return st;
+}
+
 }  // namespace b200d2
+
+extern "C" int b200d2_workspace_status(const void* d_workspace, void* stream, int* status) {
+  if (!d_workspace || !status) return B200D2_ERR_INVALID;
+  uint32_t v = 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  B200D2_CUDA_TRY(cudaMemcpyAsync(&v, d_workspace, sizeof(v), cudaMemcpyDeviceToHost, s));
+  B200D2_CUDA_TRY(cudaStreamSynchronize(s));
+  *status = (int)v;
+  return B200D2_OK;
+}

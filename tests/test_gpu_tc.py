@@ -1,0 +1,138 @@
+"""Tensor-core batch path (tcgen05) against the FP64 GPU kernel on the same
+projections, and against the FP32 drop-in.
+
+Stated tolerances (max relative diff2 error vs FP64, over every evaluation):
+  BF16x3 (hi*hi + hi*lo + lo*hi)  1e-5
+  TF32x3                          1e-5
+  TF32 (single product)           1e-3
+The argmin (o, t) must equal the FP64 argmin wherever the FP64 best-to-second
+gap exceeds twice the tolerance."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from gpu_util import DeviceProblem, argmin_consistent, ours_f64
+
+pytestmark = pytest.mark.gpu
+TOL = {"bf16x3": 1e-5, "tf32x3": 1e-5, "tf32": 1e-3}
+
+
+def prec_code(pkg, name):
+    return {"bf16x3": pkg.PREC_BF16X3, "tf32x3": pkg.PREC_TF32X3, "tf32": pkg.PREC_TF32}[name]
+
+
+def run_tc(pkg, torch, view, dp, prec, accumulate=False, init=None, stages=False):
+    pr = dp.pr
+    out = torch.zeros(pr.P * pr.O * pr.T, device="cuda")
+    if init is not None:
+        out.copy_(torch.as_tensor(np.asarray(init, np.float32).reshape(-1), device="cuda"))
+    mn = torch.empty(pr.P, device="cuda", dtype=torch.float64)
+    am = torch.empty(pr.P, device="cuda", dtype=torch.int64)
+    b = pkg.make_batch(dp.eulers, dp.tx, dp.ty, dp.re, dp.im, dp.corr, out, O=pr.O, T=pr.T, P=pr.P,
+                       N_img=pr.N_img, accumulate=accumulate, out_min=mn, out_argmin=am)
+    nb = pkg.batch_workspace_bytes(view, b, prec)
+    ws = torch.empty(nb, device="cuda", dtype=torch.uint8)
+    if stages:
+        pkg.kernel_breakdown(view, b, prec, ws, reps=1)
+    else:
+        pkg.diff2_coarse_batch(view, b, prec, ws)
+    torch.cuda.synchronize()
+    assert pkg.workspace_status(ws) == 0
+    return out.cpu().numpy().reshape(pr.P, pr.O, pr.T), mn.cpu().numpy(), am.cpu().numpy()
+
+
+def fp64_all(pkg, view, dp):
+    return np.stack([ours_f64(pkg, view, dp, p) for p in range(dp.pr.P)])
+
+
+@pytest.fixture(scope="module")
+def tiny(pkg, synth, cuda):
+    pr = synth.make_problem("tiny")
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dp = DeviceProblem(cuda, pr)
+    yield pr, view, dp, fp64_all(pkg, view, dp)
+    proj.close()
+
+
+@pytest.fixture(scope="module")
+def c1(pkg, synth, cuda):
+    pr = synth.make_problem("c1")
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dp = DeviceProblem(cuda, pr)
+    yield pr, view, dp, fp64_all(pkg, view, dp)
+    proj.close()
+
+
+def _check(pkg, oracle, cuda, case, name):
+    pr, view, dp, ref = case
+    got, mn, am = run_tc(pkg, cuda, view, dp, prec_code(pkg, name))
+    s = oracle.error_stats(got, ref)
+    print(name, pr.name, "max rel %.3g avg rel %.3g" % (s["max_rel"], s["avg_rel"]))
+    assert s["max_rel"] <= TOL[name], s
+    for p in range(pr.P):
+        ok, gap = argmin_consistent(got[p], ref[p], TOL[name])
+        assert ok, (p, gap)
+        assert am[p] == int(np.argmin(got[p].ravel()))
+        assert mn[p] == pytest.approx(float(got[p].min()), rel=1e-7)
+    return s
+
+
+@pytest.mark.parametrize("name", ["bf16x3", "tf32x3", "tf32"])
+def test_tc_tiny(pkg, oracle, cuda, tiny, name):
+    _check(pkg, oracle, cuda, tiny, name)
+
+
+@pytest.mark.parametrize("name", ["bf16x3", "tf32x3", "tf32"])
+def test_tc_c1(pkg, oracle, cuda, c1, name):
+    _check(pkg, oracle, cuda, c1, name)
+
+
+def test_tc_c2_subset(pkg, synth, oracle, cuda):
+    pr = synth.make_problem("c2", P=6)
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dp = DeviceProblem(cuda, pr)
+    ref = fp64_all(pkg, view, dp)
+    for name in ("bf16x3", "tf32x3"):
+        _check(pkg, oracle, cuda, (pr, view, dp, ref), name)
+    proj.close()
+
+
+def test_tc_accumulate_and_stages(pkg, oracle, cuda, tiny):
+    pr, view, dp, ref = tiny
+    init = np.random.default_rng(3).uniform(0, 50, (pr.P, pr.O, pr.T)).astype(np.float32)
+    got, _, _ = run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3, accumulate=True, init=init)
+    assert oracle.error_stats(got - init, ref)["max_rel"] <= 1e-5
+    got2, _, _ = run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3, stages=True)
+    np.testing.assert_array_equal(got2, run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3)[0])
+
+
+@pytest.mark.parametrize("o_lim,r2,P", [(37, 5, 1), (300, 0, 3), (257, 64, 2)])
+def test_tc_ragged(pkg, synth, oracle, cuda, o_lim, r2, P):
+    """O not a multiple of 256, P*T not a multiple of 128, T = 1 and T = 197."""
+    pr = synth.make_problem("c1", P=P, orient_limit=o_lim)
+    sh = synth.translation_grid(r2)
+    pr.shifts = sh
+    pr.trans_x = (-2 * math.pi * sh[:, 0] / pr.projector.ori_size).astype(np.float32)
+    pr.trans_y = (-2 * math.pi * sh[:, 1] / pr.projector.ori_size).astype(np.float32)
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dp = DeviceProblem(cuda, pr)
+    ref = fp64_all(pkg, view, dp)
+    got, mn, am = run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3)
+    assert got.shape == (P, o_lim, sh.shape[0])
+    assert oracle.error_stats(got, ref)["max_rel"] <= 1e-5
+    proj.close()
+
+
+def test_tc_deterministic(pkg, cuda, tiny):
+    pr, view, dp, ref = tiny
+    a = run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3)
+    b = run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3)
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[2], b[2])
