@@ -156,6 +156,8 @@ def parse():
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "tf32x3", "tf32", "fp32"])
     ap.add_argument("--config", default="c2")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--particles", type=int, default=None,
+                    help="override the particle count (small cases for profiling; not a bench line)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -215,7 +217,7 @@ def ours_arm(args):
     torch.cuda.set_device(local)
     pkg = load_package()
     synth = load_synth()
-    pr = synth.make_problem(args.config, seed=20251203 + rank)
+    pr = synth.make_problem(args.config, seed=20251203 + rank, P=args.particles)
     prec = PREC[args.precision]
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()

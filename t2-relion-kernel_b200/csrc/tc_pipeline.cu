@@ -29,6 +29,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
+#include <vector>
 
 #include "common.cuh"
 #include "tc_sm100.cuh"
@@ -243,43 +245,53 @@ __global__ void __launch_bounds__(256) tc_normx_kernel(const float* __restrict__
 
 // ------------------------------------------------------------------ stage 4
 // na[p][o] = normX[p] + sum_k w_p(k) |B_o(k)|^2, FP64 products and sums.
-// CTA tile: 32 particles x 64 orientations; thread tile 2 x 4.
+// CTA tile: 64 particles x 64 orientations over 32-pixel slabs held k-major
+// in shared memory; thread (tp, to) owns particles 4tp..4tp+3 (two 16-byte
+// broadcast loads) and orientations to + 16j (conflict-free loads), i.e. 16
+// DFMA per 6 shared loads.
 __global__ void __launch_bounds__(256) tc_norma_kernel(const float* __restrict__ corr, long long stride,
                                                        const int* __restrict__ idx, int K_c,
                                                        const float* __restrict__ q, int O, int P,
                                                        const double* __restrict__ normx, double* na) {
-  __shared__ double sw[32][33];
-  __shared__ double sq[64][33];
+  constexpr int KC = 32;
+  __shared__ __align__(16) double sw[KC][64];
+  __shared__ double sq[KC][65];
   const int tid = threadIdx.x, tp = tid >> 4, to = tid & 15;
-  const int p0 = blockIdx.y * 32, o0 = blockIdx.x * 64;
-  double acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-  for (int k0 = 0; k0 < K_c; k0 += 32) {
-    for (int e = tid; e < 32 * 32; e += 256) {
-      const int pp = e >> 5, k = e & 31;
+  const int p0 = blockIdx.y * 64, o0 = blockIdx.x * 64;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int k0 = 0; k0 < K_c; k0 += KC) {
+    for (int e = tid; e < 64 * KC; e += 256) {
+      const int pp = e % 64, k = e / 64;  // consecutive threads: consecutive particles
       double w = 0.0;
       if (p0 + pp < P && k0 + k < K_c) w = (double)corr[(long long)(p0 + pp) * stride + idx[k0 + k]] / 2.0;
-      sw[pp][k] = w;
+      sw[k][pp] = w;
     }
-    for (int e = tid; e < 64 * 32; e += 256) {
-      const int oo = e >> 5, k = e & 31;
-      sq[oo][k] = (o0 + oo < O && k0 + k < K_c) ? (double)q[(size_t)(o0 + oo) * K_c + k0 + k] : 0.0;
+    for (int e = tid; e < 64 * KC; e += 256) {
+      const int oo = e / KC, k = e % KC;
+      sq[k][oo] = (o0 + oo < O && k0 + k < K_c) ? (double)q[(size_t)(o0 + oo) * K_c + k0 + k] : 0.0;
     }
     __syncthreads();
 #pragma unroll 4
-    for (int k = 0; k < 32; ++k) {
-      const double w0 = sw[2 * tp][k], w1 = sw[2 * tp + 1][k];
+    for (int k = 0; k < KC; ++k) {
+      const double2 wa = *reinterpret_cast<const double2*>(&sw[k][4 * tp]);
+      const double2 wb = *reinterpret_cast<const double2*>(&sw[k][4 * tp + 2]);
+      const double w[4] = {wa.x, wa.y, wb.x, wb.y};
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const double qv = sq[to + 16 * j][k];
-        acc[0][j] = fma(w0, qv, acc[0][j]);
-        acc[1][j] = fma(w1, qv, acc[1][j]);
+        const double qv = sq[k][to + 16 * j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc[i][j] = fma(w[i], qv, acc[i][j]);
       }
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const int p = p0 + 2 * tp + i;
+  for (int i = 0; i < 4; ++i) {
+    const int p = p0 + 4 * tp + i;
     if (p >= P) continue;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -652,7 +664,7 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       tc_normx_kernel<<<g.P, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, g.N_img, normx);
       break;
     case 4: {
-      dim3 grid((g.O + 63) / 64, (g.P + 31) / 32);
+      dim3 grid((g.O + 63) / 64, (g.P + 63) / 64);
       tc_norma_kernel<<<grid, 256, 0, s>>>(b.d_corr, b.img_stride, idx, g.K_c, q, g.O, g.P, normx, na);
       break;
     }
@@ -754,13 +766,66 @@ int tc_run_stage(const b200d2_view& v, const b200d2_batch& b, int precision, int
   return dispatch_stage(v, b, precision, g, ws, stage, s);
 }
 
+// Side stream (and fork/join events) paired with a caller stream on the
+// current device.  Calls on one caller stream are ordered by that stream, so
+// reusing the pair's events across calls is safe; fork/join through events is
+// also what stream capture records into a graph.
+struct SidePair {
+  int device;
+  cudaStream_t user, side;
+  cudaEvent_t fork, join;
+};
+
+static std::mutex g_side_mu;
+static std::vector<SidePair> g_side;
+
+static int side_for(cudaStream_t user, SidePair* out) {
+  int dev = 0;
+  B200D2_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_side_mu);
+  for (const SidePair& sp : g_side)
+    if (sp.device == dev && sp.user == user) {
+      *out = sp;
+      return B200D2_OK;
+    }
+  SidePair sp;
+  sp.device = dev;
+  sp.user = user;
+  B200D2_CUDA_TRY(cudaStreamCreateWithFlags(&sp.side, cudaStreamNonBlocking));
+  B200D2_CUDA_TRY(cudaEventCreateWithFlags(&sp.fork, cudaEventDisableTiming));
+  B200D2_CUDA_TRY(cudaEventCreateWithFlags(&sp.join, cudaEventDisableTiming));
+  g_side.push_back(sp);
+  *out = sp;
+  return B200D2_OK;
+}
+
 int tc_run(const b200d2_view& v, const b200d2_batch& b, int precision, void* ws, size_t ws_bytes,
            cudaStream_t s) {
   int st = check_tc(v, b);
   if (st != B200D2_OK) return st;
   const TcGeom g = make_geom(v, b, precision);
   if (ws_bytes < g.total) return B200D2_ERR_INVALID;
-  for (int i = 0; i < kNumStages && st == B200D2_OK; ++i) st = dispatch_stage(v, b, precision, g, ws, i, s);
+  SidePair sp;
+  st = side_for(s, &sp);
+  if (st != B200D2_OK) return st;
+  // caller stream: pixel list -> projections -> normX -> normA ; side stream:
+  // phase tables -> operand generation; join before the contraction.
+  st = dispatch_stage(v, b, precision, g, ws, 0, s);
+  if (st != B200D2_OK) return st;
+  B200D2_CUDA_TRY(cudaEventRecord(sp.fork, s));
+  B200D2_CUDA_TRY(cudaStreamWaitEvent(sp.side, sp.fork, 0));
+  st = dispatch_stage(v, b, precision, g, ws, 1, sp.side);
+  if (st == B200D2_OK) st = dispatch_stage(v, b, precision, g, ws, 5, sp.side);
+  const cudaError_t rj = cudaEventRecord(sp.join, sp.side);
+  if (st != B200D2_OK) return st;
+  if (rj != cudaSuccess) return status_from_cuda(rj);
+  for (int i : {2, 3, 4}) {
+    st = dispatch_stage(v, b, precision, g, ws, i, s);
+    if (st != B200D2_OK) return st;
+  }
+  B200D2_CUDA_TRY(cudaStreamWaitEvent(s, sp.join, 0));
+  st = dispatch_stage(v, b, precision, g, ws, 6, s);
+  if (st == B200D2_OK) st = dispatch_stage(v, b, precision, g, ws, 7, s);
   return st;
 }
 
