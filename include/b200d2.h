@@ -104,6 +104,13 @@ int b200d2_projector_dims(const b200d2_projector* p, int* dims, float* pf);
 int b200d2_projector_view(const b200d2_projector* p, int imgX, int imgY,
                           int imgZ, int imgMaxR, int interp, b200d2_view* out);
 
+/* Central-slice projections of O orientations at K pixels (project3Dmodel,
+ * src/acc_projectorkernel_impl.h:178-252): d_out_re/d_out_im[o*K + k] for
+ * pixel (d_px[k], d_py[k]), 0 outside the projector radius. */
+int b200d2_project_pixels(const b200d2_view* view, const float* d_eulers,
+                          int O, const int* d_px, const int* d_py, int K,
+                          float* d_out_re, float* d_out_im, void* stream);
+
 /* ------------------------------------------------------------------------
  * Single-particle drop-in (replaces runDiff2KernelCoarse,
  * src/acc_helper_functions_impl.h:15-499, non-CC 3D-reference 2D-image branch)
@@ -154,6 +161,14 @@ typedef struct b200d2_batch {
   int accumulate;      /* 1: d_diff2 += diff2 (drop-in), 0: d_diff2 = diff2 */
   double* d_min;       /* optional [P]: per-particle minimum diff2 */
   long long* d_argmin; /* optional [P]: o*T + t of that minimum (lowest index on ties) */
+  /* Optional listed pixels (the reference's filtered layout, src/main.cu:88-151
+   * and the coor_xy argument of its optimised functors): when d_coor_xy is not
+   * NULL the first n_listed image entries are the pixels at integer-valued
+   * coordinates (d_coor_xy[2i], d_coor_xy[2i+1]), |x|,|y| <= 512, shared by
+   * all particles, and entries n_listed .. N_img-1 lie outside the projector
+   * radius (they add only corr/2 |X|^2).  Tensor-core precisions only. */
+  const float* d_coor_xy;
+  int n_listed;
 } b200d2_batch;
 
 /* Bytes of device scratch the batch needs for `precision` (0 for the

@@ -156,6 +156,15 @@ static inline void orc_tex_split(double u, int mode, long *i0, double *a) {
   }
 }
 
+/* Measured on the B200 (tests/test_gpu_texture.py): the 1D behaviour above
+ * (fraction rounded half-up to 1/256, weight 1.0 reachable) is exact, and
+ * the eight 3D corner weights are multiples of 1/256 summing to exactly one,
+ * but the hardware rounds them jointly in a way this separable model does
+ * not reproduce; per sample the difference is up to ~1e-2 of the voxel scale,
+ * on diff2 up to ~2e-4 relative.  Parity of the texture path is therefore
+ * pinned against the reference's own kernels and against the texture unit's
+ * own samples (orc_diff2_from_projections), not against this model. */
+
 /* Trilinear fetch of one component at texel coordinates (u, v, w), where
  * u = xp + 0.5, v = yp - mdlInitY + 0.5, w = zp - mdlInitZ + 0.5 exactly as
  * the reference forms them in float before tex3D
@@ -277,6 +286,39 @@ void orc_diff2_coarse_f64(const orc_projector *p, const float *eulers, long O,
   free(py);
   free(sre);
   free(sim);
+}
+
+/* Same FP64 sum as orc_diff2_coarse_f64, but with the projections given
+ * (prj_re/prj_im[o*N_img + i] for every image pixel i): isolates the
+ * arithmetic of cuda_kernel_diff2_coarse from the interpolation. */
+void orc_diff2_from_projections(const orc_projector *p, const float *prj_re,
+                                const float *prj_im, long O,
+                                const float *trans_x, const float *trans_y,
+                                long T, const float *fre, const float *fim,
+                                const float *corr, long N_img, double *diff2,
+                                int nthreads) {
+  long o;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 4)
+#endif
+  for (o = 0; o < O; o++) {
+    for (long t = 0; t < T; t++) {
+      double acc = 0.0;
+      for (long i = 0; i < N_img; i++) {
+        int x, y;
+        orc_pixel_coor(p, i, &x, &y);
+        double ph = x * (double)trans_x[t] + y * (double)trans_y[t];
+        double s = sin(ph), c = cos(ph);
+        double r = fre[i], m = fim[i];
+        double sr = c * r - s * m, si = c * m + s * r;
+        double dr = (double)prj_re[o * N_img + i] - sr;
+        double di = (double)prj_im[o * N_img + i] - si;
+        acc += (dr * dr + di * di) * ((double)corr[i] / 2.0);
+      }
+      diff2[o * T + t] += acc;
+    }
+  }
 }
 
 /* ---------------------------------------------------------------------------

@@ -114,6 +114,27 @@ def diff2_coarse_f64(proj: Projector, eulers, trans_x, trans_y, fre, fim, corr,
     return out
 
 
+def diff2_from_projections(proj: Projector, prj_re, prj_im, trans_x, trans_y, fre, fim, corr,
+                           nthreads: int = 0) -> np.ndarray:
+    """FP64 coarse diff2 with given projections prj[o][i] over all image pixels -> [O, T]."""
+    L = lib()
+    P_ = C.c_void_p
+    L.orc_diff2_from_projections.argtypes = [C.POINTER(OrcProjector), P_, P_, C.c_long, P_, P_, C.c_long, P_, P_,
+                                             P_, C.c_long, P_, C.c_int]
+    prj_re = np.ascontiguousarray(prj_re, np.float32)
+    prj_im = np.ascontiguousarray(prj_im, np.float32)
+    tx = np.ascontiguousarray(trans_x, np.float32)
+    ty = np.ascontiguousarray(trans_y, np.float32)
+    fre = np.ascontiguousarray(fre, np.float32)
+    fim = np.ascontiguousarray(fim, np.float32)
+    corr = np.ascontiguousarray(corr, np.float32)
+    O, T, N = prj_re.shape[0], tx.size, fre.size
+    out = np.zeros((O, T), np.float64)
+    L.orc_diff2_from_projections(C.byref(proj.s), _p(prj_re), _p(prj_im), O, _p(tx), _p(ty), T, _p(fre), _p(fim),
+                                 _p(corr), N, _p(out), nthreads)
+    return out
+
+
 def diff2_coarse_f32(proj: Projector, eulers, trans_x, trans_y, fre, fim, corr,
                      diff2_init=None, nthreads: int = 0) -> np.ndarray:
     """FP32 port of cuda_kernel_diff2_coarse (the CPU baseline) -> [O, T] float32."""

@@ -14,6 +14,10 @@
 //   runDiff2KernelCoarse                      src/acc_helper_functions_impl.h:15-499
 //   runDiff2KernelCoarseDouble                src/acc_helper_functions_impl.h:503-854
 //   CoarseMatrixKernel*::run (5 variants)     src/coarse_splitImg_*.cuh
+// The reference's texture projector is used.  Its PROJECTOR_NO_TEXTURES
+// configuration does not compile (src/diff2.cuh:16 includes
+// src/orientation_matrix_handler.cuh, which calls tex3D unconditionally at
+// :144-145), so that path cannot be run as a checker.
 #include <cuda_runtime.h>
 
 // standard headers the reference headers expect to be included first

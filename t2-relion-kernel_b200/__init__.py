@@ -56,7 +56,7 @@ class Batch(C.Structure):
                 ("T", C.c_int), ("P", C.c_int), ("N_img", C.c_int), ("d_real", C.c_void_p),
                 ("d_imag", C.c_void_p), ("d_corr", C.c_void_p), ("img_stride", C.c_longlong),
                 ("d_diff2", C.c_void_p), ("accumulate", C.c_int), ("d_min", C.c_void_p),
-                ("d_argmin", C.c_void_p)]
+                ("d_argmin", C.c_void_p), ("d_coor_xy", C.c_void_p), ("n_listed", C.c_int)]
 
 
 _lib = None
@@ -90,6 +90,7 @@ def _declare(L):
         "b200d2_diff2_coarse_f64": [C.POINTER(View), P, P, P, P, P, P, P, Z, Z, Z, I, P],
         "b200d2_diff2_coarse_batch": [C.POINTER(View), C.POINTER(Batch), I, P, Z, P],
         "b200d2_minloc": [P, C.c_longlong, I, P, P, P],
+        "b200d2_project_pixels": [C.POINTER(View), P, I, P, P, I, P, P, P],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -188,6 +189,12 @@ class Projector:
             pass
 
 
+def project_pixels(view: View, eulers, px, py, out_re, out_im, O: int, K: int, stream=None):
+    """Projections of O orientations at K pixels: out[o*K + k] (project3Dmodel)."""
+    _check(lib().b200d2_project_pixels(C.byref(view), _ptr(eulers), O, _ptr(px), _ptr(py), K, _ptr(out_re),
+                                       _ptr(out_im), _stream(stream)), "project_pixels")
+
+
 def run_diff2_kernel_coarse(view: View, trans_x, trans_y, corr, real, imag, eulers, diff2s,
                             O: int, T: int, N_img: int, stream=None, precision: int = PREC_FP32):
     """runDiff2KernelCoarse: diff2s[o*T+t] += diff2 (FP32 CUDA cores)."""
@@ -210,8 +217,11 @@ def launch_count() -> int:
 
 
 def make_batch(eulers, trans_x, trans_y, real, imag, corr, diff2, *, O: int, T: int, P: int, N_img: int,
-               img_stride: int | None = None, accumulate: bool = False, out_min=None, out_argmin=None) -> Batch:
+               img_stride: int | None = None, accumulate: bool = False, out_min=None, out_argmin=None,
+               coor_xy=None, n_listed: int = 0) -> Batch:
     b = Batch()
+    b.d_coor_xy = _ptr(coor_xy)
+    b.n_listed = n_listed if coor_xy is not None else 0
     b.d_eulers, b.O = _ptr(eulers), O
     b.d_trans_x, b.d_trans_y, b.T = _ptr(trans_x), _ptr(trans_y), T
     b.P, b.N_img = P, N_img

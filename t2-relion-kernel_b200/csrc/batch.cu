@@ -31,6 +31,7 @@ static int validate(const b200d2_view* v, const b200d2_batch* b) {
   if (v->interp == B200D2_INTERP_TEXTURE && (!v->tex_re || !v->tex_im)) return B200D2_ERR_INVALID;
   if (v->interp == B200D2_INTERP_LINEAR && (!v->lin_re || !v->lin_im)) return B200D2_ERR_INVALID;
   if (v->imgX > 32767 || v->imgY > 32767) return B200D2_ERR_UNSUPPORTED;
+  if (b->d_coor_xy && (b->n_listed < 0 || b->n_listed > b->N_img)) return B200D2_ERR_INVALID;
   return B200D2_OK;
 }
 
@@ -57,6 +58,8 @@ extern "C" int b200d2_diff2_coarse_batch(const b200d2_view* view, const b200d2_b
   int st = b200d2::validate(view, batch);
   if (st != B200D2_OK) return st;
   const b200d2_batch& b = *batch;
+  if (b.d_coor_xy && (precision == B200D2_PREC_FP32 || precision == B200D2_PREC_FP64))
+    return B200D2_ERR_UNSUPPORTED;  // listed pixels: tensor-core path only
   if (b.O == 0 || b.T == 0 || b.P == 0) return B200D2_OK;
   cudaStream_t s = (cudaStream_t)stream;
   const long long per = (long long)b.O * b.T;
@@ -103,6 +106,8 @@ extern "C" int b200d2_diff2_coarse_batch_stage(const b200d2_view* view,
   int st = b200d2::validate(view, batch);
   if (st != B200D2_OK) return st;
   const b200d2_batch& b = *batch;
+  if (b.d_coor_xy && (precision == B200D2_PREC_FP32 || precision == B200D2_PREC_FP64))
+    return B200D2_ERR_UNSUPPORTED;  // listed pixels: tensor-core path only
   if (b.O == 0 || b.T == 0 || b.P == 0) return B200D2_OK;
   cudaStream_t s = (cudaStream_t)stream;
   const long long per = (long long)b.O * b.T;

@@ -167,6 +167,37 @@ extern "C" int b200d2_projector_dims(const b200d2_projector* p, int* dims,
   return B200D2_OK;
 }
 
+namespace {
+__global__ void project_pixels_kernel(b200d2_view v, const float* __restrict__ eulers, int O,
+                                      const int* __restrict__ px, const int* __restrict__ py, int K,
+                                      float* __restrict__ out_re, float* __restrict__ out_im) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int o = blockIdx.y;
+  if (k >= K || o >= O) return;
+  const float* eo = eulers + (size_t)o * 9;
+  const float e[6] = {eo[0], eo[1], eo[3], eo[4], eo[6], eo[7]};
+  const float2 r = b200d2::project_pixel(v, (float)px[k], (float)py[k], e);
+  out_re[(size_t)o * K + k] = r.x;
+  out_im[(size_t)o * K + k] = r.y;
+}
+}  // namespace
+
+extern "C" int b200d2_project_pixels(const b200d2_view* view, const float* d_eulers, int O,
+                                     const int* d_px, const int* d_py, int K, float* d_out_re,
+                                     float* d_out_im, void* stream) {
+  if (!view || !d_eulers || !d_px || !d_py || !d_out_re || !d_out_im || O < 0 || K < 0)
+    return B200D2_ERR_INVALID;
+  if (view->interp == B200D2_INTERP_TEXTURE && (!view->tex_re || !view->tex_im)) return B200D2_ERR_INVALID;
+  if (view->interp == B200D2_INTERP_LINEAR && (!view->lin_re || !view->lin_im)) return B200D2_ERR_INVALID;
+  if (O == 0 || K == 0) return B200D2_OK;
+  if (O > 65535) return B200D2_ERR_UNSUPPORTED;
+  dim3 grid((K + 127) / 128, O);
+  project_pixels_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(*view, d_eulers, O, d_px, d_py, K, d_out_re,
+                                                                d_out_im);
+  b200d2::count_launch();
+  return b200d2::status_from_cuda(cudaGetLastError());
+}
+
 extern "C" int b200d2_projector_view(const b200d2_projector* p, int imgX,
                                      int imgY, int imgZ, int imgMaxR,
                                      int interp, b200d2_view* out) {

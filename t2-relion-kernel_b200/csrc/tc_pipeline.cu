@@ -28,6 +28,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -46,6 +47,9 @@ struct TcGeom {
 };
 
 static inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Largest |x| or |y| accepted for caller-listed pixel coordinates.
+constexpr int kListedExtent = 512;
 
 // Number of listed pixels and the largest |x| or |y| among them (the extent
 // of the phase tables).
@@ -71,7 +75,12 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec) {
   g.T = b.T;
   g.N_img = b.N_img;
   int extent = 0;
-  g.K_c = count_inside(v, b.N_img, &extent);
+  if (b.d_coor_xy) {
+    g.K_c = b.n_listed;  // caller-listed pixels (coordinates are device data)
+    extent = kListedExtent;
+  } else {
+    g.K_c = count_inside(v, b.N_img, &extent);
+  }
   g.elem = (prec == B200D2_PREC_BF16X3) ? 2 : 4;
   g.BK = 128 / g.elem;
   g.terms = (prec == B200D2_PREC_TF32) ? 1 : 3;
@@ -114,7 +123,9 @@ static inline T* ws_at(void* ws, size_t off) {
 // ------------------------------------------------------------------ stage 0
 __global__ void __launch_bounds__(1024) tc_pixel_list_kernel(b200d2_view v, int N_img, int2* xy,
                                                              int* idx, uint32_t* status,
-                                                             unsigned long long* keys, int P) {
+                                                             unsigned long long* keys, int P,
+                                                             const float* __restrict__ coor_xy,
+                                                             int n_listed, int ext) {
   __shared__ int s_cnt[32];
   __shared__ int s_base;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -123,6 +134,15 @@ __global__ void __launch_bounds__(1024) tc_pixel_list_kernel(b200d2_view v, int 
     s_base = 0;
   }
   for (int p = tid; p < P; p += blockDim.x) keys[p] = ~0ull;
+  if (coor_xy) {  // caller-listed pixels, in the caller's order
+    for (int k = tid; k < n_listed; k += blockDim.x) {
+      const int x = clampi(__float2int_rn(coor_xy[2 * k]), 0, ext);
+      const int y = clampi(__float2int_rn(coor_xy[2 * k + 1]), -ext, ext);
+      xy[k] = make_int2(x, y);
+      idx[k] = k;
+    }
+    return;
+  }
   __syncthreads();
   for (int base = 0; base < N_img; base += 1024) {
     const int i = base + tid;
@@ -353,22 +373,28 @@ __global__ void __launch_bounds__(256) tc_gen_a_kernel(
 }
 
 // ------------------------------------------------------------------ stage 6
-template <int PREC>
+// ROWB: bytes of one k-block row of an operand tile (128 -> 128-byte swizzle,
+// 64 -> 64-byte swizzle).  Narrower k-blocks give more pipeline stages in the
+// same shared memory, i.e. more TMA latency hidden behind the tensor pipe.
+template <int PREC, int ROWB>
 struct GemmCfg {
   static constexpr bool kTf32 = (PREC != B200D2_PREC_BF16X3);
   static constexpr int kElem = kTf32 ? 4 : 2;
-  static constexpr int kBK = 128 / kElem;       // elements per 128-byte k-block row
-  static constexpr int kKStep = kTf32 ? 8 : 16;  // K of one tcgen05.mma
+  static constexpr int kRowB = ROWB;
+  static constexpr int kBK = ROWB / kElem;       // elements per k-block row
+  static constexpr int kKStep = kTf32 ? 8 : 16;  // K of one tcgen05.mma (32 bytes)
   static constexpr int kTerms = (PREC == B200D2_PREC_TF32) ? 1 : 3;
   static constexpr int kPlanes = kTerms == 3 ? 2 : 1;
   static constexpr int kBM = 128, kBN = 256;
-  static constexpr int kATile = kBM * 128;
-  static constexpr int kBTile = kBN * 128;
+  static constexpr int kATile = kBM * ROWB;
+  static constexpr int kBTile = kBN * ROWB;
   static constexpr int kStageBytes = kPlanes * (kATile + kBTile);
-  static constexpr int kStages = kTerms == 3 ? 2 : 4;
+  static constexpr int kStages = (200 * 1024) / kStageBytes < 8 ? (200 * 1024) / kStageBytes : 8;
   static constexpr uint32_t kIdesc = sm100::idesc_f32acc(kTf32 ? 2u : 1u, kBM, kBN);
   static constexpr int kBarBytes = 256;
   static constexpr int kSmem = kStages * kStageBytes + kBarBytes + 1024;
+  static_assert(kStages >= 2, "at least two pipeline stages");
+  static_assert(2 * kStages * 8 + 5 * 8 + 8 <= kBarBytes, "barrier area");
 };
 
 struct GemmArgs {
@@ -390,13 +416,13 @@ __device__ __forceinline__ float from_ordered(uint32_t k) {
 
 constexpr uint64_t kWaitLimitNs = 4000000000ull;  // 4 s
 
-template <int PREC>
+template <int PREC, int ROWB>
 __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap mAhi,
                                                          const __grid_constant__ CUtensorMap mAlo,
                                                          const __grid_constant__ CUtensorMap mBhi,
                                                          const __grid_constant__ CUtensorMap mBlo,
                                                          const GemmArgs g) {
-  using C = GemmCfg<PREC>;
+  using C = GemmCfg<PREC, ROWB>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::kStages * C::kStageBytes);
@@ -505,13 +531,13 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
 #pragma unroll
           for (int ks = 0; ks < C::kBK / C::kKStep; ++ks) {
             const uint32_t koff = (uint32_t)(ks * C::kKStep * C::kElem);
-            const uint64_t dah = sm100::desc_k_sw128(a_hi + koff);
-            const uint64_t dbh = sm100::desc_k_sw128(b_hi + koff);
+            const uint64_t dah = sm100::desc_k_sw(a_hi + koff, C::kRowB);
+            const uint64_t dbh = sm100::desc_k_sw(b_hi + koff, C::kRowB);
             const uint32_t acc = (kb > 0 || ks > 0) ? 1u : 0u;
             sm100::mma<C::kTf32>(d, dah, dbh, C::kIdesc, acc);
             if (C::kTerms == 3) {
-              sm100::mma<C::kTf32>(d, dah, sm100::desc_k_sw128(b_lo + koff), C::kIdesc, 1u);
-              sm100::mma<C::kTf32>(d, sm100::desc_k_sw128(a_lo + koff), dbh, C::kIdesc, 1u);
+              sm100::mma<C::kTf32>(d, dah, sm100::desc_k_sw(b_lo + koff, C::kRowB), C::kIdesc, 1u);
+              sm100::mma<C::kTf32>(d, sm100::desc_k_sw(a_lo + koff, C::kRowB), dbh, C::kIdesc, 1u);
             }
           }
           sm100::mma_commit(&empty[s]);
@@ -609,15 +635,16 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   return fn;
 }
 
-static int make_map(CUtensorMap* m, void* base, int elem, int cols, int rows, int box_rows) {
+static int make_map(CUtensorMap* m, void* base, int elem, int cols, int rows, int box_rows, int row_bytes) {
   auto enc = get_encode();
   if (!enc) return B200D2_ERR_CUDA;
   const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)cols * elem};
-  const cuuint32_t box[2] = {(cuuint32_t)(128 / elem), (cuuint32_t)box_rows};
+  const cuuint32_t box[2] = {(cuuint32_t)(row_bytes / elem), (cuuint32_t)box_rows};
   const cuuint32_t es[2] = {1, 1};
   CUresult r = enc(m, elem == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
-                   base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   row_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? B200D2_OK : B200D2_ERR_CUDA;
 }
@@ -627,6 +654,60 @@ static int num_sms() {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   return sms;
+}
+
+// k-block row width used by the contraction (64 unless overridden by the
+// B200D2_GEMM_ROW_BYTES environment variable: 64 or 128).
+static int gemm_row_bytes() {
+  static int rb = 0;
+  if (rb == 0) {
+    const char* e = getenv("B200D2_GEMM_ROW_BYTES");
+    rb = (e && atoi(e) == 128) ? 128 : 64;
+  }
+  return rb;
+}
+
+template <int PREC, int ROWB>
+static int launch_gemm_rb(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s) {
+  using C = GemmCfg<PREC, ROWB>;
+  void* bhi = ws_at<void>(ws, g.off_bhi);
+  void* blo = ws_at<void>(ws, g.off_blo);
+  void* ahi = ws_at<void>(ws, g.off_ahi);
+  void* alo = ws_at<void>(ws, g.off_alo);
+  CUtensorMap mAhi, mAlo, mBhi, mBlo;
+  int st = make_map(&mAhi, ahi, g.elem, g.Kpad, g.Mpad, C::kBM, ROWB);
+  if (st == B200D2_OK) st = make_map(&mAlo, alo, g.elem, g.Kpad, g.Mpad, C::kBM, ROWB);
+  if (st == B200D2_OK) st = make_map(&mBhi, bhi, g.elem, g.Kpad, g.Opad, C::kBN, ROWB);
+  if (st == B200D2_OK) st = make_map(&mBlo, blo, g.elem, g.Kpad, g.Opad, C::kBN, ROWB);
+  if (st != B200D2_OK) return st;
+  GemmArgs a;
+  a.Mrows = g.Mrows;
+  a.Mtiles = g.Mpad / C::kBM;
+  a.Ntiles = g.Opad / C::kBN;
+  a.O = g.O;
+  a.T = g.T;
+  a.KB = g.Kpad / C::kBK;
+  a.accumulate = b.accumulate;
+  a.out = b.d_diff2;
+  a.na = ws_at<double>(ws, g.off_na);
+  a.keys = ws_at<unsigned long long>(ws, g.off_keys);
+  a.status = ws_at<uint32_t>(ws, g.off_status);
+  static bool attr_set = false;
+  if (!attr_set) {
+    B200D2_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<PREC, ROWB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, C::kSmem));
+    attr_set = true;
+  }
+  const int tiles = a.Mtiles * a.Ntiles;
+  const int grid = std::max(1, std::min(tiles, num_sms()));
+  tc_gemm_kernel<PREC, ROWB><<<grid, 192, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
+  count_launch();
+  return status_from_cuda(cudaGetLastError());
+}
+
+template <int PREC>
+static int launch_gemm(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s, int row_bytes) {
+  return row_bytes == 128 ? launch_gemm_rb<PREC, 128>(b, g, ws, s) : launch_gemm_rb<PREC, 64>(b, g, ws, s);
 }
 
 template <int PREC>
@@ -647,7 +728,8 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
   unsigned long long* keys = ws_at<unsigned long long>(ws, g.off_keys);
   switch (stage) {
     case 0:
-      tc_pixel_list_kernel<<<1, 1024, 0, s>>>(v, g.N_img, xy, idx, status, keys, g.P);
+      tc_pixel_list_kernel<<<1, 1024, 0, s>>>(v, g.N_img, xy, idx, status, keys, g.P, b.d_coor_xy,
+                                              g.K_c, g.maxR);
       break;
     case 1: {
       const int n = g.T * (g.exw + g.eyw);
@@ -674,37 +756,8 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
                                                  g.Kpad, ex, ey, g.T, g.maxR, g.Mrows, ahi, alo);
       break;
     }
-    case 6: {
-      using C = GemmCfg<PREC>;
-      CUtensorMap mAhi, mAlo, mBhi, mBlo;
-      int st = make_map(&mAhi, ahi, g.elem, g.Kpad, g.Mpad, C::kBM);
-      if (st == B200D2_OK) st = make_map(&mAlo, alo, g.elem, g.Kpad, g.Mpad, C::kBM);
-      if (st == B200D2_OK) st = make_map(&mBhi, bhi, g.elem, g.Kpad, g.Opad, C::kBN);
-      if (st == B200D2_OK) st = make_map(&mBlo, blo, g.elem, g.Kpad, g.Opad, C::kBN);
-      if (st != B200D2_OK) return st;
-      GemmArgs a;
-      a.Mrows = g.Mrows;
-      a.Mtiles = g.Mpad / C::kBM;
-      a.Ntiles = g.Opad / C::kBN;
-      a.O = g.O;
-      a.T = g.T;
-      a.KB = g.Kpad / C::kBK;
-      a.accumulate = b.accumulate;
-      a.out = b.d_diff2;
-      a.na = na;
-      a.keys = keys;
-      a.status = status;
-      static bool attr_set = false;
-      if (!attr_set) {
-        B200D2_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             C::kSmem));
-        attr_set = true;
-      }
-      const int tiles = a.Mtiles * a.Ntiles;
-      const int grid = std::max(1, std::min(tiles, num_sms()));
-      tc_gemm_kernel<PREC><<<grid, 192, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
-      break;
-    }
+    case 6:
+      return launch_gemm<PREC>(b, g, ws, s, gemm_row_bytes());
     case 7:
       tc_finalize_kernel<<<(g.P + 127) / 128, 128, 0, s>>>(keys, g.P, b.d_min, b.d_argmin);
       break;

@@ -177,6 +177,18 @@ __device__ __forceinline__ uint64_t desc_k_sw128(uint32_t smem_addr) {
   return d;
 }
 
+// K-major tile with rows of `row_bytes` (128 -> 128-byte swizzle, 64 -> 64-byte
+// swizzle): 8-row groups are 8 * row_bytes apart (SBO), LBO unused (1).
+__device__ __forceinline__ uint64_t desc_k_sw(uint32_t smem_addr, int row_bytes) {
+  uint64_t d = 0;
+  d |= (uint64_t)((smem_addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;
+  d |= (uint64_t)((8u * (uint32_t)row_bytes) >> 4) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)(row_bytes == 128 ? 2u : 4u) << 61;
+  return d;
+}
+
 // Instruction descriptor: F32 accumulator, A/B format `fmt` (1 = BF16 under
 // kind::f16, 2 = TF32 under kind::tf32), both K-major, M x N.
 __host__ __device__ constexpr uint32_t idesc_f32acc(uint32_t fmt, int M, int N) {

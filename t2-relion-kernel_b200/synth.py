@@ -240,6 +240,46 @@ def _noise_model(x, y, snr, signal_pow):
     return c * shape
 
 
+def write_projector_dat(path: str, pv: ProjectorVolume) -> None:
+    """projector_proc_*.dat: int32 {mdlX, mdlY, mdlZ, mdlInitY, mdlInitZ, mdlMaxR},
+    float32 padding_factor, float32 real[mdlX*mdlY*mdlZ], imag[...] (x fastest)
+    (reference reader: src/acc_projector_impl.h:300-334)."""
+    with open(path, "wb") as f:
+        np.array([pv.mdlX, pv.mdlY, pv.mdlZ, pv.mdlInitY, pv.mdlInitZ, pv.mdlMaxR], np.int32).tofile(f)
+        np.array([pv.padding_factor], np.float32).tofile(f)
+        np.ascontiguousarray(pv.re, np.float32).tofile(f)
+        np.ascontiguousarray(pv.im, np.float32).tofile(f)
+
+
+def write_coarse_dat(path: str, prob: CoarseProblem, p: int, diff2_init: np.ndarray | None = None) -> None:
+    """coarse_data*.dat for particle p: int32 {xdim, ydim, zdim, rmax, T, O, image_size},
+    float32 eulers[9*O], trans[2*T] (x block then y block), fimg[2*N] (real block
+    then imag block), corr[N], diff2s[O*T] (reference reader: src/main.cu:153-191)."""
+    N = prob.N_img
+    d2 = np.zeros(prob.O * prob.T, np.float32) if diff2_init is None else np.asarray(diff2_init, np.float32)
+    with open(path, "wb") as f:
+        np.array([prob.imgX, prob.imgY, 1, prob.imgMaxR, prob.T, prob.O, N], np.int32).tofile(f)
+        np.ascontiguousarray(prob.eulers, np.float32).tofile(f)
+        np.concatenate([prob.trans_x, prob.trans_y]).astype(np.float32).tofile(f)
+        np.concatenate([prob.fimg_re[p], prob.fimg_im[p]]).astype(np.float32).tofile(f)
+        np.ascontiguousarray(prob.corr[p], np.float32).tofile(f)
+        d2.reshape(-1).tofile(f)
+
+
+def read_coarse_dat(path: str) -> dict:
+    """Inverse of write_coarse_dat (same layout as the reference's replay files)."""
+    with open(path, "rb") as f:
+        hdr = np.fromfile(f, np.int32, 7)
+        xdim, ydim, zdim, rmax, T, O, N = (int(v) for v in hdr)
+        eul = np.fromfile(f, np.float32, 9 * O).reshape(O, 9)
+        tr = np.fromfile(f, np.float32, 2 * T)
+        fimg = np.fromfile(f, np.float32, 2 * N)
+        corr = np.fromfile(f, np.float32, N)
+        d2 = np.fromfile(f, np.float32, O * T)
+    return dict(xdim=xdim, ydim=ydim, zdim=zdim, rmax=rmax, T=T, O=O, image_size=N, eulers=eul,
+                trans_x=tr[:T], trans_y=tr[T:], fimg_re=fimg[:N], fimg_im=fimg[N:], corr=corr, diff2s=d2)
+
+
 def make_problem(name: str = "c1", seed: int = 20251203, P: int | None = None,
                  orient_limit: int | None = None) -> CoarseProblem:
     """Build a seeded synthetic coarse-pass problem.
