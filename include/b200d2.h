@@ -30,7 +30,8 @@ typedef enum b200d2_status {
   B200D2_ERR_CUDA = 3,        /* CUDA runtime error */
   B200D2_ERR_OOM = 4,         /* device allocation failed */
   B200D2_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
-  B200D2_ERR_NO_DEVICE = 6    /* no usable sm_100 device */
+  B200D2_ERR_NO_DEVICE = 6,   /* no usable sm_100 device */
+  B200D2_ERR_TOO_LARGE = 7    /* request exceeds a fixed capacity */
 } b200d2_status;
 
 /* How the projector volume is interpolated. */
@@ -182,6 +183,27 @@ size_t b200d2_diff2_coarse_batch_workspace(const b200d2_view* view,
 int b200d2_diff2_coarse_batch(const b200d2_view* view, const b200d2_batch* batch,
                               int precision, void* d_workspace,
                               size_t workspace_bytes, void* stream);
+
+/* Tensor-core batch that allocates nothing.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc: a host whose device memory is
+ * owned by another allocator (RELION's caching allocator reserves most of the
+ * card), a request path that must not pay cudaMalloc's device
+ * synchronisation, or a plug-in that receives only its input and output
+ * buffers.  Same semantics and outputs as b200d2_diff2_coarse_batch with a
+ * tensor-core precision, but the workspace is a fixed scratch area of
+ * B200D2_STATIC_SCRATCH_BYTES inside the library's device image, held by
+ * every GPU that loads the library until the process exits.  A batch whose
+ * b200d2_diff2_coarse_batch_workspace exceeds that size is rejected with
+ * B200D2_ERR_TOO_LARGE before anything runs (64 MiB holds, for example, 8
+ * particles x 576 orientations x 21 translations at image 32, or 16
+ * particles x 1536 orientations x 113 translations at image 64).  The
+ * scratch address is looked up on the first call on each device: make that
+ * call before any stream capture.  Calls share the scratch, so calls that
+ * overlap on the GPU race; serialise them.  Runs all stages on `stream`. */
+#define B200D2_STATIC_SCRATCH_BYTES (64ull << 20)
+int b200d2_diff2_coarse_batch_static(const b200d2_view* view,
+                                     const b200d2_batch* batch, int precision,
+                                     void* stream);
 
 /* Per-particle minimum and its index over d_diff2[p][0 .. n) (FP64 min,
  * lowest index on ties).  Used by the CUDA-core path; fused into the

@@ -31,7 +31,8 @@ PREC_BF16X3 = 3
 PREC_FP64 = 4
 
 _STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: "out of memory",
-           5: "device wait timed out", 6: "no device"}
+           5: "device wait timed out", 6: "no device", 7: "request exceeds a fixed capacity"}
+STATIC_SCRATCH_BYTES = 64 << 20  # B200D2_STATIC_SCRATCH_BYTES
 
 
 class B200D2Error(RuntimeError):
@@ -91,6 +92,7 @@ def _declare(L):
         "b200d2_diff2_coarse_batch": [C.POINTER(View), C.POINTER(Batch), I, P, Z, P],
         "b200d2_minloc": [P, C.c_longlong, I, P, P, P],
         "b200d2_project_pixels": [C.POINTER(View), P, I, P, P, I, P, P, P],
+        "b200d2_diff2_coarse_batch_static": [C.POINTER(View), C.POINTER(Batch), I, P],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -245,6 +247,16 @@ def diff2_coarse_batch(view: View, batch: Batch, precision: int = PREC_BF16X3, w
         workspace, int) else 0
     _check(lib().b200d2_diff2_coarse_batch(C.byref(view), C.byref(batch), precision, ws, nbytes,
                                            _stream(stream)), "diff2_coarse_batch")
+
+
+def diff2_coarse_batch_static(view: View, batch: Batch, precision: int = PREC_BF16X3, stream=None):
+    """The tensor-core batch on the library's fixed scratch (no device allocation).
+
+    For callers that cannot allocate device memory; rejects batches whose
+    workspace exceeds STATIC_SCRATCH_BYTES (B200D2Error code 7).  Calls share
+    the scratch, so they must not overlap on the GPU."""
+    _check(lib().b200d2_diff2_coarse_batch_static(C.byref(view), C.byref(batch), precision, _stream(stream)),
+           "diff2_coarse_batch_static")
 
 
 def minloc(diff2, n: int, P: int, out_min=None, out_argmin=None, stream=None):
