@@ -184,6 +184,54 @@ int b200d2_diff2_coarse_batch(const b200d2_view* view, const b200d2_batch* batch
                               int precision, void* d_workspace,
                               size_t workspace_bytes, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Plans: uneven batches in one persistent contraction launch, autotuned and
+ * captured in a CUDA graph.  Each particle has its own orientation subset
+ * (indices into the plan's orientation set) and its own translation set; its
+ * output is diff2[o_local][t] in its own buffer.  The reference scores such
+ * particles one runDiff2KernelCoarse call at a time (src/main.cu:483-503).
+ * A plan owns its workspace and tables; b200d2_plan_run replays the captured
+ * pipeline on the same device buffers, so callers refill the images in place.
+ * ---------------------------------------------------------------------- */
+typedef struct b200d2_particle_desc {
+  const float* d_real;  /* [N_img] device, CTF-folded image */
+  const float* d_imag;
+  const float* d_corr;  /* [N_img] device, Minvsigma2 * CTF^2 */
+  float* d_diff2;       /* [O][T] device output of this particle */
+  const int* h_orient;  /* host [O]: indices into the plan's orientations, NULL = 0..O-1 */
+  int O;
+  const float* h_trans_x; /* host [T] phase slopes */
+  const float* h_trans_y;
+  int T;
+} b200d2_particle_desc;
+
+enum {
+  B200D2_PLAN_AUTOTUNE = 1,   /* time the contraction variants, keep the fastest */
+  B200D2_PLAN_GRAPH = 2,      /* capture the whole pipeline in a CUDA graph */
+  B200D2_PLAN_ACCUMULATE = 4  /* add onto d_diff2 instead of overwriting */
+};
+
+typedef struct b200d2_plan_info {
+  int P, O_all, rows, tiles, tiles_dense, row_bytes, graph, stages;
+  long long evals;        /* sum over particles of O * T */
+  size_t workspace_bytes; /* plan-owned device bytes (workspace and tables) */
+  double tuned_ms[2];     /* contraction time of the 64- and 128-byte variants (0 = not timed) */
+} b200d2_plan_info;
+
+typedef struct b200d2_plan b200d2_plan;
+
+/* Build a plan for P particles against O_all orientations d_eulers[O_all][9].
+ * Host metadata is copied; device pointers must stay valid while the plan
+ * is used.  precision: a tensor-core precision.  d_min/d_argmin (optional,
+ * device [P]) receive each particle's minimum diff2 and o_local*T + t. */
+int b200d2_plan_create(const b200d2_view* view, const float* d_eulers, int O_all,
+                       int N_img, const b200d2_particle_desc* particles, int P,
+                       int precision, int flags, double* d_min,
+                       long long* d_argmin, b200d2_plan** out);
+int b200d2_plan_run(b200d2_plan* plan, void* stream);
+int b200d2_plan_get_info(const b200d2_plan* plan, b200d2_plan_info* info);
+int b200d2_plan_destroy(b200d2_plan* plan);
+
 /* Tensor-core batch that allocates nothing.  No counterpart in the reference.
  * For callers that cannot call cudaMalloc: a host whose device memory is
  * owned by another allocator (RELION's caching allocator reserves most of the

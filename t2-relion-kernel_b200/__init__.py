@@ -60,6 +60,24 @@ class Batch(C.Structure):
                 ("d_argmin", C.c_void_p), ("d_coor_xy", C.c_void_p), ("n_listed", C.c_int)]
 
 
+class ParticleDesc(C.Structure):
+    """b200d2_particle_desc: one particle of an uneven plan."""
+
+    _fields_ = [("d_real", C.c_void_p), ("d_imag", C.c_void_p), ("d_corr", C.c_void_p), ("d_diff2", C.c_void_p),
+                ("h_orient", C.c_void_p), ("O", C.c_int), ("h_trans_x", C.c_void_p), ("h_trans_y", C.c_void_p),
+                ("T", C.c_int)]
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("P", "O_all", "rows", "tiles", "tiles_dense", "row_bytes", "graph",
+                                         "stages")] + [
+        ("evals", C.c_longlong), ("workspace_bytes", C.c_size_t), ("tuned_ms", C.c_double * 2)]
+
+
+PLAN_AUTOTUNE = 1
+PLAN_GRAPH = 2
+PLAN_ACCUMULATE = 4
+
 _lib = None
 
 
@@ -93,6 +111,10 @@ def _declare(L):
         "b200d2_minloc": [P, C.c_longlong, I, P, P, P],
         "b200d2_project_pixels": [C.POINTER(View), P, I, P, P, I, P, P, P],
         "b200d2_diff2_coarse_batch_static": [C.POINTER(View), C.POINTER(Batch), I, P],
+        "b200d2_plan_create": [C.POINTER(View), P, I, I, C.POINTER(ParticleDesc), I, I, I, P, P, C.POINTER(P)],
+        "b200d2_plan_run": [P, P],
+        "b200d2_plan_get_info": [P, C.POINTER(PlanInfo)],
+        "b200d2_plan_destroy": [P],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -247,6 +269,61 @@ def diff2_coarse_batch(view: View, batch: Batch, precision: int = PREC_BF16X3, w
         workspace, int) else 0
     _check(lib().b200d2_diff2_coarse_batch(C.byref(view), C.byref(batch), precision, ws, nbytes,
                                            _stream(stream)), "diff2_coarse_batch")
+
+
+class Plan:
+    """Uneven batch in one persistent contraction launch (b200d2_plan_*).
+
+    `particles`: list of dicts with device tensors real, imag, corr, diff2
+    ([O_p*T_p]) and host numpy arrays orient (int32, or None), trans_x,
+    trans_y (float32)."""
+
+    def __init__(self, view: View, eulers, O_all: int, N_img: int, particles: list, precision: int = PREC_BF16X3,
+                 flags: int = PLAN_AUTOTUNE | PLAN_GRAPH, out_min=None, out_argmin=None):
+        self._keep = []
+        descs = (ParticleDesc * len(particles))()
+        for i, pt in enumerate(particles):
+            d = descs[i]
+            d.d_real, d.d_imag, d.d_corr, d.d_diff2 = (_ptr(pt[k]) for k in ("real", "imag", "corr", "diff2"))
+            orient = pt.get("orient")
+            if orient is not None:
+                orient = np.ascontiguousarray(orient, np.int32)
+                self._keep.append(orient)
+                d.h_orient = orient.ctypes.data_as(C.c_void_p)
+                d.O = int(orient.size)
+            else:
+                d.h_orient = None
+                d.O = int(pt["O"])
+            tx = np.ascontiguousarray(pt["trans_x"], np.float32)
+            ty = np.ascontiguousarray(pt["trans_y"], np.float32)
+            self._keep += [tx, ty]
+            d.h_trans_x = tx.ctypes.data_as(C.c_void_p)
+            d.h_trans_y = ty.ctypes.data_as(C.c_void_p)
+            d.T = int(tx.size)
+        self._h = C.c_void_p()
+        _check(lib().b200d2_plan_create(C.byref(view), _ptr(eulers), O_all, N_img, descs, len(particles), precision,
+                                        flags, _ptr(out_min), _ptr(out_argmin), C.byref(self._h)), "plan_create")
+
+    def run(self, stream=None):
+        _check(lib().b200d2_plan_run(self._h, _stream(stream)), "plan_run")
+
+    def info(self) -> dict:
+        inf = PlanInfo()
+        _check(lib().b200d2_plan_get_info(self._h, C.byref(inf)), "plan_get_info")
+        d = {n: getattr(inf, n) for n, _ in PlanInfo._fields_ if n != "tuned_ms"}
+        d["tuned_ms"] = list(inf.tuned_ms)
+        return d
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().b200d2_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def diff2_coarse_batch_static(view: View, batch: Batch, precision: int = PREC_BF16X3, stream=None):

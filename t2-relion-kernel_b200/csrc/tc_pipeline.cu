@@ -30,7 +30,9 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "common.cuh"
@@ -67,7 +69,9 @@ static int count_inside(const b200d2_view& v, int N_img, int* extent) {
   return n;
 }
 
-static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec) {
+// mrows >= 0 overrides the row count (uneven batches: the sum of every
+// particle's translations; b.T is then the number of phase tables).
+static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, int mrows = -1) {
   TcGeom g;
   memset(&g, 0, sizeof(g));
   g.P = b.P;
@@ -85,7 +89,7 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec) {
   g.BK = 128 / g.elem;
   g.terms = (prec == B200D2_PREC_TF32) ? 1 : 3;
   g.Kpad = (int)align_up((size_t)std::max(2 * g.K_c, 1), (size_t)g.BK);
-  g.Mrows = b.P * b.T;
+  g.Mrows = mrows >= 0 ? mrows : b.P * b.T;
   g.Mpad = (int)align_up((size_t)g.Mrows, 128);
   g.Opad = (int)align_up((size_t)b.O, 256);
   g.maxR = extent;  // phase tables cover x in [0, extent], y in [-extent, extent]
@@ -114,6 +118,36 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec) {
   g.total = o;
   return g;
 }
+
+// Per-particle description for uneven batches (device resident, built by a
+// plan).  Uniform batches pass no table and use base pointer + p * stride.
+struct PartDev {
+  const float* re;
+  const float* im;
+  const float* corr;
+  float* out;      // [O][T] of this particle
+  const int* inv;  // [O_all] -> index in this particle's orientation list, or -1
+  int T, O, row0, pad;
+};
+
+// Device tables of an uneven batch, owned by a plan.
+struct UnevenTabs {
+  const PartDev* parts;   // [P]
+  const int4* rows;       // [Mrows]
+  const int2* tiles;      // [ntiles]
+  int ntiles;
+  const float2* tab_txy;  // [ntab] translation of each phase table
+  int ntab;
+  int Mrows;
+};
+
+// Optional tables of an uneven batch; all null for a uniform batch.
+struct Layout {
+  const PartDev* parts;  // [P]
+  const int4* rows;      // [Mrows]: (particle, translation, phase table, 0)
+  const int2* tiles;     // [ntiles]: (m tile, n tile) that some particle needs
+  int ntiles;
+};
 
 template <typename T>
 static inline T* ws_at(void* ws, size_t off) {
@@ -173,19 +207,24 @@ __global__ void __launch_bounds__(1024) tc_pixel_list_kernel(b200d2_view v, int 
 }
 
 // ------------------------------------------------------------------ stage 1
+// T phase tables (one per translation).  With `txy` given, ntab tables whose
+// translation is txy[tab] (uneven batches: one table per distinct
+// translation of every particle); otherwise table t uses (tx[t], ty[t]).
 __global__ void tc_phase_kernel(const float* __restrict__ tx, const float* __restrict__ ty, int T,
-                                int maxR, float2* ex, float2* ey) {
+                                int maxR, float2* ex, float2* ey, const float2* __restrict__ txy) {
   const int exw = maxR + 1, eyw = 2 * maxR + 1;
   const int n1 = T * exw, n2 = T * eyw;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n1 + n2; i += gridDim.x * blockDim.x) {
     double s, c;
     if (i < n1) {
       const int t = i / exw, x = i % exw;
-      sincos((double)x * (double)tx[t], &s, &c);
+      const float sx = txy ? txy[t].x : tx[t];
+      sincos((double)x * (double)sx, &s, &c);
       ex[i] = make_float2((float)c, (float)s);
     } else {
       const int j = i - n1, t = j / eyw, y = j % eyw - maxR;
-      sincos((double)y * (double)ty[t], &s, &c);
+      const float sy = txy ? txy[t].y : ty[t];
+      sincos((double)y * (double)sy, &s, &c);
       ey[j] = make_float2((float)c, (float)s);
     }
   }
@@ -244,12 +283,16 @@ __global__ void __launch_bounds__(128) tc_project_kernel(b200d2_view v, const fl
 __global__ void __launch_bounds__(256) tc_normx_kernel(const float* __restrict__ re,
                                                        const float* __restrict__ im,
                                                        const float* __restrict__ corr,
-                                                       long long stride, int N_img, double* normx) {
+                                                       long long stride, int N_img, double* normx,
+                                                       const PartDev* __restrict__ parts) {
   const long long p = blockIdx.x;
+  const float* pre = parts ? parts[p].re : re + p * stride;
+  const float* pim = parts ? parts[p].im : im + p * stride;
+  const float* pco = parts ? parts[p].corr : corr + p * stride;
   double acc = 0.0;
   for (int i = threadIdx.x; i < N_img; i += blockDim.x) {
-    const double r = re[p * stride + i], m = im[p * stride + i];
-    acc += (r * r + m * m) * ((double)corr[p * stride + i] / 2.0);
+    const double r = pre[i], m = pim[i];
+    acc += (r * r + m * m) * ((double)pco[i] / 2.0);
   }
   __shared__ double s[8];
 #pragma unroll
@@ -272,7 +315,8 @@ __global__ void __launch_bounds__(256) tc_normx_kernel(const float* __restrict__
 __global__ void __launch_bounds__(256) tc_norma_kernel(const float* __restrict__ corr, long long stride,
                                                        const int* __restrict__ idx, int K_c,
                                                        const float* __restrict__ q, int O, int P,
-                                                       const double* __restrict__ normx, double* na) {
+                                                       const double* __restrict__ normx, double* na,
+                                                       const PartDev* __restrict__ parts) {
   constexpr int KC = 32;
   __shared__ __align__(16) double sw[KC][64];
   __shared__ double sq[KC][65];
@@ -287,7 +331,10 @@ __global__ void __launch_bounds__(256) tc_norma_kernel(const float* __restrict__
     for (int e = tid; e < 64 * KC; e += 256) {
       const int pp = e % 64, k = e / 64;  // consecutive threads: consecutive particles
       double w = 0.0;
-      if (p0 + pp < P && k0 + k < K_c) w = (double)corr[(long long)(p0 + pp) * stride + idx[k0 + k]] / 2.0;
+      if (p0 + pp < P && k0 + k < K_c) {
+        const float* pc = parts ? parts[p0 + pp].corr : corr + (long long)(p0 + pp) * stride;
+        w = (double)pc[idx[k0 + k]] / 2.0;
+      }
       sw[k][pp] = w;
     }
     for (int e = tid; e < 64 * KC; e += 256) {
@@ -328,7 +375,7 @@ __global__ void __launch_bounds__(256) tc_gen_a_kernel(
     const float* __restrict__ re, const float* __restrict__ im, const float* __restrict__ corr,
     long long stride, const int2* __restrict__ xy, const int* __restrict__ idx, int K_c, int Kpad,
     const float2* __restrict__ ex, const float2* __restrict__ ey, int T, int maxR, int Mrows,
-    void* ahi, void* alo) {
+    void* ahi, void* alo, const PartDev* __restrict__ parts, const int4* __restrict__ rows) {
   constexpr int ROWS = 32;
   const int kp = blockIdx.x * blockDim.x + threadIdx.x;
   if (kp >= Kpad / 2) return;
@@ -342,23 +389,39 @@ __global__ void __launch_bounds__(256) tc_gen_a_kernel(
   }
   const int exw = maxR + 1, eyw = 2 * maxR + 1;
   const int m0 = blockIdx.y * ROWS;
-  int p = m0 / T;
-  int t = m0 - p * T;
+  int p = rows ? 0 : m0 / T;
+  int t = rows ? 0 : m0 - p * T;
   int cur_p = -1;
   float wr = 0.f, wi = 0.f;
   for (int r = 0; r < ROWS; ++r) {
     const int m = m0 + r;
     float ar = 0.f, ai = 0.f;
     if (has && m < Mrows) {
+      int tab = t;
+      if (rows) {  // uneven batch: (particle, translation, phase table) from the row table
+        const int4 rw = rows[m];
+        p = rw.x;
+        tab = rw.z;
+      }
       if (p != cur_p) {
-        const long long at = (long long)p * stride + pix;
-        const float w = corr[at] / 2;
-        wr = w * re[at];
-        wi = w * im[at];
+        float w, xr, xi;
+        if (parts) {
+          const PartDev& pd = parts[p];
+          w = pd.corr[pix] / 2;
+          xr = pd.re[pix];
+          xi = pd.im[pix];
+        } else {
+          const long long at = (long long)p * stride + pix;
+          w = corr[at] / 2;
+          xr = re[at];
+          xi = im[at];
+        }
+        wr = w * xr;
+        wi = w * xi;
         cur_p = p;
       }
-      const float2 fx = ex[t * exw + x];
-      const float2 fy = ey[t * eyw + y + maxR];
+      const float2 fx = ex[tab * exw + x];
+      const float2 fy = ey[tab * eyw + y + maxR];
       const float pr = __fmaf_rn(fx.x, fy.x, -__fmul_rn(fx.y, fy.y));
       const float pi = __fmaf_rn(fx.x, fy.y, __fmul_rn(fx.y, fy.x));
       ar = __fmaf_rn(wr, pr, -__fmul_rn(wi, pi));
@@ -403,7 +466,21 @@ struct GemmArgs {
   const double* na;
   unsigned long long* keys;
   uint32_t* status;
+  Layout L;  // uneven batch tables (all null for a uniform batch)
 };
+
+// (m0, n0) of the tile-th work item: the work list of an uneven batch, or
+// the dense m-major order of a uniform one.
+__device__ __forceinline__ void tile_origin(const GemmArgs& g, int tile, int bm, int bn, int& m0, int& n0) {
+  if (g.L.tiles) {
+    const int2 mn = g.L.tiles[tile];
+    m0 = mn.x * bm;
+    n0 = mn.y * bn;
+  } else {
+    m0 = (tile / g.Ntiles) * bm;
+    n0 = (tile % g.Ntiles) * bn;
+  }
+}
 
 __device__ __forceinline__ uint32_t ordered_bits(float f) {
   const uint32_t u = __float_as_uint(f);
@@ -464,7 +541,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   __syncthreads();
   sm100::tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int num_tiles = g.Mtiles * g.Ntiles;
+  const int num_tiles = g.L.tiles ? g.L.ntiles : g.Mtiles * g.Ntiles;
 
   auto raise_abort = [&]() {
     *s_abort = 1;
@@ -477,7 +554,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       uint32_t gk = 0;
       bool ok = true;
       for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
-        const int m0 = (tile / g.Ntiles) * C::kBM, n0 = (tile % g.Ntiles) * C::kBN;
+        int m0, n0;
+        tile_origin(g, tile, C::kBM, C::kBN, m0, n0);
         for (int kb = 0; kb < g.KB; ++kb, ++gk) {
           const int s = gk % C::kStages;
           const uint32_t u = gk / C::kStages;
@@ -564,13 +642,30 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         break;
       }
       sm100::tc_fence_after();
-      const int m0 = (tile / g.Ntiles) * C::kBM, n0 = (tile % g.Ntiles) * C::kBN;
+      int m0, n0;
+      tile_origin(g, tile, C::kBM, C::kBN, m0, n0);
       const int m = m0 + row;
       const bool vrow = m < g.Mrows;
-      const int p = vrow ? m / g.T : 0;
-      const int t = vrow ? m - p * g.T : 0;
+      int p = 0, t = 0, Tp = g.T;
+      float* outp = g.out;
+      const int* __restrict__ inv = nullptr;  // orientation -> this particle's list index
+      if (vrow) {
+        if (g.L.rows) {
+          const int4 rw = g.L.rows[m];
+          p = rw.x;
+          t = rw.y;
+          const PartDev& pd = g.L.parts[p];
+          Tp = pd.T;
+          outp = pd.out;
+          inv = pd.inv;
+        } else {
+          p = m / g.T;
+          t = m - p * g.T;
+          outp = g.out + (size_t)p * g.O * g.T;
+        }
+      }
       const double* __restrict__ na_row = g.na + (size_t)p * g.O;
-      float* __restrict__ out_row = g.out + (size_t)p * g.O * g.T + t;
+      float* __restrict__ out_row = outp + t;
       float best = __int_as_float(0x7f800000);
       uint32_t best_idx = 0xffffffffu;
 #pragma unroll 1
@@ -584,15 +679,16 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int o = oc + j;
-            if (o < g.O) {
+            const int lo = (o < g.O) ? (inv ? inv[o] : o) : -1;
+            if (lo >= 0) {
               const double dd = fma(-2.0, (double)__uint_as_float(r[j]), na_row[o]);
               float f = (float)dd;
-              float* dst = out_row + (size_t)o * g.T;
+              float* dst = out_row + (size_t)lo * Tp;
               if (g.accumulate) f += *dst;
               *dst = f;
               if (f < best) {
                 best = f;
-                best_idx = (uint32_t)(o * g.T + t);
+                best_idx = (uint32_t)(lo * Tp + t);
               }
             }
           }
@@ -668,7 +764,8 @@ static int gemm_row_bytes() {
 }
 
 template <int PREC, int ROWB>
-static int launch_gemm_rb(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s) {
+static int launch_gemm_rb(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s,
+                          const UnevenTabs* U) {
   using C = GemmCfg<PREC, ROWB>;
   void* bhi = ws_at<void>(ws, g.off_bhi);
   void* blo = ws_at<void>(ws, g.off_blo);
@@ -692,13 +789,15 @@ static int launch_gemm_rb(const b200d2_batch& b, const TcGeom& g, void* ws, cuda
   a.na = ws_at<double>(ws, g.off_na);
   a.keys = ws_at<unsigned long long>(ws, g.off_keys);
   a.status = ws_at<uint32_t>(ws, g.off_status);
+  a.L = Layout{U ? U->parts : nullptr, U ? U->rows : nullptr, U ? U->tiles : nullptr, U ? U->ntiles : 0};
   static bool attr_set = false;
   if (!attr_set) {
     B200D2_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<PREC, ROWB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, C::kSmem));
     attr_set = true;
   }
-  const int tiles = a.Mtiles * a.Ntiles;
+  const int tiles = U ? U->ntiles : a.Mtiles * a.Ntiles;
+  if (tiles == 0) return B200D2_OK;
   const int grid = std::max(1, std::min(tiles, num_sms()));
   tc_gemm_kernel<PREC, ROWB><<<grid, 192, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
   count_launch();
@@ -706,13 +805,16 @@ static int launch_gemm_rb(const b200d2_batch& b, const TcGeom& g, void* ws, cuda
 }
 
 template <int PREC>
-static int launch_gemm(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s, int row_bytes) {
-  return row_bytes == 128 ? launch_gemm_rb<PREC, 128>(b, g, ws, s) : launch_gemm_rb<PREC, 64>(b, g, ws, s);
+static int launch_gemm(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s, int row_bytes,
+                       const UnevenTabs* U) {
+  return row_bytes == 128 ? launch_gemm_rb<PREC, 128>(b, g, ws, s, U)
+                          : launch_gemm_rb<PREC, 64>(b, g, ws, s, U);
 }
 
 template <int PREC>
 static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeom& g, void* ws, int stage,
-                        cudaStream_t s) {
+                        cudaStream_t s, const UnevenTabs* U, int row_bytes) {
+  const PartDev* parts = U ? U->parts : nullptr;
   uint32_t* status = ws_at<uint32_t>(ws, g.off_status);
   int2* xy = ws_at<int2>(ws, g.off_xy);
   int* idx = ws_at<int>(ws, g.off_idx);
@@ -734,7 +836,7 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
     case 1: {
       const int n = g.T * (g.exw + g.eyw);
       tc_phase_kernel<<<std::max(1, std::min((n + 255) / 256, 1024)), 256, 0, s>>>(
-          b.d_trans_x, b.d_trans_y, g.T, g.maxR, ex, ey);
+          b.d_trans_x, b.d_trans_y, g.T, g.maxR, ex, ey, U ? U->tab_txy : nullptr);
       break;
     }
     case 2: {
@@ -743,21 +845,22 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       break;
     }
     case 3:
-      tc_normx_kernel<<<g.P, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, g.N_img, normx);
+      tc_normx_kernel<<<g.P, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, g.N_img, normx, parts);
       break;
     case 4: {
       dim3 grid((g.O + 63) / 64, (g.P + 63) / 64);
-      tc_norma_kernel<<<grid, 256, 0, s>>>(b.d_corr, b.img_stride, idx, g.K_c, q, g.O, g.P, normx, na);
+      tc_norma_kernel<<<grid, 256, 0, s>>>(b.d_corr, b.img_stride, idx, g.K_c, q, g.O, g.P, normx, na, parts);
       break;
     }
     case 5: {
       dim3 grid((g.Kpad / 2 + 255) / 256, g.Mpad / 32);
       tc_gen_a_kernel<PREC><<<grid, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, xy, idx, g.K_c,
-                                                 g.Kpad, ex, ey, g.T, g.maxR, g.Mrows, ahi, alo);
+                                                 g.Kpad, ex, ey, g.T, g.maxR, g.Mrows, ahi, alo, parts,
+                                                 U ? U->rows : nullptr);
       break;
     }
     case 6:
-      return launch_gemm<PREC>(b, g, ws, s, gemm_row_bytes());
+      return launch_gemm<PREC>(b, g, ws, s, row_bytes > 0 ? row_bytes : gemm_row_bytes(), U);
     case 7:
       tc_finalize_kernel<<<(g.P + 127) / 128, 128, 0, s>>>(keys, g.P, b.d_min, b.d_argmin);
       break;
@@ -769,11 +872,11 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
 }
 
 static int dispatch_stage(const b200d2_view& v, const b200d2_batch& b, int prec, const TcGeom& g, void* ws,
-                          int stage, cudaStream_t s) {
+                          int stage, cudaStream_t s, const UnevenTabs* U = nullptr, int row_bytes = 0) {
   switch (prec) {
-    case B200D2_PREC_BF16X3: return launch_stage<B200D2_PREC_BF16X3>(v, b, g, ws, stage, s);
-    case B200D2_PREC_TF32X3: return launch_stage<B200D2_PREC_TF32X3>(v, b, g, ws, stage, s);
-    case B200D2_PREC_TF32: return launch_stage<B200D2_PREC_TF32>(v, b, g, ws, stage, s);
+    case B200D2_PREC_BF16X3: return launch_stage<B200D2_PREC_BF16X3>(v, b, g, ws, stage, s, U, row_bytes);
+    case B200D2_PREC_TF32X3: return launch_stage<B200D2_PREC_TF32X3>(v, b, g, ws, stage, s, U, row_bytes);
+    case B200D2_PREC_TF32: return launch_stage<B200D2_PREC_TF32>(v, b, g, ws, stage, s, U, row_bytes);
     default: return B200D2_ERR_UNSUPPORTED;
   }
 }
@@ -882,7 +985,285 @@ int tc_run(const b200d2_view& v, const b200d2_batch& b, int precision, void* ws,
   return st;
 }
 
+// ------------------------------------------------------------------ plans
+// Autotuner cache: contraction variant chosen for a problem signature.
+struct TuneKey {
+  int prec, Kpad, O, mtiles, ntiles;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(prec, Kpad, O, mtiles, ntiles) < std::tie(o.prec, o.Kpad, o.O, o.mtiles, o.ntiles);
+  }
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, int> g_tune_cache;
+
 }  // namespace b200d2
+
+struct b200d2_plan {
+  b200d2_view view;
+  b200d2_batch batch;  // shared geometry (T = number of phase tables), min/argmin outputs
+  int prec = 0, flags = 0, row_bytes = 64;
+  b200d2::TcGeom g;
+  b200d2::UnevenTabs U;
+  void* ws = nullptr;
+  b200d2::PartDev* d_parts = nullptr;
+  int4* d_rows = nullptr;
+  int2* d_tiles = nullptr;
+  float2* d_txy = nullptr;
+  int* d_inv = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  b200d2_plan_info info;
+};
+
+namespace b200d2 {
+
+static void plan_free(b200d2_plan* p) {
+  if (!p) return;
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  if (p->stream) cudaStreamDestroy(p->stream);
+  for (void* d : {(void*)p->ws, (void*)p->d_parts, (void*)p->d_rows, (void*)p->d_tiles, (void*)p->d_txy,
+                  (void*)p->d_inv})
+    if (d) cudaFree(d);
+  delete p;
+}
+
+// All stages in order on one stream (the form that is captured).
+static int plan_pipeline(b200d2_plan* p, cudaStream_t s, int row_bytes) {
+  int st = B200D2_OK;
+  for (int i = 0; i < kNumStages && st == B200D2_OK; ++i)
+    st = dispatch_stage(p->view, p->batch, p->prec, p->g, p->ws, i, s, &p->U, row_bytes);
+  return st;
+}
+
+static double time_gemm(b200d2_plan* p, int row_bytes, int reps) {
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  double best = 1e30;
+  for (int r = 0; r < reps; ++r) {
+    cudaEventRecord(a, p->stream);
+    int st = dispatch_stage(p->view, p->batch, p->prec, p->g, p->ws, 6, p->stream, &p->U, row_bytes);
+    cudaEventRecord(b, p->stream);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (st == B200D2_OK) best = std::min(best, (double)ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return best;
+}
+
+}  // namespace b200d2
+
+extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers, int O_all, int N_img,
+                                  const b200d2_particle_desc* parts, int P, int precision, int flags,
+                                  double* d_min, long long* d_argmin, b200d2_plan** out) {
+  using namespace b200d2;
+  if (!view || !d_eulers || !parts || !out || P <= 0 || O_all <= 0 || N_img <= 0) return B200D2_ERR_INVALID;
+  *out = nullptr;
+  if (precision != B200D2_PREC_BF16X3 && precision != B200D2_PREC_TF32X3 && precision != B200D2_PREC_TF32)
+    return B200D2_ERR_UNSUPPORTED;
+  if (view->mdlZ == 0 || (long long)view->imgX * view->imgY < N_img) return B200D2_ERR_INVALID;
+  for (int i = 0; i < P; ++i) {
+    const b200d2_particle_desc& d = parts[i];
+    if (!d.d_real || !d.d_imag || !d.d_corr || !d.d_diff2 || !d.h_trans_x || !d.h_trans_y) return B200D2_ERR_INVALID;
+    if (d.O <= 0 || d.T <= 0 || d.O > O_all) return B200D2_ERR_INVALID;
+    if ((long long)d.O * d.T >= 0xffffffffLL) return B200D2_ERR_UNSUPPORTED;
+    if (d.h_orient)
+      for (int k = 0; k < d.O; ++k)
+        if (d.h_orient[k] < 0 || d.h_orient[k] >= O_all) return B200D2_ERR_INVALID;
+  }
+  b200d2_plan* p = new b200d2_plan();
+  p->view = *view;
+  p->prec = precision;
+  p->flags = flags;
+
+  // distinct translation sets -> phase tables; rows (particle, t, table)
+  std::map<std::vector<std::pair<uint32_t, uint32_t>>, int> sets;
+  std::vector<float2> txy;
+  std::vector<int> tab0(P);
+  std::vector<int4> rows;
+  std::vector<PartDev> hp(P);
+  long long evals = 0;
+  for (int i = 0; i < P; ++i) {
+    const b200d2_particle_desc& d = parts[i];
+    std::vector<std::pair<uint32_t, uint32_t>> key(d.T);
+    for (int t = 0; t < d.T; ++t) {
+      uint32_t a, c;
+      memcpy(&a, &d.h_trans_x[t], 4);
+      memcpy(&c, &d.h_trans_y[t], 4);
+      key[t] = {a, c};
+    }
+    auto it = sets.find(key);
+    if (it == sets.end()) {
+      it = sets.emplace(key, (int)txy.size()).first;
+      for (int t = 0; t < d.T; ++t) txy.push_back(make_float2(d.h_trans_x[t], d.h_trans_y[t]));
+    }
+    tab0[i] = it->second;
+    hp[i].re = d.d_real;
+    hp[i].im = d.d_imag;
+    hp[i].corr = d.d_corr;
+    hp[i].out = d.d_diff2;
+    hp[i].T = d.T;
+    hp[i].O = d.O;
+    hp[i].row0 = (int)rows.size();
+    hp[i].pad = 0;
+    for (int t = 0; t < d.T; ++t) rows.push_back(make_int4(i, t, tab0[i] + t, 0));
+    evals += (long long)d.O * d.T;
+  }
+  const int Mrows = (int)rows.size();
+  const int Mtiles = (Mrows + 127) / 128, Ntiles = (O_all + 255) / 256;
+
+  // orientation -> local index maps, and the n-tiles each particle needs
+  std::vector<int> inv((size_t)P * O_all, -1);
+  std::vector<std::vector<char>> need_n(P, std::vector<char>(Ntiles, 0));
+  for (int i = 0; i < P; ++i) {
+    const b200d2_particle_desc& d = parts[i];
+    for (int k = 0; k < d.O; ++k) {
+      const int o = d.h_orient ? d.h_orient[k] : k;
+      inv[(size_t)i * O_all + o] = k;
+      need_n[i][o / 256] = 1;
+    }
+  }
+  // work list: (m tile, n tile) pairs some particle of the m tile needs, m-major
+  std::vector<int2> tiles;
+  for (int mt = 0; mt < Mtiles; ++mt) {
+    const int r0 = mt * 128, r1 = std::min(Mrows, r0 + 128);
+    std::vector<char> un(Ntiles, 0);
+    for (int pi = rows[r0].x; pi <= rows[r1 - 1].x; ++pi)
+      for (int n = 0; n < Ntiles; ++n) un[n] |= need_n[pi][n];
+    for (int n = 0; n < Ntiles; ++n)
+      if (un[n]) tiles.push_back(make_int2(mt, n));
+  }
+
+  b200d2_batch& b = p->batch;
+  memset(&b, 0, sizeof(b));
+  b.d_eulers = d_eulers;
+  b.O = O_all;
+  b.T = (int)txy.size();  // number of phase tables
+  b.P = P;
+  b.N_img = N_img;
+  b.d_real = parts[0].d_real;  // unused by the tabled kernels; kept valid
+  b.d_imag = parts[0].d_imag;
+  b.d_corr = parts[0].d_corr;
+  b.img_stride = N_img;
+  b.d_diff2 = parts[0].d_diff2;
+  b.accumulate = (flags & B200D2_PLAN_ACCUMULATE) ? 1 : 0;
+  b.d_min = d_min;
+  b.d_argmin = d_argmin;
+  p->g = make_geom(*view, b, precision, Mrows);
+
+  int st = B200D2_OK;
+  auto upload = [&](void** dst, const void* src, size_t bytes) {
+    if (st != B200D2_OK) return;
+    cudaError_t e = cudaMalloc(dst, std::max(bytes, (size_t)16));
+    if (e == cudaSuccess && bytes) e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+    st = status_from_cuda(e);
+  };
+  st = status_from_cuda(cudaMalloc(&p->ws, p->g.total));
+  upload(reinterpret_cast<void**>(&p->d_rows), rows.data(), rows.size() * sizeof(int4));
+  upload(reinterpret_cast<void**>(&p->d_tiles), tiles.data(), tiles.size() * sizeof(int2));
+  upload(reinterpret_cast<void**>(&p->d_txy), txy.data(), txy.size() * sizeof(float2));
+  upload(reinterpret_cast<void**>(&p->d_inv), inv.data(), inv.size() * sizeof(int));
+  if (st == B200D2_OK)
+    for (int i = 0; i < P; ++i) hp[i].inv = p->d_inv + (size_t)i * O_all;
+  upload(reinterpret_cast<void**>(&p->d_parts), hp.data(), hp.size() * sizeof(PartDev));
+  if (st == B200D2_OK) st = status_from_cuda(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  if (st != B200D2_OK) {
+    plan_free(p);
+    return st;
+  }
+  p->U = UnevenTabs{p->d_parts, p->d_rows, p->d_tiles, (int)tiles.size(), p->d_txy, (int)txy.size(), Mrows};
+
+  memset(&p->info, 0, sizeof(p->info));
+  p->info.P = P;
+  p->info.O_all = O_all;
+  p->info.rows = Mrows;
+  p->info.tiles = (int)tiles.size();
+  p->info.tiles_dense = Mtiles * Ntiles;
+  p->info.evals = evals;
+  p->info.stages = kNumStages;
+  p->info.workspace_bytes = p->g.total + rows.size() * sizeof(int4) + tiles.size() * sizeof(int2) +
+                            txy.size() * sizeof(float2) + inv.size() * sizeof(int) + hp.size() * sizeof(PartDev);
+
+  // warm run (also sets kernel attributes outside any capture)
+  p->row_bytes = gemm_row_bytes();
+  st = plan_pipeline(p, p->stream, p->row_bytes);
+  if (st == B200D2_OK) st = status_from_cuda(cudaStreamSynchronize(p->stream));
+  if (st == B200D2_OK && (flags & B200D2_PLAN_AUTOTUNE)) {
+    const TuneKey key{precision, p->g.Kpad, O_all, Mtiles, (int)tiles.size()};
+    int cached = 0;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end()) cached = it->second;
+    }
+    if (cached) {
+      p->row_bytes = cached;
+    } else {
+      const int cand[2] = {64, 128};
+      double best = 1e30;
+      for (int c = 0; c < 2; ++c) {
+        time_gemm(p, cand[c], 1);  // first launch of a variant sets its attributes
+        const double ms = time_gemm(p, cand[c], 3);
+        p->info.tuned_ms[c] = ms;
+        if (ms < best) {
+          best = ms;
+          p->row_bytes = cand[c];
+        }
+      }
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_tune_cache[key] = p->row_bytes;
+    }
+    // leave the outputs as one full run with the chosen variant produces them
+    st = plan_pipeline(p, p->stream, p->row_bytes);
+    if (st == B200D2_OK) st = status_from_cuda(cudaStreamSynchronize(p->stream));
+  }
+  p->info.row_bytes = p->row_bytes;
+  if (st == B200D2_OK && (flags & B200D2_PLAN_GRAPH)) {
+    st = status_from_cuda(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+    if (st == B200D2_OK) {
+      const int st2 = plan_pipeline(p, p->stream, p->row_bytes);
+      const cudaError_t e = cudaStreamEndCapture(p->stream, &p->graph);
+      st = st2 != B200D2_OK ? st2 : status_from_cuda(e);
+    }
+    if (st == B200D2_OK) st = status_from_cuda(cudaGraphInstantiate(&p->exec, p->graph, 0));
+    p->info.graph = (st == B200D2_OK) ? 1 : 0;
+  }
+  if (st != B200D2_OK) {
+    plan_free(p);
+    return st;
+  }
+  *out = p;
+  return B200D2_OK;
+}
+
+extern "C" int b200d2_plan_run(b200d2_plan* p, void* stream) {
+  if (!p) return B200D2_ERR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (p->exec) {
+    B200D2_CUDA_TRY(cudaGraphLaunch(p->exec, s));
+    b200d2::count_launch(b200d2::kNumStages);
+    return B200D2_OK;
+  }
+  return b200d2::plan_pipeline(p, s, p->row_bytes);
+}
+
+extern "C" int b200d2_plan_get_info(const b200d2_plan* p, b200d2_plan_info* info) {
+  if (!p || !info) return B200D2_ERR_INVALID;
+  *info = p->info;
+  return B200D2_OK;
+}
+
+extern "C" int b200d2_plan_destroy(b200d2_plan* p) {
+  if (!p) return B200D2_ERR_INVALID;
+  cudaStreamSynchronize(p->stream);
+  b200d2::plan_free(p);
+  return B200D2_OK;
+}
 
 extern "C" int b200d2_workspace_status(const void* d_workspace, void* stream, int* status) {
   if (!d_workspace || !status) return B200D2_ERR_INVALID;
