@@ -211,6 +211,32 @@ def reference_arm(args):
 PREC = {"fp32": 0, "tf32": 1, "tf32x3": 2, "bf16x3": 3}
 
 
+def build_plan_case(pkg, pr, dev, prec, flags):
+    """Uneven batch (per-particle orientation subsets and translation sets)
+    as one plan; outputs are slices of one buffer."""
+    import torch
+    eul = torch.as_tensor(pr.eulers.reshape(-1), device=dev)
+    re = torch.as_tensor(pr.fimg_re, device=dev)
+    im = torch.as_tensor(pr.fimg_im, device=dev)
+    corr = torch.as_tensor(pr.corr, device=dev)
+    sizes = [len(o) * len(t) for o, t in zip(pr.orient_lists, pr.trans_lists)]
+    out = torch.empty(sum(sizes), device=dev)
+    parts, off = [], 0
+    for p in range(pr.P):
+        tl = pr.trans_lists[p]
+        parts.append(dict(real=re[p], imag=im[p], corr=corr[p], diff2=out[off:off + sizes[p]],
+                          orient=pr.orient_lists[p], trans_x=tl[:, 0].copy(), trans_y=tl[:, 1].copy()))
+        off += sizes[p]
+    mn = torch.empty(pr.P, device=dev, dtype=torch.float64)
+    am = torch.empty(pr.P, device=dev, dtype=torch.int64)
+    plan = pkg.Plan(pkg_view_cache["view"], eul, pr.O, pr.N_img, parts, prec, flags=flags, out_min=mn,
+                    out_argmin=am)
+    return plan, (eul, re, im, corr, out, mn, am), sum(sizes)
+
+
+pkg_view_cache: dict = {}
+
+
 def ours_arm(args):
     import torch
     rank, world, local, dist = dist_setup(args.gpus)
@@ -234,16 +260,49 @@ def ours_arm(args):
     re = torch.as_tensor(pr.fimg_re, device=dev)
     im = torch.as_tensor(pr.fimg_im, device=dev)
     corr = torch.as_tensor(pr.corr, device=dev)
-    out = torch.empty(P * O * T, device=dev, dtype=torch.float32)
-    mn = torch.empty(P, device=dev, dtype=torch.float64)
-    am = torch.empty(P, device=dev, dtype=torch.int64)
     flush = torch.empty(2 * L2_BYTES // 4, device=dev, dtype=torch.float32)
-    batch = pkg.make_batch(eul, tx, ty, re, im, corr, out, O=O, T=T, P=P, N_img=N, out_min=mn, out_argmin=am)
-    wsb = pkg.batch_workspace_bytes(view, batch, prec)
-    ws = torch.empty(max(wsb, 16), device=dev, dtype=torch.uint8)
+    uneven = pr.orient_lists is not None
+    plan = None
+    plan_extra = {}
+    if uneven:
+        # per-particle orientation subsets and translation sets: one plan,
+        # autotuned and captured in a CUDA graph; a fixed-variant plan is
+        # timed beside it as the baseline
+        pkg_view_cache["view"] = view
+        fixed, fixed_bufs, _ = build_plan_case(pkg, pr, dev, prec, pkg.PLAN_GRAPH | pkg.PLAN_REORDER)
+        for _ in range(max(args.warmup, 1)):
+            fixed.run(stream)
+        torch.cuda.synchronize()
+        fa, fb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fa.record(stream)
+        for _ in range(max(3, min(args.steps, 10))):
+            fixed.run(stream)
+        fb.record(stream)
+        torch.cuda.synchronize()
+        plan_extra["fixed_tile_ms_per_step"] = fa.elapsed_time(fb) / max(3, min(args.steps, 10))
+        plan_extra["fixed_tile_row_bytes"] = fixed.info()["row_bytes"]
+        fixed.close()
+        del fixed_bufs
+        plan, bufs, evals_plan = build_plan_case(pkg, pr, dev, prec,
+                                                 pkg.PLAN_AUTOTUNE | pkg.PLAN_GRAPH | pkg.PLAN_REORDER)
+        eul, re, im, corr, out, mn, am = bufs
+        info = plan.info()
+        plan_extra.update({"autotuned_row_bytes": info["row_bytes"], "tuned_gemm_ms": info["tuned_ms"],
+                           "work_tiles": info["tiles"], "dense_tiles": info["tiles_dense"], "rows": info["rows"]})
+    else:
+        out = torch.empty(P * O * T, device=dev, dtype=torch.float32)
+        mn = torch.empty(P, device=dev, dtype=torch.float64)
+        am = torch.empty(P, device=dev, dtype=torch.int64)
+        batch = pkg.make_batch(eul, tx, ty, re, im, corr, out, O=O, T=T, P=P, N_img=N, out_min=mn,
+                               out_argmin=am)
+        wsb = pkg.batch_workspace_bytes(view, batch, prec)
+        ws = torch.empty(max(wsb, 16), device=dev, dtype=torch.uint8)
 
     def step():
-        pkg.diff2_coarse_batch(view, batch, prec, ws, stream)
+        if plan is not None:
+            plan.run(stream)
+        else:
+            pkg.diff2_coarse_batch(view, batch, prec, ws, stream)
 
     for _ in range(max(args.warmup, 0)):
         step()
@@ -273,11 +332,16 @@ def ours_arm(args):
         t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    evals_step = P * O * T
+    evals_step = evals_plan if uneven else P * O * T
     value = world * evals_step * args.steps / (total_ms / 1e3)
 
     # ---- dominant kernel timing (events on the launching stream) ----
-    kern = pkg.kernel_breakdown(view, batch, prec, ws, stream, reps=3) if hasattr(pkg, "kernel_breakdown") else {}
+    if uneven:
+        tuned = plan_extra["tuned_gemm_ms"][0 if plan_extra["autotuned_row_bytes"] == 64 else 1]
+        name = [n for n in pkg.stage_names(prec) if "gemm" in n][0]
+        kern = {"per_kernel_ms": {name: tuned}, "dominant": name, "dominant_ms": tuned or None, "traffic": None}
+    else:
+        kern = pkg.kernel_breakdown(view, batch, prec, ws, stream, reps=3)
 
     # ---- end to end through the public API with host buffers ----
     h_re = torch.empty_like(re, device="cpu").pin_memory()
@@ -344,11 +408,15 @@ def ours_arm(args):
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": {"fp32": "f32", "tf32": "tf32", "tf32x3": "tf32x3", "bf16x3": "bf16x3"}[args.precision],
                 "data": "synthetic (seeded blob reference, HEALPix grid, CTF, Gaussian noise)",
-                "config": {"workload": f"{args.config}: {P} particles x {O} orientations x {T} translations, "
-                                       f"image {pr.img_size} ({N} px, {K_c} in radius)",
+                "config": {"workload": (f"{args.config}: {P} particles, each a contiguous HEALPix subset of 10-100% "
+                                        f"of {O} orientations and a translation radius in 2..8 px "
+                                        f"({evals_step} evaluations), image {pr.img_size} ({N} px, {K_c} in radius)")
+                                       if uneven else
+                                       (f"{args.config}: {P} particles x {O} orientations x {T} translations, "
+                                        f"image {pr.img_size} ({N} px, {K_c} in radius)"),
                            "precision": args.precision, "particles": P, "orientations": O, "translations": T,
                            "pixels_in_radius": K_c, "l2": "flushed (256 MB write) before every timed step",
-                           "parallelism": f"replicas x{world}"},
+                           "parallelism": f"replicas x{world}", **plan_extra},
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_val, "unit": "diff2 evals/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h,

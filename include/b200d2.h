@@ -208,7 +208,11 @@ typedef struct b200d2_particle_desc {
 enum {
   B200D2_PLAN_AUTOTUNE = 1,   /* time the contraction variants, keep the fastest */
   B200D2_PLAN_GRAPH = 2,      /* capture the whole pipeline in a CUDA graph */
-  B200D2_PLAN_ACCUMULATE = 4  /* add onto d_diff2 instead of overwriting */
+  B200D2_PLAN_ACCUMULATE = 4, /* add onto d_diff2 instead of overwriting */
+  /* order orientations by viewing direction (Morton code of the projection
+   * normal) and particles by where their subsets fall, so that local
+   * orientation subsets touch few output tiles; outputs are unchanged */
+  B200D2_PLAN_REORDER = 8
 };
 
 typedef struct b200d2_plan_info {

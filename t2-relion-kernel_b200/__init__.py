@@ -77,6 +77,7 @@ class PlanInfo(C.Structure):
 PLAN_AUTOTUNE = 1
 PLAN_GRAPH = 2
 PLAN_ACCUMULATE = 4
+PLAN_REORDER = 8
 
 _lib = None
 
@@ -279,7 +280,7 @@ class Plan:
     trans_y (float32)."""
 
     def __init__(self, view: View, eulers, O_all: int, N_img: int, particles: list, precision: int = PREC_BF16X3,
-                 flags: int = PLAN_AUTOTUNE | PLAN_GRAPH, out_min=None, out_argmin=None):
+                 flags: int = PLAN_AUTOTUNE | PLAN_GRAPH | PLAN_REORDER, out_min=None, out_argmin=None):
         self._keep = []
         descs = (ParticleDesc * len(particles))()
         for i, pt in enumerate(particles):

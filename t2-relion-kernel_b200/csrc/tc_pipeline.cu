@@ -1010,6 +1010,7 @@ struct b200d2_plan {
   int2* d_tiles = nullptr;
   float2* d_txy = nullptr;
   int* d_inv = nullptr;
+  float* d_eul_perm = nullptr;
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -1024,7 +1025,7 @@ static void plan_free(b200d2_plan* p) {
   if (p->graph) cudaGraphDestroy(p->graph);
   if (p->stream) cudaStreamDestroy(p->stream);
   for (void* d : {(void*)p->ws, (void*)p->d_parts, (void*)p->d_rows, (void*)p->d_tiles, (void*)p->d_txy,
-                  (void*)p->d_inv})
+                  (void*)p->d_inv, (void*)p->d_eul_perm})
     if (d) cudaFree(d);
   delete p;
 }
@@ -1081,6 +1082,47 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   p->prec = precision;
   p->flags = flags;
 
+  // column position of every orientation: identity, or sorted by the Morton
+  // code of the viewing direction (third column of the Euler matrix, which
+  // is the same for all in-plane angles of one direction)
+  std::vector<int> pos(O_all), perm(O_all);
+  for (int o = 0; o < O_all; ++o) perm[o] = o;
+  std::vector<float> h_eul;
+  if (flags & B200D2_PLAN_REORDER) {
+    h_eul.resize((size_t)O_all * 9);
+    if (cudaMemcpy(h_eul.data(), d_eulers, h_eul.size() * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      delete p;
+      return B200D2_ERR_CUDA;
+    }
+    std::vector<uint64_t> key(O_all);
+    for (int o = 0; o < O_all; ++o) {
+      const float* e = &h_eul[(size_t)o * 9];
+      const double dz = std::max(-1.0, std::min(1.0, (double)e[8]));
+      const double ph = atan2((double)e[5], (double)e[2]);  // in (-pi, pi]
+      const uint32_t u = (uint32_t)std::min(65535.0, (dz + 1.0) * 0.5 * 65536.0);
+      const uint32_t w = (uint32_t)std::min(65535.0, (ph / (2 * 3.14159265358979323846) + 0.5) * 65536.0);
+      uint64_t m = 0;
+      for (int bit = 15; bit >= 0; --bit) m = (m << 2) | (((u >> bit) & 1u) << 1) | ((w >> bit) & 1u);
+      key[o] = m;
+    }
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int c) { return key[a] < key[c]; });
+  }
+  for (int c = 0; c < O_all; ++c) pos[perm[c]] = c;
+  // particle order: by the median column of their subsets
+  std::vector<int> ord(P);
+  for (int i = 0; i < P; ++i) ord[i] = i;
+  if (flags & B200D2_PLAN_REORDER) {
+    std::vector<double> mid(P);
+    for (int i = 0; i < P; ++i) {
+      const b200d2_particle_desc& d = parts[i];
+      std::vector<int> c(d.O);
+      for (int k = 0; k < d.O; ++k) c[k] = pos[d.h_orient ? d.h_orient[k] : k];
+      std::nth_element(c.begin(), c.begin() + d.O / 2, c.end());
+      mid[i] = c[d.O / 2];
+    }
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int c) { return mid[a] < mid[c]; });
+  }
+
   // distinct translation sets -> phase tables; rows (particle, t, table)
   std::map<std::vector<std::pair<uint32_t, uint32_t>>, int> sets;
   std::vector<float2> txy;
@@ -1088,7 +1130,8 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   std::vector<int4> rows;
   std::vector<PartDev> hp(P);
   long long evals = 0;
-  for (int i = 0; i < P; ++i) {
+  for (int oi = 0; oi < P; ++oi) {
+    const int i = ord[oi];
     const b200d2_particle_desc& d = parts[i];
     std::vector<std::pair<uint32_t, uint32_t>> key(d.T);
     for (int t = 0; t < d.T; ++t) {
@@ -1123,9 +1166,9 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   for (int i = 0; i < P; ++i) {
     const b200d2_particle_desc& d = parts[i];
     for (int k = 0; k < d.O; ++k) {
-      const int o = d.h_orient ? d.h_orient[k] : k;
-      inv[(size_t)i * O_all + o] = k;
-      need_n[i][o / 256] = 1;
+      const int c = pos[d.h_orient ? d.h_orient[k] : k];
+      inv[(size_t)i * O_all + c] = k;
+      need_n[i][c / 256] = 1;
     }
   }
   // work list: (m tile, n tile) pairs some particle of the m tile needs, m-major
@@ -1133,8 +1176,9 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   for (int mt = 0; mt < Mtiles; ++mt) {
     const int r0 = mt * 128, r1 = std::min(Mrows, r0 + 128);
     std::vector<char> un(Ntiles, 0);
-    for (int pi = rows[r0].x; pi <= rows[r1 - 1].x; ++pi)
-      for (int n = 0; n < Ntiles; ++n) un[n] |= need_n[pi][n];
+    for (int r = r0; r < r1; ++r)
+      if (r == r0 || rows[r].x != rows[r - 1].x)
+        for (int n = 0; n < Ntiles; ++n) un[n] |= need_n[rows[r].x][n];
     for (int n = 0; n < Ntiles; ++n)
       if (un[n]) tiles.push_back(make_int2(mt, n));
   }
@@ -1142,6 +1186,16 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   b200d2_batch& b = p->batch;
   memset(&b, 0, sizeof(b));
   b.d_eulers = d_eulers;
+  if (flags & B200D2_PLAN_REORDER) {  // orientations in column order
+    std::vector<float> pe((size_t)O_all * 9);
+    for (int c = 0; c < O_all; ++c) memcpy(&pe[(size_t)c * 9], &h_eul[(size_t)perm[c] * 9], 9 * sizeof(float));
+    if (cudaMalloc(&p->d_eul_perm, pe.size() * sizeof(float)) != cudaSuccess ||
+        cudaMemcpy(p->d_eul_perm, pe.data(), pe.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+      plan_free(p);
+      return B200D2_ERR_OOM;
+    }
+    b.d_eulers = p->d_eul_perm;
+  }
   b.O = O_all;
   b.T = (int)txy.size();  // number of phase tables
   b.P = P;

@@ -39,13 +39,15 @@ def _fp64_particle(pkg, torch, view, pr, part, p):
     return out.cpu().numpy()
 
 
-def test_uneven_plan_matches_fp64(pkg, synth, oracle, cuda):
+@pytest.mark.parametrize("reorder", [False, True])
+def test_uneven_plan_matches_fp64(pkg, synth, oracle, cuda, reorder):
     torch = cuda
     P = 6
     pr, proj, view, eul, parts = _plan_case(pkg, synth, torch, P)
     mn = torch.empty(P, device="cuda", dtype=torch.float64)
     am = torch.empty(P, device="cuda", dtype=torch.int64)
-    plan = pkg.Plan(view, eul, pr.O, pr.N_img, parts, pkg.PREC_BF16X3, out_min=mn, out_argmin=am)
+    flags = pkg.PLAN_AUTOTUNE | pkg.PLAN_GRAPH | (pkg.PLAN_REORDER if reorder else 0)
+    plan = pkg.Plan(view, eul, pr.O, pr.N_img, parts, pkg.PREC_BF16X3, flags=flags, out_min=mn, out_argmin=am)
     info = plan.info()
     print(info)
     assert info["graph"] == 1 and info["row_bytes"] in (64, 128)
