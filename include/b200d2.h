@@ -236,6 +236,63 @@ int b200d2_plan_run(b200d2_plan* plan, void* stream);
 int b200d2_plan_get_info(const b200d2_plan* plan, b200d2_plan_info* info);
 int b200d2_plan_destroy(b200d2_plan* plan);
 
+/* ------------------------------------------------------------------------
+ * Serving: a request loop over resident references with continuous
+ * batching.  No counterpart in the reference (it has no serving path).
+ * Requests (a set of particles scored against an orientation subset of one
+ * reference at one translation set) are queued by b200d2_server_submit and
+ * admitted by a scheduler thread as soon as a stream slot is free and their
+ * device footprint fits the HBM budget, so requests that arrive while others
+ * run start at once and overlap on the GPU.  Each admitted request copies its
+ * host inputs in, runs the tensor-core pipeline and copies its outputs out on
+ * its own stream; its device memory is released stream-ordered.
+ * ---------------------------------------------------------------------- */
+typedef struct b200d2_server b200d2_server;
+
+typedef struct b200d2_request {
+  int ref;              /* reference id from b200d2_server_add_reference */
+  int P;                /* particles */
+  const float* h_real;  /* host [P][N_img] (page-locked memory overlaps best) */
+  const float* h_imag;
+  const float* h_corr;
+  const int* h_orient;  /* host [O]: indices into the reference's orientations */
+  int O;
+  const float* h_trans_x; /* host [T] phase slopes */
+  const float* h_trans_y;
+  int T;
+  float* h_diff2;       /* optional host [P][O][T] output */
+  double* h_min;        /* optional host [P]: minimum diff2 per particle */
+  long long* h_argmin;  /* optional host [P]: o_local*T + t of that minimum */
+} b200d2_request;
+
+typedef struct b200d2_server_stats {
+  long long submitted, completed, rejected, evals;
+  int in_flight, queued, max_in_flight;
+  size_t bytes_in_use, peak_bytes;
+} b200d2_server_stats;
+
+/* slots: concurrent streams; hbm_budget_bytes: device bytes the in-flight
+ * requests may hold; precision: tensor-core precision or B200D2_PREC_FP32. */
+int b200d2_server_create(int slots, size_t hbm_budget_bytes, int precision,
+                         b200d2_server** out);
+/* Register a resident reference: a projector view and its host orientation
+ * grid h_eulers[O_all][9] (copied); image geometry from the view, N_img
+ * pixels per image. */
+int b200d2_server_add_reference(b200d2_server* s, const b200d2_view* view,
+                                const float* h_eulers, int O_all, int N_img,
+                                int* ref_id);
+/* Queue a request (host buffers must stay valid until it completes).
+ * Returns B200D2_ERR_TOO_LARGE if it can never fit the budget. */
+int b200d2_server_submit(b200d2_server* s, const b200d2_request* req,
+                         long long* ticket);
+/* Wait for a request: status of the request, its latency (submit to
+ * completion, seconds) and its device time (seconds). */
+int b200d2_server_wait(b200d2_server* s, long long ticket, double timeout_s,
+                       double* latency_s, double* device_s);
+int b200d2_server_get_stats(b200d2_server* s, b200d2_server_stats* st);
+/* Drain all requests and free the server. */
+int b200d2_server_destroy(b200d2_server* s);
+
 /* Tensor-core batch that allocates nothing.  No counterpart in the reference.
  * For callers that cannot call cudaMalloc: a host whose device memory is
  * owned by another allocator (RELION's caching allocator reserves most of the

@@ -74,6 +74,21 @@ class PlanInfo(C.Structure):
         ("evals", C.c_longlong), ("workspace_bytes", C.c_size_t), ("tuned_ms", C.c_double * 2)]
 
 
+class Request(C.Structure):
+    """b200d2_request: one serving request (host buffers)."""
+
+    _fields_ = [("ref", C.c_int), ("P", C.c_int), ("h_real", C.c_void_p), ("h_imag", C.c_void_p),
+                ("h_corr", C.c_void_p), ("h_orient", C.c_void_p), ("O", C.c_int), ("h_trans_x", C.c_void_p),
+                ("h_trans_y", C.c_void_p), ("T", C.c_int), ("h_diff2", C.c_void_p), ("h_min", C.c_void_p),
+                ("h_argmin", C.c_void_p)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("rejected", C.c_longlong),
+                ("evals", C.c_longlong), ("in_flight", C.c_int), ("queued", C.c_int), ("max_in_flight", C.c_int),
+                ("bytes_in_use", C.c_size_t), ("peak_bytes", C.c_size_t)]
+
+
 PLAN_AUTOTUNE = 1
 PLAN_GRAPH = 2
 PLAN_ACCUMULATE = 4
@@ -116,6 +131,12 @@ def _declare(L):
         "b200d2_plan_run": [P, P],
         "b200d2_plan_get_info": [P, C.POINTER(PlanInfo)],
         "b200d2_plan_destroy": [P],
+        "b200d2_server_create": [I, Z, I, C.POINTER(P)],
+        "b200d2_server_add_reference": [P, C.POINTER(View), P, I, I, C.POINTER(I)],
+        "b200d2_server_submit": [P, C.POINTER(Request), C.POINTER(C.c_longlong)],
+        "b200d2_server_wait": [P, C.c_longlong, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)],
+        "b200d2_server_get_stats": [P, C.POINTER(ServerStats)],
+        "b200d2_server_destroy": [P],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -319,6 +340,76 @@ class Plan:
         if self._h and self._h.value:
             lib().b200d2_plan_destroy(self._h)
             self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _host_ptr(a):
+    """Address of a host buffer: C-contiguous numpy array or CPU torch tensor."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise B200D2Error(1, "expected a C-contiguous host array")
+        return a.ctypes.data
+    if getattr(a, "is_cuda", False):
+        raise B200D2Error(1, "expected a host buffer")
+    return a.data_ptr()
+
+
+class Server:
+    """Request loop with continuous batching over resident references
+    (b200d2_server_*).  Host buffers of a request are kept alive until wait()."""
+
+    def __init__(self, slots: int = 4, hbm_budget: int = 32 << 30, precision: int = PREC_TF32):
+        self._h = C.c_void_p()
+        _check(lib().b200d2_server_create(slots, hbm_budget, precision, C.byref(self._h)), "server_create")
+        self._keep: dict = {}
+
+    def add_reference(self, view: View, eulers: np.ndarray, N_img: int) -> int:
+        eul = np.ascontiguousarray(eulers, np.float32).reshape(-1, 9)
+        rid = C.c_int()
+        _check(lib().b200d2_server_add_reference(self._h, C.byref(view), eul.ctypes.data_as(C.c_void_p),
+                                                 eul.shape[0], N_img, C.byref(rid)), "server_add_reference")
+        return rid.value
+
+    def submit(self, ref: int, real, imag, corr, orient, trans_x, trans_y, out_diff2=None, out_min=None,
+               out_argmin=None) -> int:
+        orient = np.ascontiguousarray(orient, np.int32)
+        tx = np.ascontiguousarray(trans_x, np.float32)
+        ty = np.ascontiguousarray(trans_y, np.float32)
+        r = Request()
+        r.ref, r.P = ref, int(real.shape[0])
+        r.h_real, r.h_imag, r.h_corr = _host_ptr(real), _host_ptr(imag), _host_ptr(corr)
+        r.h_orient, r.O = orient.ctypes.data, int(orient.size)
+        r.h_trans_x, r.h_trans_y, r.T = tx.ctypes.data, ty.ctypes.data, int(tx.size)
+        r.h_diff2, r.h_min, r.h_argmin = _host_ptr(out_diff2), _host_ptr(out_min), _host_ptr(out_argmin)
+        t = C.c_longlong()
+        _check(lib().b200d2_server_submit(self._h, C.byref(r), C.byref(t)), "server_submit")
+        self._keep[t.value] = (real, imag, corr, orient, tx, ty, out_diff2, out_min, out_argmin)
+        return t.value
+
+    def wait(self, ticket: int, timeout: float = 120.0):
+        """Returns (status, latency_s, device_s) of the request."""
+        lat, dev = C.c_double(), C.c_double()
+        st = lib().b200d2_server_wait(self._h, ticket, timeout, C.byref(lat), C.byref(dev))
+        self._keep.pop(ticket, None)
+        return st, lat.value, dev.value
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _check(lib().b200d2_server_get_stats(self._h, C.byref(s)), "server_get_stats")
+        return {n: getattr(s, n) for n, _ in ServerStats._fields_}
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().b200d2_server_destroy(self._h)
+            self._h = C.c_void_p()
+        self._keep.clear()
 
     def __del__(self):
         try:

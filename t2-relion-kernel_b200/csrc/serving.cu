@@ -1,0 +1,350 @@
+// serving.cu -- request loop with continuous batching over resident
+// references (b200d2_server_*).  No counterpart in the reference harness,
+// which scores one particle file at a time (src/main.cu:483-503).
+//
+// Requests are queued by submit() and admitted by one scheduler thread: a
+// request starts as soon as a stream slot is free and its device footprint
+// (inputs, outputs, workspace) fits the HBM budget, in arrival order with
+// later requests allowed past one that does not fit yet.  An admitted request
+// runs entirely on its slot's stream: stream-ordered allocation
+// (cudaMallocAsync), host-to-device copies, the batch pipeline, device-to-
+// host copies, stream-ordered free, and a host callback that timestamps the
+// completion and wakes the scheduler.  Requests on different slots overlap on
+// the GPU.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+size_t up256(size_t v) { return (v + 255) / 256 * 256; }
+
+struct Ref {
+  b200d2_view view;
+  std::vector<float> eulers;  // [O_all][9]
+  int O_all, N_img;
+};
+
+struct Req {
+  long long ticket = 0;
+  b200d2_request r{};
+  std::vector<float> eul;  // gathered [O][9]
+  size_t ws_bytes = 0, footprint = 0;
+  int status = -1;  // -1 pending, else a b200d2_status
+  double t_submit = 0, t_done = 0, device_s = 0;
+  int slot = -1;
+  void* dbuf = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::atomic<int> finished{0};
+  struct b200d2_server* srv = nullptr;
+};
+
+}  // namespace
+
+struct b200d2_server {
+  int slots = 1;
+  size_t budget = 0;
+  int prec = B200D2_PREC_TF32;
+  int device = 0;
+  std::vector<Ref> refs;
+  std::vector<cudaStream_t> streams;
+  std::vector<int> slot_busy;
+  std::deque<std::shared_ptr<Req>> queue;
+  std::vector<std::shared_ptr<Req>> inflight;
+  std::map<long long, std::shared_ptr<Req>> all;
+  std::mutex mu;
+  std::condition_variable cv_sched, cv_done;
+  std::thread sched;
+  bool stop = false;
+  long long next_ticket = 1;
+  b200d2_server_stats st{};
+};
+
+namespace {
+
+void CUDART_CB on_done(void* arg) {
+  Req* q = static_cast<Req*>(arg);
+  q->t_done = now_s();
+  q->finished.store(1);
+  q->srv->cv_sched.notify_all();
+}
+
+// Launch a request's work on its slot stream (called with the lock held).
+int admit(b200d2_server* s, Req& q) {
+  const Ref& ref = s->refs[q.r.ref];
+  cudaStream_t st = s->streams[q.slot];
+  const b200d2_request& r = q.r;
+  const size_t img = (size_t)r.P * ref.N_img * sizeof(float);
+  const size_t out = (size_t)r.P * r.O * r.T * sizeof(float);
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    size_t a = off;
+    off += up256(b);
+    return a;
+  };
+  const size_t o_re = take(img), o_im = take(img), o_co = take(img), o_eu = take((size_t)r.O * 9 * sizeof(float)),
+               o_tx = take((size_t)r.T * sizeof(float)), o_ty = take((size_t)r.T * sizeof(float)),
+               o_out = take(out), o_mn = take((size_t)r.P * sizeof(double)),
+               o_am = take((size_t)r.P * sizeof(long long)), o_ws = take(q.ws_bytes);
+  (void)o_ws;
+  if (cudaMallocAsync(&q.dbuf, q.footprint, st) != cudaSuccess) return B200D2_ERR_OOM;
+  uint8_t* d = static_cast<uint8_t*>(q.dbuf);
+  cudaEventRecord(q.ev0, st);
+  cudaMemcpyAsync(d + o_re, r.h_real, img, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d + o_im, r.h_imag, img, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d + o_co, r.h_corr, img, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d + o_eu, q.eul.data(), q.eul.size() * sizeof(float), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d + o_tx, r.h_trans_x, (size_t)r.T * sizeof(float), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d + o_ty, r.h_trans_y, (size_t)r.T * sizeof(float), cudaMemcpyHostToDevice, st);
+  b200d2_batch b;
+  memset(&b, 0, sizeof(b));
+  b.d_eulers = reinterpret_cast<const float*>(d + o_eu);
+  b.O = r.O;
+  b.d_trans_x = reinterpret_cast<const float*>(d + o_tx);
+  b.d_trans_y = reinterpret_cast<const float*>(d + o_ty);
+  b.T = r.T;
+  b.P = r.P;
+  b.N_img = ref.N_img;
+  b.d_real = reinterpret_cast<const float*>(d + o_re);
+  b.d_imag = reinterpret_cast<const float*>(d + o_im);
+  b.d_corr = reinterpret_cast<const float*>(d + o_co);
+  b.img_stride = ref.N_img;
+  b.d_diff2 = reinterpret_cast<float*>(d + o_out);
+  b.accumulate = 0;
+  b.d_min = reinterpret_cast<double*>(d + o_mn);
+  b.d_argmin = reinterpret_cast<long long*>(d + o_am);
+  int rc = b200d2_diff2_coarse_batch(&ref.view, &b, s->prec, q.ws_bytes ? d + o_ws : nullptr, q.ws_bytes, st);
+  if (r.h_diff2) cudaMemcpyAsync(r.h_diff2, d + o_out, out, cudaMemcpyDeviceToHost, st);
+  if (r.h_min) cudaMemcpyAsync(r.h_min, d + o_mn, (size_t)r.P * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (r.h_argmin)
+    cudaMemcpyAsync(r.h_argmin, d + o_am, (size_t)r.P * sizeof(long long), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(q.dbuf, st);
+  cudaEventRecord(q.ev1, st);
+  q.status = rc;  // final status once finished
+  const cudaError_t e = cudaLaunchHostFunc(st, on_done, &q);
+  if (e != cudaSuccess) return b200d2::status_from_cuda(e);
+  return B200D2_OK;
+}
+
+void sched_loop(b200d2_server* s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (true) {
+    bool progress = false;
+    for (size_t i = 0; i < s->inflight.size();) {
+      Req& q = *s->inflight[i];
+      if (q.finished.load()) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, q.ev0, q.ev1) == cudaSuccess) q.device_s = ms / 1e3;
+        if (q.status == -1) q.status = B200D2_OK;
+        s->slot_busy[q.slot] = 0;
+        s->st.bytes_in_use -= q.footprint;
+        s->st.completed++;
+        if (q.status == B200D2_OK) s->st.evals += (long long)q.r.P * q.r.O * q.r.T;
+        s->inflight.erase(s->inflight.begin() + i);
+        progress = true;
+      } else {
+        ++i;
+      }
+    }
+    if (progress) s->cv_done.notify_all();
+    for (auto it = s->queue.begin(); it != s->queue.end();) {
+      int slot = -1;
+      for (int k = 0; k < s->slots; ++k)
+        if (!s->slot_busy[k]) {
+          slot = k;
+          break;
+        }
+      if (slot < 0) break;
+      Req& q = **it;
+      if (s->st.bytes_in_use + q.footprint > s->budget) {
+        ++it;
+        continue;
+      }
+      q.slot = slot;
+      s->slot_busy[slot] = 1;
+      s->st.bytes_in_use += q.footprint;
+      s->st.peak_bytes = std::max(s->st.peak_bytes, s->st.bytes_in_use);
+      const int rc = admit(s, q);
+      if (rc != B200D2_OK && !q.finished.load()) {
+        // nothing was left on the stream that would signal completion
+        q.status = rc;
+        q.t_done = now_s();
+        q.finished.store(1);
+      }
+      s->inflight.push_back(*it);
+      it = s->queue.erase(it);
+      s->st.max_in_flight = std::max(s->st.max_in_flight, (int)s->inflight.size());
+      progress = true;
+    }
+    s->st.in_flight = (int)s->inflight.size();
+    s->st.queued = (int)s->queue.size();
+    if (s->stop && s->queue.empty() && s->inflight.empty()) break;
+    if (!progress) s->cv_sched.wait_for(lk, std::chrono::microseconds(200));
+  }
+}
+
+}  // namespace
+
+extern "C" int b200d2_server_create(int slots, size_t hbm_budget_bytes, int precision, b200d2_server** out) {
+  if (!out || slots <= 0 || slots > 64 || hbm_budget_bytes == 0) return B200D2_ERR_INVALID;
+  if (precision != B200D2_PREC_FP32 && precision != B200D2_PREC_TF32 && precision != B200D2_PREC_TF32X3 &&
+      precision != B200D2_PREC_BF16X3)
+    return B200D2_ERR_UNSUPPORTED;
+  *out = nullptr;
+  b200d2_server* s = new b200d2_server();
+  s->slots = slots;
+  s->budget = hbm_budget_bytes;
+  s->prec = precision;
+  cudaGetDevice(&s->device);
+  s->slot_busy.assign(slots, 0);
+  for (int k = 0; k < slots; ++k) {
+    cudaStream_t st;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+      for (cudaStream_t x : s->streams) cudaStreamDestroy(x);
+      delete s;
+      return B200D2_ERR_CUDA;
+    }
+    s->streams.push_back(st);
+  }
+  // keep freed request memory cached in the process's pool up to the budget
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
+    uint64_t thr = hbm_budget_bytes;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  s->sched = std::thread(sched_loop, s);
+  *out = s;
+  return B200D2_OK;
+}
+
+extern "C" int b200d2_server_add_reference(b200d2_server* s, const b200d2_view* view, const float* h_eulers,
+                                           int O_all, int N_img, int* ref_id) {
+  if (!s || !view || !h_eulers || O_all <= 0 || N_img <= 0 || !ref_id) return B200D2_ERR_INVALID;
+  if ((long long)view->imgX * view->imgY < N_img) return B200D2_ERR_INVALID;
+  Ref r;
+  r.view = *view;
+  r.eulers.assign(h_eulers, h_eulers + (size_t)O_all * 9);
+  r.O_all = O_all;
+  r.N_img = N_img;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->refs.push_back(std::move(r));
+  *ref_id = (int)s->refs.size() - 1;
+  return B200D2_OK;
+}
+
+extern "C" int b200d2_server_submit(b200d2_server* s, const b200d2_request* req, long long* ticket) {
+  if (!s || !req || !ticket) return B200D2_ERR_INVALID;
+  const b200d2_request& r = *req;
+  if (r.P <= 0 || r.O <= 0 || r.T <= 0 || !r.h_real || !r.h_imag || !r.h_corr || !r.h_orient || !r.h_trans_x ||
+      !r.h_trans_y)
+    return B200D2_ERR_INVALID;
+  auto q = std::make_shared<Req>();
+  q->r = r;
+  q->srv = s;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (r.ref < 0 || r.ref >= (int)s->refs.size()) return B200D2_ERR_INVALID;
+    const Ref& ref = s->refs[r.ref];
+    q->eul.resize((size_t)r.O * 9);
+    for (int k = 0; k < r.O; ++k) {
+      const int o = r.h_orient[k];
+      if (o < 0 || o >= ref.O_all) return B200D2_ERR_INVALID;
+      memcpy(&q->eul[(size_t)k * 9], &ref.eulers[(size_t)o * 9], 9 * sizeof(float));
+    }
+    // workspace of this shape (the size query needs only non-null pointers)
+    b200d2_batch b;
+    memset(&b, 0, sizeof(b));
+    const float* dummy = reinterpret_cast<const float*>(256);
+    b.d_eulers = b.d_trans_x = b.d_trans_y = b.d_real = b.d_imag = b.d_corr = dummy;
+    b.d_diff2 = const_cast<float*>(dummy);
+    b.O = r.O;
+    b.T = r.T;
+    b.P = r.P;
+    b.N_img = ref.N_img;
+    b.img_stride = ref.N_img;
+    q->ws_bytes = b200d2_diff2_coarse_batch_workspace(&ref.view, &b, s->prec);
+    const size_t img = up256((size_t)r.P * ref.N_img * sizeof(float));
+    q->footprint = 3 * img + up256((size_t)r.O * 9 * sizeof(float)) + 2 * up256((size_t)r.T * sizeof(float)) +
+                   up256((size_t)r.P * r.O * r.T * sizeof(float)) + up256((size_t)r.P * sizeof(double)) +
+                   up256((size_t)r.P * sizeof(long long)) + up256(q->ws_bytes);
+    s->st.submitted++;
+    if (q->footprint > s->budget) {
+      s->st.rejected++;
+      return B200D2_ERR_TOO_LARGE;
+    }
+    if (cudaEventCreate(&q->ev0) != cudaSuccess || cudaEventCreate(&q->ev1) != cudaSuccess) return B200D2_ERR_CUDA;
+    q->ticket = s->next_ticket++;
+    q->t_submit = now_s();
+    s->all[q->ticket] = q;
+    s->queue.push_back(q);
+    *ticket = q->ticket;
+  }
+  s->cv_sched.notify_all();
+  return B200D2_OK;
+}
+
+extern "C" int b200d2_server_wait(b200d2_server* s, long long ticket, double timeout_s, double* latency_s,
+                                  double* device_s) {
+  if (!s) return B200D2_ERR_INVALID;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->all.find(ticket);
+  if (it == s->all.end()) return B200D2_ERR_INVALID;
+  std::shared_ptr<Req> q = it->second;
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::duration<double>(timeout_s);
+  while (!(q->finished.load() && std::find(s->inflight.begin(), s->inflight.end(), q) == s->inflight.end() &&
+           std::find(s->queue.begin(), s->queue.end(), q) == s->queue.end())) {
+    if (s->cv_done.wait_until(lk, deadline) == std::cv_status::timeout) return B200D2_ERR_TIMEOUT;
+  }
+  if (latency_s) *latency_s = q->t_done - q->t_submit;
+  if (device_s) *device_s = q->device_s;
+  const int status = q->status;
+  cudaEventDestroy(q->ev0);
+  cudaEventDestroy(q->ev1);
+  q->ev0 = q->ev1 = nullptr;
+  s->all.erase(it);
+  return status;
+}
+
+extern "C" int b200d2_server_get_stats(b200d2_server* s, b200d2_server_stats* st) {
+  if (!s || !st) return B200D2_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  *st = s->st;
+  return B200D2_OK;
+}
+
+extern "C" int b200d2_server_destroy(b200d2_server* s) {
+  if (!s) return B200D2_ERR_INVALID;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_sched.notify_all();
+  if (s->sched.joinable()) s->sched.join();
+  for (cudaStream_t x : s->streams) {
+    cudaStreamSynchronize(x);
+    cudaStreamDestroy(x);
+  }
+  for (auto& kv : s->all) {
+    if (kv.second->ev0) cudaEventDestroy(kv.second->ev0);
+    if (kv.second->ev1) cudaEventDestroy(kv.second->ev1);
+  }
+  delete s;
+  return B200D2_OK;
+}

@@ -44,7 +44,7 @@ namespace b200d2 {
 struct TcGeom {
   int P, O, T, N_img, K_c, Kpad, Mrows, Mpad, Opad, maxR, exw, eyw;
   int elem, BK, terms;
-  size_t off_status, off_xy, off_idx, off_ex, off_ey, off_bhi, off_blo, off_q, off_normx, off_na,
+  size_t off_status, off_xy, off_idx, off_ex, off_ey, off_bhi, off_blo, off_q, off_w, off_normx, off_na,
       off_ahi, off_alo, off_keys, total;
 };
 
@@ -109,7 +109,8 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, i
   g.off_ey = take(sizeof(float2) * (size_t)g.T * g.eyw);
   g.off_bhi = take((size_t)g.Opad * g.Kpad * g.elem);
   g.off_blo = planes == 2 ? take((size_t)g.Opad * g.Kpad * g.elem) : g.off_bhi;
-  g.off_q = take(sizeof(float) * (size_t)g.O * std::max(g.K_c, 1));
+  g.off_q = take(sizeof(double) * (size_t)g.O * std::max(g.K_c, 1));
+  g.off_w = take(sizeof(double) * (size_t)g.P * std::max(g.K_c, 1));
   g.off_normx = take(sizeof(double) * (size_t)g.P);
   g.off_na = take(sizeof(double) * (size_t)g.P * g.O);
   g.off_ahi = take((size_t)g.Mpad * g.Kpad * g.elem);
@@ -258,7 +259,7 @@ __device__ __forceinline__ void store_split(void* hi, void* lo, size_t at, float
 template <int PREC>
 __global__ void __launch_bounds__(128) tc_project_kernel(b200d2_view v, const float* __restrict__ eulers,
                                                          int O, const int2* __restrict__ xy, int K_c,
-                                                         int Kpad, void* bhi, void* blo, float* q) {
+                                                         int Kpad, void* bhi, void* blo, double* q) {
   const int kp = blockIdx.x * blockDim.x + threadIdx.x;  // complex pixel slot
   const int o = blockIdx.y;
   if (kp >= Kpad / 2) return;
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(128) tc_project_kernel(b200d2_view v, const fl
     e[5] = eo[7];
     const int2 c = xy[kp];
     b = project_pixel(v, (float)c.x, (float)c.y, e);
-    q[(size_t)o * K_c + kp] = __fmaf_rn(b.x, b.x, __fmul_rn(b.y, b.y));
+    q[(size_t)o * K_c + kp] = (double)b.x * (double)b.x + (double)b.y * (double)b.y;
   }
   store_split<PREC>(bhi, blo, (size_t)o * (Kpad / 2) + kp, b.x, b.y);
 }
@@ -284,11 +285,14 @@ __global__ void __launch_bounds__(256) tc_normx_kernel(const float* __restrict__
                                                        const float* __restrict__ im,
                                                        const float* __restrict__ corr,
                                                        long long stride, int N_img, double* normx,
-                                                       const PartDev* __restrict__ parts) {
+                                                       const PartDev* __restrict__ parts,
+                                                       const int* __restrict__ idx, int K_c, double* wcomp) {
   const long long p = blockIdx.x;
   const float* pre = parts ? parts[p].re : re + p * stride;
   const float* pim = parts ? parts[p].im : im + p * stride;
   const float* pco = parts ? parts[p].corr : corr + p * stride;
+  // the weights of the listed pixels, compacted for the normA contraction
+  for (int k = threadIdx.x; k < K_c; k += blockDim.x) wcomp[p * K_c + k] = (double)pco[idx[k]] / 2.0;
   double acc = 0.0;
   for (int i = threadIdx.x; i < N_img; i += blockDim.x) {
     const double r = pre[i], m = pim[i];
@@ -308,57 +312,78 @@ __global__ void __launch_bounds__(256) tc_normx_kernel(const float* __restrict__
 
 // ------------------------------------------------------------------ stage 4
 // na[p][o] = normX[p] + sum_k w_p(k) |B_o(k)|^2, FP64 products and sums.
-// CTA tile: 64 particles x 64 orientations over 32-pixel slabs held k-major
-// in shared memory; thread (tp, to) owns particles 4tp..4tp+3 (two 16-byte
-// broadcast loads) and orientations to + 16j (conflict-free loads), i.e. 16
-// DFMA per 6 shared loads.
-__global__ void __launch_bounds__(256) tc_norma_kernel(const float* __restrict__ corr, long long stride,
-                                                       const int* __restrict__ idx, int K_c,
-                                                       const float* __restrict__ q, int O, int P,
-                                                       const double* __restrict__ normx, double* na,
-                                                       const PartDev* __restrict__ parts) {
-  constexpr int KC = 32;
-  __shared__ __align__(16) double sw[KC][64];
-  __shared__ double sq[KC][65];
+// The weights w[p][k] and |B|^2 q[o][k] arrive as FP64 rows (written by the
+// normX and projector stages).  CTA tile: TP particles x 64 orientations; the
+// k dimension is walked in 16-pixel slabs copied into shared memory with
+// cp.async, double-buffered so the next slab's loads overlap this slab's
+// DFMAs.  Thread (tp, to) owns particles tp*(TP/16) + i and orientations
+// to + 16j; rows are padded to 17 doubles so the loads are conflict-free.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(sm100::smem_u32(smem)), "l"(gmem),
+               "r"(pred ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int TP>
+__global__ void __launch_bounds__(256) tc_norma_kernel(const double* __restrict__ wcomp, int K_c,
+                                                       const double* __restrict__ q, int O, int P,
+                                                       const double* __restrict__ normx, double* na) {
+  constexpr int KC = 16, LD = KC + 1, PPT = TP / 16;
+  __shared__ double sw[2][TP][LD];
+  __shared__ double sq[2][64][LD];
   const int tid = threadIdx.x, tp = tid >> 4, to = tid & 15;
-  const int p0 = blockIdx.y * 64, o0 = blockIdx.x * 64;
-  double acc[4][4];
+  const int p0 = blockIdx.y * TP, o0 = blockIdx.x * 64;
+  double acc[PPT][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < PPT; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  for (int k0 = 0; k0 < K_c; k0 += KC) {
-    for (int e = tid; e < 64 * KC; e += 256) {
-      const int pp = e % 64, k = e / 64;  // consecutive threads: consecutive particles
-      double w = 0.0;
-      if (p0 + pp < P && k0 + k < K_c) {
-        const float* pc = parts ? parts[p0 + pp].corr : corr + (long long)(p0 + pp) * stride;
-        w = (double)pc[idx[k0 + k]] / 2.0;
-      }
-      sw[k][pp] = w;
+  auto stage = [&](int buf, int k0) {
+    for (int e = tid; e < TP * KC; e += 256) {
+      const int pp = e / KC, k = e % KC;
+      const bool ok = (p0 + pp < P) && (k0 + k < K_c);
+      cp_async8(&sw[buf][pp][k], ok ? wcomp + (size_t)(p0 + pp) * K_c + k0 + k : wcomp, ok);
     }
     for (int e = tid; e < 64 * KC; e += 256) {
       const int oo = e / KC, k = e % KC;
-      sq[k][oo] = (o0 + oo < O && k0 + k < K_c) ? (double)q[(size_t)(o0 + oo) * K_c + k0 + k] : 0.0;
+      const bool ok = (o0 + oo < O) && (k0 + k < K_c);
+      cp_async8(&sq[buf][oo][k], ok ? q + (size_t)(o0 + oo) * K_c + k0 + k : q, ok);
+    }
+    cp_async_commit();
+  };
+  const int nslab = (K_c + KC - 1) / KC;
+  if (nslab > 0) stage(0, 0);
+  for (int sl = 0; sl < nslab; ++sl) {
+    const int buf = sl & 1;
+    if (sl + 1 < nslab) {
+      stage(buf ^ 1, (sl + 1) * KC);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
 #pragma unroll 4
     for (int k = 0; k < KC; ++k) {
-      const double2 wa = *reinterpret_cast<const double2*>(&sw[k][4 * tp]);
-      const double2 wb = *reinterpret_cast<const double2*>(&sw[k][4 * tp + 2]);
-      const double w[4] = {wa.x, wa.y, wb.x, wb.y};
+      double w[PPT];
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) w[i] = sw[buf][tp * PPT + i][k];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const double qv = sq[k][to + 16 * j];
+        const double qv = sq[buf][to + 16 * j][k];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) acc[i][j] = fma(w[i], qv, acc[i][j]);
+        for (int i = 0; i < PPT; ++i) acc[i][j] = fma(w[i], qv, acc[i][j]);
       }
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int p = p0 + 4 * tp + i;
+  for (int i = 0; i < PPT; ++i) {
+    const int p = p0 + tp * PPT + i;
     if (p >= P) continue;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -822,7 +847,8 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
   float2* ey = ws_at<float2>(ws, g.off_ey);
   void* bhi = ws_at<void>(ws, g.off_bhi);
   void* blo = ws_at<void>(ws, g.off_blo);
-  float* q = ws_at<float>(ws, g.off_q);
+  double* q = ws_at<double>(ws, g.off_q);
+  double* wcomp = ws_at<double>(ws, g.off_w);
   double* normx = ws_at<double>(ws, g.off_normx);
   double* na = ws_at<double>(ws, g.off_na);
   void* ahi = ws_at<void>(ws, g.off_ahi);
@@ -845,11 +871,20 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       break;
     }
     case 3:
-      tc_normx_kernel<<<g.P, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, g.N_img, normx, parts);
+      tc_normx_kernel<<<g.P, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, g.N_img, normx, parts,
+                                          idx, g.K_c, wcomp);
       break;
     case 4: {
-      dim3 grid((g.O + 63) / 64, (g.P + 63) / 64);
-      tc_norma_kernel<<<grid, 256, 0, s>>>(b.d_corr, b.img_stride, idx, g.K_c, q, g.O, g.P, normx, na, parts);
+      // 64-particle tiles when they give two CTAs per SM, else 32 or 16
+      const long long otiles = (g.O + 63) / 64;
+      const int sms = num_sms();
+      if (otiles * ((g.P + 63) / 64) >= 2LL * sms) {
+        tc_norma_kernel<64><<<dim3(otiles, (g.P + 63) / 64), 256, 0, s>>>(wcomp, g.K_c, q, g.O, g.P, normx, na);
+      } else if (otiles * ((g.P + 31) / 32) >= 2LL * sms) {
+        tc_norma_kernel<32><<<dim3(otiles, (g.P + 31) / 32), 256, 0, s>>>(wcomp, g.K_c, q, g.O, g.P, normx, na);
+      } else {
+        tc_norma_kernel<16><<<dim3(otiles, (g.P + 15) / 16), 256, 0, s>>>(wcomp, g.K_c, q, g.O, g.P, normx, na);
+      }
       break;
     }
     case 5: {
