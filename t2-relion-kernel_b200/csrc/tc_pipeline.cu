@@ -329,27 +329,40 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <int TP>
-__global__ void __launch_bounds__(256) tc_norma_kernel(const double* __restrict__ wcomp, int K_c,
+// FP64 tensor-core MMA (DMMA): D[8x8] += A[8x4] * B[4x8], all FP64.  Lane l
+// holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) + {0,1}].
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// CTA tile: (2*8*WM) particles x 64 orientations, 4 warps in a 2 x 2 grid,
+// each warp WM x 4 DMMA tiles of 8 x 8; 16-pixel slabs double-buffered
+// through shared memory with cp.async.
+template <int WM>
+__global__ void __launch_bounds__(128) tc_norma_kernel(const double* __restrict__ wcomp, int K_c,
                                                        const double* __restrict__ q, int O, int P,
                                                        const double* __restrict__ normx, double* na) {
-  constexpr int KC = 16, LD = KC + 1, PPT = TP / 16;
-  __shared__ double sw[2][TP][LD];
-  __shared__ double sq[2][64][LD];
-  const int tid = threadIdx.x, tp = tid >> 4, to = tid & 15;
-  const int p0 = blockIdx.y * TP, o0 = blockIdx.x * 64;
-  double acc[PPT][4];
+  constexpr int KC = 16, LD = KC + 1, CP = 16 * WM, CO = 64;
+  __shared__ double sw[2][CP][LD];
+  __shared__ double sq[2][CO][LD];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gid = lane >> 2, tig = lane & 3;
+  const int wp0 = (warp >> 1) * 8 * WM, wo0 = (warp & 1) * 32;
+  const int p0 = blockIdx.y * CP, o0 = blockIdx.x * CO;
+  double acc[WM][4][2];
 #pragma unroll
-  for (int i = 0; i < PPT; ++i)
+  for (int i = 0; i < WM; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   auto stage = [&](int buf, int k0) {
-    for (int e = tid; e < TP * KC; e += 256) {
+    for (int e = tid; e < CP * KC; e += 128) {
       const int pp = e / KC, k = e % KC;
       const bool ok = (p0 + pp < P) && (k0 + k < K_c);
       cp_async8(&sw[buf][pp][k], ok ? wcomp + (size_t)(p0 + pp) * K_c + k0 + k : wcomp, ok);
     }
-    for (int e = tid; e < 64 * KC; e += 256) {
+    for (int e = tid; e < CO * KC; e += 128) {
       const int oo = e / KC, k = e % KC;
       const bool ok = (o0 + oo < O) && (k0 + k < K_c);
       cp_async8(&sq[buf][oo][k], ok ? q + (size_t)(o0 + oo) * K_c + k0 + k : q, ok);
@@ -367,29 +380,31 @@ __global__ void __launch_bounds__(256) tc_norma_kernel(const double* __restrict_
       cp_async_wait<0>();
     }
     __syncthreads();
-#pragma unroll 4
-    for (int k = 0; k < KC; ++k) {
-      double w[PPT];
 #pragma unroll
-      for (int i = 0; i < PPT; ++i) w[i] = sw[buf][tp * PPT + i][k];
+    for (int k4 = 0; k4 < KC; k4 += 4) {
+      double a[WM], bq[4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const double qv = sq[buf][to + 16 * j][k];
+      for (int i = 0; i < WM; ++i) a[i] = sw[buf][wp0 + 8 * i + gid][k4 + tig];
 #pragma unroll
-        for (int i = 0; i < PPT; ++i) acc[i][j] = fma(w[i], qv, acc[i][j]);
-      }
+      for (int j = 0; j < 4; ++j) bq[j] = sq[buf][wo0 + 8 * j + gid][k4 + tig];
+#pragma unroll
+      for (int i = 0; i < WM; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j], a[i], bq[j]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < PPT; ++i) {
-    const int p = p0 + tp * PPT + i;
+  for (int i = 0; i < WM; ++i) {
+    const int p = p0 + wp0 + 8 * i + gid;
     if (p >= P) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int o = o0 + to + 16 * j;
-      if (o < O) na[(size_t)p * O + o] = normx[p] + acc[i][j];
-    }
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int o = o0 + wo0 + 8 * j + 2 * tig + h;
+        if (o < O) na[(size_t)p * O + o] = normx[p] + acc[i][j][h];
+      }
   }
 }
 
@@ -879,11 +894,11 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       const long long otiles = (g.O + 63) / 64;
       const int sms = num_sms();
       if (otiles * ((g.P + 63) / 64) >= 2LL * sms) {
-        tc_norma_kernel<64><<<dim3(otiles, (g.P + 63) / 64), 256, 0, s>>>(wcomp, g.K_c, q, g.O, g.P, normx, na);
+        tc_norma_kernel<4><<<dim3(otiles, (g.P + 63) / 64), 128, 0, s>>>(wcomp, g.K_c, q, g.O, g.P, normx, na);
       } else if (otiles * ((g.P + 31) / 32) >= 2LL * sms) {
-        tc_norma_kernel<32><<<dim3(otiles, (g.P + 31) / 32), 256, 0, s>>>(wcomp, g.K_c, q, g.O, g.P, normx, na);
+        tc_norma_kernel<2><<<dim3(otiles, (g.P + 31) / 32), 128, 0, s>>>(wcomp, g.K_c, q, g.O, g.P, normx, na);
       } else {
-        tc_norma_kernel<16><<<dim3(otiles, (g.P + 15) / 16), 256, 0, s>>>(wcomp, g.K_c, q, g.O, g.P, normx, na);
+        tc_norma_kernel<1><<<dim3(otiles, (g.P + 15) / 16), 128, 0, s>>>(wcomp, g.K_c, q, g.O, g.P, normx, na);
       }
       break;
     }

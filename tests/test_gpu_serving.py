@@ -85,11 +85,12 @@ def test_serving_admission_by_budget(pkg, synth, cuda):
     prob = synth.make_problem("c1", P=4)
     proj = pkg.Projector(prob.projector, use_texture=1)
     view = proj.view(prob.imgX, prob.imgY, prob.imgMaxR)
-    srv = pkg.Server(slots=2, hbm_budget=8 << 20, precision=pkg.PREC_TF32)  # 8 MiB
+    budget = 2 << 20  # 2 MiB: one small request (~1.5 MB with its workspace) at a time
+    srv = pkg.Server(slots=2, hbm_budget=budget, precision=pkg.PREC_TF32)
     ref = srv.add_reference(view, prob.eulers, prob.N_img)
     tx = np.zeros(1, np.float32)
     big = np.arange(prob.O, dtype=np.int32)
-    with pytest.raises(pkg.B200D2Error) as e:  # 4 particles x 576 orientations x 21 t: larger than 8 MiB
+    with pytest.raises(pkg.B200D2Error) as e:  # 4 particles x 576 orientations x 21 t: ~5.5 MB
         srv.submit(ref, prob.fimg_re, prob.fimg_im, prob.corr, big,
                    np.zeros(21, np.float32), np.zeros(21, np.float32))
     assert e.value.code == 7
@@ -103,6 +104,7 @@ def test_serving_admission_by_budget(pkg, synth, cuda):
         assert srv.wait(t)[0] == 0
         assert np.isfinite(o).all() and (o > 0).all()
     st = srv.stats()
-    assert st["rejected"] == 1 and st["completed"] == 6 and st["peak_bytes"] <= 8 << 20
+    assert st["rejected"] == 1 and st["completed"] == 6 and st["peak_bytes"] <= budget
+    assert st["max_in_flight"] == 1  # the budget, not the two slots, limited concurrency
     srv.close()
     proj.close()
