@@ -34,10 +34,18 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(ROOT, "t2-relion-kernel_b200")
 METRIC = "diff2 evals/s (coarse pass)"
 L2_BYTES = 126 * 1024 * 1024
+
+# DRAM bytes (read + write) per diff2 evaluation of the contraction kernel,
+# from one ncu capture of a smaller case of the same shape (64 particles,
+# 4608 orientations, 113 translations: 514.6 MB read + 107.5 MB written for
+# 33.3 M evaluations), scaled to a launch by its evaluation count.
+GEMM_DRAM_BYTES_PER_EVAL = {("c2", "bf16x3"): (514.6e6 + 107.5e6) / 33325056}
 
 
 def load_package():
@@ -153,12 +161,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "tf32x3", "tf32", "fp32"])
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "tf32x3", "tf32", "fp16x3", "fp16", "fp32"])
     ap.add_argument("--config", default="c2")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--particles", type=int, default=None,
                     help="override the particle count (small cases for profiling; not a bench line)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--study", default=None, choices=["precision"],
+                    help="precision: error of every precision form vs the FP64 kernel (use --config c3)")
     return ap.parse_args()
 
 
@@ -208,7 +218,7 @@ def reference_arm(args):
     return 0
 
 
-PREC = {"fp32": 0, "tf32": 1, "tf32x3": 2, "bf16x3": 3}
+PREC = {"fp32": 0, "tf32": 1, "tf32x3": 2, "bf16x3": 3, "fp16": 5, "fp16x3": 6}
 
 
 def build_plan_case(pkg, pr, dev, prec, flags):
@@ -398,7 +408,14 @@ def ours_arm(args):
                     "peak": peak, "unit": "TFLOP/s",
                     "peak_source": f"{peak_src} bf16_tflops_sustained" + (" / 2 (tf32 rate)" if prec in (1, 2) else "")}
         roof["frac"] = roof["achieved"] / roof["peak"]
-        roof["traffic"] = kern.get("traffic")
+        if prec in (2, 3, 6):
+            # the split forms issue three tensor products per algorithmic product
+            roof["tensor_pipe_frac"] = 3.0 * roof["frac"]
+        bpe = GEMM_DRAM_BYTES_PER_EVAL.get((args.config, args.precision))
+        roof["traffic"] = kern.get("traffic") or (bpe * evals_step if bpe and not uneven else None)
+        if roof["traffic"]:
+            roof["traffic_note"] = ("dram__bytes_read.sum + dram__bytes_write.sum of the contraction kernel per "
+                                    "launch, ncu capture at 64 particles scaled by evaluations")
         roof["kernel"] = kern.get("dominant")
         roof["algorithmic"] = f"{evals_step} evals x 4*K_c ({K_c}) flops = {flops_per_launch:.4g} flop per launch"
 
@@ -406,7 +423,7 @@ def ours_arm(args):
         line = {"metric": METRIC, "value": value, "unit": "diff2 evals/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": {"fp32": "f32", "tf32": "tf32", "tf32x3": "tf32x3", "bf16x3": "bf16x3"}[args.precision],
+                "dtype": args.precision if args.precision != "fp32" else "f32",
                 "data": "synthetic (seeded blob reference, HEALPix grid, CTF, Gaussian noise)",
                 "config": {"workload": (f"{args.config}: {P} particles, each a contiguous HEALPix subset of 10-100% "
                                         f"of {O} orientations and a translation radius in 2..8 px "
@@ -430,8 +447,93 @@ def ours_arm(args):
     return 0
 
 
+def precision_study(args):
+    """Error of every precision form against the FP64 CUDA-core kernel on the
+    same projections (one JSON line): per-diff2 relative error, error of the
+    per-particle minimum, agreement of the best (orientation, translation),
+    and error of the normalised FP64 weights exp(-(diff2 - min)) / sum."""
+    import torch
+    pkg = load_package()
+    synth = load_synth()
+    cfg = args.config
+    pr = synth.make_problem(cfg, seed=20251203, P=args.particles)
+    dev = torch.device("cuda", 0)
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    P, O, T, N = pr.P, pr.O, pr.T, pr.N_img
+    eul = torch.as_tensor(pr.eulers.reshape(-1), device=dev)
+    tx = torch.as_tensor(pr.trans_x, device=dev)
+    ty = torch.as_tensor(pr.trans_y, device=dev)
+    re = torch.as_tensor(pr.fimg_re, device=dev)
+    im = torch.as_tensor(pr.fimg_im, device=dev)
+    corr = torch.as_tensor(pr.corr, device=dev)
+
+    # FP64 reference (texture interpolation as in every form, FP64 arithmetic)
+    ref = torch.zeros((P, O * T), device=dev, dtype=torch.float64)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for p in range(P):
+        pkg.run_diff2_kernel_coarse_double(view, tx, ty, corr[p], re[p], im[p], eul, ref[p], O, T, N)
+    e1.record()
+    torch.cuda.synchronize()
+    fp64_ms = e0.elapsed_time(e1)
+    rmin, rarg = ref.min(dim=1)
+    srt = torch.sort(ref, dim=1).values
+    gap = (srt[:, 1] - srt[:, 0]).cpu().numpy() if O * T > 1 else np.zeros(P)
+    rw = torch.exp(-(ref - rmin[:, None]))
+    rw = rw / rw.sum(dim=1, keepdim=True)
+    results = {}
+    out = torch.empty(P * O * T, device=dev, dtype=torch.float32)
+    mn = torch.empty(P, device=dev, dtype=torch.float64)
+    am = torch.empty(P, device=dev, dtype=torch.int64)
+    for name in ["fp32", "tf32", "tf32x3", "bf16x3", "fp16", "fp16x3"]:
+        prec = PREC[name]
+        b = pkg.make_batch(eul, tx, ty, re, im, corr, out, O=O, T=T, P=P, N_img=N, out_min=mn, out_argmin=am)
+        nb = pkg.batch_workspace_bytes(view, b, prec)
+        ws = torch.empty(max(nb, 1), device=dev, dtype=torch.uint8)
+        pkg.diff2_coarse_batch(view, b, prec, ws)  # warm-up
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(3):
+            pkg.diff2_coarse_batch(view, b, prec, ws)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        got = out.view(P, O * T).double()
+        rel = (got - ref).abs() / ref.abs().clamp_min(1e-300)
+        w, _ = pkg.coarse_weights(out, P, O, T, out_min=mn)
+        w = w.view(P, O * T)
+        sig = rw > 1e-3
+        wrel = ((w - rw).abs() / rw.clamp_min(1e-300))[sig]
+        max_rel = float(rel.max())
+        tol_gap = gap > 2 * max_rel * rmin.abs().cpu().numpy()
+        same = (am.cpu().numpy() == rarg.cpu().numpy())
+        results[name] = {
+            "ms_per_batch": ms, "evals_per_s": P * O * T / (ms / 1e3),
+            "diff2_max_rel": max_rel, "diff2_mean_rel": float(rel.mean()),
+            "min_abs_err": float((mn - rmin).abs().max()),
+            "min_rel_err": float(((mn - rmin).abs() / rmin.abs()).max()),
+            "argmin_identical": int(same.sum()), "particles": P,
+            "argmin_identical_where_gap_exceeds_2x_err": bool(same[tol_gap].all()),
+            "particles_with_gap_above_2x_err": int(tol_gap.sum()),
+            "weights_max_abs_err": float((w - rw).abs().max()),
+            "weights_max_rel_err_above_1e-3": float(wrel.max()) if wrel.numel() else 0.0,
+            "weights_l1_max_over_particles": float((w - rw).abs().sum(dim=1).max()),
+        }
+        del ws
+    line = {"study": "precision", "config": cfg,
+            "workload": f"{cfg}: {P} particles x {O} orientations x {T} translations, image {pr.img_size} "
+                        f"({N} px)", "reference": "FP64 CUDA-core kernel (b200d2_diff2_coarse_f64)",
+            "reference_ms": fp64_ms, "median_min_diff2": float(rmin.median()), "results": results}
+    print(json.dumps(line), flush=True)
+    proj.close()
+    return 0
+
+
 def main():
     args = parse()
+    if args.study == "precision":
+        return precision_study(args)
     if args.impl == "reference":
         return reference_arm(args)
     return ours_arm(args)

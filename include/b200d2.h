@@ -51,7 +51,13 @@ enum {
   B200D2_PREC_TF32 = 1,    /* one TF32 product, FP32 accumulation in TMEM */
   B200D2_PREC_TF32X3 = 2,  /* hi*hi + hi*lo + lo*hi TF32 split */
   B200D2_PREC_BF16X3 = 3,  /* hi*hi + hi*lo + lo*hi BF16 split */
-  B200D2_PREC_FP64 = 4     /* FP64 CUDA-core kernel (GPU oracle) */
+  B200D2_PREC_FP64 = 4,    /* FP64 CUDA-core kernel (GPU oracle) */
+  /* FP16 operands with power-of-two scales: every particle's weighted image
+   * and every orientation's projection are scaled so that their largest
+   * component lies in [2^13, 2^14); the scales are undone exactly in the FP64
+   * combine. */
+  B200D2_PREC_FP16 = 5,    /* one scaled FP16 product */
+  B200D2_PREC_FP16X3 = 6   /* hi*hi + hi*lo + lo*hi scaled FP16 split */
 };
 
 /*
@@ -319,6 +325,26 @@ int b200d2_diff2_coarse_batch_static(const b200d2_view* view,
  * tensor-core epilogue. */
 int b200d2_minloc(const float* d_diff2, long long n, int P, double* d_min,
                   long long* d_argmin, void* stream);
+
+/* Coarse weights of a scored batch, the step after the coarse pass (its
+ * RELION driver kernel_weights_exponent_coarse is a commented stub at
+ * src/utilities.h:405-443 of the reference harness):
+ *   w[p][o][t] = pdf_orient[o] * pdf_offset[t] * exp(-(diff2[p][o][t] - min_p))
+ * computed in FP64 from the FP32 diff2 block diff2[P][O][T].  min_p is
+ * d_min[p] (e.g. the batch's per-particle minimum) or, with d_min NULL, the
+ * minimum of the particle's block.  d_pdf_orient [O] / d_pdf_offset [T] may be
+ * NULL (all ones); a zero prior gives a zero weight.  d_sum[p] receives the
+ * sum of the particle's weights, added in a fixed order (bit-reproducible).
+ * With normalize != 0 the stored weights are w / d_sum[p].  d_weights may be
+ * NULL when normalize == 0 (sums only).  The workspace is
+ * b200d2_coarse_weights_workspace(P, O*T) bytes of device memory, contents
+ * ignored; one call at a time per workspace.  Asynchronous on `stream`. */
+size_t b200d2_coarse_weights_workspace(int P, long long n);
+int b200d2_coarse_weights(const float* d_diff2, int P, int O, int T,
+                          const double* d_min, const double* d_pdf_orient,
+                          const double* d_pdf_offset, int normalize,
+                          double* d_weights, double* d_sum, void* d_workspace,
+                          size_t workspace_bytes, void* stream);
 
 /* Run a single stage of the batch pipeline, so that a caller can time one
  * kernel with events on its stream.  Stages are numbered in pipeline order

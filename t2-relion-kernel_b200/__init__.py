@@ -29,6 +29,8 @@ PREC_TF32 = 1
 PREC_TF32X3 = 2
 PREC_BF16X3 = 3
 PREC_FP64 = 4
+PREC_FP16 = 5  # scaled FP16, one product
+PREC_FP16X3 = 6  # scaled FP16 hi/lo split, three products
 
 _STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: "out of memory",
            5: "device wait timed out", 6: "no device", 7: "request exceeds a fixed capacity"}
@@ -137,6 +139,7 @@ def _declare(L):
         "b200d2_server_wait": [P, C.c_longlong, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)],
         "b200d2_server_get_stats": [P, C.POINTER(ServerStats)],
         "b200d2_server_destroy": [P],
+        "b200d2_coarse_weights": [P, I, I, I, P, P, P, I, P, P, P, Z, P],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -150,6 +153,8 @@ def _declare(L):
     L.b200d2_stage_name.restype = C.c_char_p
     L.b200d2_workspace_status.argtypes = [P, P, C.POINTER(C.c_int)]
     L.b200d2_workspace_status.restype = C.c_int
+    L.b200d2_coarse_weights_workspace.argtypes = [I, C.c_longlong]
+    L.b200d2_coarse_weights_workspace.restype = C.c_size_t
     L.b200d2_launch_count.argtypes = []
     L.b200d2_launch_count.restype = C.c_ulonglong
     # optional entry points declared by later modules of the library
@@ -430,6 +435,27 @@ def diff2_coarse_batch_static(view: View, batch: Batch, precision: int = PREC_BF
 
 def minloc(diff2, n: int, P: int, out_min=None, out_argmin=None, stream=None):
     _check(lib().b200d2_minloc(_ptr(diff2), n, P, _ptr(out_min), _ptr(out_argmin), _stream(stream)), "minloc")
+
+
+def coarse_weights(diff2, P: int, O: int, T: int, out_min=None, pdf_orient=None, pdf_offset=None,
+                   normalize: bool = True, weights=None, sums=None, workspace=None, stream=None):
+    """FP64 coarse weights pdf_o * pdf_t * exp(-(diff2 - min)) per particle
+    (b200d2_coarse_weights).  diff2: CUDA float32 [P*O*T]; returns
+    (weights [P, O, T] float64, sums [P] float64), normalised by the sums
+    unless normalize is False."""
+    import torch
+    dev = diff2.device
+    if weights is None:
+        weights = torch.empty((P, O, T), dtype=torch.float64, device=dev)
+    if sums is None:
+        sums = torch.empty(P, dtype=torch.float64, device=dev)
+    nb = lib().b200d2_coarse_weights_workspace(P, O * T)
+    if workspace is None or workspace.numel() < nb:
+        workspace = torch.empty(max(nb, 1), dtype=torch.uint8, device=dev)
+    _check(lib().b200d2_coarse_weights(_ptr(diff2), P, O, T, _ptr(out_min), _ptr(pdf_orient), _ptr(pdf_offset),
+                                       1 if normalize else 0, _ptr(weights), _ptr(sums), _ptr(workspace), nb,
+                                       _stream(stream)), "coarse_weights")
+    return weights, sums
 
 
 def stage_names(precision: int) -> list[str]:

@@ -73,8 +73,7 @@ extern "C" int b200d2_diff2_coarse_batch(const b200d2_view* view, const b200d2_b
     if (b.d_min || b.d_argmin) st = b200d2::minloc(b.d_diff2, per, b.P, b.d_min, b.d_argmin, s);
     return st;
   }
-  if (precision == B200D2_PREC_TF32 || precision == B200D2_PREC_TF32X3 ||
-      precision == B200D2_PREC_BF16X3) {
+  if (b200d2::is_tc_precision(precision)) {
     const size_t need = b200d2::tc_workspace_bytes(*view, b, precision);
     if (need > 0 && (!d_workspace || workspace_bytes < need)) return B200D2_ERR_INVALID;
     return b200d2::tc_run(*view, b, precision, d_workspace, workspace_bytes, s);
@@ -93,8 +92,7 @@ extern "C" const char* b200d2_stage_name(int precision, int stage) {
     static const char* names[] = {"diff2_direct_kernel<float>", "minloc_kernel"};
     return (stage >= 0 && stage < 2) ? names[stage] : nullptr;
   }
-  if (precision == B200D2_PREC_TF32 || precision == B200D2_PREC_TF32X3 ||
-      precision == B200D2_PREC_BF16X3)
+  if (b200d2::is_tc_precision(precision))
     return b200d2::tc_stage_name(precision, stage);
   return nullptr;
 }
@@ -119,8 +117,7 @@ extern "C" int b200d2_diff2_coarse_batch_stage(const b200d2_view* view,
     if (stage == 1) return b200d2::minloc(b.d_diff2, per, b.P, b.d_min, b.d_argmin, s);
     return B200D2_ERR_INVALID;
   }
-  if (precision == B200D2_PREC_TF32 || precision == B200D2_PREC_TF32X3 ||
-      precision == B200D2_PREC_BF16X3) {
+  if (b200d2::is_tc_precision(precision)) {
     const size_t need = b200d2::tc_workspace_bytes(*view, b, precision);
     if (need > 0 && (!d_workspace || workspace_bytes < need)) return B200D2_ERR_INVALID;
     return b200d2::tc_run_stage(*view, b, precision, stage, d_workspace, workspace_bytes, s);

@@ -30,6 +30,12 @@ inline int status_from_cuda(cudaError_t e) {
   return B200D2_ERR_CUDA;
 }
 
+// Precisions served by the tensor-core pipeline.
+inline bool is_tc_precision(int p) {
+  return p == B200D2_PREC_TF32 || p == B200D2_PREC_TF32X3 || p == B200D2_PREC_BF16X3 ||
+         p == B200D2_PREC_FP16 || p == B200D2_PREC_FP16X3;
+}
+
 // Sample positions are formed with explicit, ordered fused multiply-adds so
 // that every kernel of this library (and the CPU oracle, which uses the same
 // order) sees bit-identical coordinates:

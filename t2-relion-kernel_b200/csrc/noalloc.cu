@@ -70,7 +70,7 @@ int static_scratch(void** out) {
 extern "C" int b200d2_diff2_coarse_batch_static(const b200d2_view* view, const b200d2_batch* batch,
                                                 int precision, void* stream) {
   if (!view || !batch) return B200D2_ERR_INVALID;
-  if (precision != B200D2_PREC_BF16X3 && precision != B200D2_PREC_TF32X3 && precision != B200D2_PREC_TF32)
+  if (!b200d2::is_tc_precision(precision))
     return B200D2_ERR_UNSUPPORTED;  // the CUDA-core paths need no scratch: use b200d2_diff2_coarse_batch
   if (batch->O == 0 || batch->T == 0 || batch->P == 0) return B200D2_OK;
   // the allocating entry point's size query also validates the view and batch

@@ -204,8 +204,7 @@ void sched_loop(b200d2_server* s) {
 
 extern "C" int b200d2_server_create(int slots, size_t hbm_budget_bytes, int precision, b200d2_server** out) {
   if (!out || slots <= 0 || slots > 64 || hbm_budget_bytes == 0) return B200D2_ERR_INVALID;
-  if (precision != B200D2_PREC_FP32 && precision != B200D2_PREC_TF32 && precision != B200D2_PREC_TF32X3 &&
-      precision != B200D2_PREC_BF16X3)
+  if (precision != B200D2_PREC_FP32 && !b200d2::is_tc_precision(precision))
     return B200D2_ERR_UNSUPPORTED;
   *out = nullptr;
   b200d2_server* s = new b200d2_server();

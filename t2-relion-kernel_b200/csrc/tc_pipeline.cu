@@ -5,9 +5,12 @@
 // with w = corr/2.  The cross term is a dense complex-as-real contraction:
 //   C[m = p*T + t][o] = sum_kk Aop[m][kk] * Bop[o][kk],   kk = 2*pixel + {re, im}
 // run on tcgen05 tensor cores with FP32 accumulation in TMEM.  Operands are
-// split into hi + lo parts (BF16 or TF32) and three products are accumulated
-// (hi*hi + hi*lo + lo*hi) to recover near-FP32 accuracy; the norms are
-// accumulated in FP64 and the final combination is FP64.
+// split into hi + lo parts (BF16, FP16 or TF32) and three products are
+// accumulated (hi*hi + hi*lo + lo*hi) to recover near-FP32 accuracy, or taken
+// once (TF32, FP16); the norms are accumulated in FP64 and the final
+// combination is FP64.  The FP16 forms scale each particle's rows and each
+// orientation's row by a power of two (largest component in [2^13, 2^14)) and
+// divide the scales out exactly in the combine.
 //
 // Stages (one kernel each):
 //   0 pixel_list : in-radius pixel list (FilterCoarseParamImage, src/main.cu:88-151)
@@ -24,6 +27,7 @@
 //   7 finalize   : per-particle min / argmin from the packed keys
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
@@ -45,7 +49,7 @@ struct TcGeom {
   int P, O, T, N_img, K_c, Kpad, Mrows, Mpad, Opad, maxR, exw, eyw;
   int elem, BK, terms;
   size_t off_status, off_xy, off_idx, off_ex, off_ey, off_bhi, off_blo, off_q, off_w, off_normx, off_na,
-      off_ahi, off_alo, off_keys, total;
+      off_ahi, off_alo, off_keys, off_sa, off_sb, total;
 };
 
 static inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -85,9 +89,9 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, i
   } else {
     g.K_c = count_inside(v, b.N_img, &extent);
   }
-  g.elem = (prec == B200D2_PREC_BF16X3) ? 2 : 4;
+  g.elem = (prec == B200D2_PREC_TF32 || prec == B200D2_PREC_TF32X3) ? 4 : 2;
   g.BK = 128 / g.elem;
-  g.terms = (prec == B200D2_PREC_TF32) ? 1 : 3;
+  g.terms = (prec == B200D2_PREC_TF32 || prec == B200D2_PREC_FP16) ? 1 : 3;
   g.Kpad = (int)align_up((size_t)std::max(2 * g.K_c, 1), (size_t)g.BK);
   g.Mrows = mrows >= 0 ? mrows : b.P * b.T;
   g.Mpad = (int)align_up((size_t)g.Mrows, 128);
@@ -116,6 +120,8 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, i
   g.off_ahi = take((size_t)g.Mpad * g.Kpad * g.elem);
   g.off_alo = planes == 2 ? take((size_t)g.Mpad * g.Kpad * g.elem) : g.off_ahi;
   g.off_keys = take(sizeof(unsigned long long) * (size_t)g.P);
+  g.off_sa = take(sizeof(float) * (size_t)g.P);     // FP16 forms: 1 / particle scale
+  g.off_sb = take(sizeof(float) * (size_t)g.Opad);  // FP16 forms: 1 / orientation scale
   g.total = o;
   return g;
 }
@@ -246,6 +252,14 @@ __device__ __forceinline__ void store_split(void* hi, void* lo, size_t at, float
     const __nv_bfloat162 l = __floats2bfloat162_rn(re - hf.x, im - hf.y);
     reinterpret_cast<__nv_bfloat162*>(hi)[at] = h;
     reinterpret_cast<__nv_bfloat162*>(lo)[at] = l;
+  } else if constexpr (PREC == B200D2_PREC_FP16X3) {
+    const __half2 h = __floats2half2_rn(re, im);
+    const float2 hf = __half22float2(h);
+    const __half2 l = __floats2half2_rn(re - hf.x, im - hf.y);
+    reinterpret_cast<__half2*>(hi)[at] = h;
+    reinterpret_cast<__half2*>(lo)[at] = l;
+  } else if constexpr (PREC == B200D2_PREC_FP16) {
+    reinterpret_cast<__half2*>(hi)[at] = __floats2half2_rn(re, im);
   } else if constexpr (PREC == B200D2_PREC_TF32X3) {
     const float hr = tf32_round(re), hm = tf32_round(im);
     reinterpret_cast<float2*>(hi)[at] = make_float2(hr, hm);
@@ -278,6 +292,94 @@ __global__ void __launch_bounds__(128) tc_project_kernel(b200d2_view v, const fl
     q[(size_t)o * K_c + kp] = (double)b.x * (double)b.x + (double)b.y * (double)b.y;
   }
   store_split<PREC>(bhi, blo, (size_t)o * (Kpad / 2) + kp, b.x, b.y);
+}
+
+// ------------------------------------------------------------------ FP16 scales
+// Exponent e with max_abs * 2^e in [2^13, 2^14) (0 for a zero or non-finite
+// maximum), clamped so that 2^e and 2^-e are normal FP32 numbers.
+__device__ __forceinline__ int pow2_scale_exp(float max_abs) {
+  if (!(max_abs > 0.f) || !isfinite(max_abs)) return 0;
+  int e;
+  frexpf(max_abs, &e);  // max_abs = f * 2^e, f in [0.5, 1)
+  return max(-100, min(100, 14 - e));
+}
+
+// Maximum over a CTA of blockDim.x <= 1024 threads; every thread gets it.
+__device__ __forceinline__ float block_max(float v) {
+  __shared__ float s_part[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) s_part[warp] = v;
+  __syncthreads();
+  float m = 0.f;
+  for (int w = 0; w < nw; ++w) m = fmaxf(m, s_part[w]);
+  return m;
+}
+
+// FP16 forms, stage 2: one CTA per orientation.  Pass 1 projects every listed
+// pixel, writes |B|^2 and takes the largest component; pass 2 projects again
+// (same inputs, same bits) and stores the split of the scaled projection.
+// inv_sb[o] = 2^-e is divided out in the combine.
+template <int PREC>
+__global__ void __launch_bounds__(256) tc_project_scaled_kernel(b200d2_view v, const float* __restrict__ eulers,
+                                                                int O, const int2* __restrict__ xy, int K_c,
+                                                                int Kpad, void* bhi, void* blo, double* q,
+                                                                float* inv_sb) {
+  const int o = blockIdx.x, half = Kpad / 2;
+  float e[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (o < O) {
+    const float* eo = eulers + (size_t)o * 9;
+    e[0] = eo[0];
+    e[1] = eo[1];
+    e[2] = eo[3];
+    e[3] = eo[4];
+    e[4] = eo[6];
+    e[5] = eo[7];
+  }
+  float mx = 0.f;
+  if (o < O)
+    for (int kp = threadIdx.x; kp < K_c; kp += blockDim.x) {
+      const int2 c = xy[kp];
+      const float2 b = project_pixel(v, (float)c.x, (float)c.y, e);
+      q[(size_t)o * K_c + kp] = (double)b.x * (double)b.x + (double)b.y * (double)b.y;
+      mx = fmaxf(mx, fmaxf(fabsf(b.x), fabsf(b.y)));
+    }
+  const int ex = pow2_scale_exp(block_max(mx));
+  const float sc = ldexpf(1.f, ex);
+  if (threadIdx.x == 0) inv_sb[o] = ldexpf(1.f, -ex);
+  for (int kp = threadIdx.x; kp < half; kp += blockDim.x) {
+    float2 b = make_float2(0.f, 0.f);
+    if (o < O && kp < K_c) {
+      const int2 c = xy[kp];
+      b = project_pixel(v, (float)c.x, (float)c.y, e);
+    }
+    store_split<PREC>(bhi, blo, (size_t)o * half + kp, b.x * sc, b.y * sc);
+  }
+}
+
+// FP16 forms, stage 1: per-particle scale of the A rows.  A component of a
+// row is fma(w re, c, -(w im) s) or fma(w re, s, (w im) c) with |c|, |s| <= 1,
+// so |w re| + |w im| bounds it; inv_sa[p] = 2^-e of that bound's maximum.
+__global__ void __launch_bounds__(256) tc_scale_a_kernel(const float* __restrict__ re,
+                                                         const float* __restrict__ im,
+                                                         const float* __restrict__ corr, long long stride,
+                                                         const PartDev* __restrict__ parts,
+                                                         const int* __restrict__ idx, int K_c, float* inv_sa) {
+  const long long p = blockIdx.x;
+  const float* pre = parts ? parts[p].re : re + p * stride;
+  const float* pim = parts ? parts[p].im : im + p * stride;
+  const float* pco = parts ? parts[p].corr : corr + p * stride;
+  float mx = 0.f;
+  for (int k = threadIdx.x; k < K_c; k += blockDim.x) {
+    const int pix = idx[k];
+    const float w = pco[pix] / 2;
+    mx = fmaxf(mx, fabsf(w * pre[pix]) + fabsf(w * pim[pix]));
+  }
+  // 2^-20 of headroom for the rounding of the phase factors
+  const int ex = pow2_scale_exp(block_max(mx) * (1.f + 0x1p-20f));
+  if (threadIdx.x == 0) inv_sa[p] = ldexpf(1.f, -ex);
 }
 
 // ------------------------------------------------------------------ stage 3
@@ -313,11 +415,10 @@ __global__ void __launch_bounds__(256) tc_normx_kernel(const float* __restrict__
 // ------------------------------------------------------------------ stage 4
 // na[p][o] = normX[p] + sum_k w_p(k) |B_o(k)|^2, FP64 products and sums.
 // The weights w[p][k] and |B|^2 q[o][k] arrive as FP64 rows (written by the
-// normX and projector stages).  CTA tile: TP particles x 64 orientations; the
-// k dimension is walked in 16-pixel slabs copied into shared memory with
-// cp.async, double-buffered so the next slab's loads overlap this slab's
-// DFMAs.  Thread (tp, to) owns particles tp*(TP/16) + i and orientations
-// to + 16j; rows are padded to 17 doubles so the loads are conflict-free.
+// normX and projector stages).  The product runs on the FP64 tensor-core
+// MMA (mma.sync m8n8k4 f64: FP64 operands, products and sums); the k dimension
+// is walked in 16-pixel slabs copied into shared memory with cp.async,
+// double-buffered so the next slab's loads overlap this slab's MMAs.
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(sm100::smem_u32(smem)), "l"(gmem),
                "r"(pred ? 8 : 0)
@@ -415,7 +516,8 @@ __global__ void __launch_bounds__(256) tc_gen_a_kernel(
     const float* __restrict__ re, const float* __restrict__ im, const float* __restrict__ corr,
     long long stride, const int2* __restrict__ xy, const int* __restrict__ idx, int K_c, int Kpad,
     const float2* __restrict__ ex, const float2* __restrict__ ey, int T, int maxR, int Mrows,
-    void* ahi, void* alo, const PartDev* __restrict__ parts, const int4* __restrict__ rows) {
+    void* ahi, void* alo, const PartDev* __restrict__ parts, const int4* __restrict__ rows,
+    const float* __restrict__ inv_sa) {
   constexpr int ROWS = 32;
   const int kp = blockIdx.x * blockDim.x + threadIdx.x;
   if (kp >= Kpad / 2) return;
@@ -458,6 +560,11 @@ __global__ void __launch_bounds__(256) tc_gen_a_kernel(
         }
         wr = w * xr;
         wi = w * xi;
+        if (inv_sa) {  // FP16 forms: exact power-of-two scale of the particle's rows
+          const float sc = __frcp_rn(inv_sa[p]);
+          wr *= sc;
+          wi *= sc;
+        }
         cur_p = p;
       }
       const float2 fx = ex[tab * exw + x];
@@ -481,19 +588,23 @@ __global__ void __launch_bounds__(256) tc_gen_a_kernel(
 // same shared memory, i.e. more TMA latency hidden behind the tensor pipe.
 template <int PREC, int ROWB>
 struct GemmCfg {
-  static constexpr bool kTf32 = (PREC != B200D2_PREC_BF16X3);
+  static constexpr bool kTf32 = (PREC == B200D2_PREC_TF32 || PREC == B200D2_PREC_TF32X3);
+  static constexpr bool kScaled = (PREC == B200D2_PREC_FP16 || PREC == B200D2_PREC_FP16X3);
   static constexpr int kElem = kTf32 ? 4 : 2;
   static constexpr int kRowB = ROWB;
   static constexpr int kBK = ROWB / kElem;       // elements per k-block row
   static constexpr int kKStep = kTf32 ? 8 : 16;  // K of one tcgen05.mma (32 bytes)
-  static constexpr int kTerms = (PREC == B200D2_PREC_TF32) ? 1 : 3;
+  static constexpr int kTerms = (PREC == B200D2_PREC_TF32 || PREC == B200D2_PREC_FP16) ? 1 : 3;
+  // operand format of the instruction descriptor: TF32 = 2 (kind::tf32),
+  // BF16 = 1 and F16 = 0 (kind::f16)
+  static constexpr uint32_t kFmt = kTf32 ? 2u : (PREC == B200D2_PREC_BF16X3 ? 1u : 0u);
   static constexpr int kPlanes = kTerms == 3 ? 2 : 1;
   static constexpr int kBM = 128, kBN = 256;
   static constexpr int kATile = kBM * ROWB;
   static constexpr int kBTile = kBN * ROWB;
   static constexpr int kStageBytes = kPlanes * (kATile + kBTile);
   static constexpr int kStages = (200 * 1024) / kStageBytes < 8 ? (200 * 1024) / kStageBytes : 8;
-  static constexpr uint32_t kIdesc = sm100::idesc_f32acc(kTf32 ? 2u : 1u, kBM, kBN);
+  static constexpr uint32_t kIdesc = sm100::idesc_f32acc(kFmt, kBM, kBN);
   static constexpr int kBarBytes = 256;
   static constexpr int kSmem = kStages * kStageBytes + kBarBytes + 1024;
   static_assert(kStages >= 2, "at least two pipeline stages");
@@ -506,6 +617,8 @@ struct GemmArgs {
   const double* na;
   unsigned long long* keys;
   uint32_t* status;
+  const float* inv_sa;  // FP16 forms: [P] 1 / particle scale
+  const float* inv_sb;  // FP16 forms: [Opad] 1 / orientation scale
   Layout L;  // uneven batch tables (all null for a uniform batch)
 };
 
@@ -705,6 +818,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         }
       }
       const double* __restrict__ na_row = g.na + (size_t)p * g.O;
+      // FP16 forms: -2 / (particle scale); the orientation scale is per column
+      const double m2s = C::kScaled ? -2.0 * (double)g.inv_sa[vrow ? p : 0] : -2.0;
       float* __restrict__ out_row = outp + t;
       float best = __int_as_float(0x7f800000);
       uint32_t best_idx = 0xffffffffu;
@@ -721,7 +836,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
             const int o = oc + j;
             const int lo = (o < g.O) ? (inv ? inv[o] : o) : -1;
             if (lo >= 0) {
-              const double dd = fma(-2.0, (double)__uint_as_float(r[j]), na_row[o]);
+              double cr = (double)__uint_as_float(r[j]);
+              if (C::kScaled) cr *= (double)g.inv_sb[o];
+              const double dd = fma(m2s, cr, na_row[o]);
               float f = (float)dd;
               float* dst = out_row + (size_t)lo * Tp;
               if (g.accumulate) f += *dst;
@@ -736,10 +853,20 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       }
       sm100::tc_fence_before();
       sm100::mbar_arrive(&acce[b]);
-      if (vrow && best_idx != 0xffffffffu) {
-        const unsigned long long key = ((unsigned long long)ordered_bits(best) << 32) | best_idx;
-        atomicMin(&g.keys[p], key);
+      // Per-particle minimum across the warp's 32 rows: a particle's rows are
+      // contiguous, so a segmented shuffle-down min leaves each run's minimum
+      // in its first lane, which alone issues the atomic.
+      unsigned long long key =
+          (vrow && best_idx != 0xffffffffu) ? (((unsigned long long)ordered_bits(best) << 32) | best_idx) : ~0ull;
+      const int pk = vrow ? p : -1;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const unsigned long long ok2 = __shfl_down_sync(0xffffffffu, key, off);
+        const int op = __shfl_down_sync(0xffffffffu, pk, off);
+        if (lane + off < 32 && op == pk && ok2 < key) key = ok2;
       }
+      const int prevp = __shfl_up_sync(0xffffffffu, pk, 1);
+      if (pk >= 0 && (lane == 0 || prevp != pk) && key != ~0ull) atomicMin(&g.keys[pk], key);
     }
   }
   __syncthreads();
@@ -771,14 +898,17 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   return fn;
 }
 
-static int make_map(CUtensorMap* m, void* base, int elem, int cols, int rows, int box_rows, int row_bytes) {
+static int make_map(CUtensorMap* m, void* base, int elem, int cols, int rows, int box_rows, int row_bytes,
+                    bool fp16 = false) {
   auto enc = get_encode();
   if (!enc) return B200D2_ERR_CUDA;
   const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)cols * elem};
   const cuuint32_t box[2] = {(cuuint32_t)(row_bytes / elem), (cuuint32_t)box_rows};
   const cuuint32_t es[2] = {1, 1};
-  CUresult r = enc(m, elem == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+  const CUtensorMapDataType dt = elem == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                 : (fp16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16);
+  CUresult r = enc(m, dt, 2,
                    base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                    row_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -812,10 +942,10 @@ static int launch_gemm_rb(const b200d2_batch& b, const TcGeom& g, void* ws, cuda
   void* ahi = ws_at<void>(ws, g.off_ahi);
   void* alo = ws_at<void>(ws, g.off_alo);
   CUtensorMap mAhi, mAlo, mBhi, mBlo;
-  int st = make_map(&mAhi, ahi, g.elem, g.Kpad, g.Mpad, C::kBM, ROWB);
-  if (st == B200D2_OK) st = make_map(&mAlo, alo, g.elem, g.Kpad, g.Mpad, C::kBM, ROWB);
-  if (st == B200D2_OK) st = make_map(&mBhi, bhi, g.elem, g.Kpad, g.Opad, C::kBN, ROWB);
-  if (st == B200D2_OK) st = make_map(&mBlo, blo, g.elem, g.Kpad, g.Opad, C::kBN, ROWB);
+  int st = make_map(&mAhi, ahi, g.elem, g.Kpad, g.Mpad, C::kBM, ROWB, C::kScaled);
+  if (st == B200D2_OK) st = make_map(&mAlo, alo, g.elem, g.Kpad, g.Mpad, C::kBM, ROWB, C::kScaled);
+  if (st == B200D2_OK) st = make_map(&mBhi, bhi, g.elem, g.Kpad, g.Opad, C::kBN, ROWB, C::kScaled);
+  if (st == B200D2_OK) st = make_map(&mBlo, blo, g.elem, g.Kpad, g.Opad, C::kBN, ROWB, C::kScaled);
   if (st != B200D2_OK) return st;
   GemmArgs a;
   a.Mrows = g.Mrows;
@@ -829,6 +959,8 @@ static int launch_gemm_rb(const b200d2_batch& b, const TcGeom& g, void* ws, cuda
   a.na = ws_at<double>(ws, g.off_na);
   a.keys = ws_at<unsigned long long>(ws, g.off_keys);
   a.status = ws_at<uint32_t>(ws, g.off_status);
+  a.inv_sa = ws_at<float>(ws, g.off_sa);
+  a.inv_sb = ws_at<float>(ws, g.off_sb);
   a.L = Layout{U ? U->parts : nullptr, U ? U->rows : nullptr, U ? U->tiles : nullptr, U ? U->ntiles : 0};
   static bool attr_set = false;
   if (!attr_set) {
@@ -869,6 +1001,9 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
   void* ahi = ws_at<void>(ws, g.off_ahi);
   void* alo = ws_at<void>(ws, g.off_alo);
   unsigned long long* keys = ws_at<unsigned long long>(ws, g.off_keys);
+  constexpr bool kScaled = (PREC == B200D2_PREC_FP16 || PREC == B200D2_PREC_FP16X3);
+  float* inv_sa = ws_at<float>(ws, g.off_sa);
+  float* inv_sb = ws_at<float>(ws, g.off_sb);
   switch (stage) {
     case 0:
       tc_pixel_list_kernel<<<1, 1024, 0, s>>>(v, g.N_img, xy, idx, status, keys, g.P, b.d_coor_xy,
@@ -878,11 +1013,21 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       const int n = g.T * (g.exw + g.eyw);
       tc_phase_kernel<<<std::max(1, std::min((n + 255) / 256, 1024)), 256, 0, s>>>(
           b.d_trans_x, b.d_trans_y, g.T, g.maxR, ex, ey, U ? U->tab_txy : nullptr);
+      if (kScaled) {  // the particle scales, needed by stage 5 on the same stream
+        count_launch();
+        tc_scale_a_kernel<<<g.P, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, parts, idx, g.K_c,
+                                              inv_sa);
+      }
       break;
     }
     case 2: {
-      dim3 grid((g.Kpad / 2 + 127) / 128, g.Opad);
-      tc_project_kernel<PREC><<<grid, 128, 0, s>>>(v, b.d_eulers, g.O, xy, g.K_c, g.Kpad, bhi, blo, q);
+      if (kScaled) {
+        tc_project_scaled_kernel<PREC><<<g.Opad, 256, 0, s>>>(v, b.d_eulers, g.O, xy, g.K_c, g.Kpad, bhi, blo, q,
+                                                              inv_sb);
+      } else {
+        dim3 grid((g.Kpad / 2 + 127) / 128, g.Opad);
+        tc_project_kernel<PREC><<<grid, 128, 0, s>>>(v, b.d_eulers, g.O, xy, g.K_c, g.Kpad, bhi, blo, q);
+      }
       break;
     }
     case 3:
@@ -906,7 +1051,7 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       dim3 grid((g.Kpad / 2 + 255) / 256, g.Mpad / 32);
       tc_gen_a_kernel<PREC><<<grid, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, xy, idx, g.K_c,
                                                  g.Kpad, ex, ey, g.T, g.maxR, g.Mrows, ahi, alo, parts,
-                                                 U ? U->rows : nullptr);
+                                                 U ? U->rows : nullptr, kScaled ? inv_sa : nullptr);
       break;
     }
     case 6:
@@ -927,6 +1072,8 @@ static int dispatch_stage(const b200d2_view& v, const b200d2_batch& b, int prec,
     case B200D2_PREC_BF16X3: return launch_stage<B200D2_PREC_BF16X3>(v, b, g, ws, stage, s, U, row_bytes);
     case B200D2_PREC_TF32X3: return launch_stage<B200D2_PREC_TF32X3>(v, b, g, ws, stage, s, U, row_bytes);
     case B200D2_PREC_TF32: return launch_stage<B200D2_PREC_TF32>(v, b, g, ws, stage, s, U, row_bytes);
+    case B200D2_PREC_FP16X3: return launch_stage<B200D2_PREC_FP16X3>(v, b, g, ws, stage, s, U, row_bytes);
+    case B200D2_PREC_FP16: return launch_stage<B200D2_PREC_FP16>(v, b, g, ws, stage, s, U, row_bytes);
     default: return B200D2_ERR_UNSUPPORTED;
   }
 }
@@ -947,10 +1094,20 @@ const char* tc_stage_name(int precision, int stage) {
   static const char* tf1[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_kernel<tf32>",
                               "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<tf32>",
                               "tc_gemm_kernel<tf32>", "tc_finalize_kernel"};
+  // FP16 forms: stage 1 also launches tc_scale_a_kernel, stage 2 is the
+  // two-pass tc_project_scaled_kernel
+  static const char* h3[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_scaled_kernel<fp16x3>",
+                             "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<fp16x3>",
+                             "tc_gemm_kernel<fp16x3>", "tc_finalize_kernel"};
+  static const char* h1[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_scaled_kernel<fp16>",
+                             "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<fp16>",
+                             "tc_gemm_kernel<fp16>", "tc_finalize_kernel"};
   if (stage < 0 || stage >= kNumStages) return nullptr;
   if (precision == B200D2_PREC_BF16X3) return bf16[stage];
   if (precision == B200D2_PREC_TF32X3) return tf3[stage];
   if (precision == B200D2_PREC_TF32) return tf1[stage];
+  if (precision == B200D2_PREC_FP16X3) return h3[stage];
+  if (precision == B200D2_PREC_FP16) return h1[stage];
   return nullptr;
 }
 
@@ -1115,8 +1272,7 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   using namespace b200d2;
   if (!view || !d_eulers || !parts || !out || P <= 0 || O_all <= 0 || N_img <= 0) return B200D2_ERR_INVALID;
   *out = nullptr;
-  if (precision != B200D2_PREC_BF16X3 && precision != B200D2_PREC_TF32X3 && precision != B200D2_PREC_TF32)
-    return B200D2_ERR_UNSUPPORTED;
+  if (!is_tc_precision(precision)) return B200D2_ERR_UNSUPPORTED;
   if (view->mdlZ == 0 || (long long)view->imgX * view->imgY < N_img) return B200D2_ERR_INVALID;
   for (int i = 0; i < P; ++i) {
     const b200d2_particle_desc& d = parts[i];

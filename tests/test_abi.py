@@ -37,6 +37,12 @@ def test_host_side_argument_validation(pkg):
     # NULL buffers to the drop-in
     assert lib.b200d2_diff2_coarse(C.byref(v), None, None, None, None, None, None, None, 1, 1, 1, None, 0) == 1
     assert lib.b200d2_projector_load_dat(b"/nonexistent/projector.dat", 1, C.byref(C.c_void_p())) == 1
+    # coarse weights: empty problems are a no-op, missing buffers are rejected
+    assert lib.b200d2_coarse_weights(None, 0, 10, 10, None, None, None, 1, None, None, None, 0, None) == 0
+    assert lib.b200d2_coarse_weights(None, 2, 10, 10, None, None, None, 1, None, None, None, 0, None) == 1
+    assert lib.b200d2_coarse_weights(None, -1, 10, 10, None, None, None, 1, None, None, None, 0, None) == 1
+    assert lib.b200d2_coarse_weights_workspace(0, 100) == 0
+    assert lib.b200d2_coarse_weights_workspace(3, 70000) >= 3 * 8 + 3 * 3 * 8 + 3 * 4
 
 
 def test_no_cpu_fallback_in_product():

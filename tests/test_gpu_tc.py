@@ -5,6 +5,8 @@ Stated tolerances (max relative diff2 error vs FP64, over every evaluation):
   BF16x3 (hi*hi + hi*lo + lo*hi)  1e-5
   TF32x3                          1e-5
   TF32 (single product)           1e-3
+  FP16x3 (scaled hi/lo split)     1e-5
+  FP16 (scaled, single product)   1e-3
 The argmin (o, t) must equal the FP64 argmin wherever the FP64 best-to-second
 gap exceeds twice the tolerance."""
 from __future__ import annotations
@@ -17,11 +19,13 @@ import pytest
 from gpu_util import DeviceProblem, argmin_consistent, ours_f64
 
 pytestmark = pytest.mark.gpu
-TOL = {"bf16x3": 1e-5, "tf32x3": 1e-5, "tf32": 1e-3}
+TOL = {"bf16x3": 1e-5, "tf32x3": 1e-5, "tf32": 1e-3, "fp16x3": 1e-5, "fp16": 1e-3}
+ALL = ["bf16x3", "tf32x3", "tf32", "fp16x3", "fp16"]
 
 
 def prec_code(pkg, name):
-    return {"bf16x3": pkg.PREC_BF16X3, "tf32x3": pkg.PREC_TF32X3, "tf32": pkg.PREC_TF32}[name]
+    return {"bf16x3": pkg.PREC_BF16X3, "tf32x3": pkg.PREC_TF32X3, "tf32": pkg.PREC_TF32,
+            "fp16x3": pkg.PREC_FP16X3, "fp16": pkg.PREC_FP16}[name]
 
 
 def run_tc(pkg, torch, view, dp, prec, accumulate=False, init=None, stages=False):
@@ -82,12 +86,12 @@ def _check(pkg, oracle, cuda, case, name):
     return s
 
 
-@pytest.mark.parametrize("name", ["bf16x3", "tf32x3", "tf32"])
+@pytest.mark.parametrize("name", ALL)
 def test_tc_tiny(pkg, oracle, cuda, tiny, name):
     _check(pkg, oracle, cuda, tiny, name)
 
 
-@pytest.mark.parametrize("name", ["bf16x3", "tf32x3", "tf32"])
+@pytest.mark.parametrize("name", ALL)
 def test_tc_c1(pkg, oracle, cuda, c1, name):
     _check(pkg, oracle, cuda, c1, name)
 
@@ -98,7 +102,7 @@ def test_tc_c2_subset(pkg, synth, oracle, cuda):
     view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
     dp = DeviceProblem(cuda, pr)
     ref = fp64_all(pkg, view, dp)
-    for name in ("bf16x3", "tf32x3"):
+    for name in ("bf16x3", "tf32x3", "fp16x3"):
         _check(pkg, oracle, cuda, (pr, view, dp, ref), name)
     proj.close()
 
@@ -124,9 +128,10 @@ def test_tc_ragged(pkg, synth, oracle, cuda, o_lim, r2, P):
     view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
     dp = DeviceProblem(cuda, pr)
     ref = fp64_all(pkg, view, dp)
-    got, mn, am = run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3)
-    assert got.shape == (P, o_lim, sh.shape[0])
-    assert oracle.error_stats(got, ref)["max_rel"] <= 1e-5
+    for prec in (pkg.PREC_BF16X3, pkg.PREC_FP16X3):
+        got, mn, am = run_tc(pkg, cuda, view, dp, prec)
+        assert got.shape == (P, o_lim, sh.shape[0])
+        assert oracle.error_stats(got, ref)["max_rel"] <= 1e-5
     proj.close()
 
 
