@@ -167,6 +167,9 @@ def parse():
     ap.add_argument("--particles", type=int, default=None,
                     help="override the particle count (small cases for profiling; not a bench line)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=3.0, help="c5: length of the arrival trace")
+    ap.add_argument("--serve-fp32-seconds", type=float, default=0.5,
+                    help="c5: part of the trace replayed through the FP32 baseline")
     ap.add_argument("--study", default=None, choices=["precision"],
                     help="precision: error of every precision form vs the FP64 kernel (use --config c3)")
     return ap.parse_args()
@@ -503,7 +506,7 @@ def precision_study(args):
         rel = (got - ref).abs() / ref.abs().clamp_min(1e-300)
         w, _ = pkg.coarse_weights(out, P, O, T, out_min=mn)
         w = w.view(P, O * T)
-        sig = rw > 1e-3
+        sig = rw > 1e-3 * rw.max(dim=1, keepdim=True).values  # weights within 1e-3 of the particle's best
         wrel = ((w - rw).abs() / rw.clamp_min(1e-300))[sig]
         max_rel = float(rel.max())
         tol_gap = gap > 2 * max_rel * rmin.abs().cpu().numpy()
@@ -517,7 +520,7 @@ def precision_study(args):
             "argmin_identical_where_gap_exceeds_2x_err": bool(same[tol_gap].all()),
             "particles_with_gap_above_2x_err": int(tol_gap.sum()),
             "weights_max_abs_err": float((w - rw).abs().max()),
-            "weights_max_rel_err_above_1e-3": float(wrel.max()) if wrel.numel() else 0.0,
+            "weights_max_rel_err_above_1e-3_of_max": float(wrel.max()) if wrel.numel() else 0.0,
             "weights_l1_max_over_particles": float((w - rw).abs().sum(dim=1).max()),
         }
         del ws
@@ -530,10 +533,117 @@ def precision_study(args):
     return 0
 
 
+C5_REFS = ("c5s", "c5m", "c5l")
+
+
+def serving_arm(args):
+    """Serving loop (config c5): Poisson arrivals at 200 requests/s over three
+    resident references (coarse sizes 48 / 64 / 96); each request scores a
+    contiguous run of 16-512 particles (log-uniform) from the reference's
+    particle pool against a random 10-100 % subset of its 4608 orientations
+    and the translations within a radius of 2-6 px, and returns the per-particle
+    minimum and argmin.  The same request trace is replayed through a server
+    of plain FP32 CUDA-core launches, one request at a time, as the baseline.
+    Latency = submit to completion callback (host-side clock)."""
+    import torch
+    pkg = load_package()
+    synth = load_synth()
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(20251203)
+    refs = []
+    for i, name in enumerate(C5_REFS):
+        pr = synth.make_problem(name, seed=20251203 + i)
+        proj = pkg.Projector(pr.projector, use_texture=1)
+        view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+        pin = [torch.as_tensor(a).pin_memory() for a in (pr.fimg_re, pr.fimg_im, pr.corr)]
+        refs.append(dict(pr=pr, proj=proj, view=view, pin=pin))
+    rate, horizon = 200.0, args.serve_seconds
+    trace, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > horizon:
+            break
+        r = int(rng.integers(len(refs)))
+        pr = refs[r]["pr"]
+        P = int(round(math.exp(rng.uniform(math.log(16), math.log(512)))))
+        s0 = int(rng.integers(0, pr.P - P + 1))
+        O = max(1, int(round(rng.uniform(0.1, 1.0) * pr.O)))
+        orient = np.sort(rng.choice(pr.O, O, replace=False)).astype(np.int32)
+        rad = int(rng.integers(2, 7))
+        sh = synth.translation_grid(rad * rad)
+        tx = (-2 * math.pi * sh[:, 0] / pr.projector.ori_size).astype(np.float32)
+        ty = (-2 * math.pi * sh[:, 1] / pr.projector.ori_size).astype(np.float32)
+        trace.append(dict(t=t, ref=r, s0=s0, P=P, orient=orient, tx=tx, ty=ty))
+    evals = sum(q["P"] * q["orient"].size * q["tx"].size for q in trace)
+
+    def replay(precision, slots, budget, limit_s):
+        srv = pkg.Server(slots=slots, hbm_budget=budget, precision=precision)
+        ids = [srv.add_reference(rf["view"], rf["pr"].eulers, rf["pr"].N_img) for rf in refs]
+
+        def submit(q):
+            rf = refs[q["ref"]]
+            a, b = q["s0"], q["s0"] + q["P"]
+            mn = np.empty(q["P"], np.float64)
+            am = np.empty(q["P"], np.int64)
+            return srv.submit(ids[q["ref"]], rf["pin"][0][a:b], rf["pin"][1][a:b], rf["pin"][2][a:b],
+                              q["orient"], q["tx"], q["ty"], None, mn, am), (mn, am)
+
+        for q in trace[:3]:  # warm-up: one request of each kind, waited for
+            tk, _ = submit(q)
+            srv.wait(tk)
+        t0 = time.perf_counter()
+        sent = []
+        for q in trace:
+            if q["t"] > limit_s:
+                break
+            d = t0 + q["t"] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            ts = time.perf_counter()
+            tk, keep = submit(q)
+            sent.append((tk, ts, q, keep))
+        lats, done_at, ev = [], [], 0
+        for tk, ts, q, keep in sent:
+            st, lat, dev = srv.wait(tk, timeout=600.0)
+            if st != 0:
+                raise RuntimeError(f"request failed: status {st}")
+            lats.append(lat)
+            done_at.append(ts + lat)
+            ev += q["P"] * q["orient"].size * q["tx"].size
+        stats = srv.stats()
+        srv.close()
+        span = max(done_at) - t0
+        lat_ms = np.array(lats) * 1e3
+        return {"requests": len(sent), "p50_ms": float(np.percentile(lat_ms, 50)),
+                "p99_ms": float(np.percentile(lat_ms, 99)), "mean_ms": float(lat_ms.mean()),
+                "evals": ev, "evals_per_s": ev / span, "span_s": span, "max_in_flight": stats["max_in_flight"],
+                "peak_bytes": stats["peak_bytes"]}
+
+    tc = replay(pkg.PREC_TF32, 4, 48 << 30, horizon)
+    # the FP32 baseline cannot keep up with 200 requests/s; replay the first
+    # part of the same trace so the run stays bounded
+    fp32 = replay(pkg.PREC_FP32, 1, 48 << 30, min(horizon, args.serve_fp32_seconds))
+    line = {"metric": "p99 request latency (coarse-pass serving)", "value": tc["p99_ms"], "unit": "ms",
+            "n_gpus": 1, "higher_is_better": False, "dtype": "tf32", "data": "synthetic",
+            "config": {"workload": f"c5: Poisson {rate:.0f} req/s for {horizon:.1f} s, {len(trace)} requests over "
+                                   f"3 resident references (image 48/64/96, 4608 orientations), 16-512 "
+                                   f"particles per request, 10-100 % orientation subsets, translation radius "
+                                   f"2-6 px, outputs: per-particle min/argmin",
+                       "slots": 4, "hbm_budget_gib": 48, "trace_evals": evals},
+            "tensor_core_tf32": tc, "fp32_cuda_core_per_request": fp32,
+            "evals_per_s_ratio": tc["evals_per_s"] / fp32["evals_per_s"]}
+    print(json.dumps(line), flush=True)
+    for rf in refs:
+        rf["proj"].close()
+    return 0
+
+
 def main():
     args = parse()
     if args.study == "precision":
         return precision_study(args)
+    if args.config == "c5":
+        return serving_arm(args)
     if args.impl == "reference":
         return reference_arm(args)
     return ours_arm(args)

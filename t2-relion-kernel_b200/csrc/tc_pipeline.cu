@@ -445,7 +445,9 @@ template <int WM>
 __global__ void __launch_bounds__(128) tc_norma_kernel(const double* __restrict__ wcomp, int K_c,
                                                        const double* __restrict__ q, int O, int P,
                                                        const double* __restrict__ normx, double* na) {
-  constexpr int KC = 16, LD = KC + 1, CP = 16 * WM, CO = 64;
+  // rows padded to 20 doubles: the fragment loads of a half-warp (rows g,
+  // columns t, g, t < 4) then fall on distinct bank pairs 8g + 2t
+  constexpr int KC = 16, LD = KC + 4, CP = 16 * WM, CO = 64;
   __shared__ double sw[2][CP][LD];
   __shared__ double sq[2][CO][LD];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -613,6 +615,7 @@ struct GemmCfg {
 
 struct GemmArgs {
   int Mrows, Mtiles, Ntiles, O, T, KB, accumulate;
+  int group_m;  // uniform batches: 0 = m-major tile order, else groups of group_m m-tiles, n-major inside
   float* out;
   const double* na;
   unsigned long long* keys;
@@ -629,6 +632,14 @@ __device__ __forceinline__ void tile_origin(const GemmArgs& g, int tile, int bm,
     const int2 mn = g.L.tiles[tile];
     m0 = mn.x * bm;
     n0 = mn.y * bn;
+  } else if (g.group_m > 0) {
+    // groups of group_m m-tiles whose A rows stay in L2 while every n-tile
+    // (B rows) streams past them once per group
+    const int per_group = g.group_m * g.Ntiles;
+    const int grp = tile / per_group, rem = tile - grp * per_group;
+    const int gm0 = grp * g.group_m, gsz = min(g.group_m, g.Mtiles - gm0);
+    m0 = (gm0 + rem % gsz) * bm;
+    n0 = (rem / gsz) * bn;
   } else {
     m0 = (tile / g.Ntiles) * bm;
     n0 = (tile % g.Ntiles) * bn;
@@ -955,6 +966,17 @@ static int launch_gemm_rb(const b200d2_batch& b, const TcGeom& g, void* ws, cuda
   a.T = g.T;
   a.KB = g.Kpad / C::kBK;
   a.accumulate = b.accumulate;
+  {
+    // Tile order.  m-major re-reads B (all orientations) for every wave of
+    // m-tiles: right when B stays in L2.  Otherwise group the m-tiles so a
+    // group's A rows (about 48 MB) stay in L2 while B streams once per group.
+    const double l2_budget = 48.0 * 1024 * 1024;
+    const double b_bytes = (double)g.Opad * g.Kpad * g.elem * C::kPlanes;
+    const double a_tile = (double)C::kBM * g.Kpad * g.elem * C::kPlanes;
+    a.group_m = 0;
+    if (b_bytes > 64.0 * 1024 * 1024 && a.Mtiles > 1)
+      a.group_m = std::max(1, std::min(a.Mtiles, (int)(l2_budget / a_tile)));
+  }
   a.out = b.d_diff2;
   a.na = ws_at<double>(ws, g.off_na);
   a.keys = ws_at<unsigned long long>(ws, g.off_keys);

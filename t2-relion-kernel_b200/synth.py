@@ -113,6 +113,11 @@ CONFIGS = {
     "c3": dict(box=256, img=96, pf=2, order=3, n_psi=48, r2_trans=16, P=64, snr=0.02, ctf=True),
     "c4": dict(box=128, img=64, pf=2, order=2, n_psi=24, r2_trans=64, P=1024, snr=0.05, ctf=True,
                uneven=True),
+    # serving: three resident references (coarse sizes 48 / 64 / 96 from 96^3,
+    # 128^3, 192^3 volumes), a 512-particle pool each; requests take subsets
+    "c5s": dict(box=96, img=48, pf=2, order=2, n_psi=24, r2_trans=36, P=512, snr=0.05, ctf=True),
+    "c5m": dict(box=128, img=64, pf=2, order=2, n_psi=24, r2_trans=36, P=512, snr=0.05, ctf=True),
+    "c5l": dict(box=192, img=96, pf=2, order=2, n_psi=24, r2_trans=36, P=512, snr=0.05, ctf=True),
 }
 
 
