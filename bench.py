@@ -133,7 +133,7 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 def cpu_sample(pr, budget_s: float, max_particles: int | None = None) -> dict:
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle  # the checker's C restatement; measured here as the CPU baseline only
+    import oracle  # the oracle's C restatement; measured here as the CPU baseline only
     nthreads = os.cpu_count() or 1
     op = oracle.projector_for(pr)
     t0 = time.perf_counter()
@@ -293,14 +293,18 @@ def ours_arm(args):
         fb.record(stream)
         torch.cuda.synchronize()
         plan_extra["fixed_tile_ms_per_step"] = fa.elapsed_time(fb) / max(3, min(args.steps, 10))
-        plan_extra["fixed_tile_row_bytes"] = fixed.info()["row_bytes"]
+        fi = fixed.info()
+        plan_extra["fixed_variant"] = {"row_bytes": fi["row_bytes"], "tile_n": fi["tile_n"], "split": fi["split"]}
         fixed.close()
         del fixed_bufs
         plan, bufs, evals_plan = build_plan_case(pkg, pr, dev, prec,
                                                  pkg.PLAN_AUTOTUNE | pkg.PLAN_GRAPH | pkg.PLAN_REORDER)
         eul, re, im, corr, out, mn, am = bufs
         info = plan.info()
-        plan_extra.update({"autotuned_row_bytes": info["row_bytes"], "tuned_gemm_ms": info["tuned_ms"],
+        plan_extra.update({"autotuned_variant": {"row_bytes": info["row_bytes"], "tile_n": info["tile_n"],
+                                                 "split": info["split"]},
+                           "tuned_gemm_ms": {f"rb{v[0]}_n{v[1]}_s{v[2]}": ms for v, ms in info["tuned"]},
+                           "work_tiles_n128": info["tiles_n128"],
                            "work_tiles": info["tiles"], "dense_tiles": info["tiles_dense"], "rows": info["rows"]})
     else:
         out = torch.empty(P * O * T, device=dev, dtype=torch.float32)
@@ -350,7 +354,8 @@ def ours_arm(args):
 
     # ---- dominant kernel timing (events on the launching stream) ----
     if uneven:
-        tuned = plan_extra["tuned_gemm_ms"][0 if plan_extra["autotuned_row_bytes"] == 64 else 1]
+        av = plan_extra["autotuned_variant"]
+        tuned = plan_extra["tuned_gemm_ms"].get(f"rb{av['row_bytes']}_n{av['tile_n']}_s{av['split']}")
         name = [n for n in pkg.stage_names(prec) if "gemm" in n][0]
         kern = {"per_kernel_ms": {name: tuned}, "dominant": name, "dominant_ms": tuned or None, "traffic": None}
     else:

@@ -147,7 +147,7 @@ int b200d2_diff2_coarse_f64(const b200d2_view* view, const float* d_trans_x,
                             void* stream);
 
 /* ------------------------------------------------------------------------
- * Batched coarse pass (north-star layout diff2[p][o][t]).  The reference
+ * Batched coarse pass (layout diff2[p][o][t]).  The reference
  * launches one runDiff2KernelCoarse per particle (src/main.cu:483-503); this
  * call scores P particles that share the orientation and translation sets in
  * one pass.  Image p lives at d_real/d_imag/d_corr + p * img_stride.
@@ -221,11 +221,20 @@ enum {
   B200D2_PLAN_REORDER = 8
 };
 
+#define B200D2_PLAN_MAX_VARIANTS 16
 typedef struct b200d2_plan_info {
   int P, O_all, rows, tiles, tiles_dense, row_bytes, graph, stages;
   long long evals;        /* sum over particles of O * T */
   size_t workspace_bytes; /* plan-owned device bytes (workspace and tables) */
-  double tuned_ms[2];     /* contraction time of the 64- and 128-byte variants (0 = not timed) */
+  /* chosen contraction variant: tile width (orientations per tile) and
+   * k-splits per tile (row_bytes above is its k-block row width) */
+  int tile_n, split;
+  int tiles_n128;         /* work-list length with 128-wide tiles */
+  /* autotuner: variants timed, each (row_bytes, tile_n, split) and its
+   * contraction time in ms (n_tuned = 0 without B200D2_PLAN_AUTOTUNE) */
+  int n_tuned;
+  int tuned_variant[B200D2_PLAN_MAX_VARIANTS][3];
+  double tuned_ms[B200D2_PLAN_MAX_VARIANTS];
 } b200d2_plan_info;
 
 typedef struct b200d2_plan b200d2_plan;
@@ -345,6 +354,15 @@ int b200d2_coarse_weights(const float* d_diff2, int P, int O, int T,
                           const double* d_pdf_offset, int normalize,
                           double* d_weights, double* d_sum, void* d_workspace,
                           size_t workspace_bytes, void* stream);
+
+/* Contraction variant used by the tensor-core batch entry points
+ * (b200d2_diff2_coarse_batch, _stage, _static and the server), process-wide:
+ * row_bytes 64 or 128 (k-block row width), tile_n 256 or 128 (orientations
+ * per tile), split = k-splits per tile (partial sums added in split order in
+ * FP64).  0 in any field restores the default (64-byte rows, 256-wide tiles,
+ * k-splits chosen from the tile count, at most the workspace's capacity).
+ * Plans choose their own variant (B200D2_PLAN_AUTOTUNE). */
+int b200d2_set_gemm_variant(int row_bytes, int tile_n, int split);
 
 /* Run a single stage of the batch pipeline, so that a caller can time one
  * kernel with events on its stream.  Stages are numbered in pipeline order

@@ -70,10 +70,15 @@ class ParticleDesc(C.Structure):
                 ("T", C.c_int)]
 
 
+PLAN_MAX_VARIANTS = 16
+
+
 class PlanInfo(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("P", "O_all", "rows", "tiles", "tiles_dense", "row_bytes", "graph",
                                          "stages")] + [
-        ("evals", C.c_longlong), ("workspace_bytes", C.c_size_t), ("tuned_ms", C.c_double * 2)]
+        ("evals", C.c_longlong), ("workspace_bytes", C.c_size_t), ("tile_n", C.c_int), ("split", C.c_int),
+        ("tiles_n128", C.c_int), ("n_tuned", C.c_int), ("tuned_variant", (C.c_int * 3) * PLAN_MAX_VARIANTS),
+        ("tuned_ms", C.c_double * PLAN_MAX_VARIANTS)]
 
 
 class Request(C.Structure):
@@ -140,6 +145,7 @@ def _declare(L):
         "b200d2_server_get_stats": [P, C.POINTER(ServerStats)],
         "b200d2_server_destroy": [P],
         "b200d2_coarse_weights": [P, I, I, I, P, P, P, I, P, P, P, Z, P],
+        "b200d2_set_gemm_variant": [I, I, I],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -337,8 +343,9 @@ class Plan:
     def info(self) -> dict:
         inf = PlanInfo()
         _check(lib().b200d2_plan_get_info(self._h, C.byref(inf)), "plan_get_info")
-        d = {n: getattr(inf, n) for n, _ in PlanInfo._fields_ if n != "tuned_ms"}
-        d["tuned_ms"] = list(inf.tuned_ms)
+        d = {n: getattr(inf, n) for n, _ in PlanInfo._fields_ if n not in ("tuned_ms", "tuned_variant")}
+        # autotuner record: ((row_bytes, tile_n, split), ms) per variant timed
+        d["tuned"] = [(tuple(inf.tuned_variant[i]), inf.tuned_ms[i]) for i in range(inf.n_tuned)]
         return d
 
     def close(self):
@@ -456,6 +463,11 @@ def coarse_weights(diff2, P: int, O: int, T: int, out_min=None, pdf_orient=None,
                                        1 if normalize else 0, _ptr(weights), _ptr(sums), _ptr(workspace), nb,
                                        _stream(stream)), "coarse_weights")
     return weights, sums
+
+
+def set_gemm_variant(row_bytes: int = 0, tile_n: int = 0, split: int = 0) -> None:
+    """Contraction variant of the batch entry points (0 = default)."""
+    _check(lib().b200d2_set_gemm_variant(row_bytes, tile_n, split), "set_gemm_variant")
 
 
 def stage_names(precision: int) -> list[str]:

@@ -14,7 +14,8 @@ int direct_batch(const b200d2_view& view, const float* eulers, const float* tx,
                  long long out_stride, int O, int T, int N_img, int P,
                  bool fp64, int filter_img, cudaStream_t s);
 int minloc(const float* d, long long n, int P, double* mn, long long* arg, cudaStream_t s);
-size_t tc_workspace_bytes(const b200d2_view& view, const b200d2_batch& b, int precision);
+size_t tc_workspace_bytes(const b200d2_view& view, const b200d2_batch& b, int precision,
+                          bool allow_split = true);
 int tc_run(const b200d2_view& view, const b200d2_batch& b, int precision, void* ws,
            size_t ws_bytes, cudaStream_t s);
 
@@ -84,7 +85,7 @@ extern "C" int b200d2_diff2_coarse_batch(const b200d2_view* view, const b200d2_b
 namespace b200d2 {
 const char* tc_stage_name(int precision, int stage);
 int tc_run_stage(const b200d2_view& view, const b200d2_batch& b, int precision, int stage,
-                 void* ws, size_t ws_bytes, cudaStream_t s);
+                 void* ws, size_t ws_bytes, cudaStream_t s, bool allow_split = true);
 }  // namespace b200d2
 
 extern "C" const char* b200d2_stage_name(int precision, int stage) {

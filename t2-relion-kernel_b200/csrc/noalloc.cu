@@ -34,9 +34,10 @@
 #include "common.cuh"
 
 namespace b200d2 {
-size_t tc_workspace_bytes(const b200d2_view& view, const b200d2_batch& b, int precision);
+size_t tc_workspace_bytes(const b200d2_view& view, const b200d2_batch& b, int precision,
+                          bool allow_split = true);
 int tc_run_stage(const b200d2_view& view, const b200d2_batch& b, int precision, int stage, void* ws,
-                 size_t ws_bytes, cudaStream_t s);
+                 size_t ws_bytes, cudaStream_t s, bool allow_split = true);
 const char* tc_stage_name(int precision, int stage);
 }  // namespace b200d2
 
@@ -74,15 +75,17 @@ extern "C" int b200d2_diff2_coarse_batch_static(const b200d2_view* view, const b
     return B200D2_ERR_UNSUPPORTED;  // the CUDA-core paths need no scratch: use b200d2_diff2_coarse_batch
   if (batch->O == 0 || batch->T == 0 || batch->P == 0) return B200D2_OK;
   // the allocating entry point's size query also validates the view and batch
-  const size_t need = b200d2_diff2_coarse_batch_workspace(view, batch, precision);
-  if (need == 0) return B200D2_ERR_INVALID;
+  if (b200d2_diff2_coarse_batch_workspace(view, batch, precision) == 0) return B200D2_ERR_INVALID;
+  // the scratch is sized for the contraction without k-splits (no partial sums)
+  const size_t need = b200d2::tc_workspace_bytes(*view, *batch, precision, false);
   if (need > (size_t)B200D2_STATIC_SCRATCH_BYTES) return B200D2_ERR_TOO_LARGE;
   void* ws = nullptr;
   int st = static_scratch(&ws);
   if (st != B200D2_OK) return st;
   cudaStream_t s = (cudaStream_t)stream;
   for (int stage = 0; b200d2::tc_stage_name(precision, stage) != nullptr; ++stage) {
-    st = b200d2::tc_run_stage(*view, *batch, precision, stage, ws, (size_t)B200D2_STATIC_SCRATCH_BYTES, s);
+    st = b200d2::tc_run_stage(*view, *batch, precision, stage, ws, (size_t)B200D2_STATIC_SCRATCH_BYTES, s,
+                              false);
     if (st != B200D2_OK) return st;
   }
   return B200D2_OK;

@@ -32,6 +32,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -49,8 +50,12 @@ struct TcGeom {
   int P, O, T, N_img, K_c, Kpad, Mrows, Mpad, Opad, maxR, exw, eyw;
   int elem, BK, terms;
   size_t off_status, off_xy, off_idx, off_ex, off_ey, off_bhi, off_blo, off_q, off_w, off_normx, off_na,
-      off_ahi, off_alo, off_keys, off_sa, off_sb, total;
+      off_ahi, off_alo, off_keys, off_sa, off_sb, off_part, off_cnt, total;
+  int split_max;  // largest k-split the workspace holds partial sums for
+  int n_cnt;      // split arrival counters
 };
+
+static int num_sms();
 
 static inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -75,7 +80,8 @@ static int count_inside(const b200d2_view& v, int N_img, int* extent) {
 
 // mrows >= 0 overrides the row count (uneven batches: the sum of every
 // particle's translations; b.T is then the number of phase tables).
-static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, int mrows = -1) {
+static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, int mrows = -1,
+                        bool allow_split = true) {
   TcGeom g;
   memset(&g, 0, sizeof(g));
   g.P = b.P;
@@ -122,6 +128,20 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, i
   g.off_keys = take(sizeof(unsigned long long) * (size_t)g.P);
   g.off_sa = take(sizeof(float) * (size_t)g.P);     // FP16 forms: 1 / particle scale
   g.off_sb = take(sizeof(float) * (size_t)g.Opad);  // FP16 forms: 1 / orientation scale
+  // split-K: partial sums when the 256-wide tiles do not fill the GPU (the
+  // 128-wide tiling needs the same bytes: twice the tiles, half the width)
+  {
+    const int mt = g.Mpad / 128, tiles256 = mt * (g.Opad / 256);
+    const int kb = g.Kpad / g.BK;  // k-blocks of the 128-byte rows (fewest)
+    g.split_max = 1;
+    const int sms = num_sms();
+    if (allow_split && tiles256 < sms)
+      while (g.split_max * 2 <= 8 && (long long)tiles256 * g.split_max * 2 <= 2LL * sms && kb / (g.split_max * 2) >= 2)
+        g.split_max *= 2;
+    g.off_part = take(g.split_max > 1 ? (size_t)g.split_max * tiles256 * 256 * 128 * sizeof(float) : 0);
+    g.n_cnt = 4 * mt * (g.Opad / 128);
+    g.off_cnt = take(sizeof(unsigned) * (size_t)g.n_cnt);
+  }
   g.total = o;
   return g;
 }
@@ -141,8 +161,8 @@ struct PartDev {
 struct UnevenTabs {
   const PartDev* parts;   // [P]
   const int4* rows;       // [Mrows]
-  const int2* tiles;      // [ntiles]
-  int ntiles;
+  const int2* tiles[2];   // work lists of 256- and 128-wide tiles
+  int ntiles[2];
   const float2* tab_txy;  // [ntab] translation of each phase table
   int ntab;
   int Mrows;
@@ -166,7 +186,7 @@ __global__ void __launch_bounds__(1024) tc_pixel_list_kernel(b200d2_view v, int 
                                                              int* idx, uint32_t* status,
                                                              unsigned long long* keys, int P,
                                                              const float* __restrict__ coor_xy,
-                                                             int n_listed, int ext) {
+                                                             int n_listed, int ext, unsigned* cnt, int n_cnt) {
   __shared__ int s_cnt[32];
   __shared__ int s_base;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -175,6 +195,7 @@ __global__ void __launch_bounds__(1024) tc_pixel_list_kernel(b200d2_view v, int 
     s_base = 0;
   }
   for (int p = tid; p < P; p += blockDim.x) keys[p] = ~0ull;
+  for (int i = tid; i < n_cnt; i += blockDim.x) cnt[i] = 0u;  // split-K arrival counters
   if (coor_xy) {  // caller-listed pixels, in the caller's order
     for (int k = tid; k < n_listed; k += blockDim.x) {
       const int x = clampi(__float2int_rn(coor_xy[2 * k]), 0, ext);
@@ -588,7 +609,9 @@ __global__ void __launch_bounds__(256) tc_gen_a_kernel(
 // ROWB: bytes of one k-block row of an operand tile (128 -> 128-byte swizzle,
 // 64 -> 64-byte swizzle).  Narrower k-blocks give more pipeline stages in the
 // same shared memory, i.e. more TMA latency hidden behind the tensor pipe.
-template <int PREC, int ROWB>
+// BN: orientations per tile (256 or 128; the accumulator is double-buffered
+// in TMEM, 2 x BN columns).
+template <int PREC, int ROWB, int BN>
 struct GemmCfg {
   static constexpr bool kTf32 = (PREC == B200D2_PREC_TF32 || PREC == B200D2_PREC_TF32X3);
   static constexpr bool kScaled = (PREC == B200D2_PREC_FP16 || PREC == B200D2_PREC_FP16X3);
@@ -601,7 +624,8 @@ struct GemmCfg {
   // BF16 = 1 and F16 = 0 (kind::f16)
   static constexpr uint32_t kFmt = kTf32 ? 2u : (PREC == B200D2_PREC_BF16X3 ? 1u : 0u);
   static constexpr int kPlanes = kTerms == 3 ? 2 : 1;
-  static constexpr int kBM = 128, kBN = 256;
+  static constexpr int kBM = 128, kBN = BN;
+  static constexpr int kTmemCols = 2 * BN;  // a power of two >= 32
   static constexpr int kATile = kBM * ROWB;
   static constexpr int kBTile = kBN * ROWB;
   static constexpr int kStageBytes = kPlanes * (kATile + kBTile);
@@ -611,22 +635,26 @@ struct GemmCfg {
   static constexpr int kSmem = kStages * kStageBytes + kBarBytes + 1024;
   static_assert(kStages >= 2, "at least two pipeline stages");
   static_assert(2 * kStages * 8 + 5 * 8 + 8 <= kBarBytes, "barrier area");
+  static_assert(BN == 128 || BN == 256, "tile width");
 };
 
 struct GemmArgs {
   int Mrows, Mtiles, Ntiles, O, T, KB, accumulate;
   int group_m;  // uniform batches: 0 = m-major tile order, else groups of group_m m-tiles, n-major inside
+  int split;    // k-splits per tile (>= 1)
   float* out;
   const double* na;
   unsigned long long* keys;
   uint32_t* status;
   const float* inv_sa;  // FP16 forms: [P] 1 / particle scale
   const float* inv_sb;  // FP16 forms: [Opad] 1 / orientation scale
+  float* part;          // split > 1: [tiles * split][BN][128] FP32 partial sums
+  unsigned* cnt;        // split > 1: [tiles][4] arrivals per (tile, TMEM lane quadrant)
   Layout L;  // uneven batch tables (all null for a uniform batch)
 };
 
-// (m0, n0) of the tile-th work item: the work list of an uneven batch, or
-// the dense m-major order of a uniform one.
+// (m0, n0) of the tile-th tile: the work list of an uneven batch, or the
+// dense order of a uniform one.
 __device__ __forceinline__ void tile_origin(const GemmArgs& g, int tile, int bm, int bn, int& m0, int& n0) {
   if (g.L.tiles) {
     const int2 mn = g.L.tiles[tile];
@@ -646,6 +674,12 @@ __device__ __forceinline__ void tile_origin(const GemmArgs& g, int tile, int bm,
   }
 }
 
+// k-blocks [kb0, kb1) of split s of a tile
+__device__ __forceinline__ void split_range(const GemmArgs& g, int s, int& kb0, int& kb1) {
+  kb0 = (int)(((long long)g.KB * s) / g.split);
+  kb1 = (int)(((long long)g.KB * (s + 1)) / g.split);
+}
+
 __device__ __forceinline__ uint32_t ordered_bits(float f) {
   const uint32_t u = __float_as_uint(f);
   return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
@@ -657,13 +691,21 @@ __device__ __forceinline__ float from_ordered(uint32_t k) {
 
 constexpr uint64_t kWaitLimitNs = 4000000000ull;  // 4 s
 
-template <int PREC, int ROWB>
+// Persistent contraction.  Work items are (tile, k-split) pairs, item =
+// tile * split + s, handed out round-robin over the grid.  Warp 0 streams the
+// operand k-blocks with TMA into a ring of shared-memory stages, warp 1 issues
+// the tcgen05 MMAs into one of two TMEM accumulators, warps 2-5 (one per TMEM
+// lane quadrant) drain the other accumulator.  With split == 1 the epilogue
+// combines directly; with split > 1 each split stores its FP32 partial and the
+// last split to arrive for a (tile, quadrant) adds all partials in split order
+// (FP64) and combines, so the result does not depend on arrival order.
+template <int PREC, int ROWB, int BN>
 __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap mAhi,
                                                          const __grid_constant__ CUtensorMap mAlo,
                                                          const __grid_constant__ CUtensorMap mBhi,
                                                          const __grid_constant__ CUtensorMap mBlo,
                                                          const GemmArgs g) {
-  using C = GemmCfg<PREC, ROWB>;
+  using C = GemmCfg<PREC, ROWB, BN>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::kStages * C::kStageBytes);
@@ -698,7 +740,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     }
   }
   if (warp == 1) {
-    sm100::tmem_alloc(tmem_slot, 512);
+    sm100::tmem_alloc(tmem_slot, C::kTmemCols);
     sm100::tmem_relinquish();
   }
   sm100::tc_fence_before();
@@ -706,6 +748,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   sm100::tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   const int num_tiles = g.L.tiles ? g.L.ntiles : g.Mtiles * g.Ntiles;
+  const int num_items = num_tiles * g.split;
 
   auto raise_abort = [&]() {
     *s_abort = 1;
@@ -717,10 +760,12 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     if (lane == 0) {
       uint32_t gk = 0;
       bool ok = true;
-      for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
-        int m0, n0;
+      for (int item = blockIdx.x; item < num_items && ok; item += gridDim.x) {
+        const int tile = item / g.split;
+        int m0, n0, kb0, kb1;
         tile_origin(g, tile, C::kBM, C::kBN, m0, n0);
-        for (int kb = 0; kb < g.KB; ++kb, ++gk) {
+        split_range(g, item - tile * g.split, kb0, kb1);
+        for (int kb = kb0; kb < kb1; ++kb, ++gk) {
           const int s = gk % C::kStages;
           const uint32_t u = gk / C::kStages;
           if (u > 0 && !sm100::mbar_wait_bounded(&empty[s], (u - 1) & 1, s_abort, kWaitLimitNs)) {
@@ -749,7 +794,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       uint32_t gk = 0;
       int i = 0;
       bool ok = true;
-      for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x, ++i) {
+      for (int item = blockIdx.x; item < num_items && ok; item += gridDim.x, ++i) {
         const int b = i & 1;
         const uint32_t v = (uint32_t)(i >> 1);
         if (v > 0 && !sm100::mbar_wait_bounded(&acce[b], (v - 1) & 1, s_abort, kWaitLimitNs)) {
@@ -758,7 +803,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         }
         sm100::tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(b * C::kBN);
-        for (int kb = 0; kb < g.KB; ++kb, ++gk) {
+        int kb0, kb1;
+        split_range(g, item - (item / g.split) * g.split, kb0, kb1);
+        for (int kb = kb0; kb < kb1; ++kb, ++gk) {
           const int s = gk % C::kStages;
           const uint32_t u = gk / C::kStages;
           if (!sm100::mbar_wait_bounded(&full[s], u & 1, s_abort, kWaitLimitNs)) {
@@ -775,7 +822,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
             const uint32_t koff = (uint32_t)(ks * C::kKStep * C::kElem);
             const uint64_t dah = sm100::desc_k_sw(a_hi + koff, C::kRowB);
             const uint64_t dbh = sm100::desc_k_sw(b_hi + koff, C::kRowB);
-            const uint32_t acc = (kb > 0 || ks > 0) ? 1u : 0u;
+            const uint32_t acc = (kb > kb0 || ks > 0) ? 1u : 0u;
             sm100::mma<C::kTf32>(d, dah, dbh, C::kIdesc, acc);
             if (C::kTerms == 3) {
               sm100::mma<C::kTf32>(d, dah, sm100::desc_k_sw(b_lo + koff, C::kRowB), C::kIdesc, 1u);
@@ -795,7 +842,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     const int qd = warp & 3;  // TMEM lane quadrant this warp may access
     const int row = qd * 32 + lane;
     int i = 0;
-    for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x, ++i) {
+    for (int item = blockIdx.x; item < num_items; item += gridDim.x, ++i) {
       const int b = i & 1;
       const uint32_t v = (uint32_t)(i >> 1);
       int ok = 1;
@@ -806,6 +853,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         break;
       }
       sm100::tc_fence_after();
+      const int tile = item / g.split;
       int m0, n0;
       tile_origin(g, tile, C::kBM, C::kBN, m0, n0);
       const int m = m0 + row;
@@ -829,61 +877,97 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         }
       }
       const double* __restrict__ na_row = g.na + (size_t)p * g.O;
+      float* __restrict__ out_row = outp + t;
       // FP16 forms: -2 / (particle scale); the orientation scale is per column
       const double m2s = C::kScaled ? -2.0 * (double)g.inv_sa[vrow ? p : 0] : -2.0;
-      float* __restrict__ out_row = outp + t;
       float best = __int_as_float(0x7f800000);
       uint32_t best_idx = 0xffffffffu;
+      // FP64 combine of one accumulator value, store and running minimum
+      auto consume = [&](int o, double cr) {
+        const int lo = (o < g.O) ? (inv ? inv[o] : o) : -1;
+        if (lo < 0) return;
+        if (C::kScaled) cr *= (double)g.inv_sb[o];
+        const double dd = fma(m2s, cr, na_row[o]);
+        float f = (float)dd;
+        float* dst = out_row + (size_t)lo * Tp;
+        if (g.accumulate) f += *dst;
+        *dst = f;
+        if (f < best) {
+          best = f;
+          best_idx = (uint32_t)(lo * Tp + t);
+        }
+      };
+      bool mine = true;  // this warp's rows are combined by this item
+      if (g.split == 1) {
 #pragma unroll 1
-      for (int c = 0; c < C::kBN / 32; ++c) {
-        uint32_t r[32];
-        __syncwarp();
-        sm100::tmem_ld_32x32b_x32(tmem + (uint32_t)(b * C::kBN + c * 32) + ((uint32_t)(qd * 32) << 16), r);
-        sm100::tmem_ld_wait();
-        const int oc = n0 + c * 32;
-        if (vrow) {
+        for (int c = 0; c < C::kBN / 32; ++c) {
+          uint32_t r[32];
+          __syncwarp();
+          sm100::tmem_ld_32x32b_x32(tmem + (uint32_t)(b * C::kBN + c * 32) + ((uint32_t)(qd * 32) << 16), r);
+          sm100::tmem_ld_wait();
+          if (vrow)
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int o = oc + j;
-            const int lo = (o < g.O) ? (inv ? inv[o] : o) : -1;
-            if (lo >= 0) {
-              double cr = (double)__uint_as_float(r[j]);
-              if (C::kScaled) cr *= (double)g.inv_sb[o];
-              const double dd = fma(m2s, cr, na_row[o]);
-              float f = (float)dd;
-              float* dst = out_row + (size_t)lo * Tp;
-              if (g.accumulate) f += *dst;
-              *dst = f;
-              if (f < best) {
-                best = f;
-                best_idx = (uint32_t)(lo * Tp + t);
-              }
+            for (int j = 0; j < 32; ++j) consume(n0 + c * 32 + j, (double)__uint_as_float(r[j]));
+        }
+        sm100::tc_fence_before();
+        sm100::mbar_arrive(&acce[b]);
+      } else {
+        // store this split's partial: [item][column][row], coalesced over rows
+        float* part = g.part + (size_t)item * C::kBN * 128 + row;
+#pragma unroll 1
+        for (int c = 0; c < C::kBN / 32; ++c) {
+          uint32_t r[32];
+          __syncwarp();
+          sm100::tmem_ld_32x32b_x32(tmem + (uint32_t)(b * C::kBN + c * 32) + ((uint32_t)(qd * 32) << 16), r);
+          sm100::tmem_ld_wait();
+#pragma unroll
+          for (int j = 0; j < 32; ++j) part[(size_t)(c * 32 + j) * 128] = __uint_as_float(r[j]);
+        }
+        sm100::tc_fence_before();
+        sm100::mbar_arrive(&acce[b]);
+        __threadfence();
+        __syncwarp();
+        unsigned last = 0;
+        if (lane == 0) last = atomicAdd(&g.cnt[tile * 4 + qd], 1u) == (unsigned)(g.split - 1) ? 1u : 0u;
+        last = __shfl_sync(0xffffffffu, last, 0);
+        mine = last != 0;
+        if (mine) {
+          __threadfence();
+          const float* base = g.part + (size_t)tile * g.split * C::kBN * 128 + row;
+          if (vrow) {
+#pragma unroll 1
+            for (int col = 0; col < C::kBN; ++col) {
+              double acc = 0.0;
+              for (int s2 = 0; s2 < g.split; ++s2) acc += (double)__ldcg(base + ((size_t)s2 * C::kBN + col) * 128);
+              consume(n0 + col, acc);
             }
           }
+          __syncwarp();
+          if (lane == 0) g.cnt[tile * 4 + qd] = 0;  // ready for the next launch
         }
       }
-      sm100::tc_fence_before();
-      sm100::mbar_arrive(&acce[b]);
-      // Per-particle minimum across the warp's 32 rows: a particle's rows are
-      // contiguous, so a segmented shuffle-down min leaves each run's minimum
-      // in its first lane, which alone issues the atomic.
-      unsigned long long key =
-          (vrow && best_idx != 0xffffffffu) ? (((unsigned long long)ordered_bits(best) << 32) | best_idx) : ~0ull;
-      const int pk = vrow ? p : -1;
+      if (mine) {
+        // Per-particle minimum across the warp's 32 rows: a particle's rows
+        // are contiguous, so a segmented shuffle-down min leaves each run's
+        // minimum in its first lane, which alone issues the atomic.
+        unsigned long long key =
+            (vrow && best_idx != 0xffffffffu) ? (((unsigned long long)ordered_bits(best) << 32) | best_idx) : ~0ull;
+        const int pk = vrow ? p : -1;
 #pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const unsigned long long ok2 = __shfl_down_sync(0xffffffffu, key, off);
-        const int op = __shfl_down_sync(0xffffffffu, pk, off);
-        if (lane + off < 32 && op == pk && ok2 < key) key = ok2;
+        for (int off = 1; off < 32; off <<= 1) {
+          const unsigned long long ok2 = __shfl_down_sync(0xffffffffu, key, off);
+          const int op = __shfl_down_sync(0xffffffffu, pk, off);
+          if (lane + off < 32 && op == pk && ok2 < key) key = ok2;
+        }
+        const int prevp = __shfl_up_sync(0xffffffffu, pk, 1);
+        if (pk >= 0 && (lane == 0 || prevp != pk) && key != ~0ull) atomicMin(&g.keys[pk], key);
       }
-      const int prevp = __shfl_up_sync(0xffffffffu, pk, 1);
-      if (pk >= 0 && (lane == 0 || prevp != pk) && key != ~0ull) atomicMin(&g.keys[pk], key);
     }
   }
   __syncthreads();
   if (warp == 1) {
     sm100::tc_fence_after();
-    sm100::tmem_dealloc(tmem, 512);
+    sm100::tmem_dealloc(tmem, C::kTmemCols);
   }
 }
 
@@ -944,10 +1028,32 @@ static int gemm_row_bytes() {
   return rb;
 }
 
-template <int PREC, int ROWB>
-static int launch_gemm_rb(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s,
-                          const UnevenTabs* U) {
-  using C = GemmCfg<PREC, ROWB>;
+// Contraction variant: k-block row width, tile width and k-splits per tile.
+struct GemmVariant {
+  int row_bytes = 0;  // 64 or 128; 0 = library default
+  int bn = 0;         // orientations per tile: 256 or 128; 0 = library default (256)
+  int split = 0;      // k-splits per tile; 0 = chosen from the tile count
+};
+
+// Process-wide variant of the batch entry points (b200d2_set_gemm_variant);
+// plans carry their own.
+static std::atomic<int> g_var_rb{0}, g_var_bn{0}, g_var_split{0};
+
+// k-splits for `tiles` tiles of KB k-blocks: 1 when the tiles fill the GPU,
+// else the largest power of two (<= cap) keeping two work items per SM at
+// most and at least two k-blocks per split.
+static int auto_split(int tiles, int KB, int cap) {
+  const int sms = num_sms();
+  int sp = 1;
+  if (tiles >= sms) return 1;
+  while (sp * 2 <= cap && (long long)tiles * sp * 2 <= 2LL * sms && KB / (sp * 2) >= 2) sp *= 2;
+  return sp;
+}
+
+template <int PREC, int ROWB, int BN>
+static int launch_gemm_v(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s,
+                         const UnevenTabs* U, int split) {
+  using C = GemmCfg<PREC, ROWB, BN>;
   void* bhi = ws_at<void>(ws, g.off_bhi);
   void* blo = ws_at<void>(ws, g.off_blo);
   void* ahi = ws_at<void>(ws, g.off_ahi);
@@ -958,6 +1064,7 @@ static int launch_gemm_rb(const b200d2_batch& b, const TcGeom& g, void* ws, cuda
   if (st == B200D2_OK) st = make_map(&mBhi, bhi, g.elem, g.Kpad, g.Opad, C::kBN, ROWB, C::kScaled);
   if (st == B200D2_OK) st = make_map(&mBlo, blo, g.elem, g.Kpad, g.Opad, C::kBN, ROWB, C::kScaled);
   if (st != B200D2_OK) return st;
+  const int wl = BN == 256 ? 0 : 1;  // work list of this tile width
   GemmArgs a;
   a.Mrows = g.Mrows;
   a.Mtiles = g.Mpad / C::kBM;
@@ -977,37 +1084,55 @@ static int launch_gemm_rb(const b200d2_batch& b, const TcGeom& g, void* ws, cuda
     if (b_bytes > 64.0 * 1024 * 1024 && a.Mtiles > 1)
       a.group_m = std::max(1, std::min(a.Mtiles, (int)(l2_budget / a_tile)));
   }
+  const int tiles = U ? U->ntiles[wl] : a.Mtiles * a.Ntiles;
+  if (tiles == 0) return B200D2_OK;
+  a.split = split > 0 ? std::min(split, g.split_max) : auto_split(tiles, a.KB, g.split_max);
+  a.split = std::max(1, std::min(a.split, a.KB));
   a.out = b.d_diff2;
   a.na = ws_at<double>(ws, g.off_na);
   a.keys = ws_at<unsigned long long>(ws, g.off_keys);
   a.status = ws_at<uint32_t>(ws, g.off_status);
   a.inv_sa = ws_at<float>(ws, g.off_sa);
   a.inv_sb = ws_at<float>(ws, g.off_sb);
-  a.L = Layout{U ? U->parts : nullptr, U ? U->rows : nullptr, U ? U->tiles : nullptr, U ? U->ntiles : 0};
-  static bool attr_set = false;
-  if (!attr_set) {
-    B200D2_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<PREC, ROWB>,
+  a.part = ws_at<float>(ws, g.off_part);
+  a.cnt = ws_at<unsigned>(ws, g.off_cnt);
+  a.L = Layout{U ? U->parts : nullptr, U ? U->rows : nullptr, U ? U->tiles[wl] : nullptr, U ? U->ntiles[wl] : 0};
+  // the shared-memory opt-in is a per-device function attribute
+  static std::atomic<unsigned long long> attr_dev{0};
+  int dev = 0;
+  B200D2_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(attr_dev.load() & bit)) {
+    B200D2_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<PREC, ROWB, BN>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, C::kSmem));
-    attr_set = true;
+    attr_dev.fetch_or(bit);
   }
-  const int tiles = U ? U->ntiles : a.Mtiles * a.Ntiles;
-  if (tiles == 0) return B200D2_OK;
-  const int grid = std::max(1, std::min(tiles, num_sms()));
-  tc_gemm_kernel<PREC, ROWB><<<grid, 192, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
+  const long long items = (long long)tiles * a.split;
+  const int grid = (int)std::max(1LL, std::min(items, (long long)num_sms()));
+  tc_gemm_kernel<PREC, ROWB, BN><<<grid, 192, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
   count_launch();
   return status_from_cuda(cudaGetLastError());
 }
 
 template <int PREC>
-static int launch_gemm(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s, int row_bytes,
+static int launch_gemm(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s, GemmVariant var,
                        const UnevenTabs* U) {
-  return row_bytes == 128 ? launch_gemm_rb<PREC, 128>(b, g, ws, s, U)
-                          : launch_gemm_rb<PREC, 64>(b, g, ws, s, U);
+  if (!U) {  // batch entry points: the process-wide setting fills unset fields
+    if (var.row_bytes <= 0) var.row_bytes = g_var_rb.load();
+    if (var.bn <= 0) var.bn = g_var_bn.load();
+    if (var.split <= 0) var.split = g_var_split.load();
+  }
+  const int rb = var.row_bytes > 0 ? var.row_bytes : gemm_row_bytes();
+  if (var.bn == 128)
+    return rb == 128 ? launch_gemm_v<PREC, 128, 128>(b, g, ws, s, U, var.split)
+                     : launch_gemm_v<PREC, 64, 128>(b, g, ws, s, U, var.split);
+  return rb == 128 ? launch_gemm_v<PREC, 128, 256>(b, g, ws, s, U, var.split)
+                   : launch_gemm_v<PREC, 64, 256>(b, g, ws, s, U, var.split);
 }
 
 template <int PREC>
 static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeom& g, void* ws, int stage,
-                        cudaStream_t s, const UnevenTabs* U, int row_bytes) {
+                        cudaStream_t s, const UnevenTabs* U, GemmVariant var) {
   const PartDev* parts = U ? U->parts : nullptr;
   uint32_t* status = ws_at<uint32_t>(ws, g.off_status);
   int2* xy = ws_at<int2>(ws, g.off_xy);
@@ -1029,7 +1154,7 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
   switch (stage) {
     case 0:
       tc_pixel_list_kernel<<<1, 1024, 0, s>>>(v, g.N_img, xy, idx, status, keys, g.P, b.d_coor_xy,
-                                              g.K_c, g.maxR);
+                                              g.K_c, g.maxR, ws_at<unsigned>(ws, g.off_cnt), g.n_cnt);
       break;
     case 1: {
       const int n = g.T * (g.exw + g.eyw);
@@ -1077,7 +1202,7 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       break;
     }
     case 6:
-      return launch_gemm<PREC>(b, g, ws, s, row_bytes > 0 ? row_bytes : gemm_row_bytes(), U);
+      return launch_gemm<PREC>(b, g, ws, s, var, U);
     case 7:
       tc_finalize_kernel<<<(g.P + 127) / 128, 128, 0, s>>>(keys, g.P, b.d_min, b.d_argmin);
       break;
@@ -1089,21 +1214,22 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
 }
 
 static int dispatch_stage(const b200d2_view& v, const b200d2_batch& b, int prec, const TcGeom& g, void* ws,
-                          int stage, cudaStream_t s, const UnevenTabs* U = nullptr, int row_bytes = 0) {
+                          int stage, cudaStream_t s, const UnevenTabs* U = nullptr,
+                          GemmVariant var = GemmVariant()) {
   switch (prec) {
-    case B200D2_PREC_BF16X3: return launch_stage<B200D2_PREC_BF16X3>(v, b, g, ws, stage, s, U, row_bytes);
-    case B200D2_PREC_TF32X3: return launch_stage<B200D2_PREC_TF32X3>(v, b, g, ws, stage, s, U, row_bytes);
-    case B200D2_PREC_TF32: return launch_stage<B200D2_PREC_TF32>(v, b, g, ws, stage, s, U, row_bytes);
-    case B200D2_PREC_FP16X3: return launch_stage<B200D2_PREC_FP16X3>(v, b, g, ws, stage, s, U, row_bytes);
-    case B200D2_PREC_FP16: return launch_stage<B200D2_PREC_FP16>(v, b, g, ws, stage, s, U, row_bytes);
+    case B200D2_PREC_BF16X3: return launch_stage<B200D2_PREC_BF16X3>(v, b, g, ws, stage, s, U, var);
+    case B200D2_PREC_TF32X3: return launch_stage<B200D2_PREC_TF32X3>(v, b, g, ws, stage, s, U, var);
+    case B200D2_PREC_TF32: return launch_stage<B200D2_PREC_TF32>(v, b, g, ws, stage, s, U, var);
+    case B200D2_PREC_FP16X3: return launch_stage<B200D2_PREC_FP16X3>(v, b, g, ws, stage, s, U, var);
+    case B200D2_PREC_FP16: return launch_stage<B200D2_PREC_FP16>(v, b, g, ws, stage, s, U, var);
     default: return B200D2_ERR_UNSUPPORTED;
   }
 }
 
 static constexpr int kNumStages = 8;
 
-size_t tc_workspace_bytes(const b200d2_view& v, const b200d2_batch& b, int precision) {
-  return make_geom(v, b, precision).total;
+size_t tc_workspace_bytes(const b200d2_view& v, const b200d2_batch& b, int precision, bool allow_split) {
+  return make_geom(v, b, precision, -1, allow_split).total;
 }
 
 const char* tc_stage_name(int precision, int stage) {
@@ -1143,10 +1269,10 @@ static int check_tc(const b200d2_view& v, const b200d2_batch& b) {
 }
 
 int tc_run_stage(const b200d2_view& v, const b200d2_batch& b, int precision, int stage, void* ws,
-                 size_t ws_bytes, cudaStream_t s) {
+                 size_t ws_bytes, cudaStream_t s, bool allow_split) {
   int st = check_tc(v, b);
   if (st != B200D2_OK) return st;
-  const TcGeom g = make_geom(v, b, precision);
+  const TcGeom g = make_geom(v, b, precision, -1, allow_split);
   if (ws_bytes < g.total) return B200D2_ERR_INVALID;
   return dispatch_stage(v, b, precision, g, ws, stage, s);
 }
@@ -1223,20 +1349,22 @@ struct TuneKey {
   }
 };
 static std::mutex g_tune_mu;
-static std::map<TuneKey, int> g_tune_cache;
+static std::map<TuneKey, GemmVariant> g_tune_cache;
 
 }  // namespace b200d2
 
 struct b200d2_plan {
   b200d2_view view;
   b200d2_batch batch;  // shared geometry (T = number of phase tables), min/argmin outputs
-  int prec = 0, flags = 0, row_bytes = 64;
+  int prec = 0, flags = 0;
+  b200d2::GemmVariant var;  // contraction variant in use
   b200d2::TcGeom g;
   b200d2::UnevenTabs U;
   void* ws = nullptr;
   b200d2::PartDev* d_parts = nullptr;
   int4* d_rows = nullptr;
-  int2* d_tiles = nullptr;
+  int2* d_tiles = nullptr;     // work list, 256-wide tiles
+  int2* d_tiles128 = nullptr;  // work list, 128-wide tiles
   float2* d_txy = nullptr;
   int* d_inv = nullptr;
   float* d_eul_perm = nullptr;
@@ -1253,28 +1381,28 @@ static void plan_free(b200d2_plan* p) {
   if (p->exec) cudaGraphExecDestroy(p->exec);
   if (p->graph) cudaGraphDestroy(p->graph);
   if (p->stream) cudaStreamDestroy(p->stream);
-  for (void* d : {(void*)p->ws, (void*)p->d_parts, (void*)p->d_rows, (void*)p->d_tiles, (void*)p->d_txy,
-                  (void*)p->d_inv, (void*)p->d_eul_perm})
+  for (void* d : {(void*)p->ws, (void*)p->d_parts, (void*)p->d_rows, (void*)p->d_tiles, (void*)p->d_tiles128,
+                  (void*)p->d_txy, (void*)p->d_inv, (void*)p->d_eul_perm})
     if (d) cudaFree(d);
   delete p;
 }
 
 // All stages in order on one stream (the form that is captured).
-static int plan_pipeline(b200d2_plan* p, cudaStream_t s, int row_bytes) {
+static int plan_pipeline(b200d2_plan* p, cudaStream_t s, GemmVariant var) {
   int st = B200D2_OK;
   for (int i = 0; i < kNumStages && st == B200D2_OK; ++i)
-    st = dispatch_stage(p->view, p->batch, p->prec, p->g, p->ws, i, s, &p->U, row_bytes);
+    st = dispatch_stage(p->view, p->batch, p->prec, p->g, p->ws, i, s, &p->U, var);
   return st;
 }
 
-static double time_gemm(b200d2_plan* p, int row_bytes, int reps) {
+static double time_gemm(b200d2_plan* p, GemmVariant var, int reps) {
   cudaEvent_t a, b;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
   double best = 1e30;
   for (int r = 0; r < reps; ++r) {
     cudaEventRecord(a, p->stream);
-    int st = dispatch_stage(p->view, p->batch, p->prec, p->g, p->ws, 6, p->stream, &p->U, row_bytes);
+    int st = dispatch_stage(p->view, p->batch, p->prec, p->g, p->ws, 6, p->stream, &p->U, var);
     cudaEventRecord(b, p->stream);
     cudaEventSynchronize(b);
     float ms = 0.f;
@@ -1386,29 +1514,32 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
     evals += (long long)d.O * d.T;
   }
   const int Mrows = (int)rows.size();
-  const int Mtiles = (Mrows + 127) / 128, Ntiles = (O_all + 255) / 256;
+  const int Mtiles = (Mrows + 127) / 128, Ntiles = (O_all + 255) / 256, Ntiles128 = (O_all + 127) / 128;
 
   // orientation -> local index maps, and the n-tiles each particle needs
   std::vector<int> inv((size_t)P * O_all, -1);
-  std::vector<std::vector<char>> need_n(P, std::vector<char>(Ntiles, 0));
+  std::vector<std::vector<char>> need_n(P, std::vector<char>(Ntiles128, 0));  // 128-wide column blocks
   for (int i = 0; i < P; ++i) {
     const b200d2_particle_desc& d = parts[i];
     for (int k = 0; k < d.O; ++k) {
       const int c = pos[d.h_orient ? d.h_orient[k] : k];
       inv[(size_t)i * O_all + c] = k;
-      need_n[i][c / 256] = 1;
+      need_n[i][c / 128] = 1;
     }
   }
-  // work list: (m tile, n tile) pairs some particle of the m tile needs, m-major
-  std::vector<int2> tiles;
+  // work lists: (m tile, n tile) pairs some particle of the m tile needs,
+  // m-major, for 256- and 128-wide tiles
+  std::vector<int2> tiles, tiles128;
   for (int mt = 0; mt < Mtiles; ++mt) {
     const int r0 = mt * 128, r1 = std::min(Mrows, r0 + 128);
-    std::vector<char> un(Ntiles, 0);
+    std::vector<char> un(Ntiles128, 0);
     for (int r = r0; r < r1; ++r)
       if (r == r0 || rows[r].x != rows[r - 1].x)
-        for (int n = 0; n < Ntiles; ++n) un[n] |= need_n[rows[r].x][n];
+        for (int n = 0; n < Ntiles128; ++n) un[n] |= need_n[rows[r].x][n];
     for (int n = 0; n < Ntiles; ++n)
-      if (un[n]) tiles.push_back(make_int2(mt, n));
+      if (un[2 * n] || (2 * n + 1 < Ntiles128 && un[2 * n + 1])) tiles.push_back(make_int2(mt, n));
+    for (int n = 0; n < Ntiles128; ++n)
+      if (un[n]) tiles128.push_back(make_int2(mt, n));
   }
 
   b200d2_batch& b = p->batch;
@@ -1448,6 +1579,7 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   st = status_from_cuda(cudaMalloc(&p->ws, p->g.total));
   upload(reinterpret_cast<void**>(&p->d_rows), rows.data(), rows.size() * sizeof(int4));
   upload(reinterpret_cast<void**>(&p->d_tiles), tiles.data(), tiles.size() * sizeof(int2));
+  upload(reinterpret_cast<void**>(&p->d_tiles128), tiles128.data(), tiles128.size() * sizeof(int2));
   upload(reinterpret_cast<void**>(&p->d_txy), txy.data(), txy.size() * sizeof(float2));
   upload(reinterpret_cast<void**>(&p->d_inv), inv.data(), inv.size() * sizeof(int));
   if (st == B200D2_OK)
@@ -1458,7 +1590,8 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
     plan_free(p);
     return st;
   }
-  p->U = UnevenTabs{p->d_parts, p->d_rows, p->d_tiles, (int)tiles.size(), p->d_txy, (int)txy.size(), Mrows};
+  p->U = UnevenTabs{p->d_parts, p->d_rows, {p->d_tiles, p->d_tiles128}, {(int)tiles.size(), (int)tiles128.size()},
+                    p->d_txy, (int)txy.size(), Mrows};
 
   memset(&p->info, 0, sizeof(p->info));
   p->info.P = P;
@@ -1468,47 +1601,77 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   p->info.tiles_dense = Mtiles * Ntiles;
   p->info.evals = evals;
   p->info.stages = kNumStages;
-  p->info.workspace_bytes = p->g.total + rows.size() * sizeof(int4) + tiles.size() * sizeof(int2) +
+  p->info.tiles_n128 = (int)tiles128.size();
+  p->info.workspace_bytes = p->g.total + rows.size() * sizeof(int4) + (tiles.size() + tiles128.size()) * sizeof(int2) +
                             txy.size() * sizeof(float2) + inv.size() * sizeof(int) + hp.size() * sizeof(PartDev);
 
   // warm run (also sets kernel attributes outside any capture)
-  p->row_bytes = gemm_row_bytes();
-  st = plan_pipeline(p, p->stream, p->row_bytes);
+  p->var = GemmVariant();
+  p->var.row_bytes = gemm_row_bytes();
+  p->var.split = 1;
+  st = plan_pipeline(p, p->stream, p->var);
   if (st == B200D2_OK) st = status_from_cuda(cudaStreamSynchronize(p->stream));
   if (st == B200D2_OK && (flags & B200D2_PLAN_AUTOTUNE)) {
+    // autotuner: time every (k-block row width, tile width, k-split) variant
+    // on this plan's own work lists and keep the fastest; results are cached
+    // per problem signature for later plans
     const TuneKey key{precision, p->g.Kpad, O_all, Mtiles, (int)tiles.size()};
-    int cached = 0;
+    bool cached = false;
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
       auto it = g_tune_cache.find(key);
-      if (it != g_tune_cache.end()) cached = it->second;
+      if (it != g_tune_cache.end()) {
+        p->var = it->second;
+        cached = true;
+      }
     }
-    if (cached) {
-      p->row_bytes = cached;
-    } else {
-      const int cand[2] = {64, 128};
+    if (!cached) {
+      std::vector<GemmVariant> cand;
+      const int sms = num_sms();
+      for (int rb : {64, 128})
+        for (int bn : {256, 128}) {
+          const int nt = bn == 256 ? (int)tiles.size() : (int)tiles128.size();
+          for (int sp = 1; sp <= p->g.split_max; sp *= 2) {
+            if (sp > 1 && (long long)nt * sp > 2LL * sms) break;  // splits only while the GPU is not full
+            GemmVariant v;
+            v.row_bytes = rb;
+            v.bn = bn;
+            v.split = sp;
+            cand.push_back(v);
+          }
+        }
       double best = 1e30;
-      for (int c = 0; c < 2; ++c) {
-        time_gemm(p, cand[c], 1);  // first launch of a variant sets its attributes
-        const double ms = time_gemm(p, cand[c], 3);
-        p->info.tuned_ms[c] = ms;
+      int n = 0;
+      for (const GemmVariant& v : cand) {
+        time_gemm(p, v, 1);  // first launch of a variant sets its attributes
+        const double ms = time_gemm(p, v, 3);
+        if (n < B200D2_PLAN_MAX_VARIANTS) {
+          p->info.tuned_variant[n][0] = v.row_bytes;
+          p->info.tuned_variant[n][1] = v.bn;
+          p->info.tuned_variant[n][2] = v.split;
+          p->info.tuned_ms[n] = ms;
+          ++n;
+        }
         if (ms < best) {
           best = ms;
-          p->row_bytes = cand[c];
+          p->var = v;
         }
       }
+      p->info.n_tuned = n;
       std::lock_guard<std::mutex> lk(g_tune_mu);
-      g_tune_cache[key] = p->row_bytes;
+      g_tune_cache[key] = p->var;
     }
     // leave the outputs as one full run with the chosen variant produces them
-    st = plan_pipeline(p, p->stream, p->row_bytes);
+    st = plan_pipeline(p, p->stream, p->var);
     if (st == B200D2_OK) st = status_from_cuda(cudaStreamSynchronize(p->stream));
   }
-  p->info.row_bytes = p->row_bytes;
+  p->info.row_bytes = p->var.row_bytes;
+  p->info.tile_n = p->var.bn;
+  p->info.split = p->var.split;
   if (st == B200D2_OK && (flags & B200D2_PLAN_GRAPH)) {
     st = status_from_cuda(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
     if (st == B200D2_OK) {
-      const int st2 = plan_pipeline(p, p->stream, p->row_bytes);
+      const int st2 = plan_pipeline(p, p->stream, p->var);
       const cudaError_t e = cudaStreamEndCapture(p->stream, &p->graph);
       st = st2 != B200D2_OK ? st2 : status_from_cuda(e);
     }
@@ -1531,7 +1694,7 @@ extern "C" int b200d2_plan_run(b200d2_plan* p, void* stream) {
     b200d2::count_launch(b200d2::kNumStages);
     return B200D2_OK;
   }
-  return b200d2::plan_pipeline(p, s, p->row_bytes);
+  return b200d2::plan_pipeline(p, s, p->var);
 }
 
 extern "C" int b200d2_plan_get_info(const b200d2_plan* p, b200d2_plan_info* info) {
@@ -1554,5 +1717,15 @@ extern "C" int b200d2_workspace_status(const void* d_workspace, void* stream, in
   B200D2_CUDA_TRY(cudaMemcpyAsync(&v, d_workspace, sizeof(v), cudaMemcpyDeviceToHost, s));
   B200D2_CUDA_TRY(cudaStreamSynchronize(s));
   *status = (int)v;
+  return B200D2_OK;
+}
+
+extern "C" int b200d2_set_gemm_variant(int row_bytes, int tile_n, int split) {
+  if ((row_bytes != 0 && row_bytes != 64 && row_bytes != 128) || (tile_n != 0 && tile_n != 128 && tile_n != 256) ||
+      split < 0 || split > 64)
+    return B200D2_ERR_INVALID;
+  b200d2::g_var_rb.store(row_bytes);
+  b200d2::g_var_bn.store(tile_n);
+  b200d2::g_var_split.store(split);
   return B200D2_OK;
 }

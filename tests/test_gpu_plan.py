@@ -51,6 +51,14 @@ def test_uneven_plan_matches_fp64(pkg, synth, oracle, cuda, reorder):
     info = plan.info()
     print(info)
     assert info["graph"] == 1 and info["row_bytes"] in (64, 128)
+    assert info["tile_n"] in (128, 256) and info["split"] >= 1
+    # the autotuner timed every variant and kept the fastest (a plan with the
+    # same problem signature as an earlier one reuses its choice untimed)
+    if info["n_tuned"]:
+        assert info["n_tuned"] >= 4
+        best = min(info["tuned"], key=lambda x: x[1])[0]
+        assert best == (info["row_bytes"], info["tile_n"], info["split"])
+    assert 0 < info["tiles_n128"] <= 2 * info["tiles"]
     assert info["evals"] == sum(len(p["orient"]) * len(p["trans_x"]) for p in parts)
     assert 0 < info["tiles"] <= info["tiles_dense"]
     for rep in range(2):  # the graph replays on the same buffers

@@ -141,3 +141,26 @@ def test_tc_deterministic(pkg, cuda, tiny):
     b = run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3)
     np.testing.assert_array_equal(a[0], b[0])
     np.testing.assert_array_equal(a[2], b[2])
+
+
+@pytest.mark.parametrize("rb,tn,split", [(64, 256, 1), (64, 256, 2), (64, 256, 4), (128, 256, 2),
+                                         (64, 128, 1), (64, 128, 4), (128, 128, 1)])
+def test_tc_gemm_variants(pkg, oracle, cuda, c1, rb, tn, split):
+    """Every contraction variant (k-block row width, tile width, k-splits with
+    FP64 addition of the partials) meets the same tolerance, and a split
+    run is reproducible bit for bit."""
+    pr, view, dp, ref = c1
+    pkg.set_gemm_variant(rb, tn, split)
+    try:
+        got, mn, am = run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3)
+        again, _, _ = run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3)
+    finally:
+        pkg.set_gemm_variant(0, 0, 0)
+    np.testing.assert_array_equal(got, again)
+    s = oracle.error_stats(got, ref)
+    assert s["max_rel"] <= TOL["bf16x3"], s
+    for p in range(pr.P):
+        assert am[p] == int(np.argmin(got[p].ravel()))
+        ok, gap = argmin_consistent(got[p], ref[p], TOL["bf16x3"])
+        assert ok, (p, gap)
+
