@@ -1608,6 +1608,7 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   // warm run (also sets kernel attributes outside any capture)
   p->var = GemmVariant();
   p->var.row_bytes = gemm_row_bytes();
+  p->var.bn = 256;
   p->var.split = 1;
   st = plan_pipeline(p, p->stream, p->var);
   if (st == B200D2_OK) st = status_from_cuda(cudaStreamSynchronize(p->stream));

@@ -85,12 +85,12 @@ def test_serving_admission_by_budget(pkg, synth, cuda):
     prob = synth.make_problem("c1", P=4)
     proj = pkg.Projector(prob.projector, use_texture=1)
     view = proj.view(prob.imgX, prob.imgY, prob.imgMaxR)
-    budget = 2 << 20  # 2 MiB: one small request (~1.5 MB with its workspace) at a time
+    budget = 4 << 20  # 4 MiB: one small request (~2.5 MiB with its workspace) at a time
     srv = pkg.Server(slots=2, hbm_budget=budget, precision=pkg.PREC_TF32)
     ref = srv.add_reference(view, prob.eulers, prob.N_img)
     tx = np.zeros(1, np.float32)
     big = np.arange(prob.O, dtype=np.int32)
-    with pytest.raises(pkg.B200D2Error) as e:  # 4 particles x 576 orientations x 21 t: ~5.5 MB
+    with pytest.raises(pkg.B200D2Error) as e:  # 4 particles x 576 orientations x 21 t: ~8 MiB
         srv.submit(ref, prob.fimg_re, prob.fimg_im, prob.corr, big,
                    np.zeros(21, np.float32), np.zeros(21, np.float32))
     assert e.value.code == 7
