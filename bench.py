@@ -256,6 +256,8 @@ def ours_arm(args):
     torch.cuda.set_device(local)
     pkg = load_package()
     synth = load_synth()
+    import importlib
+    replicas = importlib.import_module("relion_b200.replicas")
     pr = synth.make_problem(args.config, seed=20251203 + rank, P=args.particles)
     prec = PREC[args.precision]
     dev = torch.device("cuda", local)
@@ -344,13 +346,10 @@ def ours_arm(args):
         dist.barrier()
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
     evals_step = evals_plan if uneven else P * O * T
-    value = world * evals_step * args.steps / (total_ms / 1e3)
+    # whole job: every rank's evaluations over the slowest rank's device time
+    value = replicas.job_rate(evals_step * args.steps, sum(step_ms), dist, dev)
+    total_ms = replicas.slowest(sum(step_ms), dist, dev)
 
     # ---- dominant kernel timing (events on the launching stream) ----
     if uneven:
@@ -384,12 +383,7 @@ def ours_arm(args):
         h_am.copy_(am, non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_val = world * evals_step * e2e_steps / (e2e_ms / 1e3)
+    e2e_val = replicas.job_rate(evals_step * e2e_steps, e0.elapsed_time(e1), dist, dev)
     h2d = 3 * P * N * 4
     d2h = P * (8 + 8)
 

@@ -335,6 +335,31 @@ int b200d2_diff2_coarse_batch_static(const b200d2_view* view,
 int b200d2_minloc(const float* d_diff2, long long n, int P, double* d_min,
                   long long* d_argmin, void* stream);
 
+/* Batched multi-particle CTF folding (no counterpart in the reference, which
+ * receives folded inputs from RELION): for P raw particle transforms X
+ * (d_real/d_imag + p * img_stride, N_img half-plane pixels in
+ * pixel_index2coor order) and each particle's CTF d_ctf[p] (device array),
+ *   Fimg = X / CTF  (X where |CTF| <= 1e-8),   corr = Minvsigma2 * CTF^2
+ * into d_fimg_real/d_fimg_imag/d_corr (same layout), the inputs of the coarse
+ * pass.  CTF = -(sqrt(1-Q^2) sin(chi) + Q cos(chi)) * scale * exp(-B k^2/4),
+ * chi = pi lambda dz k^2 - pi/2 Cs lambda^3 k^4 + phase_shift, dz the
+ * astigmatic defocus at the pixel's azimuth, k = (x, y) / (ori_size *
+ * pixel_A), all in FP64.  d_minvsigma2 is one row per particle
+ * (minvsigma2_stride = N_img or more) or one row shared by all (stride 0).
+ * maxR is the image radius used by pixel_index2coor. */
+typedef struct b200d2_ctf {
+  float defocus_u_A, defocus_v_A, defocus_angle_deg; /* astigmatic defocus (A) */
+  float voltage_kV, cs_mm, amp_contrast, phase_shift_deg;
+  float bfactor; /* envelope exp(-B k^2 / 4); 0 = none */
+  float scale;   /* 0 is taken as 1 */
+} b200d2_ctf;
+int b200d2_ctf_fold(const float* d_real, const float* d_imag, long long img_stride,
+                    int P, int N_img, int imgX, int imgY, int maxR, int ori_size,
+                    float pixel_A, const b200d2_ctf* d_ctf,
+                    const float* d_minvsigma2, long long minvsigma2_stride,
+                    float* d_fimg_real, float* d_fimg_imag, float* d_corr,
+                    void* stream);
+
 /* Coarse weights of a scored batch, the step after the coarse pass (its
  * RELION driver kernel_weights_exponent_coarse is a commented stub at
  * src/utilities.h:405-443 of the reference harness):

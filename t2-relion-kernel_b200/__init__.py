@@ -70,6 +70,13 @@ class ParticleDesc(C.Structure):
                 ("T", C.c_int)]
 
 
+class CTF(C.Structure):
+    """b200d2_ctf: one particle's CTF parameters."""
+
+    _fields_ = [(n, C.c_float) for n in ("defocus_u_A", "defocus_v_A", "defocus_angle_deg", "voltage_kV", "cs_mm",
+                                         "amp_contrast", "phase_shift_deg", "bfactor", "scale")]
+
+
 PLAN_MAX_VARIANTS = 16
 
 
@@ -146,6 +153,7 @@ def _declare(L):
         "b200d2_server_destroy": [P],
         "b200d2_coarse_weights": [P, I, I, I, P, P, P, I, P, P, P, Z, P],
         "b200d2_set_gemm_variant": [I, I, I],
+        "b200d2_ctf_fold": [P, P, C.c_longlong, I, I, I, I, I, I, F, P, P, C.c_longlong, P, P, P, P],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -463,6 +471,33 @@ def coarse_weights(diff2, P: int, O: int, T: int, out_min=None, pdf_orient=None,
                                        1 if normalize else 0, _ptr(weights), _ptr(sums), _ptr(workspace), nb,
                                        _stream(stream)), "coarse_weights")
     return weights, sums
+
+
+def ctf_fold(real, imag, ctf_params: list, minvsigma2, *, imgX: int, imgY: int, maxR: int, ori_size: int,
+             pixel_A: float, out_real=None, out_imag=None, out_corr=None, stream=None):
+    """Fold each particle's CTF into its image and weights on the device
+    (b200d2_ctf_fold).  real/imag: CUDA float32 [P, N_img]; ctf_params: P
+    dicts of CTF fields; minvsigma2: CUDA float32 [N_img] (shared) or
+    [P, N_img].  Returns (Fimg_real, Fimg_imag, corr)."""
+    import torch
+    P, N = int(real.shape[0]), int(real.shape[1])
+    arr = (CTF * max(P, 1))()
+    for i, c in enumerate(ctf_params):
+        for k, v in c.items():
+            setattr(arr[i], k, float(v))
+    d_ctf = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8).to(real.device)
+    out_real = torch.empty_like(real) if out_real is None else out_real
+    out_imag = torch.empty_like(imag) if out_imag is None else out_imag
+    out_corr = torch.empty_like(real) if out_corr is None else out_corr
+    ms = 0 if minvsigma2.dim() == 1 else int(minvsigma2.stride(0))
+    _check(lib().b200d2_ctf_fold(_ptr(real), _ptr(imag), int(real.stride(0)), P, N, imgX, imgY, maxR, ori_size,
+                                 pixel_A, _ptr(d_ctf), _ptr(minvsigma2), ms, _ptr(out_real), _ptr(out_imag),
+                                 _ptr(out_corr), _stream(stream)), "ctf_fold")
+    if stream is None:
+        torch.cuda.current_stream().synchronize()  # d_ctf is a temporary
+    else:
+        stream.synchronize()
+    return out_real, out_imag, out_corr
 
 
 def set_gemm_variant(row_bytes: int = 0, tile_n: int = 0, split: int = 0) -> None:

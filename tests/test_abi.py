@@ -41,6 +41,12 @@ def test_host_side_argument_validation(pkg):
     assert lib.b200d2_coarse_weights(None, 0, 10, 10, None, None, None, 1, None, None, None, 0, None) == 0
     assert lib.b200d2_coarse_weights(None, 2, 10, 10, None, None, None, 1, None, None, None, 0, None) == 1
     assert lib.b200d2_coarse_weights(None, -1, 10, 10, None, None, None, 1, None, None, None, 0, None) == 1
+    assert lib.b200d2_ctf_fold(None, None, 10, 0, 10, 6, 10, 5, 10, 1.5, None, None, 0, None, None, None,
+                               None) == 0
+    assert lib.b200d2_ctf_fold(None, None, 10, 2, 10, 6, 10, 5, 10, 1.5, None, None, 0, None, None, None,
+                               None) == 1
+    assert lib.b200d2_set_gemm_variant(96, 0, 0) == 1 and lib.b200d2_set_gemm_variant(0, 192, 0) == 1
+    assert lib.b200d2_set_gemm_variant(0, 0, 0) == 0
     assert lib.b200d2_coarse_weights_workspace(0, 100) == 0
     assert lib.b200d2_coarse_weights_workspace(3, 70000) >= 3 * 8 + 3 * 3 * 8 + 3 * 4
 
