@@ -12,6 +12,7 @@ pytestmark = pytest.mark.gpu
 
 
 def ctf_ref(x, y, ori_size, pixel_A, c):
+    c = {k: float(np.float32(v)) for k, v in c.items()}  # the device receives FP32 parameters
     volt = c["voltage_kV"] * 1e3
     lam = 12.2643247 / math.sqrt(volt * (1.0 + volt * 0.978466e-6))
     kx = x.astype(np.float64) / (ori_size * pixel_A)
