@@ -49,6 +49,7 @@ namespace b200d2 {
 struct TcGeom {
   int P, O, T, N_img, K_c, Kpad, Mrows, Mpad, Opad, maxR, exw, eyw;
   int elem, BK, terms;
+  int Kq;  // row stride (doubles) of |B|^2 and of the compacted weights: Kpad / 2, zero padded
   size_t off_status, off_xy, off_idx, off_ex, off_ey, off_bhi, off_blo, off_q, off_w, off_normx, off_na,
       off_ahi, off_alo, off_keys, off_sa, off_sb, off_part, off_cnt, total;
   int split_max;  // largest k-split the workspace holds partial sums for
@@ -119,8 +120,9 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, i
   g.off_ey = take(sizeof(float2) * (size_t)g.T * g.eyw);
   g.off_bhi = take((size_t)g.Opad * g.Kpad * g.elem);
   g.off_blo = planes == 2 ? take((size_t)g.Opad * g.Kpad * g.elem) : g.off_bhi;
-  g.off_q = take(sizeof(double) * (size_t)g.O * std::max(g.K_c, 1));
-  g.off_w = take(sizeof(double) * (size_t)g.P * std::max(g.K_c, 1));
+  g.Kq = g.Kpad / 2;  // a multiple of 16
+  g.off_q = take(sizeof(double) * (size_t)g.O * g.Kq);
+  g.off_w = take(sizeof(double) * (size_t)g.P * g.Kq);
   g.off_normx = take(sizeof(double) * (size_t)g.P);
   g.off_na = take(sizeof(double) * (size_t)g.P * g.O);
   g.off_ahi = take((size_t)g.Mpad * g.Kpad * g.elem);
@@ -299,6 +301,7 @@ __global__ void __launch_bounds__(128) tc_project_kernel(b200d2_view v, const fl
   const int o = blockIdx.y;
   if (kp >= Kpad / 2) return;
   float2 b = make_float2(0.f, 0.f);
+  if (o < O && kp >= K_c) q[(size_t)o * (Kpad / 2) + kp] = 0.0;  // zero padding of the |B|^2 row
   if (o < O && kp < K_c) {
     float e[6];
     const float* eo = eulers + (size_t)o * 9;
@@ -310,7 +313,7 @@ __global__ void __launch_bounds__(128) tc_project_kernel(b200d2_view v, const fl
     e[5] = eo[7];
     const int2 c = xy[kp];
     b = project_pixel(v, (float)c.x, (float)c.y, e);
-    q[(size_t)o * K_c + kp] = (double)b.x * (double)b.x + (double)b.y * (double)b.y;
+    q[(size_t)o * (Kpad / 2) + kp] = (double)b.x * (double)b.x + (double)b.y * (double)b.y;
   }
   store_split<PREC>(bhi, blo, (size_t)o * (Kpad / 2) + kp, b.x, b.y);
 }
@@ -364,9 +367,11 @@ __global__ void __launch_bounds__(256) tc_project_scaled_kernel(b200d2_view v, c
     for (int kp = threadIdx.x; kp < K_c; kp += blockDim.x) {
       const int2 c = xy[kp];
       const float2 b = project_pixel(v, (float)c.x, (float)c.y, e);
-      q[(size_t)o * K_c + kp] = (double)b.x * (double)b.x + (double)b.y * (double)b.y;
+      q[(size_t)o * half + kp] = (double)b.x * (double)b.x + (double)b.y * (double)b.y;
       mx = fmaxf(mx, fmaxf(fabsf(b.x), fabsf(b.y)));
     }
+  if (o < O)
+    for (int kp = K_c + threadIdx.x; kp < half; kp += blockDim.x) q[(size_t)o * half + kp] = 0.0;
   const int ex = pow2_scale_exp(block_max(mx));
   const float sc = ldexpf(1.f, ex);
   if (threadIdx.x == 0) inv_sb[o] = ldexpf(1.f, -ex);
@@ -409,13 +414,14 @@ __global__ void __launch_bounds__(256) tc_normx_kernel(const float* __restrict__
                                                        const float* __restrict__ corr,
                                                        long long stride, int N_img, double* normx,
                                                        const PartDev* __restrict__ parts,
-                                                       const int* __restrict__ idx, int K_c, double* wcomp) {
+                                                       const int* __restrict__ idx, int K_c, int Kq,
+                                                       double* wcomp) {
   const long long p = blockIdx.x;
   const float* pre = parts ? parts[p].re : re + p * stride;
   const float* pim = parts ? parts[p].im : im + p * stride;
   const float* pco = parts ? parts[p].corr : corr + p * stride;
   // the weights of the listed pixels, compacted for the normA contraction
-  for (int k = threadIdx.x; k < K_c; k += blockDim.x) wcomp[p * K_c + k] = (double)pco[idx[k]] / 2.0;
+  for (int k = threadIdx.x; k < Kq; k += blockDim.x) wcomp[p * Kq + k] = k < K_c ? (double)pco[idx[k]] / 2.0 : 0.0;
   double acc = 0.0;
   for (int i = threadIdx.x; i < N_img; i += blockDim.x) {
     const double r = pre[i], m = pim[i];
@@ -445,6 +451,11 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pre
                "r"(pred ? 8 : 0)
                : "memory");
 }
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sm100::smem_u32(smem)), "l"(gmem),
+               "r"(pred ? 16 : 0)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -463,14 +474,16 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
 // each warp WM x 4 DMMA tiles of 8 x 8; 16-pixel slabs double-buffered
 // through shared memory with cp.async.
 template <int WM>
-__global__ void __launch_bounds__(128) tc_norma_kernel(const double* __restrict__ wcomp, int K_c,
+__global__ void __launch_bounds__(128) tc_norma_kernel(const double* __restrict__ wcomp, int Kq,
                                                        const double* __restrict__ q, int O, int P,
                                                        const double* __restrict__ normx, double* na) {
-  // rows padded to 20 doubles: the fragment loads of a half-warp (rows g,
-  // columns t, g, t < 4) then fall on distinct bank pairs 8g + 2t
+  // Kq: row stride of wcomp and q, a multiple of 16, zero padded.  Shared
+  // rows padded to 20 doubles (160 B, 16-byte aligned): the fragment loads
+  // of a half-warp (rows g, columns t, g, t < 4) fall on distinct bank pairs
+  // 8g + 2t.
   constexpr int KC = 16, LD = KC + 4, CP = 16 * WM, CO = 64;
-  __shared__ double sw[2][CP][LD];
-  __shared__ double sq[2][CO][LD];
+  __shared__ __align__(16) double sw[2][CP][LD];
+  __shared__ __align__(16) double sq[2][CO][LD];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gid = lane >> 2, tig = lane & 3;
   const int wp0 = (warp >> 1) * 8 * WM, wo0 = (warp & 1) * 32;
@@ -481,19 +494,20 @@ __global__ void __launch_bounds__(128) tc_norma_kernel(const double* __restrict_
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   auto stage = [&](int buf, int k0) {
-    for (int e = tid; e < CP * KC; e += 128) {
-      const int pp = e / KC, k = e % KC;
-      const bool ok = (p0 + pp < P) && (k0 + k < K_c);
-      cp_async8(&sw[buf][pp][k], ok ? wcomp + (size_t)(p0 + pp) * K_c + k0 + k : wcomp, ok);
+    // 16-byte pieces (two doubles); rows past P or O are zero-filled
+    for (int e = tid; e < CP * (KC / 2); e += 128) {
+      const int pp = e / (KC / 2), k = 2 * (e % (KC / 2));
+      const bool ok = p0 + pp < P;
+      cp_async16(&sw[buf][pp][k], ok ? wcomp + (size_t)(p0 + pp) * Kq + k0 + k : wcomp, ok);
     }
-    for (int e = tid; e < CO * KC; e += 128) {
-      const int oo = e / KC, k = e % KC;
-      const bool ok = (o0 + oo < O) && (k0 + k < K_c);
-      cp_async8(&sq[buf][oo][k], ok ? q + (size_t)(o0 + oo) * K_c + k0 + k : q, ok);
+    for (int e = tid; e < CO * (KC / 2); e += 128) {
+      const int oo = e / (KC / 2), k = 2 * (e % (KC / 2));
+      const bool ok = o0 + oo < O;
+      cp_async16(&sq[buf][oo][k], ok ? q + (size_t)(o0 + oo) * Kq + k0 + k : q, ok);
     }
     cp_async_commit();
   };
-  const int nslab = (K_c + KC - 1) / KC;
+  const int nslab = Kq / KC;
   if (nslab > 0) stage(0, 0);
   for (int sl = 0; sl < nslab; ++sl) {
     const int buf = sl & 1;
@@ -1179,18 +1193,18 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
     }
     case 3:
       tc_normx_kernel<<<g.P, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, g.N_img, normx, parts,
-                                          idx, g.K_c, wcomp);
+                                          idx, g.K_c, g.Kq, wcomp);
       break;
     case 4: {
-      // 64-particle tiles when they give two CTAs per SM, else 32 or 16
+      // the largest particle tile (64, 32, 16) that still gives every SM a CTA
       const long long otiles = (g.O + 63) / 64;
       const int sms = num_sms();
-      if (otiles * ((g.P + 63) / 64) >= 2LL * sms) {
-        tc_norma_kernel<4><<<dim3(otiles, (g.P + 63) / 64), 128, 0, s>>>(wcomp, g.K_c, q, g.O, g.P, normx, na);
-      } else if (otiles * ((g.P + 31) / 32) >= 2LL * sms) {
-        tc_norma_kernel<2><<<dim3(otiles, (g.P + 31) / 32), 128, 0, s>>>(wcomp, g.K_c, q, g.O, g.P, normx, na);
+      if (otiles * ((g.P + 63) / 64) >= sms) {
+        tc_norma_kernel<4><<<dim3(otiles, (g.P + 63) / 64), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na);
+      } else if (otiles * ((g.P + 31) / 32) >= sms) {
+        tc_norma_kernel<2><<<dim3(otiles, (g.P + 31) / 32), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na);
       } else {
-        tc_norma_kernel<1><<<dim3(otiles, (g.P + 15) / 16), 128, 0, s>>>(wcomp, g.K_c, q, g.O, g.P, normx, na);
+        tc_norma_kernel<1><<<dim3(otiles, (g.P + 15) / 16), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na);
       }
       break;
     }
