@@ -170,6 +170,8 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="c5: length of the arrival trace")
     ap.add_argument("--serve-fp32-seconds", type=float, default=0.5,
                     help="c5: part of the trace replayed through the FP32 baseline")
+    ap.add_argument("--gemm-variant", default=None,
+                    help="row_bytes,tile_n,split,pair for the contraction (0 = default; pair 1 = CTA pairs)")
     ap.add_argument("--study", default=None, choices=["precision"],
                     help="precision: error of every precision form vs the FP64 kernel (use --config c3)")
     return ap.parse_args()
@@ -261,6 +263,8 @@ def ours_arm(args):
     pr = synth.make_problem(args.config, seed=20251203 + rank, P=args.particles)
     prec = PREC[args.precision]
     dev = torch.device("cuda", local)
+    if args.gemm_variant:
+        pkg.set_gemm_variant(*[int(x) for x in args.gemm_variant.split(",")])
     stream = torch.cuda.current_stream()
 
     proj = pkg.Projector(pr.projector, use_texture=1)

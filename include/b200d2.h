@@ -384,10 +384,13 @@ int b200d2_coarse_weights(const float* d_diff2, int P, int O, int T,
  * (b200d2_diff2_coarse_batch, _stage, _static and the server), process-wide:
  * row_bytes 64 or 128 (k-block row width), tile_n 256 or 128 (orientations
  * per tile), split = k-splits per tile (partial sums added in split order in
- * FP64).  0 in any field restores the default (64-byte rows, 256-wide tiles,
- * k-splits chosen from the tile count, at most the workspace's capacity).
- * Plans choose their own variant (B200D2_PLAN_AUTOTUNE). */
-int b200d2_set_gemm_variant(int row_bytes, int tile_n, int split);
+ * FP64), pair = 1 for CTA-pair tiles (a cluster of two CTAs computes a
+ * 256 x 256 tile with cta_group::2 MMAs; 256-wide, no k-splits), 2 for
+ * single-CTA tiles.  0 in any field restores the default (64-byte rows,
+ * 256-wide tiles, k-splits chosen from the tile count, at most the
+ * workspace's capacity, CTA pairs when the pair tiles fill the GPU).  Plans
+ * choose their own variant (B200D2_PLAN_AUTOTUNE). */
+int b200d2_set_gemm_variant(int row_bytes, int tile_n, int split, int pair);
 
 /* Run a single stage of the batch pipeline, so that a caller can time one
  * kernel with events on its stream.  Stages are numbered in pipeline order

@@ -152,7 +152,7 @@ def _declare(L):
         "b200d2_server_get_stats": [P, C.POINTER(ServerStats)],
         "b200d2_server_destroy": [P],
         "b200d2_coarse_weights": [P, I, I, I, P, P, P, I, P, P, P, Z, P],
-        "b200d2_set_gemm_variant": [I, I, I],
+        "b200d2_set_gemm_variant": [I, I, I, I],
         "b200d2_ctf_fold": [P, P, C.c_longlong, I, I, I, I, I, I, F, P, P, C.c_longlong, P, P, P, P],
     }
     for name, args in sig.items():
@@ -500,9 +500,10 @@ def ctf_fold(real, imag, ctf_params: list, minvsigma2, *, imgX: int, imgY: int, 
     return out_real, out_imag, out_corr
 
 
-def set_gemm_variant(row_bytes: int = 0, tile_n: int = 0, split: int = 0) -> None:
-    """Contraction variant of the batch entry points (0 = default)."""
-    _check(lib().b200d2_set_gemm_variant(row_bytes, tile_n, split), "set_gemm_variant")
+def set_gemm_variant(row_bytes: int = 0, tile_n: int = 0, split: int = 0, pair: int = 0) -> None:
+    """Contraction variant of the batch entry points (0 = default; pair: 1 =
+    CTA-pair 256 x 256 tiles, 2 = single-CTA tiles)."""
+    _check(lib().b200d2_set_gemm_variant(row_bytes, tile_n, split, pair), "set_gemm_variant")
 
 
 def stage_names(precision: int) -> list[str]:

@@ -101,7 +101,7 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, i
   g.terms = (prec == B200D2_PREC_TF32 || prec == B200D2_PREC_FP16) ? 1 : 3;
   g.Kpad = (int)align_up((size_t)std::max(2 * g.K_c, 1), (size_t)g.BK);
   g.Mrows = mrows >= 0 ? mrows : b.P * b.T;
-  g.Mpad = (int)align_up((size_t)g.Mrows, 128);
+  g.Mpad = (int)align_up((size_t)g.Mrows, 256);  // whole 256-row tiles for the CTA-pair contraction
   g.Opad = (int)align_up((size_t)b.O, 256);
   g.maxR = extent;  // phase tables cover x in [0, extent], y in [-extent, extent]
   g.exw = extent + 1;
@@ -985,6 +985,250 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   }
 }
 
+// CTA-pair variant (cta_group::2): a cluster of two CTAs computes a 256 x 256
+// tile.  Each CTA loads its 128 rows of A and its 128-row half of B into its
+// own shared memory; the even CTA issues one M = 256, N = 256 MMA per k-step
+// that reads both CTAs' tiles, and each CTA's TMEM receives its own 128 rows
+// of the accumulator.  Per SM the operand stream from L2 and the tensor core's
+// shared-memory reads are a third lower than with a 128 x 256 tile per CTA.
+// Uniform batches only; no k-splits.
+template <int PREC, int ROWB>
+struct GemmCfgPair {
+  using Base = GemmCfg<PREC, ROWB, 256>;
+  static constexpr bool kTf32 = Base::kTf32;
+  static constexpr bool kScaled = Base::kScaled;
+  static constexpr int kElem = Base::kElem, kBK = Base::kBK, kKStep = Base::kKStep, kTerms = Base::kTerms;
+  static constexpr int kPlanes = Base::kPlanes, kRowB = ROWB;
+  static constexpr int kBM = 128;  // rows of A per CTA (256 per pair)
+  static constexpr int kBNh = 128;  // rows of B per CTA (N = 256 per pair)
+  static constexpr int kATile = kBM * ROWB, kBTile = kBNh * ROWB;
+  static constexpr int kStageBytes = kPlanes * (kATile + kBTile);
+  static constexpr int kStages = (200 * 1024) / kStageBytes < 8 ? (200 * 1024) / kStageBytes : 8;
+  static constexpr uint32_t kIdesc = sm100::idesc_f32acc(Base::kFmt, 256, 256);
+  static constexpr int kTmemCols = 512;
+  static constexpr int kBarBytes = 256;
+  static constexpr int kSmem = kStages * kStageBytes + kBarBytes + 1024;
+  static_assert(kStages >= 2, "at least two pipeline stages");
+  static_assert(2 * kStages * 8 + 5 * 8 + 8 <= kBarBytes, "barrier area");
+};
+
+template <int PREC, int ROWB>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
+    tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
+                        const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo,
+                        const GemmArgs g) {
+  using C = GemmCfgPair<PREC, ROWB>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::kStages * C::kStageBytes);
+  uint64_t* empty = full + C::kStages;
+  uint64_t* accf = empty + C::kStages;
+  uint64_t* acce = accf + 2;
+  uint64_t* drain = acce + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile uint32_t* s_abort = tmem_slot + 1;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = sm100::cluster_ctarank();  // 0 issues the MMAs
+  const bool lead = rank == 0;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C::kStages; ++s) {
+      sm100::mbar_init(&full[s], 1);   // used in the even CTA: its own arrive + both CTAs' bytes
+      sm100::mbar_init(&empty[s], 1);  // one multicast commit per use
+    }
+    for (int b = 0; b < 2; ++b) {
+      sm100::mbar_init(&accf[b], 1);
+      sm100::mbar_init(&acce[b], 256);  // even CTA: the epilogue threads of both CTAs
+    }
+    sm100::mbar_init(drain, 1);
+    *s_abort = 0;
+    sm100::fence_barrier_init();
+    sm100::fence_proxy_async_smem();
+  }
+  if (warp == 0 && lane == 0) {
+    sm100::prefetch_tensormap(&mAhi);
+    sm100::prefetch_tensormap(&mBhi);
+    if (C::kPlanes == 2) {
+      sm100::prefetch_tensormap(&mAlo);
+      sm100::prefetch_tensormap(&mBlo);
+    }
+  }
+  if (warp == 1) {
+    sm100::tmem_alloc_pair(tmem_slot, C::kTmemCols);
+    sm100::tmem_relinquish_pair();
+  }
+  sm100::tc_fence_before();
+  __syncthreads();
+  sm100::cluster_sync();  // both CTAs' barriers initialised before any remote use
+  sm100::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int num_tiles = g.Mtiles * g.Ntiles;
+  const int cl = blockIdx.x >> 1, ncl = gridDim.x >> 1;
+  const uint32_t full0 = sm100::map_to_rank(full, 0);  // the even CTA's full[0]
+  const uint32_t acce0 = sm100::map_to_rank(acce, 0);
+
+  auto raise_abort = [&]() {
+    *s_abort = 1;
+    atomicExch(g.status, (uint32_t)B200D2_ERR_TIMEOUT);
+  };
+
+  if (warp == 0) {
+    // ------------------------------------------------ TMA producer (both CTAs)
+    if (lane == 0) {
+      uint32_t gk = 0;
+      bool ok = true;
+      for (int tile = cl; tile < num_tiles && ok; tile += ncl) {
+        int m0, n0;
+        tile_origin(g, tile, 256, 256, m0, n0);
+        for (int kb = 0; kb < g.KB; ++kb, ++gk) {
+          const int s = gk % C::kStages;
+          const uint32_t u = gk / C::kStages;
+          if (u > 0 && !sm100::mbar_wait_bounded(&empty[s], (u - 1) & 1, s_abort, kWaitLimitNs)) {
+            raise_abort();
+            ok = false;
+            break;
+          }
+          if (lead) sm100::mbar_arrive_expect_tx(&full[s], 2 * C::kStageBytes);
+          uint8_t* st = smem + s * C::kStageBytes;
+          const uint32_t fb = full0 + 8u * (uint32_t)s;
+          const int kc = kb * C::kBK;
+          sm100::tma_load_2d_pair(st, &mAhi, fb, kc, m0 + 128 * (int)rank);
+          if (C::kPlanes == 2) sm100::tma_load_2d_pair(st + C::kATile, &mAlo, fb, kc, m0 + 128 * (int)rank);
+          uint8_t* sb = st + C::kPlanes * C::kATile;
+          sm100::tma_load_2d_pair(sb, &mBhi, fb, kc, n0 + 128 * (int)rank);
+          if (C::kPlanes == 2) sm100::tma_load_2d_pair(sb + C::kBTile, &mBlo, fb, kc, n0 + 128 * (int)rank);
+        }
+      }
+      // the even CTA's full barriers count both CTAs' bytes: let every copy
+      // in flight land before either CTA can leave (the final cluster
+      // barrier holds the odd CTA until then)
+      if (lead) {
+        const uint32_t issued = gk;
+        for (uint32_t j = (issued > (uint32_t)C::kStages ? issued - C::kStages : 0); j < issued; ++j)
+          sm100::mbar_wait_bounded(&full[j % C::kStages], (j / C::kStages) & 1, s_abort, kWaitLimitNs);
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------ MMA issuer (even CTA)
+    if (lead && lane == 0) {
+      uint32_t gk = 0;
+      int i = 0;
+      bool ok = true;
+      for (int tile = cl; tile < num_tiles && ok; tile += ncl, ++i) {
+        const int b = i & 1;
+        const uint32_t v = (uint32_t)(i >> 1);
+        if (v > 0 && !sm100::mbar_wait_bounded(&acce[b], (v - 1) & 1, s_abort, kWaitLimitNs)) {
+          raise_abort();
+          break;
+        }
+        sm100::tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(b * 256);
+        for (int kb = 0; kb < g.KB; ++kb, ++gk) {
+          const int s = gk % C::kStages;
+          const uint32_t u = gk / C::kStages;
+          if (!sm100::mbar_wait_bounded(&full[s], u & 1, s_abort, kWaitLimitNs)) {
+            raise_abort();
+            ok = false;
+            break;
+          }
+          sm100::tc_fence_after();
+          const uint32_t st = sm100::smem_u32(smem + s * C::kStageBytes);
+          const uint32_t a_hi = st, a_lo = st + C::kATile;
+          const uint32_t b_hi = st + C::kPlanes * C::kATile, b_lo = b_hi + C::kBTile;
+#pragma unroll
+          for (int ks = 0; ks < C::kBK / C::kKStep; ++ks) {
+            const uint32_t koff = (uint32_t)(ks * C::kKStep * C::kElem);
+            const uint64_t dah = sm100::desc_k_sw(a_hi + koff, C::kRowB);
+            const uint64_t dbh = sm100::desc_k_sw(b_hi + koff, C::kRowB);
+            const uint32_t acc = (kb > 0 || ks > 0) ? 1u : 0u;
+            sm100::mma_pair<C::kTf32>(d, dah, dbh, C::kIdesc, acc);
+            if (C::kTerms == 3) {
+              sm100::mma_pair<C::kTf32>(d, dah, sm100::desc_k_sw(b_lo + koff, C::kRowB), C::kIdesc, 1u);
+              sm100::mma_pair<C::kTf32>(d, sm100::desc_k_sw(a_lo + koff, C::kRowB), dbh, C::kIdesc, 1u);
+            }
+          }
+          sm100::mma_commit_pair(&empty[s], (uint16_t)3);  // frees stage s in both CTAs
+        }
+        if (ok) sm100::mma_commit_pair(&accf[b], (uint16_t)3);
+      }
+      sm100::mma_commit_pair(drain, (uint16_t)1);
+      if (!sm100::mbar_wait_bounded(drain, 0, s_abort, kWaitLimitNs)) raise_abort();
+    }
+  } else {
+    // ------------------------------------------------ epilogue (warps 2..5, both CTAs)
+    const int qd = warp & 3;
+    const int row = qd * 32 + lane;
+    int i = 0;
+    for (int tile = cl; tile < num_tiles; tile += ncl, ++i) {
+      const int b = i & 1;
+      const uint32_t v = (uint32_t)(i >> 1);
+      int ok = 1;
+      if (lane == 0) ok = sm100::mbar_wait_bounded(&accf[b], v & 1, s_abort, kWaitLimitNs) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        if (lane == 0) raise_abort();
+        break;
+      }
+      sm100::tc_fence_after();
+      int m0, n0;
+      tile_origin(g, tile, 256, 256, m0, n0);
+      const int m = m0 + 128 * (int)rank + row;
+      const bool vrow = m < g.Mrows;
+      const int p = vrow ? m / g.T : 0;
+      const int t = vrow ? m - p * g.T : 0;
+      const double* __restrict__ na_row = g.na + (size_t)p * g.O;
+      float* __restrict__ out_row = g.out + (size_t)p * g.O * g.T + t;
+      const double m2s = C::kScaled ? -2.0 * (double)g.inv_sa[p] : -2.0;
+      float best = __int_as_float(0x7f800000);
+      uint32_t best_idx = 0xffffffffu;
+#pragma unroll 1
+      for (int c = 0; c < 256 / 32; ++c) {
+        uint32_t r[32];
+        __syncwarp();
+        sm100::tmem_ld_32x32b_x32(tmem + (uint32_t)(b * 256 + c * 32) + ((uint32_t)(qd * 32) << 16), r);
+        sm100::tmem_ld_wait();
+        if (vrow) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int o = n0 + c * 32 + j;
+            if (o < g.O) {
+              double cr = (double)__uint_as_float(r[j]);
+              if (C::kScaled) cr *= (double)g.inv_sb[o];
+              float f = (float)fma(m2s, cr, na_row[o]);
+              float* dst = out_row + (size_t)o * g.T;
+              if (g.accumulate) f += *dst;
+              *dst = f;
+              if (f < best) {
+                best = f;
+                best_idx = (uint32_t)(o * g.T + t);
+              }
+            }
+          }
+        }
+      }
+      sm100::tc_fence_before();
+      sm100::mbar_arrive_cluster(acce0 + 8u * (uint32_t)b);  // the even CTA may reuse buffer b
+      unsigned long long key =
+          (vrow && best_idx != 0xffffffffu) ? (((unsigned long long)ordered_bits(best) << 32) | best_idx) : ~0ull;
+      const int pk = vrow ? p : -1;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const unsigned long long ok2 = __shfl_down_sync(0xffffffffu, key, off);
+        const int op = __shfl_down_sync(0xffffffffu, pk, off);
+        if (lane + off < 32 && op == pk && ok2 < key) key = ok2;
+      }
+      const int prevp = __shfl_up_sync(0xffffffffu, pk, 1);
+      if (pk >= 0 && (lane == 0 || prevp != pk) && key != ~0ull) atomicMin(&g.keys[pk], key);
+    }
+  }
+  __syncthreads();
+  sm100::cluster_sync();  // no CTA leaves while its pair may still touch its memory
+  if (warp == 1) {
+    sm100::tc_fence_after();
+    sm100::tmem_dealloc_pair(tmem, C::kTmemCols);
+  }
+}
+
 // ------------------------------------------------------------------ stage 7
 __global__ void tc_finalize_kernel(const unsigned long long* keys, int P, double* mn, long long* arg) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1047,11 +1291,12 @@ struct GemmVariant {
   int row_bytes = 0;  // 64 or 128; 0 = library default
   int bn = 0;         // orientations per tile: 256 or 128; 0 = library default (256)
   int split = 0;      // k-splits per tile; 0 = chosen from the tile count
+  int pair = 0;       // 1: CTA-pair 256 x 256 tiles (uniform batches, no k-splits); 0: one CTA per tile
 };
 
 // Process-wide variant of the batch entry points (b200d2_set_gemm_variant);
 // plans carry their own.
-static std::atomic<int> g_var_rb{0}, g_var_bn{0}, g_var_split{0};
+static std::atomic<int> g_var_rb{0}, g_var_bn{0}, g_var_split{0}, g_var_pair{0};
 
 // k-splits for `tiles` tiles of KB k-blocks: 1 when the tiles fill the GPU,
 // else the largest power of two (<= cap) keeping two work items per SM at
@@ -1128,6 +1373,57 @@ static int launch_gemm_v(const b200d2_batch& b, const TcGeom& g, void* ws, cudaS
   return status_from_cuda(cudaGetLastError());
 }
 
+template <int PREC, int ROWB>
+static int launch_gemm_pair(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s) {
+  using C = GemmCfgPair<PREC, ROWB>;
+  CUtensorMap mAhi, mAlo, mBhi, mBlo;
+  int st = make_map(&mAhi, ws_at<void>(ws, g.off_ahi), g.elem, g.Kpad, g.Mpad, 128, ROWB, C::kScaled);
+  if (st == B200D2_OK) st = make_map(&mAlo, ws_at<void>(ws, g.off_alo), g.elem, g.Kpad, g.Mpad, 128, ROWB, C::kScaled);
+  if (st == B200D2_OK) st = make_map(&mBhi, ws_at<void>(ws, g.off_bhi), g.elem, g.Kpad, g.Opad, 128, ROWB, C::kScaled);
+  if (st == B200D2_OK) st = make_map(&mBlo, ws_at<void>(ws, g.off_blo), g.elem, g.Kpad, g.Opad, 128, ROWB, C::kScaled);
+  if (st != B200D2_OK) return st;
+  GemmArgs a;
+  memset(&a, 0, sizeof(a));
+  a.Mrows = g.Mrows;
+  a.Mtiles = g.Mpad / 256;
+  a.Ntiles = g.Opad / 256;
+  a.O = g.O;
+  a.T = g.T;
+  a.KB = g.Kpad / C::kBK;
+  a.accumulate = b.accumulate;
+  a.split = 1;
+  {
+    // tile order as for single-CTA tiles, with 256-row m-tiles
+    const double b_bytes = (double)g.Opad * g.Kpad * g.elem * C::kPlanes;
+    const double a_tile = 256.0 * g.Kpad * g.elem * C::kPlanes;
+    a.group_m = 0;
+    if (b_bytes > 64.0 * 1024 * 1024 && a.Mtiles > 1)
+      a.group_m = std::max(1, std::min(a.Mtiles, (int)(48.0 * 1024 * 1024 / a_tile)));
+  }
+  a.out = b.d_diff2;
+  a.na = ws_at<double>(ws, g.off_na);
+  a.keys = ws_at<unsigned long long>(ws, g.off_keys);
+  a.status = ws_at<uint32_t>(ws, g.off_status);
+  a.inv_sa = ws_at<float>(ws, g.off_sa);
+  a.inv_sb = ws_at<float>(ws, g.off_sb);
+  a.L = Layout{nullptr, nullptr, nullptr, 0};
+  static std::atomic<unsigned long long> attr_dev{0};
+  int dev = 0;
+  B200D2_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(attr_dev.load() & bit)) {
+    B200D2_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_pair_kernel<PREC, ROWB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, C::kSmem));
+    attr_dev.fetch_or(bit);
+  }
+  const int tiles = a.Mtiles * a.Ntiles;
+  if (tiles == 0) return B200D2_OK;
+  const int pairs = std::max(1, std::min(tiles, num_sms() / 2));
+  tc_gemm_pair_kernel<PREC, ROWB><<<2 * pairs, 192, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
+  count_launch();
+  return status_from_cuda(cudaGetLastError());
+}
+
 template <int PREC>
 static int launch_gemm(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s, GemmVariant var,
                        const UnevenTabs* U) {
@@ -1135,8 +1431,11 @@ static int launch_gemm(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStr
     if (var.row_bytes <= 0) var.row_bytes = g_var_rb.load();
     if (var.bn <= 0) var.bn = g_var_bn.load();
     if (var.split <= 0) var.split = g_var_split.load();
+    if (var.pair <= 0) var.pair = g_var_pair.load();
   }
   const int rb = var.row_bytes > 0 ? var.row_bytes : gemm_row_bytes();
+  if (var.pair == 1 && !U && (var.bn <= 0 || var.bn == 256) && var.split <= 1)
+    return rb == 128 ? launch_gemm_pair<PREC, 128>(b, g, ws, s) : launch_gemm_pair<PREC, 64>(b, g, ws, s);
   if (var.bn == 128)
     return rb == 128 ? launch_gemm_v<PREC, 128, 128>(b, g, ws, s, U, var.split)
                      : launch_gemm_v<PREC, 64, 128>(b, g, ws, s, U, var.split);
@@ -1735,12 +2034,13 @@ extern "C" int b200d2_workspace_status(const void* d_workspace, void* stream, in
   return B200D2_OK;
 }
 
-extern "C" int b200d2_set_gemm_variant(int row_bytes, int tile_n, int split) {
+extern "C" int b200d2_set_gemm_variant(int row_bytes, int tile_n, int split, int pair) {
   if ((row_bytes != 0 && row_bytes != 64 && row_bytes != 128) || (tile_n != 0 && tile_n != 128 && tile_n != 256) ||
-      split < 0 || split > 64)
+      split < 0 || split > 64 || pair < 0 || pair > 2)
     return B200D2_ERR_INVALID;
   b200d2::g_var_rb.store(row_bytes);
   b200d2::g_var_bn.store(tile_n);
   b200d2::g_var_split.store(split);
+  b200d2::g_var_pair.store(pair);
   return B200D2_OK;
 }

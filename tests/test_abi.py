@@ -45,8 +45,9 @@ def test_host_side_argument_validation(pkg):
                                None) == 0
     assert lib.b200d2_ctf_fold(None, None, 10, 2, 10, 6, 10, 5, 10, 1.5, None, None, 0, None, None, None,
                                None) == 1
-    assert lib.b200d2_set_gemm_variant(96, 0, 0) == 1 and lib.b200d2_set_gemm_variant(0, 192, 0) == 1
-    assert lib.b200d2_set_gemm_variant(0, 0, 0) == 0
+    assert lib.b200d2_set_gemm_variant(96, 0, 0, 0) == 1 and lib.b200d2_set_gemm_variant(0, 192, 0, 0) == 1
+    assert lib.b200d2_set_gemm_variant(0, 0, 0, 3) == 1
+    assert lib.b200d2_set_gemm_variant(0, 0, 0, 0) == 0
     assert lib.b200d2_coarse_weights_workspace(0, 100) == 0
     assert lib.b200d2_coarse_weights_workspace(3, 70000) >= 3 * 8 + 3 * 3 * 8 + 3 * 4
 

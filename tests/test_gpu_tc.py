@@ -143,19 +143,20 @@ def test_tc_deterministic(pkg, cuda, tiny):
     np.testing.assert_array_equal(a[2], b[2])
 
 
-@pytest.mark.parametrize("rb,tn,split", [(64, 256, 1), (64, 256, 2), (64, 256, 4), (128, 256, 2),
-                                         (64, 128, 1), (64, 128, 4), (128, 128, 1)])
-def test_tc_gemm_variants(pkg, oracle, cuda, c1, rb, tn, split):
+@pytest.mark.parametrize("rb,tn,split,pair", [(64, 256, 1, 2), (64, 256, 2, 2), (64, 256, 4, 2), (128, 256, 2, 2),
+                                              (64, 128, 1, 2), (64, 128, 4, 2), (128, 128, 1, 2),
+                                              (64, 256, 1, 1), (128, 256, 1, 1)])
+def test_tc_gemm_variants(pkg, oracle, cuda, c1, rb, tn, split, pair):
     """Every contraction variant (k-block row width, tile width, k-splits with
-    FP64 addition of the partials) meets the same tolerance, and a split
-    run is reproducible bit for bit."""
+    FP64 addition of the partials, CTA-pair tiles) meets the same tolerance,
+    and a run is reproducible bit for bit."""
     pr, view, dp, ref = c1
-    pkg.set_gemm_variant(rb, tn, split)
+    pkg.set_gemm_variant(rb, tn, split, pair)
     try:
         got, mn, am = run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3)
         again, _, _ = run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3)
     finally:
-        pkg.set_gemm_variant(0, 0, 0)
+        pkg.set_gemm_variant(0, 0, 0, 0)
     np.testing.assert_array_equal(got, again)
     s = oracle.error_stats(got, ref)
     assert s["max_rel"] <= TOL["bf16x3"], s
@@ -163,4 +164,21 @@ def test_tc_gemm_variants(pkg, oracle, cuda, c1, rb, tn, split):
         assert am[p] == int(np.argmin(got[p].ravel()))
         ok, gap = argmin_consistent(got[p], ref[p], TOL["bf16x3"])
         assert ok, (p, gap)
+
+
+@pytest.mark.parametrize("name", ["bf16x3", "tf32", "fp16x3"])
+def test_tc_pair_tiles_c2_subset(pkg, synth, oracle, cuda, name):
+    """CTA-pair tiles (cta_group::2) on a C2 subset: several 256 x 256 tiles
+    per pair, O not a multiple of 256 handled by the epilogue."""
+    pr = synth.make_problem("c2", P=5, orient_limit=1000)
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dp = DeviceProblem(cuda, pr)
+    ref = fp64_all(pkg, view, dp)
+    pkg.set_gemm_variant(0, 0, 1, 1)
+    try:
+        _check(pkg, oracle, cuda, (pr, view, dp, ref), name)
+    finally:
+        pkg.set_gemm_variant(0, 0, 0, 0)
+    proj.close()
 
