@@ -300,7 +300,8 @@ def ours_arm(args):
         torch.cuda.synchronize()
         plan_extra["fixed_tile_ms_per_step"] = fa.elapsed_time(fb) / max(3, min(args.steps, 10))
         fi = fixed.info()
-        plan_extra["fixed_variant"] = {"row_bytes": fi["row_bytes"], "tile_n": fi["tile_n"], "split": fi["split"]}
+        plan_extra["fixed_variant"] = {"row_bytes": fi["row_bytes"], "tile_n": fi["tile_n"], "split": fi["split"],
+                                       "pair": fi["pair"]}
         fixed.close()
         del fixed_bufs
         plan, bufs, evals_plan = build_plan_case(pkg, pr, dev, prec,
@@ -308,8 +309,9 @@ def ours_arm(args):
         eul, re, im, corr, out, mn, am = bufs
         info = plan.info()
         plan_extra.update({"autotuned_variant": {"row_bytes": info["row_bytes"], "tile_n": info["tile_n"],
-                                                 "split": info["split"]},
-                           "tuned_gemm_ms": {f"rb{v[0]}_n{v[1]}_s{v[2]}": ms for v, ms in info["tuned"]},
+                                                 "split": info["split"], "pair": info["pair"]},
+                           "tuned_gemm_ms": {f"rb{v[0]}_n{v[1]}_s{v[2]}_p{v[3]}": ms for v, ms in info["tuned"]},
+                           "work_tiles_pair": info["tiles_pair"],
                            "work_tiles_n128": info["tiles_n128"],
                            "work_tiles": info["tiles"], "dense_tiles": info["tiles_dense"], "rows": info["rows"]})
     else:
@@ -358,7 +360,8 @@ def ours_arm(args):
     # ---- dominant kernel timing (events on the launching stream) ----
     if uneven:
         av = plan_extra["autotuned_variant"]
-        tuned = plan_extra["tuned_gemm_ms"].get(f"rb{av['row_bytes']}_n{av['tile_n']}_s{av['split']}")
+        tuned = plan_extra["tuned_gemm_ms"].get(
+            f"rb{av['row_bytes']}_n{av['tile_n']}_s{av['split']}_p{1 if av['pair'] else 2}")
         name = [n for n in pkg.stage_names(prec) if "gemm" in n][0]
         kern = {"per_kernel_ms": {name: tuned}, "dominant": name, "dominant_ms": tuned or None, "traffic": None}
     else:

@@ -229,11 +229,13 @@ typedef struct b200d2_plan_info {
   /* chosen contraction variant: tile width (orientations per tile) and
    * k-splits per tile (row_bytes above is its k-block row width) */
   int tile_n, split;
+  int pair;               /* 1: CTA-pair 256 x 256 tiles */
   int tiles_n128;         /* work-list length with 128-wide tiles */
-  /* autotuner: variants timed, each (row_bytes, tile_n, split) and its
+  int tiles_pair;         /* work-list length with 256 x 256 tiles */
+  /* autotuner: variants timed, each (row_bytes, tile_n, split, pair) and its
    * contraction time in ms (n_tuned = 0 without B200D2_PLAN_AUTOTUNE) */
   int n_tuned;
-  int tuned_variant[B200D2_PLAN_MAX_VARIANTS][3];
+  int tuned_variant[B200D2_PLAN_MAX_VARIANTS][4];
   double tuned_ms[B200D2_PLAN_MAX_VARIANTS];
 } b200d2_plan_info;
 
@@ -389,7 +391,8 @@ int b200d2_coarse_weights(const float* d_diff2, int P, int O, int T,
  * single-CTA tiles.  0 in any field restores the default (64-byte rows,
  * 256-wide tiles, k-splits chosen from the tile count, at most the
  * workspace's capacity, CTA pairs when the pair tiles fill the GPU).  Plans
- * choose their own variant (B200D2_PLAN_AUTOTUNE). */
+ * created with B200D2_PLAN_AUTOTUNE choose their own variant; other plans take
+ * this setting at creation (single-CTA 256-wide tiles when it is 0). */
 int b200d2_set_gemm_variant(int row_bytes, int tile_n, int split, int pair);
 
 /* Run a single stage of the batch pipeline, so that a caller can time one

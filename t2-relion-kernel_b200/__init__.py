@@ -84,7 +84,8 @@ class PlanInfo(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("P", "O_all", "rows", "tiles", "tiles_dense", "row_bytes", "graph",
                                          "stages")] + [
         ("evals", C.c_longlong), ("workspace_bytes", C.c_size_t), ("tile_n", C.c_int), ("split", C.c_int),
-        ("tiles_n128", C.c_int), ("n_tuned", C.c_int), ("tuned_variant", (C.c_int * 3) * PLAN_MAX_VARIANTS),
+        ("pair", C.c_int), ("tiles_n128", C.c_int), ("tiles_pair", C.c_int), ("n_tuned", C.c_int),
+        ("tuned_variant", (C.c_int * 4) * PLAN_MAX_VARIANTS),
         ("tuned_ms", C.c_double * PLAN_MAX_VARIANTS)]
 
 

@@ -163,8 +163,8 @@ struct PartDev {
 struct UnevenTabs {
   const PartDev* parts;   // [P]
   const int4* rows;       // [Mrows]
-  const int2* tiles[2];   // work lists of 256- and 128-wide tiles
-  int ntiles[2];
+  const int2* tiles[3];   // work lists: 128 x 256, 128 x 128 and (CTA pairs) 256 x 256 tiles
+  int ntiles[3];
   const float2* tab_txy;  // [ntab] translation of each phase table
   int ntab;
   int Mrows;
@@ -991,7 +991,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
 // that reads both CTAs' tiles, and each CTA's TMEM receives its own 128 rows
 // of the accumulator.  Per SM the operand stream from L2 and the tensor core's
 // shared-memory reads are a third lower than with a 128 x 256 tile per CTA.
-// Uniform batches only; no k-splits.
+// No k-splits; uneven batches through a work list of 256-row m-tiles.
 template <int PREC, int ROWB>
 struct GemmCfgPair {
   using Base = GemmCfg<PREC, ROWB, 256>;
@@ -1062,7 +1062,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
   sm100::cluster_sync();  // both CTAs' barriers initialised before any remote use
   sm100::tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int num_tiles = g.Mtiles * g.Ntiles;
+  const int num_tiles = g.L.tiles ? g.L.ntiles : g.Mtiles * g.Ntiles;
   const int cl = blockIdx.x >> 1, ncl = gridDim.x >> 1;
   const uint32_t full0 = sm100::map_to_rank(full, 0);  // the even CTA's full[0]
   const uint32_t acce0 = sm100::map_to_rank(acce, 0);
@@ -1174,10 +1174,26 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       tile_origin(g, tile, 256, 256, m0, n0);
       const int m = m0 + 128 * (int)rank + row;
       const bool vrow = m < g.Mrows;
-      const int p = vrow ? m / g.T : 0;
-      const int t = vrow ? m - p * g.T : 0;
+      int p = 0, t = 0, Tp = g.T;
+      float* outp = g.out;
+      const int* __restrict__ inv = nullptr;  // orientation -> this particle's list index
+      if (vrow) {
+        if (g.L.rows) {
+          const int4 rw = g.L.rows[m];
+          p = rw.x;
+          t = rw.y;
+          const PartDev& pd = g.L.parts[p];
+          Tp = pd.T;
+          outp = pd.out;
+          inv = pd.inv;
+        } else {
+          p = m / g.T;
+          t = m - p * g.T;
+          outp = g.out + (size_t)p * g.O * g.T;
+        }
+      }
       const double* __restrict__ na_row = g.na + (size_t)p * g.O;
-      float* __restrict__ out_row = g.out + (size_t)p * g.O * g.T + t;
+      float* __restrict__ out_row = outp + t;
       const double m2s = C::kScaled ? -2.0 * (double)g.inv_sa[p] : -2.0;
       float best = __int_as_float(0x7f800000);
       uint32_t best_idx = 0xffffffffu;
@@ -1191,16 +1207,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int o = n0 + c * 32 + j;
-            if (o < g.O) {
+            const int lo = (o < g.O) ? (inv ? inv[o] : o) : -1;
+            if (lo >= 0) {
               double cr = (double)__uint_as_float(r[j]);
               if (C::kScaled) cr *= (double)g.inv_sb[o];
               float f = (float)fma(m2s, cr, na_row[o]);
-              float* dst = out_row + (size_t)o * g.T;
+              float* dst = out_row + (size_t)lo * Tp;
               if (g.accumulate) f += *dst;
               *dst = f;
               if (f < best) {
                 best = f;
-                best_idx = (uint32_t)(o * g.T + t);
+                best_idx = (uint32_t)(lo * Tp + t);
               }
             }
           }
@@ -1374,7 +1391,8 @@ static int launch_gemm_v(const b200d2_batch& b, const TcGeom& g, void* ws, cudaS
 }
 
 template <int PREC, int ROWB>
-static int launch_gemm_pair(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s) {
+static int launch_gemm_pair(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s,
+                            const UnevenTabs* U) {
   using C = GemmCfgPair<PREC, ROWB>;
   CUtensorMap mAhi, mAlo, mBhi, mBlo;
   int st = make_map(&mAhi, ws_at<void>(ws, g.off_ahi), g.elem, g.Kpad, g.Mpad, 128, ROWB, C::kScaled);
@@ -1406,7 +1424,7 @@ static int launch_gemm_pair(const b200d2_batch& b, const TcGeom& g, void* ws, cu
   a.status = ws_at<uint32_t>(ws, g.off_status);
   a.inv_sa = ws_at<float>(ws, g.off_sa);
   a.inv_sb = ws_at<float>(ws, g.off_sb);
-  a.L = Layout{nullptr, nullptr, nullptr, 0};
+  a.L = Layout{U ? U->parts : nullptr, U ? U->rows : nullptr, U ? U->tiles[2] : nullptr, U ? U->ntiles[2] : 0};
   static std::atomic<unsigned long long> attr_dev{0};
   int dev = 0;
   B200D2_CUDA_TRY(cudaGetDevice(&dev));
@@ -1416,7 +1434,7 @@ static int launch_gemm_pair(const b200d2_batch& b, const TcGeom& g, void* ws, cu
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, C::kSmem));
     attr_dev.fetch_or(bit);
   }
-  const int tiles = a.Mtiles * a.Ntiles;
+  const int tiles = U ? U->ntiles[2] : a.Mtiles * a.Ntiles;
   if (tiles == 0) return B200D2_OK;
   const int pairs = std::max(1, std::min(tiles, num_sms() / 2));
   tc_gemm_pair_kernel<PREC, ROWB><<<2 * pairs, 192, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
@@ -1433,9 +1451,16 @@ static int launch_gemm(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStr
     if (var.split <= 0) var.split = g_var_split.load();
     if (var.pair <= 0) var.pair = g_var_pair.load();
   }
+  // CTA pairs by default for uniform batches whose 256 x 256 tiles fill the
+  // GPU (one tile per pair of SMs at least); their default rows are 128 bytes
+  bool pair = var.pair == 1;
+  if (var.pair == 0 && !U && (var.bn <= 0 || var.bn == 256) && var.split <= 1)
+    pair = (long long)(g.Mpad / 256) * (g.Opad / 256) >= num_sms() / 2;
+  if (pair && (var.bn <= 0 || var.bn == 256) && var.split <= 1) {
+    const int prb = var.row_bytes > 0 ? var.row_bytes : 128;
+    return prb == 128 ? launch_gemm_pair<PREC, 128>(b, g, ws, s, U) : launch_gemm_pair<PREC, 64>(b, g, ws, s, U);
+  }
   const int rb = var.row_bytes > 0 ? var.row_bytes : gemm_row_bytes();
-  if (var.pair == 1 && !U && (var.bn <= 0 || var.bn == 256) && var.split <= 1)
-    return rb == 128 ? launch_gemm_pair<PREC, 128>(b, g, ws, s) : launch_gemm_pair<PREC, 64>(b, g, ws, s);
   if (var.bn == 128)
     return rb == 128 ? launch_gemm_v<PREC, 128, 128>(b, g, ws, s, U, var.split)
                      : launch_gemm_v<PREC, 64, 128>(b, g, ws, s, U, var.split);
@@ -1548,21 +1573,21 @@ size_t tc_workspace_bytes(const b200d2_view& v, const b200d2_batch& b, int preci
 const char* tc_stage_name(int precision, int stage) {
   static const char* bf16[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_kernel<bf16x3>",
                                "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<bf16x3>",
-                               "tc_gemm_kernel<bf16x3>", "tc_finalize_kernel"};
+                               "tc_gemm[_pair]_kernel<bf16x3>", "tc_finalize_kernel"};
   static const char* tf3[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_kernel<tf32x3>",
                               "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<tf32x3>",
-                              "tc_gemm_kernel<tf32x3>", "tc_finalize_kernel"};
+                              "tc_gemm[_pair]_kernel<tf32x3>", "tc_finalize_kernel"};
   static const char* tf1[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_kernel<tf32>",
                               "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<tf32>",
-                              "tc_gemm_kernel<tf32>", "tc_finalize_kernel"};
+                              "tc_gemm[_pair]_kernel<tf32>", "tc_finalize_kernel"};
   // FP16 forms: stage 1 also launches tc_scale_a_kernel, stage 2 is the
   // two-pass tc_project_scaled_kernel
   static const char* h3[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_scaled_kernel<fp16x3>",
                              "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<fp16x3>",
-                             "tc_gemm_kernel<fp16x3>", "tc_finalize_kernel"};
+                             "tc_gemm[_pair]_kernel<fp16x3>", "tc_finalize_kernel"};
   static const char* h1[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_scaled_kernel<fp16>",
                              "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<fp16>",
-                             "tc_gemm_kernel<fp16>", "tc_finalize_kernel"};
+                             "tc_gemm[_pair]_kernel<fp16>", "tc_finalize_kernel"};
   if (stage < 0 || stage >= kNumStages) return nullptr;
   if (precision == B200D2_PREC_BF16X3) return bf16[stage];
   if (precision == B200D2_PREC_TF32X3) return tf3[stage];
@@ -1678,6 +1703,7 @@ struct b200d2_plan {
   int4* d_rows = nullptr;
   int2* d_tiles = nullptr;     // work list, 256-wide tiles
   int2* d_tiles128 = nullptr;  // work list, 128-wide tiles
+  int2* d_tiles_pair = nullptr;  // work list, 256 x 256 tiles of CTA pairs
   float2* d_txy = nullptr;
   int* d_inv = nullptr;
   float* d_eul_perm = nullptr;
@@ -1695,7 +1721,7 @@ static void plan_free(b200d2_plan* p) {
   if (p->graph) cudaGraphDestroy(p->graph);
   if (p->stream) cudaStreamDestroy(p->stream);
   for (void* d : {(void*)p->ws, (void*)p->d_parts, (void*)p->d_rows, (void*)p->d_tiles, (void*)p->d_tiles128,
-                  (void*)p->d_txy, (void*)p->d_inv, (void*)p->d_eul_perm})
+                  (void*)p->d_tiles_pair, (void*)p->d_txy, (void*)p->d_inv, (void*)p->d_eul_perm})
     if (d) cudaFree(d);
   delete p;
 }
@@ -1842,7 +1868,16 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   }
   // work lists: (m tile, n tile) pairs some particle of the m tile needs,
   // m-major, for 256- and 128-wide tiles
-  std::vector<int2> tiles, tiles128;
+  std::vector<int2> tiles, tiles128, tiles_pair;
+  for (int mt = 0; mt < (Mtiles + 1) / 2; ++mt) {  // 256-row m-tiles for CTA pairs
+    const int r0 = mt * 256, r1 = std::min(Mrows, r0 + 256);
+    std::vector<char> un(Ntiles128, 0);
+    for (int r = r0; r < r1; ++r)
+      if (r == r0 || rows[r].x != rows[r - 1].x)
+        for (int n = 0; n < Ntiles128; ++n) un[n] |= need_n[rows[r].x][n];
+    for (int n = 0; n < Ntiles; ++n)
+      if (un[2 * n] || (2 * n + 1 < Ntiles128 && un[2 * n + 1])) tiles_pair.push_back(make_int2(mt, n));
+  }
   for (int mt = 0; mt < Mtiles; ++mt) {
     const int r0 = mt * 128, r1 = std::min(Mrows, r0 + 128);
     std::vector<char> un(Ntiles128, 0);
@@ -1893,6 +1928,7 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   upload(reinterpret_cast<void**>(&p->d_rows), rows.data(), rows.size() * sizeof(int4));
   upload(reinterpret_cast<void**>(&p->d_tiles), tiles.data(), tiles.size() * sizeof(int2));
   upload(reinterpret_cast<void**>(&p->d_tiles128), tiles128.data(), tiles128.size() * sizeof(int2));
+  upload(reinterpret_cast<void**>(&p->d_tiles_pair), tiles_pair.data(), tiles_pair.size() * sizeof(int2));
   upload(reinterpret_cast<void**>(&p->d_txy), txy.data(), txy.size() * sizeof(float2));
   upload(reinterpret_cast<void**>(&p->d_inv), inv.data(), inv.size() * sizeof(int));
   if (st == B200D2_OK)
@@ -1903,8 +1939,13 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
     plan_free(p);
     return st;
   }
-  p->U = UnevenTabs{p->d_parts, p->d_rows, {p->d_tiles, p->d_tiles128}, {(int)tiles.size(), (int)tiles128.size()},
-                    p->d_txy, (int)txy.size(), Mrows};
+  p->U = UnevenTabs{p->d_parts,
+                    p->d_rows,
+                    {p->d_tiles, p->d_tiles128, p->d_tiles_pair},
+                    {(int)tiles.size(), (int)tiles128.size(), (int)tiles_pair.size()},
+                    p->d_txy,
+                    (int)txy.size(),
+                    Mrows};
 
   memset(&p->info, 0, sizeof(p->info));
   p->info.P = P;
@@ -1915,14 +1956,19 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   p->info.evals = evals;
   p->info.stages = kNumStages;
   p->info.tiles_n128 = (int)tiles128.size();
-  p->info.workspace_bytes = p->g.total + rows.size() * sizeof(int4) + (tiles.size() + tiles128.size()) * sizeof(int2) +
+  p->info.tiles_pair = (int)tiles_pair.size();
+  p->info.workspace_bytes = p->g.total + rows.size() * sizeof(int4) +
+                            (tiles.size() + tiles128.size() + tiles_pair.size()) * sizeof(int2) +
                             txy.size() * sizeof(float2) + inv.size() * sizeof(int) + hp.size() * sizeof(PartDev);
 
   // warm run (also sets kernel attributes outside any capture)
+  // without the autotuner a plan takes the process-wide variant
+  // (b200d2_set_gemm_variant), single-CTA 256-wide tiles by default
   p->var = GemmVariant();
-  p->var.row_bytes = gemm_row_bytes();
-  p->var.bn = 256;
-  p->var.split = 1;
+  p->var.row_bytes = g_var_rb.load() > 0 ? g_var_rb.load() : gemm_row_bytes();
+  p->var.bn = g_var_bn.load() > 0 ? g_var_bn.load() : 256;
+  p->var.split = g_var_split.load() > 0 ? std::min(g_var_split.load(), p->g.split_max) : 1;
+  p->var.pair = g_var_pair.load() == 1 && p->var.bn == 256 && p->var.split == 1 ? 1 : 2;
   st = plan_pipeline(p, p->stream, p->var);
   if (st == B200D2_OK) st = status_from_cuda(cudaStreamSynchronize(p->stream));
   if (st == B200D2_OK && (flags & B200D2_PLAN_AUTOTUNE)) {
@@ -1942,6 +1988,14 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
     if (!cached) {
       std::vector<GemmVariant> cand;
       const int sms = num_sms();
+      for (int rb : {64, 128}) {  // CTA-pair 256 x 256 tiles
+        GemmVariant v;
+        v.row_bytes = rb;
+        v.bn = 256;
+        v.split = 1;
+        v.pair = 1;
+        cand.push_back(v);
+      }
       for (int rb : {64, 128})
         for (int bn : {256, 128}) {
           const int nt = bn == 256 ? (int)tiles.size() : (int)tiles128.size();
@@ -1951,6 +2005,7 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
             v.row_bytes = rb;
             v.bn = bn;
             v.split = sp;
+            v.pair = 2;
             cand.push_back(v);
           }
         }
@@ -1963,6 +2018,7 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
           p->info.tuned_variant[n][0] = v.row_bytes;
           p->info.tuned_variant[n][1] = v.bn;
           p->info.tuned_variant[n][2] = v.split;
+          p->info.tuned_variant[n][3] = v.pair;
           p->info.tuned_ms[n] = ms;
           ++n;
         }
@@ -1982,6 +2038,7 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   p->info.row_bytes = p->var.row_bytes;
   p->info.tile_n = p->var.bn;
   p->info.split = p->var.split;
+  p->info.pair = p->var.pair == 1 ? 1 : 0;
   if (st == B200D2_OK && (flags & B200D2_PLAN_GRAPH)) {
     st = status_from_cuda(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
     if (st == B200D2_OK) {

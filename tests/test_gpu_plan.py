@@ -57,7 +57,7 @@ def test_uneven_plan_matches_fp64(pkg, synth, oracle, cuda, reorder):
     if info["n_tuned"]:
         assert info["n_tuned"] >= 4
         best = min(info["tuned"], key=lambda x: x[1])[0]
-        assert best == (info["row_bytes"], info["tile_n"], info["split"])
+        assert best == (info["row_bytes"], info["tile_n"], info["split"], 1 if info["pair"] else 2)
     assert 0 < info["tiles_n128"] <= 2 * info["tiles"]
     assert info["evals"] == sum(len(p["orient"]) * len(p["trans_x"]) for p in parts)
     assert 0 < info["tiles"] <= info["tiles_dense"]
@@ -109,3 +109,35 @@ def test_plan_uniform_matches_batch_api(pkg, synth, oracle, cuda):
         assert oracle.error_stats(parts[p]["diff2"].cpu().numpy(), ref[p])["max_rel"] <= 1e-6
     plan.close()
     proj.close()
+
+
+@pytest.mark.parametrize("variant", [(128, 256, 1, 1), (64, 128, 1, 2)])
+def test_uneven_plan_fixed_variants(pkg, synth, oracle, cuda, variant):
+    """Plans without the autotuner take the process-wide contraction variant:
+    CTA-pair 256 x 256 tiles and 128-wide single-CTA tiles on uneven work lists."""
+    torch = cuda
+    P = 5
+    pr, proj, view, eul, parts = _plan_case(pkg, synth, torch, P)
+    mn = torch.empty(P, device="cuda", dtype=torch.float64)
+    am = torch.empty(P, device="cuda", dtype=torch.int64)
+    pkg.set_gemm_variant(*variant)
+    try:
+        plan = pkg.Plan(view, eul, pr.O, pr.N_img, parts, pkg.PREC_BF16X3, flags=pkg.PLAN_GRAPH | pkg.PLAN_REORDER,
+                        out_min=mn, out_argmin=am)
+    finally:
+        pkg.set_gemm_variant(0, 0, 0, 0)
+    info = plan.info()
+    assert info["pair"] == (1 if variant[3] == 1 else 0) and info["tile_n"] == variant[1]
+    assert info["tiles_pair"] > 0
+    for pt in parts:
+        pt["diff2"].fill_(-7.0)
+    plan.run()
+    torch.cuda.synchronize()
+    for p, pt in enumerate(parts):
+        got = pt["diff2"].cpu().numpy()
+        ref = _fp64_particle(pkg, torch, view, pr, pt, p)
+        assert oracle.error_stats(got, ref)["max_rel"] <= TOL, p
+        assert am[p].item() == int(np.argmin(got))
+    plan.close()
+    proj.close()
+
