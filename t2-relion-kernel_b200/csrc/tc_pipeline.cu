@@ -101,7 +101,7 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, i
   g.terms = (prec == B200D2_PREC_TF32 || prec == B200D2_PREC_FP16) ? 1 : 3;
   g.Kpad = (int)align_up((size_t)std::max(2 * g.K_c, 1), (size_t)g.BK);
   g.Mrows = mrows >= 0 ? mrows : b.P * b.T;
-  g.Mpad = (int)align_up((size_t)g.Mrows, 256);  // whole 256-row tiles for the CTA-pair contraction
+  g.Mpad = (int)align_up((size_t)g.Mrows, 128);
   g.Opad = (int)align_up((size_t)b.O, 256);
   g.maxR = extent;  // phase tables cover x in [0, extent], y in [-extent, extent]
   g.exw = extent + 1;
@@ -1403,7 +1403,7 @@ static int launch_gemm_pair(const b200d2_batch& b, const TcGeom& g, void* ws, cu
   GemmArgs a;
   memset(&a, 0, sizeof(a));
   a.Mrows = g.Mrows;
-  a.Mtiles = g.Mpad / 256;
+  a.Mtiles = (g.Mpad + 255) / 256;  // a last half tile reads rows past Mpad as zeros (TMA fill)
   a.Ntiles = g.Opad / 256;
   a.O = g.O;
   a.T = g.T;
@@ -1455,7 +1455,7 @@ static int launch_gemm(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStr
   // GPU (one tile per pair of SMs at least); their default rows are 128 bytes
   bool pair = var.pair == 1;
   if (var.pair == 0 && !U && (var.bn <= 0 || var.bn == 256) && var.split <= 1)
-    pair = (long long)(g.Mpad / 256) * (g.Opad / 256) >= num_sms() / 2;
+    pair = (long long)((g.Mpad + 255) / 256) * (g.Opad / 256) >= num_sms() / 2;
   if (pair && (var.bn <= 0 || var.bn == 256) && var.split <= 1) {
     const int prb = var.row_bytes > 0 ? var.row_bytes : 128;
     return prb == 128 ? launch_gemm_pair<PREC, 128>(b, g, ws, s, U) : launch_gemm_pair<PREC, 64>(b, g, ws, s, U);
