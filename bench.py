@@ -170,6 +170,8 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="c5: length of the arrival trace")
     ap.add_argument("--serve-fp32-seconds", type=float, default=0.5,
                     help="c5: part of the trace replayed through the FP32 baseline")
+    ap.add_argument("--combine", default="df32", choices=["df32", "fp64"],
+                    help="final combination nA - 2 cross: double-float (default) or FP64")
     ap.add_argument("--gemm-variant", default=None,
                     help="row_bytes,tile_n,split,pair for the contraction (0 = default; pair 1 = CTA pairs)")
     ap.add_argument("--study", default=None, choices=["precision"],
@@ -265,6 +267,7 @@ def ours_arm(args):
     dev = torch.device("cuda", local)
     if args.gemm_variant:
         pkg.set_gemm_variant(*[int(x) for x in args.gemm_variant.split(",")])
+    pkg.set_combine(pkg.COMBINE_FP64 if args.combine == "fp64" else pkg.COMBINE_DF32)
     stream = torch.cuda.current_stream()
 
     proj = pkg.Projector(pr.projector, use_texture=1)
@@ -440,7 +443,8 @@ def ours_arm(args):
                                        if uneven else
                                        (f"{args.config}: {P} particles x {O} orientations x {T} translations, "
                                         f"image {pr.img_size} ({N} px, {K_c} in radius)"),
-                           "precision": args.precision, "particles": P, "orientations": O, "translations": T,
+                           "precision": args.precision, "combine": args.combine,
+                           "particles": P, "orientations": O, "translations": T,
                            "pixels_in_radius": K_c, "l2": "flushed (256 MB write) before every timed step",
                            "parallelism": f"replicas x{world}", **plan_extra},
                 "roofline": roof, "cpu_baseline": cpu,

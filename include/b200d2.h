@@ -382,6 +382,16 @@ int b200d2_coarse_weights(const float* d_diff2, int P, int O, int T,
                           double* d_weights, double* d_sum, void* d_workspace,
                           size_t workspace_bytes, void* stream);
 
+/* Final combination diff2 = nA - 2 cross of the tensor-core forms, where nA =
+ * sum w|X|^2 + sum w|A|^2 is accumulated in FP64 and cross comes from the
+ * FP32 tensor-core accumulator.  B200D2_COMBINE_DF32 (default): nA is kept as
+ * an unevaluated sum of two floats (48-bit significand) and the combine is
+ * one FMA and one add, within 2 ulp of the FP64 combine rounded to FP32;
+ * B200D2_COMBINE_FP64: FP64 arithmetic, rounded once.  Process-wide; read
+ * when a contraction is launched (plans capture it in their graph). */
+enum { B200D2_COMBINE_DF32 = 0, B200D2_COMBINE_FP64 = 1 };
+int b200d2_set_combine(int mode);
+
 /* Contraction variant used by the tensor-core batch entry points
  * (b200d2_diff2_coarse_batch, _stage, _static and the server), process-wide:
  * row_bytes 64 or 128 (k-block row width), tile_n 256 or 128 (orientations

@@ -154,6 +154,7 @@ def _declare(L):
         "b200d2_server_destroy": [P],
         "b200d2_coarse_weights": [P, I, I, I, P, P, P, I, P, P, P, Z, P],
         "b200d2_set_gemm_variant": [I, I, I, I],
+        "b200d2_set_combine": [I],
         "b200d2_ctf_fold": [P, P, C.c_longlong, I, I, I, I, I, I, F, P, P, C.c_longlong, P, P, P, P],
     }
     for name, args in sig.items():
@@ -499,6 +500,16 @@ def ctf_fold(real, imag, ctf_params: list, minvsigma2, *, imgX: int, imgY: int, 
     else:
         stream.synchronize()
     return out_real, out_imag, out_corr
+
+
+COMBINE_DF32 = 0
+COMBINE_FP64 = 1
+
+
+def set_combine(mode: int) -> None:
+    """Final combination of the tensor-core forms: COMBINE_DF32 (default,
+    double-float) or COMBINE_FP64."""
+    _check(lib().b200d2_set_combine(mode), "set_combine")
 
 
 def set_gemm_variant(row_bytes: int = 0, tile_n: int = 0, split: int = 0, pair: int = 0) -> None:

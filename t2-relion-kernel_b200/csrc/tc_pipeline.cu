@@ -50,7 +50,7 @@ struct TcGeom {
   int P, O, T, N_img, K_c, Kpad, Mrows, Mpad, Opad, maxR, exw, eyw;
   int elem, BK, terms;
   int Kq;  // row stride (doubles) of |B|^2 and of the compacted weights: Kpad / 2, zero padded
-  size_t off_status, off_xy, off_idx, off_ex, off_ey, off_bhi, off_blo, off_q, off_w, off_normx, off_na,
+  size_t off_status, off_xy, off_idx, off_ex, off_ey, off_bhi, off_blo, off_q, off_w, off_normx, off_na, off_nahl,
       off_ahi, off_alo, off_keys, off_sa, off_sb, off_part, off_cnt, total;
   int split_max;  // largest k-split the workspace holds partial sums for
   int n_cnt;      // split arrival counters
@@ -125,6 +125,7 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, i
   g.off_w = take(sizeof(double) * (size_t)g.P * g.Kq);
   g.off_normx = take(sizeof(double) * (size_t)g.P);
   g.off_na = take(sizeof(double) * (size_t)g.P * g.O);
+  g.off_nahl = take(sizeof(float2) * (size_t)g.P * g.O);  // nA as an unevaluated sum hi + lo of two floats
   g.off_ahi = take((size_t)g.Mpad * g.Kpad * g.elem);
   g.off_alo = planes == 2 ? take((size_t)g.Mpad * g.Kpad * g.elem) : g.off_ahi;
   g.off_keys = take(sizeof(unsigned long long) * (size_t)g.P);
@@ -476,7 +477,8 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
 template <int WM>
 __global__ void __launch_bounds__(128) tc_norma_kernel(const double* __restrict__ wcomp, int Kq,
                                                        const double* __restrict__ q, int O, int P,
-                                                       const double* __restrict__ normx, double* na) {
+                                                       const double* __restrict__ normx, double* na,
+                                                       float2* na_hl) {
   // Kq: row stride of wcomp and q, a multiple of 16, zero padded.  Shared
   // rows padded to 20 doubles (160 B, 16-byte aligned): the fragment loads
   // of a half-warp (rows g, columns t, g, t < 4) fall on distinct bank pairs
@@ -541,7 +543,12 @@ __global__ void __launch_bounds__(128) tc_norma_kernel(const double* __restrict_
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int o = o0 + wo0 + 8 * j + 2 * tig + h;
-        if (o < O) na[(size_t)p * O + o] = normx[p] + acc[i][j][h];
+        if (o < O) {
+          const double v = normx[p] + acc[i][j][h];
+          na[(size_t)p * O + o] = v;
+          const float hi = (float)v;  // v = hi + lo to 48 bits: the combine's double-float operand
+          na_hl[(size_t)p * O + o] = make_float2(hi, (float)(v - (double)hi));
+        }
       }
   }
 }
@@ -658,6 +665,8 @@ struct GemmArgs {
   int split;    // k-splits per tile (>= 1)
   float* out;
   const double* na;
+  const float2* na_hl;  // nA = hi + lo (double-float)
+  int combine64;        // 1: FP64 combine; 0: double-float combine
   unsigned long long* keys;
   uint32_t* status;
   const float* inv_sa;  // FP16 forms: [P] 1 / particle scale
@@ -772,6 +781,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   if (warp == 0) {
     // ------------------------------------------------ TMA producer
     if (lane == 0) {
+      // projections (B) are re-read by every m-tile: keep them in L2
+      const uint64_t keep = sm100::policy_evict_last();
       uint32_t gk = 0;
       bool ok = true;
       for (int item = blockIdx.x; item < num_items && ok; item += gridDim.x) {
@@ -793,8 +804,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
           sm100::tma_load_2d(st, &mAhi, &full[s], kc, m0);
           if (C::kPlanes == 2) sm100::tma_load_2d(st + C::kATile, &mAlo, &full[s], kc, m0);
           uint8_t* sb = st + C::kPlanes * C::kATile;
-          sm100::tma_load_2d(sb, &mBhi, &full[s], kc, n0);
-          if (C::kPlanes == 2) sm100::tma_load_2d(sb + C::kBTile, &mBlo, &full[s], kc, n0);
+          sm100::tma_load_2d_hint(sb, &mBhi, &full[s], kc, n0, keep);
+          if (C::kPlanes == 2) sm100::tma_load_2d_hint(sb + C::kBTile, &mBlo, &full[s], kc, n0, keep);
         }
       }
       // let the copies in flight land before the CTA can exit
@@ -891,21 +902,33 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         }
       }
       const double* __restrict__ na_row = g.na + (size_t)p * g.O;
+      const float2* __restrict__ nh_row = g.na_hl + (size_t)p * g.O;
       float* __restrict__ out_row = outp + t;
       // FP16 forms: -2 / (particle scale); the orientation scale is per column
       const double m2s = C::kScaled ? -2.0 * (double)g.inv_sa[vrow ? p : 0] : -2.0;
+      const float m2f = (float)m2s;  // a power of two: exact
       float best = __int_as_float(0x7f800000);
       uint32_t best_idx = 0xffffffffu;
-      // FP64 combine of one accumulator value, store and running minimum
-      auto consume = [&](int o, double cr) {
+      // Combine of one accumulator value c: diff2 = nA - 2c, store and running
+      // minimum.  nA carries 48 bits (FP64 norms); the default double-float
+      // form rounds nA_hi - 2c once (FMA) and adds nA_lo, within 2 ulp of the
+      // FP64 combine rounded to FP32, at a tenth of its cost on this GPU.
+      auto consume = [&](int o, float c) {
         const int lo = (o < g.O) ? (inv ? inv[o] : o) : -1;
         if (lo < 0) return;
-        if (C::kScaled) cr *= (double)g.inv_sb[o];
-        const double dd = fma(m2s, cr, na_row[o]);
-        float f = (float)dd;
+        float f;
+        if (g.combine64) {
+          double cr = (double)c;
+          if (C::kScaled) cr *= (double)g.inv_sb[o];
+          f = (float)fma(m2s, cr, na_row[o]);
+        } else {
+          const float2 nh = nh_row[o];
+          const float sc = C::kScaled ? m2f * g.inv_sb[o] : m2f;  // product of powers of two: exact
+          f = __fadd_rn(__fmaf_rn(sc, c, nh.x), nh.y);
+        }
         float* dst = out_row + (size_t)lo * Tp;
-        if (g.accumulate) f += *dst;
-        *dst = f;
+        if (g.accumulate) f += __ldcs(dst);
+        __stcs(dst, f);  // streamed: the output must not evict the operands from L2
         if (f < best) {
           best = f;
           best_idx = (uint32_t)(lo * Tp + t);
@@ -921,7 +944,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
           sm100::tmem_ld_wait();
           if (vrow)
 #pragma unroll
-            for (int j = 0; j < 32; ++j) consume(n0 + c * 32 + j, (double)__uint_as_float(r[j]));
+            for (int j = 0; j < 32; ++j) consume(n0 + c * 32 + j, __uint_as_float(r[j]));
         }
         sm100::tc_fence_before();
         sm100::mbar_arrive(&acce[b]);
@@ -953,7 +976,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
             for (int col = 0; col < C::kBN; ++col) {
               double acc = 0.0;
               for (int s2 = 0; s2 < g.split; ++s2) acc += (double)__ldcg(base + ((size_t)s2 * C::kBN + col) * 128);
-              consume(n0 + col, acc);
+              consume(n0 + col, (float)acc);
             }
           }
           __syncwarp();
@@ -1075,6 +1098,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
   if (warp == 0) {
     // ------------------------------------------------ TMA producer (both CTAs)
     if (lane == 0) {
+      const uint64_t keep = sm100::policy_evict_last();  // B is re-read by every m-tile
       uint32_t gk = 0;
       bool ok = true;
       for (int tile = cl; tile < num_tiles && ok; tile += ncl) {
@@ -1095,8 +1119,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
           sm100::tma_load_2d_pair(st, &mAhi, fb, kc, m0 + 128 * (int)rank);
           if (C::kPlanes == 2) sm100::tma_load_2d_pair(st + C::kATile, &mAlo, fb, kc, m0 + 128 * (int)rank);
           uint8_t* sb = st + C::kPlanes * C::kATile;
-          sm100::tma_load_2d_pair(sb, &mBhi, fb, kc, n0 + 128 * (int)rank);
-          if (C::kPlanes == 2) sm100::tma_load_2d_pair(sb + C::kBTile, &mBlo, fb, kc, n0 + 128 * (int)rank);
+          sm100::tma_load_2d_pair_hint(sb, &mBhi, fb, kc, n0 + 128 * (int)rank, keep);
+          if (C::kPlanes == 2) sm100::tma_load_2d_pair_hint(sb + C::kBTile, &mBlo, fb, kc, n0 + 128 * (int)rank, keep);
         }
       }
       // the even CTA's full barriers count both CTAs' bytes: let every copy
@@ -1193,8 +1217,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
         }
       }
       const double* __restrict__ na_row = g.na + (size_t)p * g.O;
+      const float2* __restrict__ nh_row = g.na_hl + (size_t)p * g.O;
       float* __restrict__ out_row = outp + t;
       const double m2s = C::kScaled ? -2.0 * (double)g.inv_sa[p] : -2.0;
+      const float m2f = (float)m2s;
       float best = __int_as_float(0x7f800000);
       uint32_t best_idx = 0xffffffffu;
 #pragma unroll 1
@@ -1209,12 +1235,20 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
             const int o = n0 + c * 32 + j;
             const int lo = (o < g.O) ? (inv ? inv[o] : o) : -1;
             if (lo >= 0) {
-              double cr = (double)__uint_as_float(r[j]);
-              if (C::kScaled) cr *= (double)g.inv_sb[o];
-              float f = (float)fma(m2s, cr, na_row[o]);
+              const float c = __uint_as_float(r[j]);
+              float f;
+              if (g.combine64) {  // FP64 combine
+                double cr = (double)c;
+                if (C::kScaled) cr *= (double)g.inv_sb[o];
+                f = (float)fma(m2s, cr, na_row[o]);
+              } else {  // double-float combine (see tc_gemm_kernel)
+                const float2 nh = nh_row[o];
+                const float sc = C::kScaled ? m2f * g.inv_sb[o] : m2f;
+                f = __fadd_rn(__fmaf_rn(sc, c, nh.x), nh.y);
+              }
               float* dst = out_row + (size_t)lo * Tp;
-              if (g.accumulate) f += *dst;
-              *dst = f;
+              if (g.accumulate) f += __ldcs(dst);
+              __stcs(dst, f);  // streamed: the output must not evict the operands from L2
               if (f < best) {
                 best = f;
                 best_idx = (uint32_t)(lo * Tp + t);
@@ -1314,6 +1348,7 @@ struct GemmVariant {
 // Process-wide variant of the batch entry points (b200d2_set_gemm_variant);
 // plans carry their own.
 static std::atomic<int> g_var_rb{0}, g_var_bn{0}, g_var_split{0}, g_var_pair{0};
+static std::atomic<int> g_combine64{0};  // b200d2_set_combine
 
 // k-splits for `tiles` tiles of KB k-blocks: 1 when the tiles fill the GPU,
 // else the largest power of two (<= cap) keeping two work items per SM at
@@ -1366,6 +1401,8 @@ static int launch_gemm_v(const b200d2_batch& b, const TcGeom& g, void* ws, cudaS
   a.split = std::max(1, std::min(a.split, a.KB));
   a.out = b.d_diff2;
   a.na = ws_at<double>(ws, g.off_na);
+  a.na_hl = ws_at<float2>(ws, g.off_nahl);
+  a.combine64 = g_combine64.load();
   a.keys = ws_at<unsigned long long>(ws, g.off_keys);
   a.status = ws_at<uint32_t>(ws, g.off_status);
   a.inv_sa = ws_at<float>(ws, g.off_sa);
@@ -1420,6 +1457,8 @@ static int launch_gemm_pair(const b200d2_batch& b, const TcGeom& g, void* ws, cu
   }
   a.out = b.d_diff2;
   a.na = ws_at<double>(ws, g.off_na);
+  a.na_hl = ws_at<float2>(ws, g.off_nahl);
+  a.combine64 = g_combine64.load();
   a.keys = ws_at<unsigned long long>(ws, g.off_keys);
   a.status = ws_at<uint32_t>(ws, g.off_status);
   a.inv_sa = ws_at<float>(ws, g.off_sa);
@@ -1483,6 +1522,7 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
   double* wcomp = ws_at<double>(ws, g.off_w);
   double* normx = ws_at<double>(ws, g.off_normx);
   double* na = ws_at<double>(ws, g.off_na);
+  float2* na_hl = ws_at<float2>(ws, g.off_nahl);
   void* ahi = ws_at<void>(ws, g.off_ahi);
   void* alo = ws_at<void>(ws, g.off_alo);
   unsigned long long* keys = ws_at<unsigned long long>(ws, g.off_keys);
@@ -1524,11 +1564,11 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       const long long otiles = (g.O + 63) / 64;
       const int sms = num_sms();
       if (otiles * ((g.P + 63) / 64) >= sms) {
-        tc_norma_kernel<4><<<dim3(otiles, (g.P + 63) / 64), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na);
+        tc_norma_kernel<4><<<dim3(otiles, (g.P + 63) / 64), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl);
       } else if (otiles * ((g.P + 31) / 32) >= sms) {
-        tc_norma_kernel<2><<<dim3(otiles, (g.P + 31) / 32), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na);
+        tc_norma_kernel<2><<<dim3(otiles, (g.P + 31) / 32), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl);
       } else {
-        tc_norma_kernel<1><<<dim3(otiles, (g.P + 15) / 16), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na);
+        tc_norma_kernel<1><<<dim3(otiles, (g.P + 15) / 16), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl);
       }
       break;
     }
@@ -2099,5 +2139,11 @@ extern "C" int b200d2_set_gemm_variant(int row_bytes, int tile_n, int split, int
   b200d2::g_var_bn.store(tile_n);
   b200d2::g_var_split.store(split);
   b200d2::g_var_pair.store(pair);
+  return B200D2_OK;
+}
+
+extern "C" int b200d2_set_combine(int mode) {
+  if (mode != B200D2_COMBINE_DF32 && mode != B200D2_COMBINE_FP64) return B200D2_ERR_INVALID;
+  b200d2::g_combine64.store(mode == B200D2_COMBINE_FP64 ? 1 : 0);
   return B200D2_OK;
 }

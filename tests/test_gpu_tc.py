@@ -182,3 +182,28 @@ def test_tc_pair_tiles_c2_subset(pkg, synth, oracle, cuda, name):
         pkg.set_gemm_variant(0, 0, 0, 0)
     proj.close()
 
+
+@pytest.mark.parametrize("case,variant", [("c1", (0, 0, 0, 0)), ("c1", (64, 256, 1, 2)), ("c2", (0, 0, 1, 1))])
+def test_combine_df32_matches_fp64_combine(pkg, synth, oracle, cuda, case, variant):
+    """The double-float combine (nA as hi + lo floats, one FMA and one add)
+    stays within 2 ulp of the FP64 combine rounded to FP32, on the split-K,
+    single-CTA and CTA-pair contractions."""
+    pr = synth.make_problem(case, P=5 if case == "c2" else None, orient_limit=700 if case == "c2" else None)
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dp = DeviceProblem(cuda, pr)
+    pkg.set_gemm_variant(*variant)
+    try:
+        pkg.set_combine(pkg.COMBINE_FP64)
+        d64, mn64, am64 = run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3)
+        pkg.set_combine(pkg.COMBINE_DF32)
+        d32, mn32, am32 = run_tc(pkg, cuda, view, dp, pkg.PREC_BF16X3)
+    finally:
+        pkg.set_combine(pkg.COMBINE_DF32)
+        pkg.set_gemm_variant(0, 0, 0, 0)
+    ulp = np.spacing(np.abs(d64).astype(np.float32))
+    assert np.all(np.abs(d32.astype(np.float64) - d64) <= 2 * ulp)
+    ref = fp64_all(pkg, view, dp)
+    assert oracle.error_stats(d32, ref)["max_rel"] <= TOL["bf16x3"]
+    proj.close()
+
