@@ -54,8 +54,8 @@ enum {
   B200D2_PREC_FP64 = 4,    /* FP64 CUDA-core kernel (GPU oracle) */
   /* FP16 operands with power-of-two scales: every particle's weighted image
    * and every orientation's projection are scaled so that their largest
-   * component lies in [2^13, 2^14); the scales are undone exactly in the FP64
-   * combine. */
+   * component lies in [2^13, 2^14); the scales are undone exactly in the
+   * final combination. */
   B200D2_PREC_FP16 = 5,    /* one scaled FP16 product */
   B200D2_PREC_FP16X3 = 6   /* hi*hi + hi*lo + lo*hi scaled FP16 split */
 };
@@ -322,7 +322,7 @@ int b200d2_server_destroy(b200d2_server* s);
  * b200d2_diff2_coarse_batch_workspace exceeds that size is rejected with
  * B200D2_ERR_TOO_LARGE before anything runs (64 MiB holds, for example, 8
  * particles x 576 orientations x 21 translations at image 32, or 16
- * particles x 1536 orientations x 113 translations at image 64).  The
+ * particles x 1024 orientations x 113 translations at image 64).  The
  * scratch address is looked up on the first call on each device: make that
  * call before any stream capture.  Calls share the scratch, so calls that
  * overlap on the GPU race; serialise them.  Runs all stages on `stream`. */

@@ -142,7 +142,7 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, i
       while (g.split_max * 2 <= 8 && (long long)tiles256 * g.split_max * 2 <= 2LL * sms && kb / (g.split_max * 2) >= 2)
         g.split_max *= 2;
     g.off_part = take(g.split_max > 1 ? (size_t)g.split_max * tiles256 * 256 * 128 * sizeof(float) : 0);
-    g.n_cnt = 4 * mt * (g.Opad / 128);
+    g.n_cnt = 8 * mt * (g.Opad / 128);  // per (tile, column half, lane quadrant) of 128-wide tiles
     g.off_cnt = take(sizeof(unsigned) * (size_t)g.n_cnt);
   }
   g.total = o;
@@ -672,7 +672,7 @@ struct GemmArgs {
   const float* inv_sa;  // FP16 forms: [P] 1 / particle scale
   const float* inv_sb;  // FP16 forms: [Opad] 1 / orientation scale
   float* part;          // split > 1: [tiles * split][BN][128] FP32 partial sums
-  unsigned* cnt;        // split > 1: [tiles][4] arrivals per (tile, TMEM lane quadrant)
+  unsigned* cnt;        // split > 1: [tiles][8] arrivals per (tile, column half, TMEM lane quadrant)
   Layout L;  // uneven batch tables (all null for a uniform batch)
 };
 
@@ -714,6 +714,88 @@ __device__ __forceinline__ float from_ordered(uint32_t k) {
 
 constexpr uint64_t kWaitLimitNs = 4000000000ull;  // 4 s
 
+// Epilogue warps of the contraction kernels: two per TMEM lane quadrant, each
+// draining half of the accumulator's columns.
+constexpr int kEpiWarps = 8;
+constexpr int kGemmThreads = 64 + 32 * kEpiWarps;  // TMA warp, MMA warp, epilogue warps
+
+// One row of a tile in the epilogue: where its diff2 values go and what they
+// combine with.
+struct EpiRow {
+  float* out_row;          // diff2 of (particle, translation) at orientation list index 0
+  const double* na_row;    // FP64 nA of the particle, per orientation
+  const float2* nh_row;    // the same as hi + lo floats
+  const int* inv;          // orientation -> list index of the particle (uneven batches), or null
+  int Tp, t;               // translations of the particle, this row's translation
+  double m2s;              // -2 / (particle scale of the FP16 forms), else -2
+  float m2f;
+};
+
+// Combine one accumulator value c of orientation o: diff2 = nA - 2c, stored,
+// with the running minimum (value and orientation list index).  nA carries 48
+// bits (FP64 norms); the default double-float form rounds nA_hi - 2c once
+// (FMA) and adds nA_lo, within 2 ulp of the FP64 combine rounded to FP32, at
+// about a tenth of its cost on this GPU.
+template <bool SCALED>
+__device__ __forceinline__ void epi_combine(const GemmArgs& g, const EpiRow& x, int o, float c, float& best,
+                                            int& best_lo) {
+  const int lo = (o < g.O) ? (x.inv ? x.inv[o] : o) : -1;
+  if (lo < 0) return;
+  float f;
+  if (g.combine64) {
+    double cr = (double)c;
+    if (SCALED) cr *= (double)g.inv_sb[o];
+    f = (float)fma(x.m2s, cr, x.na_row[o]);
+  } else {
+    const float2 nh = x.nh_row[o];
+    const float sc = SCALED ? x.m2f * g.inv_sb[o] : x.m2f;  // product of powers of two: exact
+    f = __fadd_rn(__fmaf_rn(sc, c, nh.x), nh.y);
+  }
+  float* dst = x.out_row + (size_t)lo * x.Tp;
+  if (g.accumulate) f += __ldcs(dst);
+  __stcs(dst, f);  // streamed: the output must not evict the operands from L2
+  if (f < best) {
+    best = f;
+    best_lo = lo;
+  }
+}
+
+// Drain NCH 32-column chunks of one TMEM lane quadrant starting at `taddr`
+// (orientations from o0) into diff2.  `fast`: a uniform batch whose columns
+// all exist, overwritten, double-float combine (no per-element branches).
+template <bool SCALED, int NCH>
+__device__ __forceinline__ void epi_drain(const GemmArgs& g, const EpiRow& x, uint32_t taddr, int o0, bool vrow,
+                                          bool fast, float& best, int& best_lo) {
+  uint32_t ra[32];
+  auto use = [&](const uint32_t (&r)[32], int oc) {
+    if (!vrow) return;
+    if (fast) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int o = oc + j;
+        const float2 nh = x.nh_row[o];
+        const float sc = SCALED ? x.m2f * g.inv_sb[o] : x.m2f;
+        const float f = __fadd_rn(__fmaf_rn(sc, __uint_as_float(r[j]), nh.x), nh.y);
+        __stcs(x.out_row + (size_t)o * x.Tp, f);
+        if (f < best) {
+          best = f;
+          best_lo = o;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) epi_combine<SCALED>(g, x, oc + j, __uint_as_float(r[j]), best, best_lo);
+    }
+  };
+#pragma unroll 1
+  for (int c = 0; c < NCH; ++c) {
+    __syncwarp();
+    sm100::tmem_ld_32x32b_x32(taddr + (uint32_t)(c * 32), ra);
+    sm100::tmem_ld_wait_regs(ra);
+    use(ra, o0 + c * 32);
+  }
+}
+
 // Persistent contraction.  Work items are (tile, k-split) pairs, item =
 // tile * split + s, handed out round-robin over the grid.  Warp 0 streams the
 // operand k-blocks with TMA into a ring of shared-memory stages, warp 1 issues
@@ -723,7 +805,7 @@ constexpr uint64_t kWaitLimitNs = 4000000000ull;  // 4 s
 // last split to arrive for a (tile, quadrant) adds all partials in split order
 // (FP64) and combines, so the result does not depend on arrival order.
 template <int PREC, int ROWB, int BN>
-__global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap mAhi,
+__global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap mAhi,
                                                          const __grid_constant__ CUtensorMap mAlo,
                                                          const __grid_constant__ CUtensorMap mBhi,
                                                          const __grid_constant__ CUtensorMap mBlo,
@@ -747,7 +829,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     }
     for (int b = 0; b < 2; ++b) {
       sm100::mbar_init(&accf[b], 1);
-      sm100::mbar_init(&acce[b], 128);
+      sm100::mbar_init(&acce[b], 32 * kEpiWarps);
     }
     sm100::mbar_init(drain, 1);
     *s_abort = 0;
@@ -863,9 +945,13 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       if (!sm100::mbar_wait_bounded(drain, 0, s_abort, kWaitLimitNs)) raise_abort();
     }
   } else {
-    // ------------------------------------------------ epilogue (warps 2..5)
-    const int qd = warp & 3;  // TMEM lane quadrant this warp may access
+    // ------------------------------------------------ epilogue (warps 2..9)
+    // warp w may read TMEM lanes 32 (w % 4) .. +31; warps 2-5 drain the
+    // first half of the columns, warps 6-9 the second half
+    const int qd = warp & 3;
+    const int half = (warp - 2) >> 2;
     const int row = qd * 32 + lane;
+    constexpr int kCols = C::kBN / 2;  // columns per epilogue warp
     int i = 0;
     for (int item = blockIdx.x; item < num_items; item += gridDim.x, ++i) {
       const int b = i & 1;
@@ -883,80 +969,52 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       tile_origin(g, tile, C::kBM, C::kBN, m0, n0);
       const int m = m0 + row;
       const bool vrow = m < g.Mrows;
-      int p = 0, t = 0, Tp = g.T;
-      float* outp = g.out;
-      const int* __restrict__ inv = nullptr;  // orientation -> this particle's list index
+      int p = 0;
+      EpiRow x;
+      x.t = 0;
+      x.Tp = g.T;
+      x.out_row = g.out;
+      x.inv = nullptr;
       if (vrow) {
         if (g.L.rows) {
           const int4 rw = g.L.rows[m];
           p = rw.x;
-          t = rw.y;
+          x.t = rw.y;
           const PartDev& pd = g.L.parts[p];
-          Tp = pd.T;
-          outp = pd.out;
-          inv = pd.inv;
+          x.Tp = pd.T;
+          x.out_row = pd.out;
+          x.inv = pd.inv;
         } else {
           p = m / g.T;
-          t = m - p * g.T;
-          outp = g.out + (size_t)p * g.O * g.T;
+          x.t = m - p * g.T;
+          x.out_row = g.out + (size_t)p * g.O * g.T;
         }
       }
-      const double* __restrict__ na_row = g.na + (size_t)p * g.O;
-      const float2* __restrict__ nh_row = g.na_hl + (size_t)p * g.O;
-      float* __restrict__ out_row = outp + t;
+      x.out_row += x.t;
+      x.na_row = g.na + (size_t)p * g.O;
+      x.nh_row = g.na_hl + (size_t)p * g.O;
       // FP16 forms: -2 / (particle scale); the orientation scale is per column
-      const double m2s = C::kScaled ? -2.0 * (double)g.inv_sa[vrow ? p : 0] : -2.0;
-      const float m2f = (float)m2s;  // a power of two: exact
+      x.m2s = C::kScaled ? -2.0 * (double)g.inv_sa[p] : -2.0;
+      x.m2f = (float)x.m2s;  // a power of two: exact
+      const int o0 = n0 + half * kCols;
+      const bool fast = !x.inv && !g.accumulate && !g.combine64 && o0 + kCols <= g.O;
       float best = __int_as_float(0x7f800000);
-      uint32_t best_idx = 0xffffffffu;
-      // Combine of one accumulator value c: diff2 = nA - 2c, store and running
-      // minimum.  nA carries 48 bits (FP64 norms); the default double-float
-      // form rounds nA_hi - 2c once (FMA) and adds nA_lo, within 2 ulp of the
-      // FP64 combine rounded to FP32, at a tenth of its cost on this GPU.
-      auto consume = [&](int o, float c) {
-        const int lo = (o < g.O) ? (inv ? inv[o] : o) : -1;
-        if (lo < 0) return;
-        float f;
-        if (g.combine64) {
-          double cr = (double)c;
-          if (C::kScaled) cr *= (double)g.inv_sb[o];
-          f = (float)fma(m2s, cr, na_row[o]);
-        } else {
-          const float2 nh = nh_row[o];
-          const float sc = C::kScaled ? m2f * g.inv_sb[o] : m2f;  // product of powers of two: exact
-          f = __fadd_rn(__fmaf_rn(sc, c, nh.x), nh.y);
-        }
-        float* dst = out_row + (size_t)lo * Tp;
-        if (g.accumulate) f += __ldcs(dst);
-        __stcs(dst, f);  // streamed: the output must not evict the operands from L2
-        if (f < best) {
-          best = f;
-          best_idx = (uint32_t)(lo * Tp + t);
-        }
-      };
-      bool mine = true;  // this warp's rows are combined by this item
+      int best_lo = -1;
+      bool mine = true;  // this warp's rows and columns are combined by this item
+      const uint32_t taddr = tmem + (uint32_t)(b * C::kBN + half * kCols) + ((uint32_t)(qd * 32) << 16);
       if (g.split == 1) {
-#pragma unroll 1
-        for (int c = 0; c < C::kBN / 32; ++c) {
-          uint32_t r[32];
-          __syncwarp();
-          sm100::tmem_ld_32x32b_x32(tmem + (uint32_t)(b * C::kBN + c * 32) + ((uint32_t)(qd * 32) << 16), r);
-          sm100::tmem_ld_wait();
-          if (vrow)
-#pragma unroll
-            for (int j = 0; j < 32; ++j) consume(n0 + c * 32 + j, __uint_as_float(r[j]));
-        }
+        epi_drain<C::kScaled, kCols / 32>(g, x, taddr, o0, vrow, fast, best, best_lo);
         sm100::tc_fence_before();
         sm100::mbar_arrive(&acce[b]);
       } else {
         // store this split's partial: [item][column][row], coalesced over rows
-        float* part = g.part + (size_t)item * C::kBN * 128 + row;
+        float* part = g.part + (size_t)item * C::kBN * 128 + (size_t)(half * kCols) * 128 + row;
 #pragma unroll 1
-        for (int c = 0; c < C::kBN / 32; ++c) {
+        for (int c = 0; c < kCols / 32; ++c) {
           uint32_t r[32];
           __syncwarp();
-          sm100::tmem_ld_32x32b_x32(tmem + (uint32_t)(b * C::kBN + c * 32) + ((uint32_t)(qd * 32) << 16), r);
-          sm100::tmem_ld_wait();
+          sm100::tmem_ld_32x32b_x32(taddr + (uint32_t)(c * 32), r);
+          sm100::tmem_ld_wait_regs(r);
 #pragma unroll
           for (int j = 0; j < 32; ++j) part[(size_t)(c * 32 + j) * 128] = __uint_as_float(r[j]);
         }
@@ -964,8 +1022,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         sm100::mbar_arrive(&acce[b]);
         __threadfence();
         __syncwarp();
+        const int ci = tile * 8 + half * 4 + qd;  // arrivals per (tile, column half, lane quadrant)
         unsigned last = 0;
-        if (lane == 0) last = atomicAdd(&g.cnt[tile * 4 + qd], 1u) == (unsigned)(g.split - 1) ? 1u : 0u;
+        if (lane == 0) last = atomicAdd(&g.cnt[ci], 1u) == (unsigned)(g.split - 1) ? 1u : 0u;
         last = __shfl_sync(0xffffffffu, last, 0);
         mine = last != 0;
         if (mine) {
@@ -973,14 +1032,14 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
           const float* base = g.part + (size_t)tile * g.split * C::kBN * 128 + row;
           if (vrow) {
 #pragma unroll 1
-            for (int col = 0; col < C::kBN; ++col) {
+            for (int col = half * kCols; col < (half + 1) * kCols; ++col) {
               double acc = 0.0;
               for (int s2 = 0; s2 < g.split; ++s2) acc += (double)__ldcg(base + ((size_t)s2 * C::kBN + col) * 128);
-              consume(n0 + col, (float)acc);
+              epi_combine<C::kScaled>(g, x, n0 + col, (float)acc, best, best_lo);
             }
           }
           __syncwarp();
-          if (lane == 0) g.cnt[tile * 4 + qd] = 0;  // ready for the next launch
+          if (lane == 0) g.cnt[ci] = 0;  // ready for the next launch
         }
       }
       if (mine) {
@@ -988,7 +1047,9 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         // are contiguous, so a segmented shuffle-down min leaves each run's
         // minimum in its first lane, which alone issues the atomic.
         unsigned long long key =
-            (vrow && best_idx != 0xffffffffu) ? (((unsigned long long)ordered_bits(best) << 32) | best_idx) : ~0ull;
+            (vrow && best_lo >= 0)
+                ? (((unsigned long long)ordered_bits(best) << 32) | (uint32_t)(best_lo * x.Tp + x.t))
+                : ~0ull;
         const int pk = vrow ? p : -1;
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
@@ -1036,7 +1097,7 @@ struct GemmCfgPair {
 };
 
 template <int PREC, int ROWB>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
     tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
                         const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo,
                         const GemmArgs g) {
@@ -1061,7 +1122,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
     }
     for (int b = 0; b < 2; ++b) {
       sm100::mbar_init(&accf[b], 1);
-      sm100::mbar_init(&acce[b], 256);  // even CTA: the epilogue threads of both CTAs
+      sm100::mbar_init(&acce[b], 2 * 32 * kEpiWarps);  // even CTA: the epilogue threads of both CTAs
     }
     sm100::mbar_init(drain, 1);
     *s_abort = 0;
@@ -1179,8 +1240,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       if (!sm100::mbar_wait_bounded(drain, 0, s_abort, kWaitLimitNs)) raise_abort();
     }
   } else {
-    // ------------------------------------------------ epilogue (warps 2..5, both CTAs)
-    const int qd = warp & 3;
+    // ------------------------------------------------ epilogue (warps 2..9, both CTAs)
+    const int qd = warp & 3;            // TMEM lane quadrant this warp may access
+    const int half = (warp - 2) >> 2;  // column half of the 256-wide tile
     const int row = qd * 32 + lane;
     int i = 0;
     for (int tile = cl; tile < num_tiles; tile += ncl, ++i) {
@@ -1198,69 +1260,44 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
       tile_origin(g, tile, 256, 256, m0, n0);
       const int m = m0 + 128 * (int)rank + row;
       const bool vrow = m < g.Mrows;
-      int p = 0, t = 0, Tp = g.T;
-      float* outp = g.out;
-      const int* __restrict__ inv = nullptr;  // orientation -> this particle's list index
+      int p = 0;
+      EpiRow x;
+      x.t = 0;
+      x.Tp = g.T;
+      x.out_row = g.out;
+      x.inv = nullptr;
       if (vrow) {
         if (g.L.rows) {
           const int4 rw = g.L.rows[m];
           p = rw.x;
-          t = rw.y;
+          x.t = rw.y;
           const PartDev& pd = g.L.parts[p];
-          Tp = pd.T;
-          outp = pd.out;
-          inv = pd.inv;
+          x.Tp = pd.T;
+          x.out_row = pd.out;
+          x.inv = pd.inv;
         } else {
           p = m / g.T;
-          t = m - p * g.T;
-          outp = g.out + (size_t)p * g.O * g.T;
+          x.t = m - p * g.T;
+          x.out_row = g.out + (size_t)p * g.O * g.T;
         }
       }
-      const double* __restrict__ na_row = g.na + (size_t)p * g.O;
-      const float2* __restrict__ nh_row = g.na_hl + (size_t)p * g.O;
-      float* __restrict__ out_row = outp + t;
-      const double m2s = C::kScaled ? -2.0 * (double)g.inv_sa[p] : -2.0;
-      const float m2f = (float)m2s;
+      x.out_row += x.t;
+      x.na_row = g.na + (size_t)p * g.O;
+      x.nh_row = g.na_hl + (size_t)p * g.O;
+      x.m2s = C::kScaled ? -2.0 * (double)g.inv_sa[p] : -2.0;
+      x.m2f = (float)x.m2s;
+      const int o0 = n0 + half * 128;
+      const bool fast = !x.inv && !g.accumulate && !g.combine64 && o0 + 128 <= g.O;
       float best = __int_as_float(0x7f800000);
-      uint32_t best_idx = 0xffffffffu;
-#pragma unroll 1
-      for (int c = 0; c < 256 / 32; ++c) {
-        uint32_t r[32];
-        __syncwarp();
-        sm100::tmem_ld_32x32b_x32(tmem + (uint32_t)(b * 256 + c * 32) + ((uint32_t)(qd * 32) << 16), r);
-        sm100::tmem_ld_wait();
-        if (vrow) {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int o = n0 + c * 32 + j;
-            const int lo = (o < g.O) ? (inv ? inv[o] : o) : -1;
-            if (lo >= 0) {
-              const float c = __uint_as_float(r[j]);
-              float f;
-              if (g.combine64) {  // FP64 combine
-                double cr = (double)c;
-                if (C::kScaled) cr *= (double)g.inv_sb[o];
-                f = (float)fma(m2s, cr, na_row[o]);
-              } else {  // double-float combine (see tc_gemm_kernel)
-                const float2 nh = nh_row[o];
-                const float sc = C::kScaled ? m2f * g.inv_sb[o] : m2f;
-                f = __fadd_rn(__fmaf_rn(sc, c, nh.x), nh.y);
-              }
-              float* dst = out_row + (size_t)lo * Tp;
-              if (g.accumulate) f += __ldcs(dst);
-              __stcs(dst, f);  // streamed: the output must not evict the operands from L2
-              if (f < best) {
-                best = f;
-                best_idx = (uint32_t)(lo * Tp + t);
-              }
-            }
-          }
-        }
-      }
+      int best_lo = -1;
+      epi_drain<C::kScaled, 4>(g, x, tmem + (uint32_t)(b * 256 + half * 128) + ((uint32_t)(qd * 32) << 16), o0,
+                               vrow, fast, best, best_lo);
       sm100::tc_fence_before();
       sm100::mbar_arrive_cluster(acce0 + 8u * (uint32_t)b);  // the even CTA may reuse buffer b
       unsigned long long key =
-          (vrow && best_idx != 0xffffffffu) ? (((unsigned long long)ordered_bits(best) << 32) | best_idx) : ~0ull;
+          (vrow && best_lo >= 0)
+              ? (((unsigned long long)ordered_bits(best) << 32) | (uint32_t)(best_lo * x.Tp + x.t))
+              : ~0ull;
       const int pk = vrow ? p : -1;
 #pragma unroll
       for (int off = 1; off < 32; off <<= 1) {
@@ -1422,7 +1459,7 @@ static int launch_gemm_v(const b200d2_batch& b, const TcGeom& g, void* ws, cudaS
   }
   const long long items = (long long)tiles * a.split;
   const int grid = (int)std::max(1LL, std::min(items, (long long)num_sms()));
-  tc_gemm_kernel<PREC, ROWB, BN><<<grid, 192, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
+  tc_gemm_kernel<PREC, ROWB, BN><<<grid, kGemmThreads, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
   count_launch();
   return status_from_cuda(cudaGetLastError());
 }
@@ -1476,7 +1513,7 @@ static int launch_gemm_pair(const b200d2_batch& b, const TcGeom& g, void* ws, cu
   const int tiles = U ? U->ntiles[2] : a.Mtiles * a.Ntiles;
   if (tiles == 0) return B200D2_OK;
   const int pairs = std::max(1, std::min(tiles, num_sms() / 2));
-  tc_gemm_pair_kernel<PREC, ROWB><<<2 * pairs, 192, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
+  tc_gemm_pair_kernel<PREC, ROWB><<<2 * pairs, kGemmThreads, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
   count_launch();
   return status_from_cuda(cudaGetLastError());
 }

@@ -182,6 +182,14 @@ __device__ __forceinline__ void tmem_ld_wait() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Wait for the loads in flight, then tie the 32 destination registers of one
+// load to that point so that no use of them is scheduled before the wait.
+__device__ __forceinline__ void tmem_ld_wait_regs(uint32_t (&r)[32]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 32; ++j) asm volatile("" : "+r"(r[j]));
+}
+
 // Shared-memory matrix descriptor for a K-major tile with 128-byte swizzle:
 // rows of 128 bytes, 8-row groups 1024 bytes apart (SBO), LBO unused (1).
 __device__ __forceinline__ uint64_t desc_k_sw128(uint32_t smem_addr) {

@@ -80,15 +80,15 @@ def test_static_scratch_rejects_oversized_batches(pkg, synth, cuda):
     assert e.value.code == 7
     torch.cuda.synchronize()
     assert float(d.max().item()) == -1.0  # nothing ran
-    # the header's example shape fits: 16 particles x 1536 orientations x
+    # the header's example shape fits: 16 particles x 1024 orientations x
     # 113 translations at image 64 (the scratch holds the contraction without
     # k-splits, so its need can be below the allocating entry point's query)
     P16 = 16
     re16 = dp.re[:1].expand(P16, -1).contiguous()
     im16 = dp.im[:1].expand(P16, -1).contiguous()
     co16 = dp.corr[:1].expand(P16, -1).contiguous()
-    d16 = torch.full((P16 * 1536 * pr.T,), -1.0, device="cuda")
-    small = pkg.make_batch(dp.eulers, dp.tx, dp.ty, re16, im16, co16, d16, O=1536, T=pr.T, P=P16,
+    d16 = torch.full((P16 * 1024 * pr.T,), -1.0, device="cuda")
+    small = pkg.make_batch(dp.eulers, dp.tx, dp.ty, re16, im16, co16, d16, O=1024, T=pr.T, P=P16,
                            N_img=pr.N_img)
     pkg.diff2_coarse_batch_static(view, small, pkg.PREC_BF16X3)
     torch.cuda.synchronize()
