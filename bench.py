@@ -41,11 +41,11 @@ PKG_DIR = os.path.join(ROOT, "t2-relion-kernel_b200")
 METRIC = "diff2 evals/s (coarse pass)"
 L2_BYTES = 126 * 1024 * 1024
 
-# DRAM bytes (read + write) per diff2 evaluation of the contraction kernel,
-# from one ncu capture of a smaller case of the same shape (64 particles,
-# 4608 orientations, 113 translations: 514.6 MB read + 107.5 MB written for
-# 33.3 M evaluations), scaled to a launch by its evaluation count.
-GEMM_DRAM_BYTES_PER_EVAL = {("c2", "bf16x3"): (514.6e6 + 107.5e6) / 33325056}
+# DRAM bytes (read + write) per diff2 evaluation of the contraction kernel
+# (CTA-pair form), from one ncu capture of a smaller case of the same shape (64
+# particles, 4608 orientations, 113 translations: 531.4 MB read + 121.9 MB
+# written for 33.3 M evaluations), scaled to a launch by its evaluation count.
+GEMM_DRAM_BYTES_PER_EVAL = {("c2", "bf16x3"): (531.4e6 + 121.9e6) / 33325056}
 
 
 def load_package():
