@@ -148,7 +148,7 @@ def cpu_sample(pr, budget_s: float, max_particles: int | None = None) -> dict:
         el = time.perf_counter() - t0
         if el >= budget_s or (max_particles is not None and done >= max_particles):
             break
-    return {"value": evals / el, "unit": "diff2 evals/s", "cores": nthreads, "kind": "port",
+    return {"value": evals / el, "unit": "diff2 evals/s", "cores": nthreads, "kind": "port", "particles": done,
             "sample": f"{done} particle(s) x {pr.O} orientations x {pr.T} translations of the same "
                       f"workload, FP32 C restatement of cuda_kernel_diff2_coarse, {nthreads} threads, "
                       f"{el:.1f} s"}
@@ -202,12 +202,12 @@ def reference_arm(args):
     per_step_particles = 2
     # warm-up steps (untimed), then K timed steps, each a bounded sample
     for _ in range(args.warmup):
-        cpu_sample(pr, 0.0, max_particles=1)
+        cpu_sample(pr, float("inf"), max_particles=1)
     t0 = time.perf_counter()
     evals = 0
     for k in range(args.steps):
-        s = cpu_sample(pr, 0.0, max_particles=per_step_particles)
-        evals += per_step_particles * pr.O * pr.T
+        s = cpu_sample(pr, float("inf"), max_particles=per_step_particles)  # exactly per_step_particles
+        evals += s["particles"] * pr.O * pr.T
     el = time.perf_counter() - t0
     v = evals / el
     cores = os.cpu_count() or 1
