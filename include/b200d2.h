@@ -146,6 +146,24 @@ int b200d2_diff2_coarse_f64(const b200d2_view* view, const float* d_trans_x,
                             size_t T, size_t N_img, int filter_img,
                             void* stream);
 
+/* Fine-pass diff2 over a job list (replaces cuda_kernel_diff2_fine,
+ * src/diff2.cuh:540-682, 2D image against a 3D reference; the reference has
+ * no host wrapper for it).  Job j (j < todo_blocks) scores orientation
+ * d_rot_idx[d_job_idx[j]] of d_eulers[][9] against the d_job_num[j]
+ * consecutive translations starting at d_trans_idx[d_job_idx[j]] and writes
+ *   d_diff2s[d_job_idx[j] + i] = sum_init + sum_px corr/2 |proj - shift_i(img)|^2
+ * over all image_size pixels (the fine kernel's pixel mapping).  FP32, like
+ * the reference.  Any number of translations per job.  Index arrays are
+ * device uint64 (the reference's unsigned long). */
+int b200d2_diff2_fine(const b200d2_view* view, const float* d_eulers,
+                      const float* d_real, const float* d_imag,
+                      const float* d_trans_x, const float* d_trans_y,
+                      const float* d_corr, float* d_diff2s, size_t image_size,
+                      float sum_init, size_t todo_blocks,
+                      const uint64_t* d_rot_idx, const uint64_t* d_trans_idx,
+                      const uint64_t* d_job_idx, const uint64_t* d_job_num,
+                      void* stream);
+
 /* ------------------------------------------------------------------------
  * Batched coarse pass (layout diff2[p][o][t]).  The reference
  * launches one runDiff2KernelCoarse per particle (src/main.cu:483-503); this

@@ -211,6 +211,9 @@ def ref_lib():
         L.refshim_variant_workspace_bytes.argtypes = [C.c_int] * 6
         L.refshim_variant_workspace_bytes.restype = C.c_size_t
         L.refshim_variant_run.argtypes = [C.c_int, P] + [C.c_int] * 4 + [P] * 9 + [C.c_int] * 5 + [P]
+        if hasattr(L, "refshim_diff2_fine"):
+            L.refshim_diff2_fine.argtypes = ([P] + [C.c_int] * 4 + [P] * 7 + [C.c_long, C.c_float] + [C.c_long] * 3 +
+                                             [P] * 4 + [P])
         _ref = L
     return _ref
 

@@ -14,6 +14,7 @@
 //   runDiff2KernelCoarse                      src/acc_helper_functions_impl.h:15-499
 //   runDiff2KernelCoarseDouble                src/acc_helper_functions_impl.h:503-854
 //   CoarseMatrixKernel*::run (5 variants)     src/coarse_splitImg_*.cuh
+//   cuda_kernel_diff2_fine (no host wrapper)  src/diff2.cuh:540-682
 // The reference's texture projector is used.  Its PROJECTOR_NO_TEXTURES
 // configuration does not compile (src/diff2.cuh:16 includes
 // src/orientation_matrix_handler.cuh, which calls tex3D unconditionally at
@@ -51,7 +52,7 @@ AccProjectorKernel make_view(RefProjector* p, int imgX, int imgY, int imgZ,
 
 extern "C" {
 
-int refshim_abi_version(void) { return 2; }
+int refshim_abi_version(void) { return 3; }
 
 void* refshim_projector_create(int mdlX, int mdlY, int mdlZ, int initY,
                                int initZ, int maxR, float pf, const float* re,
@@ -156,6 +157,22 @@ int refshim_variant_run(int variant, void* h, int imgX, int imgY, int imgZ,
     default:
       return -1;
   }
+  return (int)cudaGetLastError();
+}
+
+// The fine-pass kernel has no host wrapper in the reference; this launches
+// it for a 3D reference and 2D images with 128-thread blocks and up to 16
+// translations per job (its shared-memory buffer is block_sz * chunk_sz).
+int refshim_diff2_fine(void* h, int imgX, int imgY, int imgZ, int imgMaxR, float* d_eulers, float* d_re,
+                       float* d_im, float* d_tx, float* d_ty, float* d_corr, float* d_diff2s, long image_size,
+                       float sum_init, long O, long T, long todo_blocks, unsigned long* d_rot_idx,
+                       unsigned long* d_trans_idx, unsigned long* d_job_idx, unsigned long* d_job_num,
+                       void* stream) {
+  RefProjector* p = reinterpret_cast<RefProjector*>(h);
+  AccProjectorKernel k = make_view(p, imgX, imgY, imgZ, imgMaxR);
+  cuda_kernel_diff2_fine<true, false, 128, 16><<<(unsigned)todo_blocks, 128, 0, (cudaStream_t)stream>>>(
+      d_eulers, d_re, d_im, d_tx, d_ty, nullptr, k, d_corr, d_diff2s, (unsigned)image_size, sum_init,
+      (unsigned long)O, (unsigned long)T, (unsigned long)todo_blocks, d_rot_idx, d_trans_idx, d_job_idx, d_job_num);
   return (int)cudaGetLastError();
 }
 

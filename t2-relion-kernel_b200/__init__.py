@@ -155,6 +155,7 @@ def _declare(L):
         "b200d2_coarse_weights": [P, I, I, I, P, P, P, I, P, P, P, Z, P],
         "b200d2_set_gemm_variant": [I, I, I, I],
         "b200d2_set_combine": [I],
+        "b200d2_diff2_fine": [C.POINTER(View), P, P, P, P, P, P, P, Z, F, Z, P, P, P, P, P],
         "b200d2_ctf_fold": [P, P, C.c_longlong, I, I, I, I, I, I, F, P, P, C.c_longlong, P, P, P, P],
     }
     for name, args in sig.items():
@@ -452,6 +453,16 @@ def diff2_coarse_batch_static(view: View, batch: Batch, precision: int = PREC_BF
 
 def minloc(diff2, n: int, P: int, out_min=None, out_argmin=None, stream=None):
     _check(lib().b200d2_minloc(_ptr(diff2), n, P, _ptr(out_min), _ptr(out_argmin), _stream(stream)), "minloc")
+
+
+def diff2_fine(view: View, eulers, real, imag, trans_x, trans_y, corr, diff2s, *, rot_idx, trans_idx, job_idx,
+               job_num, image_size: int, sum_init: float = 0.0, stream=None):
+    """Fine-pass diff2 over a job list (b200d2_diff2_fine); index tensors are
+    CUDA int64 [jobs] (rot_idx / trans_idx indexed by job_idx)."""
+    _check(lib().b200d2_diff2_fine(C.byref(view), _ptr(eulers), _ptr(real), _ptr(imag), _ptr(trans_x),
+                                   _ptr(trans_y), _ptr(corr), _ptr(diff2s), image_size, sum_init,
+                                   int(job_idx.numel()), _ptr(rot_idx), _ptr(trans_idx), _ptr(job_idx),
+                                   _ptr(job_num), _stream(stream)), "diff2_fine")
 
 
 def coarse_weights(diff2, P: int, O: int, T: int, out_min=None, pdf_orient=None, pdf_offset=None,

@@ -1,0 +1,123 @@
+// fine.cu -- fine-pass diff2 over a job list (b200d2_diff2_fine).
+//
+// Replaces cuda_kernel_diff2_fine (src/diff2.cuh:540-682, 2D image against a
+// 3D reference).  After the coarse pass, RELION rescores only the significant
+// samples on oversampled orientation and translation grids.  The work arrives
+// as jobs: job j scores orientation rot_idx[job_idx[j]] against the job_num[j]
+// consecutive translations starting at trans_idx[job_idx[j]], and writes
+//   diff2s[job_idx[j] + i] = sum_init + sum_px corr/2 |proj - shift_i(img)|^2
+// for i < job_num[j] (written, not accumulated, as the reference does).
+//
+// One CTA per job.  Each thread projects its pixels once (texture or linear
+// projector, the same sample positions as the coarse kernels) and keeps the
+// job's translations in registers (up to kFineMaxTrans per pass; longer jobs
+// take several passes over the pixels), so the projection is shared by all of
+// the job's translations; the per-translation sums are reduced with warp
+// shuffles and one shared-memory step in a fixed order.  Pixel coordinates
+// follow the fine kernel's mapping (src/diff2.cuh:612-626): rows past maxR
+// wrap to negative y when they lie within maxR of the end, otherwise their x
+// is set to maxR (outside the projector radius).
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace b200d2 {
+
+constexpr int kFineThreads = 128;
+constexpr int kFineMaxTrans = 16;
+
+__device__ __forceinline__ void fine_pixel_coor(int pixel, int imgX, int imgY, int maxR, int& x, int& y) {
+  x = pixel % imgX;
+  y = pixel / imgX;
+  if (y > maxR) {
+    if (y >= imgY - maxR)
+      y -= imgY;
+    else
+      x = maxR;
+  }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kFineThreads) diff2_fine_kernel(
+    b200d2_view v, const float* __restrict__ eulers, const float* __restrict__ re, const float* __restrict__ im,
+    const float* __restrict__ tx, const float* __restrict__ ty, const float* __restrict__ corr,
+    float* __restrict__ diff2s, int image_size, float sum_init, const uint64_t* __restrict__ rot_idx,
+    const uint64_t* __restrict__ trans_idx, const uint64_t* __restrict__ job_idx,
+    const uint64_t* __restrict__ job_num) {
+  const uint64_t jb = job_idx[blockIdx.x];
+  const int ntrans = (int)job_num[blockIdx.x];
+  const uint64_t o = rot_idx[jb];
+  const uint64_t t0 = trans_idx[jb];
+  const float* eo = eulers + o * 9;
+  float e[6] = {eo[0], eo[1], eo[3], eo[4], eo[6], eo[7]};
+  __shared__ float s_part[kFineThreads / 32][NT];
+  for (int base = 0; base < ntrans; base += NT) {  // passes of NT translations
+    const int nt = min(NT, ntrans - base);
+    float ftx[NT], fty[NT], acc[NT];
+#pragma unroll
+    for (int i = 0; i < NT; ++i) {
+      ftx[i] = i < nt ? tx[t0 + base + i] : 0.f;
+      fty[i] = i < nt ? ty[t0 + base + i] : 0.f;
+      acc[i] = 0.f;
+    }
+    for (int pixel = threadIdx.x; pixel < image_size; pixel += kFineThreads) {
+      int x, y;
+      fine_pixel_coor(pixel, v.imgX, v.imgY, v.maxR, x, y);
+      const float2 a = project_pixel(v, (float)x, (float)y, e);
+      const float xr = re[pixel], xi = im[pixel];
+      const float w = 0.5f * corr[pixel];
+#pragma unroll
+      for (int i = 0; i < NT; ++i) {
+        if (i < nt) {
+          float s, c;
+          sincosf(__fmaf_rn((float)x, ftx[i], __fmul_rn((float)y, fty[i])), &s, &c);
+          const float dr = a.x - __fmaf_rn(c, xr, -__fmul_rn(s, xi));
+          const float di = a.y - __fmaf_rn(c, xi, __fmul_rn(s, xr));
+          acc[i] = __fmaf_rn(__fmaf_rn(dr, dr, __fmul_rn(di, di)), w, acc[i]);
+        }
+      }
+    }
+    // fixed-order reduction: shuffle tree inside each warp, then warps in order
+#pragma unroll
+    for (int i = 0; i < NT; ++i) {
+      float vsum = acc[i];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) vsum += __shfl_xor_sync(0xffffffffu, vsum, off);
+      if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5][i] = vsum;
+    }
+    __syncthreads();
+    if (threadIdx.x < nt) {
+      float tot = 0.f;
+#pragma unroll
+      for (int w = 0; w < kFineThreads / 32; ++w) tot += s_part[w][threadIdx.x];
+      diff2s[jb + base + threadIdx.x] = tot + sum_init;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace b200d2
+
+extern "C" int b200d2_diff2_fine(const b200d2_view* view, const float* d_eulers, const float* d_real,
+                                 const float* d_imag, const float* d_trans_x, const float* d_trans_y,
+                                 const float* d_corr, float* d_diff2s, size_t image_size, float sum_init,
+                                 size_t todo_blocks, const uint64_t* d_rot_idx, const uint64_t* d_trans_idx,
+                                 const uint64_t* d_job_idx, const uint64_t* d_job_num, void* stream) {
+  using namespace b200d2;
+  if (!view) return B200D2_ERR_INVALID;
+  if (todo_blocks == 0 || image_size == 0) return B200D2_OK;
+  if (!d_eulers || !d_real || !d_imag || !d_trans_x || !d_trans_y || !d_corr || !d_diff2s || !d_rot_idx ||
+      !d_trans_idx || !d_job_idx || !d_job_num)
+    return B200D2_ERR_INVALID;
+  if (view->mdlZ == 0) return B200D2_ERR_UNSUPPORTED;  // 2D references are outside the ported branch
+  if ((long long)view->imgX * view->imgY < (long long)image_size || image_size > 0x7fffffffull)
+    return B200D2_ERR_INVALID;
+  if (view->interp == B200D2_INTERP_TEXTURE && (!view->tex_re || !view->tex_im)) return B200D2_ERR_INVALID;
+  if (view->interp == B200D2_INTERP_LINEAR && (!view->lin_re || !view->lin_im)) return B200D2_ERR_INVALID;
+  if (todo_blocks > 0x7fffffffull) return B200D2_ERR_UNSUPPORTED;
+  diff2_fine_kernel<kFineMaxTrans><<<(unsigned)todo_blocks, kFineThreads, 0, (cudaStream_t)stream>>>(
+      *view, d_eulers, d_real, d_imag, d_trans_x, d_trans_y, d_corr, d_diff2s, (int)image_size, sum_init,
+      d_rot_idx, d_trans_idx, d_job_idx, d_job_num);
+  count_launch();
+  return status_from_cuda(cudaGetLastError());
+}

@@ -1,0 +1,89 @@
+"""Fine-pass diff2 over a job list (b200d2_diff2_fine) against the
+reference's own cuda_kernel_diff2_fine (src/diff2.cuh:540-682, compiled into
+oracle/_ref) on the same device buffers and job lists, and against this
+library's FP64 coarse kernel (every (orientation, translation) pair scored
+over all pixels, plus sum_init).  Tolerance: 1e-5 relative (both FP32 sums,
+different summation orders)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from gpu_util import DeviceProblem
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def _jobs(rng, O, T, n_jobs, max_chunk):
+    """Random significant samples grouped the way RELION's fine scheduler
+    does: one orientation and a run of consecutive translations per job."""
+    rot, trans, jidx, jnum = [], [], [], []
+    pos = 0
+    for _ in range(n_jobs):
+        o = int(rng.integers(O))
+        n = int(rng.integers(1, max_chunk + 1))
+        t0 = int(rng.integers(0, T - n + 1))
+        for i in range(n):  # per-sample tables, indexed by the job's first sample
+            rot.append(o)
+            trans.append(t0 + i)
+        jidx.append(pos)
+        jnum.append(n)
+        pos += n
+    return (np.array(rot, np.uint64), np.array(trans, np.uint64), np.array(jidx, np.uint64),
+            np.array(jnum, np.uint64))
+
+
+@pytest.mark.parametrize("case,max_chunk", [("c1", 16), ("tiny", 16), ("c1", 40)])
+def test_fine_matches_reference_and_fp64(pkg, synth, oracle, cuda, case, max_chunk):
+    torch = cuda
+    pr = synth.make_problem(case, P=2)
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dp = DeviceProblem(torch, pr)
+    rng = np.random.default_rng(7)
+    rot, trans, jidx, jnum = _jobs(rng, pr.O, pr.T, 37, min(max_chunk, pr.T))
+    dev = lambda a: torch.as_tensor(a.astype(np.int64), device="cuda")  # noqa: E731
+    d_rot, d_trans, d_jidx, d_jnum = dev(rot), dev(trans), dev(jidx), dev(jnum)
+    n_out = int(jnum.sum())
+    sum_init = 3.25
+    for p in range(pr.P):
+        out = torch.full((n_out,), -1.0, device="cuda")
+        pkg.diff2_fine(view, dp.eulers, dp.re[p], dp.im[p], dp.tx, dp.ty, dp.corr[p], out, rot_idx=d_rot,
+                       trans_idx=d_trans, job_idx=d_jidx, job_num=d_jnum, image_size=pr.N_img, sum_init=sum_init)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        # FP64 coarse scores of every (o, t), then picked per sample
+        f64 = torch.zeros(pr.O * pr.T, device="cuda", dtype=torch.float64)
+        pkg.run_diff2_kernel_coarse_double(view, dp.tx, dp.ty, dp.corr[p], dp.re[p], dp.im[p], dp.eulers, f64,
+                                           pr.O, pr.T, pr.N_img)
+        torch.cuda.synchronize()
+        ref64 = f64.cpu().numpy().reshape(pr.O, pr.T)[rot.astype(np.int64), trans.astype(np.int64)] + sum_init
+        assert oracle.error_stats(got, ref64)["max_rel"] <= TOL
+        if max_chunk <= 16:  # the reference kernel holds at most 16 translations per job
+            L = oracle.ref_lib()
+            h = L.refshim_projector_create(pr.projector.mdlX, pr.projector.mdlY, pr.projector.mdlZ,
+                                           pr.projector.mdlInitY, pr.projector.mdlInitZ, pr.projector.mdlMaxR,
+                                           pr.projector.padding_factor,
+                                           np.ascontiguousarray(pr.projector.re, np.float32).ctypes.data,
+                                           np.ascontiguousarray(pr.projector.im, np.float32).ctypes.data)
+            assert h
+            rout = torch.full((n_out,), -1.0, device="cuda")
+            st = L.refshim_diff2_fine(h, pr.imgX, pr.imgY, 1, pr.imgMaxR, dp.eulers.data_ptr(), dp.re[p].data_ptr(),
+                                      dp.im[p].data_ptr(), dp.tx.data_ptr(), dp.ty.data_ptr(), dp.corr[p].data_ptr(),
+                                      rout.data_ptr(), pr.N_img, sum_init, pr.O, pr.T, len(jidx), d_rot.data_ptr(),
+                                      d_trans.data_ptr(), d_jidx.data_ptr(), d_jnum.data_ptr(), None)
+            torch.cuda.synchronize()
+            L.refshim_projector_destroy(h)
+            assert st == 0
+            assert oracle.error_stats(got, rout.cpu().numpy())["max_rel"] <= TOL
+    proj.close()
+
+
+def test_fine_rejects_bad_arguments(pkg, cuda):
+    import ctypes as C
+    v = pkg.View()
+    assert pkg.lib().b200d2_diff2_fine(C.byref(v), None, None, None, None, None, None, None, 10, 0.0, 3,
+                                       None, None, None, None, None) == 1
+    assert pkg.lib().b200d2_diff2_fine(C.byref(v), None, None, None, None, None, None, None, 10, 0.0, 0,
+                                       None, None, None, None, None) == 0
