@@ -174,7 +174,7 @@ def parse():
                     help="final combination nA - 2 cross: double-float (default) or FP64")
     ap.add_argument("--gemm-variant", default=None,
                     help="row_bytes,tile_n,split,pair for the contraction (0 = default; pair 1 = CTA pairs)")
-    ap.add_argument("--study", default=None, choices=["precision"],
+    ap.add_argument("--study", default=None, choices=["precision", "fine"],
                     help="precision: error of every precision form vs the FP64 kernel (use --config c3)")
     return ap.parse_args()
 
@@ -543,6 +543,84 @@ def precision_study(args):
     return 0
 
 
+def fine_study(args):
+    """Fine pass over job lists (one JSON line): this library's
+    b200d2_diff2_fine against the reference's cuda_kernel_diff2_fine on the
+    same device buffers.  Workload: C2 particles (image 64, 2112 pixels), a
+    job list per particle of 2048 jobs, each one orientation of the 4608 and a
+    run of 16 consecutive translations of the 113 (32768 samples per
+    particle, the order of RELION's significant samples after the coarse
+    pass); 16 particles, CUDA events."""
+    import ctypes as C
+
+    import torch
+    pkg = load_package()
+    synth = load_synth()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the reference's own kernels, built from its sources into oracle/_ref
+    pr = synth.make_problem("c2", seed=20251203, P=16)
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dev = "cuda"
+    eul = torch.as_tensor(pr.eulers.reshape(-1), device=dev)
+    tx, ty = torch.as_tensor(pr.trans_x, device=dev), torch.as_tensor(pr.trans_y, device=dev)
+    re, im, co = (torch.as_tensor(a, device=dev) for a in (pr.fimg_re, pr.fimg_im, pr.corr))
+    rng = np.random.default_rng(11)
+    n_jobs, chunk = 2048, 16
+    o = rng.integers(0, pr.O, n_jobs)
+    t0 = rng.integers(0, pr.T - chunk + 1, n_jobs)
+    rot = np.repeat(o, chunk).astype(np.int64)
+    trans = (t0[:, None] + np.arange(chunk)[None, :]).reshape(-1).astype(np.int64)
+    jidx = (np.arange(n_jobs) * chunk).astype(np.int64)
+    jnum = np.full(n_jobs, chunk, np.int64)
+    d = {k: torch.as_tensor(v, device=dev) for k, v in dict(rot=rot, trans=trans, jidx=jidx, jnum=jnum).items()}
+    n_out = n_jobs * chunk
+    out = torch.empty((pr.P, n_out), device=dev)
+    rout = torch.empty((pr.P, n_out), device=dev)
+
+    def ours():
+        for p in range(pr.P):
+            pkg.diff2_fine(view, eul, re[p], im[p], tx, ty, co[p], out[p], rot_idx=d["rot"], trans_idx=d["trans"],
+                           job_idx=d["jidx"], job_num=d["jnum"], image_size=pr.N_img)
+
+    L = oracle.ref_lib()
+    pv = pr.projector
+    h = L.refshim_projector_create(pv.mdlX, pv.mdlY, pv.mdlZ, pv.mdlInitY, pv.mdlInitZ, pv.mdlMaxR,
+                                   pv.padding_factor, np.ascontiguousarray(pv.re, np.float32).ctypes.data,
+                                   np.ascontiguousarray(pv.im, np.float32).ctypes.data)
+
+    def ref():
+        for p in range(pr.P):
+            L.refshim_diff2_fine(h, pr.imgX, pr.imgY, 1, pr.imgMaxR, eul.data_ptr(), re[p].data_ptr(),
+                                 im[p].data_ptr(), tx.data_ptr(), ty.data_ptr(), co[p].data_ptr(),
+                                 rout[p].data_ptr(), pr.N_img, 0.0, pr.O, pr.T, n_jobs, d["rot"].data_ptr(),
+                                 d["trans"].data_ptr(), d["jidx"].data_ptr(), d["jnum"].data_ptr(), None)
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_ours, ms_ref = timed(ours), timed(ref)
+    rel = float(((out - rout).abs() / rout.abs().clamp_min(1e-30)).max())
+    L.refshim_projector_destroy(h)
+    evals = pr.P * n_out
+    line = {"study": "fine", "workload": f"16 C2 particles (image 64, {pr.N_img} px) x {n_jobs} jobs x {chunk} "
+                                         f"translations ({evals} samples)",
+            "ours_ms": ms_ours, "reference_ms": ms_ref, "ours_evals_per_s": evals / (ms_ours / 1e3),
+            "reference_evals_per_s": evals / (ms_ref / 1e3), "speedup": ms_ref / ms_ours,
+            "max_rel_diff_vs_reference": rel}
+    print(json.dumps(line), flush=True)
+    proj.close()
+    return 0
+
+
 C5_REFS = ("c5s", "c5m", "c5l")
 
 
@@ -652,6 +730,8 @@ def main():
     args = parse()
     if args.study == "precision":
         return precision_study(args)
+    if args.study == "fine":
+        return fine_study(args)
     if args.config == "c5":
         return serving_arm(args)
     if args.impl == "reference":

@@ -13,11 +13,17 @@
 // job's translations in registers (up to kFineMaxTrans per pass; longer jobs
 // take several passes over the pixels), so the projection is shared by all of
 // the job's translations; the per-translation sums are reduced with warp
-// shuffles and one shared-memory step in a fixed order.  Pixel coordinates
+// shuffles and one shared-memory step in a fixed order.  The phase shift
+// e^{i(x tx + y ty)} is the product of two table entries e^{i x tx} and
+// e^{i y ty}, built per pass in shared memory (one sincos per table entry,
+// not per pixel); jobs on images too large for the tables take sincosf per
+// pixel as the reference does.  Pixel coordinates
 // follow the fine kernel's mapping (src/diff2.cuh:612-626): rows past maxR
 // wrap to negative y when they lie within maxR of the end, otherwise their x
 // is set to maxR (outside the projector radius).
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "common.cuh"
 
@@ -25,6 +31,7 @@ namespace b200d2 {
 
 constexpr int kFineThreads = 128;
 constexpr int kFineMaxTrans = 16;
+constexpr size_t kFineTableBytes = 96 * 1024;  // largest phase-table area per CTA
 
 __device__ __forceinline__ void fine_pixel_coor(int pixel, int imgX, int imgY, int maxR, int& x, int& y) {
   x = pixel % imgX;
@@ -37,7 +44,7 @@ __device__ __forceinline__ void fine_pixel_coor(int pixel, int imgX, int imgY, i
   }
 }
 
-template <int NT>
+template <int NT, bool TABLES>
 __global__ void __launch_bounds__(kFineThreads) diff2_fine_kernel(
     b200d2_view v, const float* __restrict__ eulers, const float* __restrict__ re, const float* __restrict__ im,
     const float* __restrict__ tx, const float* __restrict__ ty, const float* __restrict__ corr,
@@ -51,6 +58,13 @@ __global__ void __launch_bounds__(kFineThreads) diff2_fine_kernel(
   const float* eo = eulers + o * 9;
   float e[6] = {eo[0], eo[1], eo[3], eo[4], eo[6], eo[7]};
   __shared__ float s_part[kFineThreads / 32][NT];
+  // TABLES: [NT][exw] e^{i x tx} for x in [0, exw), then [NT][eyw] e^{i y ty}
+  // for y in [-maxR, imgY); fine_pixel_coor yields x < max(imgX, maxR + 1)
+  // and -maxR <= y < imgY.
+  extern __shared__ float2 s_tab[];
+  const int exw = max(v.imgX, v.maxR + 1), eyw = v.imgY + v.maxR;
+  float2* s_ex = s_tab;
+  float2* s_ey = s_tab + NT * exw;
   for (int base = 0; base < ntrans; base += NT) {  // passes of NT translations
     const int nt = min(NT, ntrans - base);
     float ftx[NT], fty[NT], acc[NT];
@@ -59,6 +73,21 @@ __global__ void __launch_bounds__(kFineThreads) diff2_fine_kernel(
       ftx[i] = i < nt ? tx[t0 + base + i] : 0.f;
       fty[i] = i < nt ? ty[t0 + base + i] : 0.f;
       acc[i] = 0.f;
+    }
+    if (TABLES) {
+      for (int e2 = threadIdx.x; e2 < NT * (exw + eyw); e2 += kFineThreads) {
+        float sn = 0.f, cs = 1.f;
+        if (e2 < NT * exw) {
+          const int i = e2 / exw, x = e2 - i * exw;
+          if (i < nt) sincosf(__fmul_rn((float)x, tx[t0 + base + i]), &sn, &cs);
+          s_ex[e2] = make_float2(cs, sn);
+        } else {
+          const int j = e2 - NT * exw, i = j / eyw, y = j - i * eyw - v.maxR;
+          if (i < nt) sincosf(__fmul_rn((float)y, ty[t0 + base + i]), &sn, &cs);
+          s_ey[j] = make_float2(cs, sn);
+        }
+      }
+      __syncthreads();
     }
     for (int pixel = threadIdx.x; pixel < image_size; pixel += kFineThreads) {
       int x, y;
@@ -70,7 +99,13 @@ __global__ void __launch_bounds__(kFineThreads) diff2_fine_kernel(
       for (int i = 0; i < NT; ++i) {
         if (i < nt) {
           float s, c;
-          sincosf(__fmaf_rn((float)x, ftx[i], __fmul_rn((float)y, fty[i])), &s, &c);
+          if (TABLES) {
+            const float2 ex = s_ex[i * exw + x], ey = s_ey[i * eyw + y + v.maxR];
+            c = __fmaf_rn(ex.x, ey.x, -__fmul_rn(ex.y, ey.y));
+            s = __fmaf_rn(ex.x, ey.y, __fmul_rn(ex.y, ey.x));
+          } else {
+            sincosf(__fmaf_rn((float)x, ftx[i], __fmul_rn((float)y, fty[i])), &s, &c);
+          }
           const float dr = a.x - __fmaf_rn(c, xr, -__fmul_rn(s, xi));
           const float di = a.y - __fmaf_rn(c, xi, __fmul_rn(s, xr));
           acc[i] = __fmaf_rn(__fmaf_rn(dr, dr, __fmul_rn(di, di)), w, acc[i]);
@@ -115,9 +150,23 @@ extern "C" int b200d2_diff2_fine(const b200d2_view* view, const float* d_eulers,
   if (view->interp == B200D2_INTERP_TEXTURE && (!view->tex_re || !view->tex_im)) return B200D2_ERR_INVALID;
   if (view->interp == B200D2_INTERP_LINEAR && (!view->lin_re || !view->lin_im)) return B200D2_ERR_INVALID;
   if (todo_blocks > 0x7fffffffull) return B200D2_ERR_UNSUPPORTED;
-  diff2_fine_kernel<kFineMaxTrans><<<(unsigned)todo_blocks, kFineThreads, 0, (cudaStream_t)stream>>>(
-      *view, d_eulers, d_real, d_imag, d_trans_x, d_trans_y, d_corr, d_diff2s, (int)image_size, sum_init,
-      d_rot_idx, d_trans_idx, d_job_idx, d_job_num);
+  const size_t exw = (size_t)std::max(view->imgX, view->maxR + 1);
+  const size_t tab_bytes = sizeof(float2) * kFineMaxTrans * (exw + view->imgY + view->maxR);
+  if (view->maxR >= 0 && view->imgX > 0 && view->imgY > 0 && tab_bytes <= kFineTableBytes) {
+    static bool attr = false;  // the opt-in above 48 KB of dynamic shared memory
+    if (!attr) {
+      B200D2_CUDA_TRY(cudaFuncSetAttribute(diff2_fine_kernel<kFineMaxTrans, true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFineTableBytes));
+      attr = true;
+    }
+    diff2_fine_kernel<kFineMaxTrans, true><<<(unsigned)todo_blocks, kFineThreads, tab_bytes, (cudaStream_t)stream>>>(
+        *view, d_eulers, d_real, d_imag, d_trans_x, d_trans_y, d_corr, d_diff2s, (int)image_size, sum_init,
+        d_rot_idx, d_trans_idx, d_job_idx, d_job_num);
+  } else {
+    diff2_fine_kernel<kFineMaxTrans, false><<<(unsigned)todo_blocks, kFineThreads, 0, (cudaStream_t)stream>>>(
+        *view, d_eulers, d_real, d_imag, d_trans_x, d_trans_y, d_corr, d_diff2s, (int)image_size, sum_init,
+        d_rot_idx, d_trans_idx, d_job_idx, d_job_num);
+  }
   count_launch();
   return status_from_cuda(cudaGetLastError());
 }

@@ -34,49 +34,85 @@ def _jobs(rng, O, T, n_jobs, max_chunk):
             np.array(jnum, np.uint64))
 
 
+def _check_fine(pkg, oracle, torch, pr, view, imgX, imgY, imgMaxR, N, eulers, tx, ty, re, im, corr, max_chunk,
+                seed=7):
+    """Score 37 random jobs through b200d2_diff2_fine and compare with the
+    FP64 coarse kernel and, for jobs of at most 16 translations, with the
+    reference's fine kernel.  Returns the largest relative difference seen."""
+    O, T = eulers.numel() // 9, tx.numel()
+    rng = np.random.default_rng(seed)
+    rot, trans, jidx, jnum = _jobs(rng, O, T, 37, min(max_chunk, T))
+    dev = lambda a: torch.as_tensor(a.astype(np.int64), device="cuda")  # noqa: E731
+    d_rot, d_trans, d_jidx, d_jnum = dev(rot), dev(trans), dev(jidx), dev(jnum)
+    n_out = int(jnum.sum())
+    sum_init = 3.25
+    out = torch.full((n_out,), -1.0, device="cuda")
+    pkg.diff2_fine(view, eulers, re, im, tx, ty, corr, out, rot_idx=d_rot, trans_idx=d_trans, job_idx=d_jidx,
+                   job_num=d_jnum, image_size=N, sum_init=sum_init)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    # FP64 coarse scores of every (o, t), then picked per sample
+    f64 = torch.zeros(O * T, device="cuda", dtype=torch.float64)
+    pkg.run_diff2_kernel_coarse_double(view, tx, ty, corr, re, im, eulers, f64, O, T, N)
+    torch.cuda.synchronize()
+    ref64 = f64.cpu().numpy().reshape(O, T)[rot.astype(np.int64), trans.astype(np.int64)] + sum_init
+    worst = oracle.error_stats(got, ref64)["max_rel"]
+    assert worst <= TOL
+    if max_chunk <= 16:  # the reference kernel holds at most 16 translations per job
+        L = oracle.ref_lib()
+        h = L.refshim_projector_create(pr.projector.mdlX, pr.projector.mdlY, pr.projector.mdlZ,
+                                       pr.projector.mdlInitY, pr.projector.mdlInitZ, pr.projector.mdlMaxR,
+                                       pr.projector.padding_factor,
+                                       np.ascontiguousarray(pr.projector.re, np.float32).ctypes.data,
+                                       np.ascontiguousarray(pr.projector.im, np.float32).ctypes.data)
+        assert h
+        rout = torch.full((n_out,), -1.0, device="cuda")
+        st = L.refshim_diff2_fine(h, imgX, imgY, 1, imgMaxR, eulers.data_ptr(), re.data_ptr(), im.data_ptr(),
+                                  tx.data_ptr(), ty.data_ptr(), corr.data_ptr(), rout.data_ptr(), N, sum_init, O, T,
+                                  len(jidx), d_rot.data_ptr(), d_trans.data_ptr(), d_jidx.data_ptr(),
+                                  d_jnum.data_ptr(), None)
+        torch.cuda.synchronize()
+        L.refshim_projector_destroy(h)
+        assert st == 0
+        d = oracle.error_stats(got, rout.cpu().numpy())["max_rel"]
+        assert d <= TOL
+        worst = max(worst, d)
+    return worst
+
+
 @pytest.mark.parametrize("case,max_chunk", [("c1", 16), ("tiny", 16), ("c1", 40)])
 def test_fine_matches_reference_and_fp64(pkg, synth, oracle, cuda, case, max_chunk):
+    """Coarse-sized images: the phase shifts come from the per-pass tables."""
     torch = cuda
     pr = synth.make_problem(case, P=2)
     proj = pkg.Projector(pr.projector, use_texture=1)
     view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
     dp = DeviceProblem(torch, pr)
-    rng = np.random.default_rng(7)
-    rot, trans, jidx, jnum = _jobs(rng, pr.O, pr.T, 37, min(max_chunk, pr.T))
-    dev = lambda a: torch.as_tensor(a.astype(np.int64), device="cuda")  # noqa: E731
-    d_rot, d_trans, d_jidx, d_jnum = dev(rot), dev(trans), dev(jidx), dev(jnum)
-    n_out = int(jnum.sum())
-    sum_init = 3.25
     for p in range(pr.P):
-        out = torch.full((n_out,), -1.0, device="cuda")
-        pkg.diff2_fine(view, dp.eulers, dp.re[p], dp.im[p], dp.tx, dp.ty, dp.corr[p], out, rot_idx=d_rot,
-                       trans_idx=d_trans, job_idx=d_jidx, job_num=d_jnum, image_size=pr.N_img, sum_init=sum_init)
-        torch.cuda.synchronize()
-        got = out.cpu().numpy()
-        # FP64 coarse scores of every (o, t), then picked per sample
-        f64 = torch.zeros(pr.O * pr.T, device="cuda", dtype=torch.float64)
-        pkg.run_diff2_kernel_coarse_double(view, dp.tx, dp.ty, dp.corr[p], dp.re[p], dp.im[p], dp.eulers, f64,
-                                           pr.O, pr.T, pr.N_img)
-        torch.cuda.synchronize()
-        ref64 = f64.cpu().numpy().reshape(pr.O, pr.T)[rot.astype(np.int64), trans.astype(np.int64)] + sum_init
-        assert oracle.error_stats(got, ref64)["max_rel"] <= TOL
-        if max_chunk <= 16:  # the reference kernel holds at most 16 translations per job
-            L = oracle.ref_lib()
-            h = L.refshim_projector_create(pr.projector.mdlX, pr.projector.mdlY, pr.projector.mdlZ,
-                                           pr.projector.mdlInitY, pr.projector.mdlInitZ, pr.projector.mdlMaxR,
-                                           pr.projector.padding_factor,
-                                           np.ascontiguousarray(pr.projector.re, np.float32).ctypes.data,
-                                           np.ascontiguousarray(pr.projector.im, np.float32).ctypes.data)
-            assert h
-            rout = torch.full((n_out,), -1.0, device="cuda")
-            st = L.refshim_diff2_fine(h, pr.imgX, pr.imgY, 1, pr.imgMaxR, dp.eulers.data_ptr(), dp.re[p].data_ptr(),
-                                      dp.im[p].data_ptr(), dp.tx.data_ptr(), dp.ty.data_ptr(), dp.corr[p].data_ptr(),
-                                      rout.data_ptr(), pr.N_img, sum_init, pr.O, pr.T, len(jidx), d_rot.data_ptr(),
-                                      d_trans.data_ptr(), d_jidx.data_ptr(), d_jnum.data_ptr(), None)
-            torch.cuda.synchronize()
-            L.refshim_projector_destroy(h)
-            assert st == 0
-            assert oracle.error_stats(got, rout.cpu().numpy())["max_rel"] <= TOL
+        _check_fine(pkg, oracle, torch, pr, view, pr.imgX, pr.imgY, pr.imgMaxR, pr.N_img, dp.eulers, dp.tx, dp.ty,
+                    dp.re[p], dp.im[p], dp.corr[p], max_chunk)
+    proj.close()
+
+
+@pytest.mark.parametrize("imgX,imgY,imgMaxR", [(65, 128, 64), (257, 512, 256)])
+def test_fine_images_beyond_projector_radius(pkg, synth, oracle, cuda, imgX, imgY, imgMaxR):
+    """Images larger than the c1 projector's radius (16): the view's maxR is
+    the projector's, so rows between maxR and imgY - maxR take the fine
+    kernel's x = maxR mapping.  At 128 pixels the phase tables fit; at 512
+    (257 x 512 half-transform) they would exceed the shared-memory area and
+    the kernel takes sincos per pixel.  Random image data; pixels beyond the
+    projector's radius score against a zero projection."""
+    torch = cuda
+    pr = synth.make_problem("c1", P=1, orient_limit=64)
+    N = imgX * imgY
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(imgX, imgY, imgMaxR)
+    rng = np.random.default_rng(11)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device="cuda")  # noqa: E731
+    re, im = t(rng.normal(0, 1e-3, N)), t(rng.normal(0, 1e-3, N))
+    corr = t(rng.uniform(0.5, 2.0, N))
+    _check_fine(pkg, oracle, torch, pr, view, imgX, imgY, imgMaxR, N, t(pr.eulers.reshape(-1)), t(pr.trans_x),
+                t(pr.trans_y), re, im, corr, 16, seed=3)
     proj.close()
 
 
