@@ -174,7 +174,7 @@ def parse():
                     help="final combination nA - 2 cross: double-float (default) or FP64")
     ap.add_argument("--gemm-variant", default=None,
                     help="row_bytes,tile_n,split,pair for the contraction (0 = default; pair 1 = CTA pairs)")
-    ap.add_argument("--study", default=None, choices=["precision", "fine"],
+    ap.add_argument("--study", default=None, choices=["precision", "fine", "significance"],
                     help="precision: error of every precision form vs the FP64 kernel (use --config c3)")
     return ap.parse_args()
 
@@ -621,6 +621,99 @@ def fine_study(args):
     return 0
 
 
+def significance_study(args):
+    """Significance after the coarse weights (one JSON line): b200d2_significance
+    on the FP64 weights of the C2 batch (256 particles x 4608 orientations x
+    113 translations = 520704 samples per particle, adaptive fraction 0.999),
+    against RELION's device sequence around the reference's own kernels: per
+    particle the positive weights filtered, sorted and scanned in FP64 (torch),
+    then the reference's cuda_kernel_find_threshold_idx_in_cumulative and
+    cuda_kernel_array_over_threshold.  CUDA events; the weights (1.07 GB)
+    exceed L2."""
+    import torch
+    pkg = load_package()
+    synth = load_synth()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the reference's own kernels, built from its sources into oracle/_ref
+    pr = synth.make_problem("c2")
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dev = "cuda"
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)  # noqa: E731
+    eul, tx, ty = t(pr.eulers.reshape(-1)), t(pr.trans_x), t(pr.trans_y)
+    re, im, co = t(pr.fimg_re), t(pr.fimg_im), t(pr.corr)
+    n = pr.O * pr.T
+    d2 = torch.empty(pr.P * n, device=dev)
+    b = pkg.make_batch(eul, tx, ty, re, im, co, d2, O=pr.O, T=pr.T, P=pr.P, N_img=pr.N_img)
+    ws = torch.empty(pkg.batch_workspace_bytes(view, b, pkg.PREC_BF16X3), device=dev, dtype=torch.uint8)
+    pkg.diff2_coarse_batch(view, b, pkg.PREC_BF16X3, ws)
+    del ws
+    w, sums = pkg.coarse_weights(d2, pr.P, pr.O, pr.T, normalize=False)
+    w = w.reshape(pr.P, n)
+    del d2
+    frac = 0.999
+    sig = torch.empty(pr.P, dtype=torch.float64, device=dev)
+    nsig = torch.empty(pr.P, dtype=torch.int64, device=dev)
+    mask = torch.empty((pr.P, n), dtype=torch.uint8, device=dev)
+    sws = torch.empty(pkg.lib().b200d2_significance_workspace(pr.P, n), dtype=torch.uint8, device=dev)
+
+    def ours():
+        pkg.significance(w, sums, frac, 0, passed=mask, sig_weight=sig, nsig=nsig, workspace=sws)
+
+    L = oracle.ref_lib()
+    rsig = np.zeros(pr.P)
+    rnsig = np.zeros(pr.P, np.int64)
+    rmask = torch.empty((pr.P, n), dtype=torch.bool, device=dev)
+    d_idx = torch.zeros(pr.P, dtype=torch.int64, device=dev)
+    thr = ((1.0 - frac) * sums).cpu().numpy()
+
+    def ref():
+        for p in range(pr.P):
+            pos = torch.sort(w[p][w[p] > 0]).values
+            cum = torch.cumsum(pos, 0)
+            L.refshim_find_threshold_idx(cum.data_ptr(), float(thr[p]), pos.numel(), d_idx[p:].data_ptr(), None)
+            idx = int(d_idx[p].item())  # RELION reads the index back to the host here
+            rsig[p] = float(pos[idx].item())
+            rnsig[p] = pos.numel() - idx
+            L.refshim_array_over_threshold(w[p].data_ptr(), rmask[p].data_ptr(), rsig[p], n, None)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    l0 = pkg.launch_count()
+    ms_ours = timed(ours, 10)
+    launches = (pkg.launch_count() - l0) // 11
+    ms_ref = timed(ref, 2)
+    same_sig = int((sig.cpu().numpy() == rsig).sum())
+    same_nsig = int((nsig.cpu().numpy() == rnsig).sum())
+    same_mask = bool(torch.equal(mask.bool(), rmask))
+    peaks, src = measured_peaks()
+    bytes_alg = pr.P * n * (8 + 1)  # read every weight once, write the mask
+    ach = bytes_alg / (ms_ours / 1e3) / 1e9
+    line = {"study": "significance",
+            "workload": f"C2 batch weights: {pr.P} particles x {n} samples (FP64, 1.07 GB), adaptive fraction {frac}",
+            "ours_ms": ms_ours, "reference_sequence_ms": ms_ref, "speedup": ms_ref / ms_ours,
+            "launches_per_call": launches,
+            "median_nsig": float(np.median(nsig.cpu().numpy())),
+            "particles_equal_sig": same_sig, "particles_equal_nsig": same_nsig, "mask_equal": same_mask,
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": ach / peaks["hbm_gbs"], "peak_source": src,
+                         "algorithmic_bytes": bytes_alg,
+                         "note": "algorithmic bytes = one read of the weights + the mask; the kernels read the "
+                                 "weights twice (exponent histogram; mask and binade compaction)"}}
+    print(json.dumps(line), flush=True)
+    proj.close()
+    return 0
+
+
 C5_REFS = ("c5s", "c5m", "c5l")
 
 
@@ -732,6 +825,8 @@ def main():
         return precision_study(args)
     if args.study == "fine":
         return fine_study(args)
+    if args.study == "significance":
+        return significance_study(args)
     if args.config == "c5":
         return serving_arm(args)
     if args.impl == "reference":

@@ -400,6 +400,33 @@ int b200d2_coarse_weights(const float* d_diff2, int P, int O, int T,
                           double* d_weights, double* d_sum, void* d_workspace,
                           size_t workspace_bytes, void* stream);
 
+/* Significant samples of a weighted batch, the step after the coarse weights
+ * (RELION's pass-0 significance; its device kernels in the reference harness
+ * are cuda_kernel_find_threshold_idx_in_cumulative and
+ * cuda_kernel_array_over_threshold, src/cuda_device_utils.cuh:238-266).  For
+ * particle p, over its weights d_weights[p][0..n) that are > 0 and finite,
+ * sorted ascending with inclusive cumulative sums c_k:
+ *   thr  = (1 - adaptive_fraction) * d_sum[p]
+ *   idx  = i + 1 for the i with c_i <= thr < c_{i+1}, else 0
+ *   nsig = count - idx; if max_significants > 0 and nsig > max_significants:
+ *          nsig = max_significants, idx = count - nsig
+ *   d_sig_weight[p] = sorted[idx],  d_nsig[p] = nsig,
+ *   d_passed[p][i]  = d_weights[p][i] >= d_sig_weight[p]   (0 or 1; optional)
+ * The cumulative sums are taken exactly (no sort: radix selection with exact
+ * integer bucket sums, double-double across buckets), so the result is that
+ * of exact arithmetic; a particle with no positive weight gets nsig = 0 and
+ * d_sig_weight = +inf (nothing passes).  n < 2^27 per particle.  The
+ * workspace is b200d2_significance_workspace(P, n) bytes of device memory
+ * (about 8 bytes per weight), contents ignored; one call at a time per
+ * workspace.  Asynchronous on `stream`. */
+size_t b200d2_significance_workspace(int P, long long n);
+int b200d2_significance(const double* d_weights, int P, long long n,
+                        const double* d_sum, double adaptive_fraction,
+                        long long max_significants, double* d_sig_weight,
+                        long long* d_nsig, uint8_t* d_passed,
+                        void* d_workspace, size_t workspace_bytes,
+                        void* stream);
+
 /* Final combination diff2 = nA - 2 cross of the tensor-core forms, where nA =
  * sum w|X|^2 + sum w|A|^2 is accumulated in FP64 and cross comes from the
  * FP32 tensor-core accumulator.  B200D2_COMBINE_DF32 (default): nA is kept as

@@ -188,6 +188,51 @@ def weights_from_diff2(d: np.ndarray) -> tuple[float, np.ndarray]:
     return mn, w / w.sum()
 
 
+def significance(w: np.ndarray, total: float, adaptive_fraction: float, max_significants: int = 0):
+    """Significant samples of one particle's weights, RELION's pass-0 steps
+    around the reference's cuda_kernel_find_threshold_idx_in_cumulative and
+    cuda_kernel_array_over_threshold (src/cuda_device_utils.cuh:238-266):
+    keep the weights > 0 (finite), sort them ascending, take inclusive
+    cumulative sums c_k, idx = i + 1 for the i with c_i <= thr < c_{i+1}
+    (else 0) at thr = (1 - adaptive_fraction) * total, nsig = count - idx
+    capped at max_significants (idx = count - nsig), threshold weight
+    sorted[idx], mask w >= threshold.
+
+    The cumulative sums are exact: every double is an integer multiple of a
+    common power of two, added as Python integers.  Returns (sig_weight,
+    nsig, passed, margin), margin = min |c_k - thr| / max(|c_k|, |thr|) over
+    the two sums either side of the crossing (how far the decision is from a
+    tie)."""
+    import bisect
+    import itertools
+    w = np.asarray(w, np.float64).ravel()
+    pos = np.sort(w[(w > 0) & np.isfinite(w)])
+    cnt = int(pos.size)
+    if cnt == 0:
+        return float("inf"), 0, np.zeros(w.size, np.uint8), float("inf")
+    thr = float(np.float64(1.0 - adaptive_fraction) * np.float64(total))
+    mant, expo = np.frexp(pos)
+    M = (mant * 2.0 ** 53).astype(np.int64)
+    E = expo.astype(np.int64) - 53
+    tm, te = np.frexp(thr)
+    tM, tE = int(tm * 2.0 ** 53), int(te) - 53
+    base = int(min(E.min(), tE))
+    vals = [int(m) << int(e - base) for m, e in zip(M.tolist(), E.tolist())]
+    cum = list(itertools.accumulate(vals))
+    thr_i = tM << (tE - base) if tM >= 0 else -((-tM) << (tE - base))
+    k = bisect.bisect_right(cum, thr_i)  # number of c_i <= thr
+    idx = k if 1 <= k <= cnt - 1 else 0
+    # distance of the decision from a tie, relative to the sums compared
+    margin = min((abs(cum[j] - thr_i) / max(abs(cum[j]), abs(thr_i)) for j in (k - 1, k) if 0 <= j < cnt),
+                 default=float("inf"))
+    nsig = cnt - idx
+    if max_significants > 0 and nsig > max_significants:
+        nsig = int(max_significants)
+        idx = cnt - nsig
+    sig = float(pos[idx])
+    return sig, nsig, (w >= sig).astype(np.uint8), margin
+
+
 # --------------------------------------------------------------------------
 # the reference project's own kernels (GPU), compiled into oracle/_ref
 # --------------------------------------------------------------------------
@@ -211,6 +256,9 @@ def ref_lib():
         L.refshim_variant_workspace_bytes.argtypes = [C.c_int] * 6
         L.refshim_variant_workspace_bytes.restype = C.c_size_t
         L.refshim_variant_run.argtypes = [C.c_int, P] + [C.c_int] * 4 + [P] * 9 + [C.c_int] * 5 + [P]
+        if hasattr(L, "refshim_find_threshold_idx"):
+            L.refshim_find_threshold_idx.argtypes = [P, C.c_double, C.c_long, P, P]
+            L.refshim_array_over_threshold.argtypes = [P, P, C.c_double, C.c_long, P]
         if hasattr(L, "refshim_diff2_fine"):
             L.refshim_diff2_fine.argtypes = ([P] + [C.c_int] * 4 + [P] * 7 + [C.c_long, C.c_float] + [C.c_long] * 3 +
                                              [P] * 4 + [P])

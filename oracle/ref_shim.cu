@@ -15,6 +15,8 @@
 //   runDiff2KernelCoarseDouble                src/acc_helper_functions_impl.h:503-854
 //   CoarseMatrixKernel*::run (5 variants)     src/coarse_splitImg_*.cuh
 //   cuda_kernel_diff2_fine (no host wrapper)  src/diff2.cuh:540-682
+//   cuda_kernel_find_threshold_idx_in_cumulative,
+//   cuda_kernel_array_over_threshold          src/cuda_device_utils.cuh:238-266
 // The reference's texture projector is used.  Its PROJECTOR_NO_TEXTURES
 // configuration does not compile (src/diff2.cuh:16 includes
 // src/orientation_matrix_handler.cuh, which calls tex3D unconditionally at
@@ -52,7 +54,7 @@ AccProjectorKernel make_view(RefProjector* p, int imgX, int imgY, int imgZ,
 
 extern "C" {
 
-int refshim_abi_version(void) { return 3; }
+int refshim_abi_version(void) { return 4; }
 
 void* refshim_projector_create(int mdlX, int mdlY, int mdlZ, int initY,
                                int initZ, int maxR, float pf, const float* re,
@@ -173,6 +175,30 @@ int refshim_diff2_fine(void* h, int imgX, int imgY, int imgZ, int imgMaxR, float
   cuda_kernel_diff2_fine<true, false, 128, 16><<<(unsigned)todo_blocks, 128, 0, (cudaStream_t)stream>>>(
       d_eulers, d_re, d_im, d_tx, d_ty, nullptr, k, d_corr, d_diff2s, (unsigned)image_size, sum_init,
       (unsigned long)O, (unsigned long)T, (unsigned long)todo_blocks, d_rot_idx, d_trans_idx, d_job_idx, d_job_num);
+  return (int)cudaGetLastError();
+}
+
+// The significance kernels, launched the way RELION's host helpers
+// (findThresholdIdxInCumulativeSum, arrayOverThreshold) do: a grid over the
+// array, the index word cleared first; block size 256.
+int refshim_find_threshold_idx(double* d_cum, double thr, long size, unsigned long* d_idx, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(d_idx, 0, sizeof(size_t), s);
+  if (e != cudaSuccess) return (int)e;
+  const int bs = 256;
+  const long grid = size > 1 ? (size - 1 + bs - 1) / bs : 0;
+  if (grid == 0) return 0;
+  cuda_kernel_find_threshold_idx_in_cumulative<double><<<(unsigned)grid, bs, 0, s>>>(
+      d_cum, thr, (size_t)(size - 1), reinterpret_cast<size_t*>(d_idx), bs);
+  return (int)cudaGetLastError();
+}
+
+int refshim_array_over_threshold(double* d_data, bool* d_passed, double thr, long size, void* stream) {
+  const int bs = 256;
+  const long grid = (size + bs - 1) / bs;
+  if (grid == 0) return 0;
+  cuda_kernel_array_over_threshold<double><<<(unsigned)grid, bs, 0, (cudaStream_t)stream>>>(
+      d_data, d_passed, thr, (size_t)size, bs);
   return (int)cudaGetLastError();
 }
 

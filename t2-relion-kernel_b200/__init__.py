@@ -153,6 +153,7 @@ def _declare(L):
         "b200d2_server_get_stats": [P, C.POINTER(ServerStats)],
         "b200d2_server_destroy": [P],
         "b200d2_coarse_weights": [P, I, I, I, P, P, P, I, P, P, P, Z, P],
+        "b200d2_significance": [P, I, C.c_longlong, P, C.c_double, C.c_longlong, P, P, P, P, Z, P],
         "b200d2_set_gemm_variant": [I, I, I, I],
         "b200d2_set_combine": [I],
         "b200d2_diff2_fine": [C.POINTER(View), P, P, P, P, P, P, P, Z, F, Z, P, P, P, P, P],
@@ -172,6 +173,8 @@ def _declare(L):
     L.b200d2_workspace_status.restype = C.c_int
     L.b200d2_coarse_weights_workspace.argtypes = [I, C.c_longlong]
     L.b200d2_coarse_weights_workspace.restype = C.c_size_t
+    L.b200d2_significance_workspace.argtypes = [I, C.c_longlong]
+    L.b200d2_significance_workspace.restype = C.c_size_t
     L.b200d2_launch_count.argtypes = []
     L.b200d2_launch_count.restype = C.c_ulonglong
     # optional entry points declared by later modules of the library
@@ -484,6 +487,35 @@ def coarse_weights(diff2, P: int, O: int, T: int, out_min=None, pdf_orient=None,
                                        1 if normalize else 0, _ptr(weights), _ptr(sums), _ptr(workspace), nb,
                                        _stream(stream)), "coarse_weights")
     return weights, sums
+
+
+def significance(weights, sums, adaptive_fraction: float, max_significants: int = 0, *, passed=True,
+                 sig_weight=None, nsig=None, workspace=None, stream=None):
+    """Significant samples per particle (b200d2_significance).  weights: CUDA
+    float64 [P, n] (any shape with P rows); sums: CUDA float64 [P].  Returns
+    (sig_weight [P] float64, nsig [P] int64, passed [P, n] uint8 or None):
+    the threshold weight sorted[idx] of the positive weights in ascending
+    order, the number of significant samples, and the mask w >= sig_weight."""
+    import torch
+    P = int(weights.shape[0])
+    n = int(weights.numel() // max(P, 1))
+    dev = weights.device
+    if sig_weight is None:
+        sig_weight = torch.empty(P, dtype=torch.float64, device=dev)
+    if nsig is None:
+        nsig = torch.empty(P, dtype=torch.int64, device=dev)
+    mask = None
+    if passed is True:
+        mask = torch.empty((P, n), dtype=torch.uint8, device=dev)
+    elif passed is not None and passed is not False:
+        mask = passed
+    nb = lib().b200d2_significance_workspace(P, n)
+    if workspace is None or workspace.numel() < nb:
+        workspace = torch.empty(max(nb, 1), dtype=torch.uint8, device=dev)
+    _check(lib().b200d2_significance(_ptr(weights), P, n, _ptr(sums), float(adaptive_fraction), int(max_significants),
+                                     _ptr(sig_weight), _ptr(nsig), _ptr(mask), _ptr(workspace), nb, _stream(stream)),
+           "significance")
+    return sig_weight, nsig, mask
 
 
 def ctf_fold(real, imag, ctf_params: list, minvsigma2, *, imgX: int, imgY: int, maxR: int, ori_size: int,

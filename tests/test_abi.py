@@ -48,6 +48,15 @@ def test_host_side_argument_validation(pkg):
     assert lib.b200d2_set_gemm_variant(96, 0, 0, 0) == 1 and lib.b200d2_set_gemm_variant(0, 192, 0, 0) == 1
     assert lib.b200d2_set_gemm_variant(0, 0, 0, 3) == 1
     assert lib.b200d2_set_gemm_variant(0, 0, 0, 0) == 0
+    # significance: nothing to do for no particles; missing outputs, NaN
+    # fraction, oversized rows and short workspaces rejected before any launch
+    assert lib.b200d2_significance(None, 0, 10, None, 0.999, 0, None, None, None, None, 0, None) == 0
+    assert lib.b200d2_significance(None, 2, 10, None, 0.999, 0, None, None, None, None, 0, None) == 1
+    assert lib.b200d2_significance(None, 2, 10, None, float("nan"), 0, 8, 8, None, None, 0, None) == 1
+    assert lib.b200d2_significance(8, 2, 1 << 27, 8, 0.999, 0, 8, 8, None, 8, 1 << 40, None) == 2
+    assert lib.b200d2_significance(8, 2, 10, 8, 0.999, 0, 8, 8, None, 8, 16, None) == 1
+    assert lib.b200d2_significance_workspace(0, 10) == 0
+    assert lib.b200d2_significance_workspace(2, 1000) >= 2 * 1000 * 8
     assert lib.b200d2_coarse_weights_workspace(0, 100) == 0
     assert lib.b200d2_coarse_weights_workspace(3, 70000) >= 3 * 8 + 3 * 3 * 8 + 3 * 4
 

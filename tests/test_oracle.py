@@ -96,6 +96,60 @@ def test_weights_normalised(oracle):
     assert mn == 1.0 and w.sum() == pytest.approx(1.0) and np.argmax(w) == 1
 
 
+def _naive_significance(w, total, frac, maxsig):
+    """The same steps with a floating-point cumulative sum (numpy, sequential)."""
+    pos = np.sort(w[(w > 0) & np.isfinite(w)])
+    if pos.size == 0:
+        return float("inf"), 0
+    c = np.cumsum(pos)
+    k = int(np.searchsorted(c, (1.0 - frac) * total, side="right"))
+    idx = k if 1 <= k <= pos.size - 1 else 0
+    nsig = pos.size - idx
+    if maxsig > 0 and nsig > maxsig:
+        nsig, idx = maxsig, pos.size - maxsig
+    return float(pos[idx]), nsig
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_significance_oracle_matches_sorted_scan(oracle, seed):
+    """Away from ties the exact-sum restatement equals a sort + FP64 scan."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(1, 20000))
+    w = np.exp(-rng.exponential(rng.uniform(1, 200), n))
+    w[rng.random(n) < 0.2] = 0.0
+    frac = float(rng.choice([0.999, 0.99, 0.5, 1.0, 0.0]))
+    maxsig = int(rng.choice([0, 5, 1000]))
+    sig, nsig, passed, margin = oracle.significance(w, w.sum(), frac, maxsig)
+    if margin > 1e-9:
+        assert (sig, nsig) == _naive_significance(w, w.sum(), frac, maxsig)
+    assert passed.sum() >= nsig and (passed == (w >= sig)).all()
+
+
+def test_significance_oracle_edge_cases(oracle):
+    inf = float("inf")
+    # no positive weight: nothing significant
+    assert oracle.significance(np.zeros(5), 0.0, 0.999)[:2] == (inf, 0)
+    # fraction 0: thr equals the total, no crossing, idx 0, every positive weight
+    w = np.array([0.0, 1.0, 2.0, 3.0])
+    assert oracle.significance(w, 6.0, 0.0)[:2] == (1.0, 3)
+    # fraction 1: thr = 0 < c_0, idx 0
+    assert oracle.significance(w, 6.0, 1.0)[:2] == (1.0, 3)
+    # thr = 1.5: c = 1, 3, 6 -> idx 1, threshold 2, two significant
+    assert oracle.significance(w, 6.0, 0.75)[:2] == (2.0, 2)
+    # a cumulative sum equal to thr counts as below it (c_i <= thr)
+    assert oracle.significance(w, 6.0, 0.5)[:2] == (3.0, 1)
+    # ties: [1, 1, 1, 1], thr = 2.5 -> c = 1, 2, 3, 4, idx 2, threshold 1, nsig 2,
+    # but all four pass the mask (w >= 1)
+    sig, nsig, passed, _ = oracle.significance(np.ones(4), 4.0, 0.375)
+    assert (sig, nsig, int(passed.sum())) == (1.0, 2, 4)
+    # cap at two: idx = 3 - 2 = 1
+    assert oracle.significance(w, 6.0, 1.0, 2)[:2] == (2.0, 2)
+    # negative, NaN and infinite weights take no part in the sums
+    w2 = np.array([-1.0, np.nan, np.inf, 1.0, 2.0])
+    sig, nsig, passed, _ = oracle.significance(w2, 3.0, 0.5)
+    assert (sig, nsig) == (2.0, 1) and passed.tolist() == [0, 0, 1, 0, 1]
+
+
 def test_healpix_grid(synth):
     import importlib
     hp = importlib.import_module("relion_b200.healpix")
