@@ -174,7 +174,7 @@ def parse():
                     help="final combination nA - 2 cross: double-float (default) or FP64")
     ap.add_argument("--gemm-variant", default=None,
                     help="row_bytes,tile_n,split,pair for the contraction (0 = default; pair 1 = CTA pairs)")
-    ap.add_argument("--study", default=None, choices=["precision", "fine", "significance"],
+    ap.add_argument("--study", default=None, choices=["precision", "fine", "significance", "cc"],
                     help="precision: error of every precision form vs the FP64 kernel (use --config c3)")
     return ap.parse_args()
 
@@ -714,6 +714,93 @@ def significance_study(args):
     return 0
 
 
+def cc_study(args):
+    """Cross-correlation coarse score (one JSON line): the C2 batch (256
+    particles x 4608 orientations x 113 translations at image 64) scored with
+    B200D2_SCORE_CC on the tensor cores (BF16x3, TF32x3) and on the FP32 CUDA-core
+    kernel, against the reference's own CC path (runDiff2KernelCoarse with
+    do_CC, one launch per particle) timed on 8 particles and scaled to the
+    batch; the error is measured against the FP64 CC kernel on 4 particles."""
+    import torch
+    pkg = load_package()
+    synth = load_synth()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the reference's own kernels, built from its sources into oracle/_ref
+    pr = synth.make_problem("c2")
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dev = "cuda"
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)  # noqa: E731
+    eul, tx, ty = t(pr.eulers.reshape(-1)), t(pr.trans_x), t(pr.trans_y)
+    re, im, co = t(pr.fimg_re), t(pr.fimg_im), t(pr.corr)
+    n = pr.O * pr.T
+    evals = pr.P * n
+    outs = {}
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    res = {}
+    for name, prec, reps in (("bf16x3", pkg.PREC_BF16X3, 10), ("tf32x3", pkg.PREC_TF32X3, 10),
+                             ("fp32", pkg.PREC_FP32, 2)):
+        out = torch.empty(evals, device=dev)
+        mn = torch.empty(pr.P, device=dev, dtype=torch.float64)
+        am = torch.empty(pr.P, device=dev, dtype=torch.int64)
+        b = pkg.make_batch(eul, tx, ty, re, im, co, out, O=pr.O, T=pr.T, P=pr.P, N_img=pr.N_img, out_min=mn,
+                           out_argmin=am, score=pkg.SCORE_CC)
+        ws = torch.empty(max(pkg.batch_workspace_bytes(view, b, prec), 1), device=dev, dtype=torch.uint8)
+        ms = timed(lambda: pkg.diff2_coarse_batch(view, b, prec, ws), reps)
+        outs[name] = out
+        res[name] = {"ms": ms, "evals_per_s": evals / (ms / 1e3)}
+        del ws
+    # the reference's CC path, 8 particles
+    L = oracle.ref_lib()
+    pv = pr.projector
+    h = L.refshim_projector_create(pv.mdlX, pv.mdlY, pv.mdlZ, pv.mdlInitY, pv.mdlInitZ, pv.mdlMaxR,
+                                   pv.padding_factor, np.ascontiguousarray(pv.re, np.float32).ctypes.data,
+                                   np.ascontiguousarray(pv.im, np.float32).ctypes.data)
+    sample = 8
+    rout = torch.empty((sample, n), device=dev)
+
+    def ref():
+        for p in range(sample):
+            L.refshim_diff2_coarse_cc(h, pr.imgX, pr.imgY, 1, pr.imgMaxR, eul.data_ptr(), tx.data_ptr(),
+                                      ty.data_ptr(), co[p].data_ptr(), re[p].data_ptr(), im[p].data_ptr(),
+                                      rout[p].data_ptr(), pr.O, pr.T, pr.N_img, None)
+
+    ms_ref = timed(ref, 1) * pr.P / sample
+    L.refshim_projector_destroy(h)
+    # errors against FP64 on 4 particles, relative to each particle's largest magnitude
+    errs = {k: 0.0 for k in outs}
+    errs["reference"] = 0.0
+    for p in range(4):
+        r64 = torch.zeros(n, device=dev, dtype=torch.float64)
+        pkg.run_diff2_kernel_coarse_cc_double(view, tx, ty, co[p], re[p], im[p], eul, r64, pr.O, pr.T, pr.N_img)
+        scale = float(r64.abs().max())
+        for k, o in outs.items():
+            errs[k] = max(errs[k], float((o[p * n:(p + 1) * n].double() - r64).abs().max()) / scale)
+        errs["reference"] = max(errs["reference"], float((rout[p].double() - r64).abs().max()) / scale)
+    res["reference"] = {"ms": ms_ref, "evals_per_s": evals / (ms_ref / 1e3),
+                        "note": f"timed on {sample} particles, scaled to {pr.P}"}
+    line = {"study": "cc", "workload": f"C2: {pr.P} particles x {pr.O} orientations x {pr.T} translations "
+                                       f"(image 64), CC score", "results": res,
+            "speedup_bf16x3_vs_reference": ms_ref / res["bf16x3"]["ms"],
+            "speedup_tf32x3_vs_reference": ms_ref / res["tf32x3"]["ms"],
+            "speedup_fp32_vs_reference": ms_ref / res["fp32"]["ms"],
+            "max_err_vs_fp64_rel_to_max": errs}
+    print(json.dumps(line), flush=True)
+    proj.close()
+    return 0
+
+
 C5_REFS = ("c5s", "c5m", "c5l")
 
 
@@ -827,6 +914,8 @@ def main():
         return fine_study(args)
     if args.study == "significance":
         return significance_study(args)
+    if args.study == "cc":
+        return cc_study(args)
     if args.config == "c5":
         return serving_arm(args)
     if args.impl == "reference":

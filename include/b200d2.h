@@ -146,6 +146,25 @@ int b200d2_diff2_coarse_f64(const b200d2_view* view, const float* d_trans_x,
                             size_t T, size_t N_img, int filter_img,
                             void* stream);
 
+/* Cross-correlation coarse score (replaces the do_CC branch of
+ * runDiff2KernelCoarse, src/acc_helper_functions_impl.h:441-498, 3D reference
+ * and 2D images: cuda_kernel_diff2_CC_coarse, src/diff2.cuh:691-809):
+ *   d_diff2s[o*T + t] = -(sum_px corr Re(conj(A_o) S_t)) / sqrt(sum_px corr |A_o|^2)
+ * written, not accumulated (as the reference does).  Pixels outside the
+ * projector radius have A = 0 and take no part.  FP32 sums
+ * (precision B200D2_PREC_FP32); the _f64 form sums in FP64.  The reference's
+ * local_sqrtXi2 argument is not used by its kernel and is not taken here. */
+int b200d2_diff2_coarse_cc(const b200d2_view* view, const float* d_trans_x,
+                           const float* d_trans_y, const float* d_corr,
+                           const float* d_real, const float* d_imag,
+                           const float* d_eulers, float* d_diff2s, size_t O,
+                           size_t T, size_t N_img, void* stream, int precision);
+int b200d2_diff2_coarse_cc_f64(const b200d2_view* view, const float* d_trans_x,
+                               const float* d_trans_y, const float* d_corr,
+                               const float* d_real, const float* d_imag,
+                               const float* d_eulers, double* d_diff2s, size_t O,
+                               size_t T, size_t N_img, void* stream);
+
 /* Fine-pass diff2 over a job list (replaces cuda_kernel_diff2_fine,
  * src/diff2.cuh:540-682, 2D image against a 3D reference; the reference has
  * no host wrapper for it).  Job j (j < todo_blocks) scores orientation
@@ -194,7 +213,15 @@ typedef struct b200d2_batch {
    * radius (they add only corr/2 |X|^2).  Tensor-core precisions only. */
   const float* d_coor_xy;
   int n_listed;
+  /* B200D2_SCORE_DIFF2 (0): diff2 as above.  B200D2_SCORE_CC (1): the
+   * cross-correlation score of cuda_kernel_diff2_CC_coarse
+   * (src/diff2.cuh:691-809), d_diff2[p][o][t] = -sum corr Re(conj(A_o) S_t)
+   * / sqrt(sum corr |A_o|^2), with d_min / d_argmin the most negative score.
+   * FP32 CUDA cores and the tensor-core forms (norms in FP64). */
+  int score;
 } b200d2_batch;
+
+enum { B200D2_SCORE_DIFF2 = 0, B200D2_SCORE_CC = 1 };
 
 /* Bytes of device scratch the batch needs for `precision` (0 for the
  * CUDA-core paths). */

@@ -12,7 +12,8 @@
 // Differences a caller may notice:
 //   * errors throw b200d2_relion_error (the reference raises SIGSEGV through
 //     HANDLE_ERROR, src/common.h:20-36);
-//   * the do_CC and data_is_3D branches are not provided (they throw);
+//   * do_CC runs the CC score (b200d2_diff2_coarse_cc); the data_is_3D
+//     branches are not provided (they throw);
 //   * the optimised functor runs the tensor-core pipeline (BF16 3-term split
 //     by default, B200D2_RELION_FUNCTOR_PRECISION to change) and its
 //     workspace needs no 0xff pre-fill.
@@ -157,14 +158,22 @@ class AccProjectorKernel {
   }
 };
 
-// diff2s[o*T + t] += diff2(o, t)  (FP32 CUDA cores, asynchronous on `stream`)
+// diff2s[o*T + t] += diff2(o, t)  (FP32 CUDA cores, asynchronous on `stream`);
+// with do_CC, diff2s[o*T + t] = -cross / sqrt(norm) as cuda_kernel_diff2_CC_coarse
+// (src/diff2.cuh:691-809) writes it.
 inline void runDiff2KernelCoarse(AccProjectorKernel& projector, XFLOAT* trans_x, XFLOAT* trans_y,
                                  XFLOAT* /*trans_z*/, XFLOAT* corr_img, XFLOAT* Fimg_real, XFLOAT* Fimg_imag,
                                  XFLOAT* d_eulers, XFLOAT* diff2s, XFLOAT /*local_sqrtXi2*/,
                                  unsigned long orientation_num, unsigned long translation_num,
                                  unsigned long image_size, cudaStream_t stream, bool do_CC, bool data_is_3D) {
-  if (do_CC) throw b200d2_relion_error("runDiff2KernelCoarse: do_CC", B200D2_ERR_UNSUPPORTED);
   if (data_is_3D) throw b200d2_relion_error("runDiff2KernelCoarse: data_is_3D", B200D2_ERR_UNSUPPORTED);
+  if (do_CC) {
+    b200d2_relion_detail::check(
+        b200d2_diff2_coarse_cc(&projector.view, trans_x, trans_y, corr_img, Fimg_real, Fimg_imag, d_eulers, diff2s,
+                               orientation_num, translation_num, image_size, stream, B200D2_PREC_FP32),
+        "runDiff2KernelCoarse(do_CC)");
+    return;
+  }
   b200d2_relion_detail::check(
       b200d2_diff2_coarse(&projector.view, trans_x, trans_y, corr_img, Fimg_real, Fimg_imag, d_eulers, diff2s,
                           orientation_num, translation_num, image_size, stream, B200D2_PREC_FP32),
@@ -177,7 +186,9 @@ inline void runDiff2KernelCoarseDouble(AccProjectorKernel& projector, XFLOAT* tr
                                        XFLOAT /*local_sqrtXi2*/, unsigned long orientation_num,
                                        unsigned long translation_num, unsigned long image_size,
                                        cudaStream_t stream, bool do_CC, bool data_is_3D, bool filter_img = false) {
-  if (do_CC) throw b200d2_relion_error("runDiff2KernelCoarseDouble: do_CC", B200D2_ERR_UNSUPPORTED);
+  // the reference's FP64 dispatcher has no CC branch: do_CC is ignored there
+  // (src/acc_helper_functions_impl.h:503-854), and here
+  (void)do_CC;
   if (data_is_3D) throw b200d2_relion_error("runDiff2KernelCoarseDouble: data_is_3D", B200D2_ERR_UNSUPPORTED);
   b200d2_relion_detail::check(
       b200d2_diff2_coarse_f64(&projector.view, trans_x, trans_y, corr_img, Fimg_real, Fimg_imag, d_eulers,

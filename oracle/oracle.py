@@ -151,6 +151,39 @@ def diff2_coarse_f32(proj: Projector, eulers, trans_x, trans_y, fre, fim, corr,
     return out
 
 
+def cc_coarse_f64(proj: Projector, eulers, trans_x, trans_y, fre, fim, corr, projections=None) -> np.ndarray:
+    """FP64 restatement of cuda_kernel_diff2_CC_coarse (src/diff2.cuh:691-809)
+    for one particle: cc[o][t] = -sum corr Re(conj(A_o) S_t) / sqrt(sum corr
+    |A_o|^2) over the pixels inside the projector radius (elsewhere A = 0).
+    Projections are the oracle's (project3Dmodel restatement); the phase shift
+    is translatePixel's (src/cuda_device_utils.cuh:110-129) in FP64.
+    projections: optional (re, im) [O][N_img] samples to use instead (e.g.
+    the texture unit's own, to compare arithmetic without the texture-weight
+    model)."""
+    v = proj.s
+    n = fre.size
+    x = np.arange(n) % v.imgX
+    y = np.arange(n) // v.imgX
+    y = np.where(y > v.maxR, y - v.imgY, y)
+    # every pixel is projected (0 outside the radius), so the sums are exact
+    inside = np.ones(n, bool)
+    px, py = x.astype(np.int32), y.astype(np.int32)
+    O = eulers.reshape(-1, 9).shape[0]
+    ar, ai = project_pixels(proj, eulers, px, py) if projections is None else projections
+    ar = ar.reshape(O, -1).astype(np.float64)
+    ai = ai.reshape(O, -1).astype(np.float64)
+    w = np.asarray(corr, np.float64)[inside]
+    xr = np.asarray(fre, np.float64)[inside]
+    xi = np.asarray(fim, np.float64)[inside]
+    ph = np.outer(np.asarray(trans_x, np.float64), px) + np.outer(np.asarray(trans_y, np.float64), py)
+    c, s = np.cos(ph), np.sin(ph)
+    sr = c * xr - s * xi  # [T][K]
+    si = c * xi + s * xr
+    cross = (ar * w) @ sr.T + (ai * w) @ si.T  # [O][T]
+    norm = (ar * ar + ai * ai) @ w
+    return -cross / np.sqrt(norm)[:, None]
+
+
 def filter_image(proj: Projector, fre, fim, corr):
     """FilterCoarseParamImage restatement -> (re, im, corr, coor_xy, n_inside)."""
     N = fre.size
@@ -252,6 +285,8 @@ def ref_lib():
         L.refshim_projector_create.restype = P
         L.refshim_projector_destroy.argtypes = [P]
         L.refshim_diff2_coarse.argtypes = [P] + [C.c_int] * 4 + [P] * 7 + [C.c_long] * 3 + [P]
+        if hasattr(L, "refshim_diff2_coarse_cc"):
+            L.refshim_diff2_coarse_cc.argtypes = [P] + [C.c_int] * 4 + [P] * 7 + [C.c_long] * 3 + [P]
         L.refshim_diff2_coarse_double.argtypes = [P] + [C.c_int] * 4 + [P] * 7 + [C.c_long] * 3 + [C.c_int, P]
         L.refshim_variant_workspace_bytes.argtypes = [C.c_int] * 6
         L.refshim_variant_workspace_bytes.restype = C.c_size_t

@@ -15,6 +15,7 @@
 //   runDiff2KernelCoarseDouble                src/acc_helper_functions_impl.h:503-854
 //   CoarseMatrixKernel*::run (5 variants)     src/coarse_splitImg_*.cuh
 //   cuda_kernel_diff2_fine (no host wrapper)  src/diff2.cuh:540-682
+//   runDiff2KernelCoarse with do_CC           src/acc_helper_functions_impl.h:441-498
 //   cuda_kernel_find_threshold_idx_in_cumulative,
 //   cuda_kernel_array_over_threshold          src/cuda_device_utils.cuh:238-266
 // The reference's texture projector is used.  Its PROJECTOR_NO_TEXTURES
@@ -54,7 +55,7 @@ AccProjectorKernel make_view(RefProjector* p, int imgX, int imgY, int imgZ,
 
 extern "C" {
 
-int refshim_abi_version(void) { return 4; }
+int refshim_abi_version(void) { return 5; }
 
 void* refshim_projector_create(int mdlX, int mdlY, int mdlZ, int initY,
                                int initZ, int maxR, float pf, const float* re,
@@ -83,6 +84,21 @@ int refshim_diff2_coarse(void* h, int imgX, int imgY, int imgZ, int imgMaxR,
   runDiff2KernelCoarse(k, d_tx, d_ty, nullptr, d_corr, d_re, d_im, d_eulers,
                        d_diff2s, 1.f, (unsigned long)O, (unsigned long)T,
                        (unsigned long)N_img, (cudaStream_t)stream, false,
+                       false);
+  return (int)cudaGetLastError();
+}
+
+// runDiff2KernelCoarse with do_CC (cuda_kernel_diff2_CC_coarse, src/diff2.cuh:691-809)
+int refshim_diff2_coarse_cc(void* h, int imgX, int imgY, int imgZ, int imgMaxR,
+                            float* d_eulers, float* d_tx, float* d_ty,
+                            float* d_corr, float* d_re, float* d_im,
+                            float* d_diff2s, long O, long T, long N_img,
+                            void* stream) {
+  RefProjector* p = reinterpret_cast<RefProjector*>(h);
+  AccProjectorKernel k = make_view(p, imgX, imgY, imgZ, imgMaxR);
+  runDiff2KernelCoarse(k, d_tx, d_ty, nullptr, d_corr, d_re, d_im, d_eulers,
+                       d_diff2s, 1.f, (unsigned long)O, (unsigned long)T,
+                       (unsigned long)N_img, (cudaStream_t)stream, true,
                        false);
   return (int)cudaGetLastError();
 }

@@ -59,7 +59,12 @@ class Batch(C.Structure):
                 ("T", C.c_int), ("P", C.c_int), ("N_img", C.c_int), ("d_real", C.c_void_p),
                 ("d_imag", C.c_void_p), ("d_corr", C.c_void_p), ("img_stride", C.c_longlong),
                 ("d_diff2", C.c_void_p), ("accumulate", C.c_int), ("d_min", C.c_void_p),
-                ("d_argmin", C.c_void_p), ("d_coor_xy", C.c_void_p), ("n_listed", C.c_int)]
+                ("d_argmin", C.c_void_p), ("d_coor_xy", C.c_void_p), ("n_listed", C.c_int),
+                ("score", C.c_int)]
+
+
+SCORE_DIFF2 = 0
+SCORE_CC = 1
 
 
 class ParticleDesc(C.Structure):
@@ -138,6 +143,8 @@ def _declare(L):
         "b200d2_projector_view": [P, I, I, I, I, I, C.POINTER(View)],
         "b200d2_diff2_coarse": [C.POINTER(View), P, P, P, P, P, P, P, Z, Z, Z, P, I],
         "b200d2_diff2_coarse_f64": [C.POINTER(View), P, P, P, P, P, P, P, Z, Z, Z, I, P],
+        "b200d2_diff2_coarse_cc": [C.POINTER(View), P, P, P, P, P, P, P, Z, Z, Z, P, I],
+        "b200d2_diff2_coarse_cc_f64": [C.POINTER(View), P, P, P, P, P, P, P, Z, Z, Z, P],
         "b200d2_diff2_coarse_batch": [C.POINTER(View), C.POINTER(Batch), I, P, Z, P],
         "b200d2_minloc": [P, C.c_longlong, I, P, P, P],
         "b200d2_project_pixels": [C.POINTER(View), P, I, P, P, I, P, P, P],
@@ -282,6 +289,22 @@ def run_diff2_kernel_coarse_double(view: View, trans_x, trans_y, corr, real, ima
                                          1 if filter_img else 0, _stream(stream)), "diff2_coarse_f64")
 
 
+def run_diff2_kernel_coarse_cc(view: View, trans_x, trans_y, corr, real, imag, eulers, diff2s,
+                               O: int, T: int, N_img: int, stream=None, precision: int = PREC_FP32):
+    """runDiff2KernelCoarse with do_CC: diff2s[o*T+t] = -cross / sqrt(norm) (written)."""
+    _check(lib().b200d2_diff2_coarse_cc(C.byref(view), _ptr(trans_x), _ptr(trans_y), _ptr(corr), _ptr(real),
+                                        _ptr(imag), _ptr(eulers), _ptr(diff2s), O, T, N_img, _stream(stream),
+                                        precision), "diff2_coarse_cc")
+
+
+def run_diff2_kernel_coarse_cc_double(view: View, trans_x, trans_y, corr, real, imag, eulers, diff2s,
+                                      O: int, T: int, N_img: int, stream=None):
+    """The CC score summed in FP64 (diff2s double, written)."""
+    _check(lib().b200d2_diff2_coarse_cc_f64(C.byref(view), _ptr(trans_x), _ptr(trans_y), _ptr(corr), _ptr(real),
+                                            _ptr(imag), _ptr(eulers), _ptr(diff2s), O, T, N_img, _stream(stream)),
+           "diff2_coarse_cc_f64")
+
+
 def launch_count() -> int:
     """Kernels launched by libb200d2 in this process so far."""
     return int(lib().b200d2_launch_count())
@@ -289,8 +312,9 @@ def launch_count() -> int:
 
 def make_batch(eulers, trans_x, trans_y, real, imag, corr, diff2, *, O: int, T: int, P: int, N_img: int,
                img_stride: int | None = None, accumulate: bool = False, out_min=None, out_argmin=None,
-               coor_xy=None, n_listed: int = 0) -> Batch:
+               coor_xy=None, n_listed: int = 0, score: int = SCORE_DIFF2) -> Batch:
     b = Batch()
+    b.score = score
     b.d_coor_xy = _ptr(coor_xy)
     b.n_listed = n_listed if coor_xy is not None else 0
     b.d_eulers, b.O = _ptr(eulers), O

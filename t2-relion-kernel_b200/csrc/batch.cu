@@ -12,7 +12,7 @@ int direct_batch(const b200d2_view& view, const float* eulers, const float* tx,
                  const float* ty, const float* re, const float* im,
                  const float* corr, long long img_stride, void* out,
                  long long out_stride, int O, int T, int N_img, int P,
-                 bool fp64, int filter_img, cudaStream_t s);
+                 bool fp64, int filter_img, cudaStream_t s, int cc, int accumulate);
 int minloc(const float* d, long long n, int P, double* mn, long long* arg, cudaStream_t s);
 size_t tc_workspace_bytes(const b200d2_view& view, const b200d2_batch& b, int precision,
                           bool allow_split = true);
@@ -33,6 +33,7 @@ static int validate(const b200d2_view* v, const b200d2_batch* b) {
   if (v->interp == B200D2_INTERP_LINEAR && (!v->lin_re || !v->lin_im)) return B200D2_ERR_INVALID;
   if (v->imgX > 32767 || v->imgY > 32767) return B200D2_ERR_UNSUPPORTED;
   if (b->d_coor_xy && (b->n_listed < 0 || b->n_listed > b->N_img)) return B200D2_ERR_INVALID;
+  if (b->score != B200D2_SCORE_DIFF2 && b->score != B200D2_SCORE_CC) return B200D2_ERR_INVALID;
   return B200D2_OK;
 }
 
@@ -65,11 +66,12 @@ extern "C" int b200d2_diff2_coarse_batch(const b200d2_view* view, const b200d2_b
   cudaStream_t s = (cudaStream_t)stream;
   const long long per = (long long)b.O * b.T;
   if (precision == B200D2_PREC_FP32) {
-    if (!b.accumulate)
+    const int cc = b.score == B200D2_SCORE_CC;
+    if (!b.accumulate && !cc)  // the diff2 kernel adds; the CC kernel writes unless told to add
       B200D2_CUDA_TRY(cudaMemsetAsync(b.d_diff2, 0, sizeof(float) * per * b.P, s));
     st = b200d2::direct_batch(*view, b.d_eulers, b.d_trans_x, b.d_trans_y, b.d_real, b.d_imag,
                               b.d_corr, b.img_stride, b.d_diff2, per, b.O, b.T, b.N_img, b.P,
-                              false, 0, s);
+                              false, 0, s, cc, b.accumulate);
     if (st != B200D2_OK) return st;
     if (b.d_min || b.d_argmin) st = b200d2::minloc(b.d_diff2, per, b.P, b.d_min, b.d_argmin, s);
     return st;
@@ -114,7 +116,7 @@ extern "C" int b200d2_diff2_coarse_batch_stage(const b200d2_view* view,
     if (stage == 0)
       return b200d2::direct_batch(*view, b.d_eulers, b.d_trans_x, b.d_trans_y, b.d_real,
                                   b.d_imag, b.d_corr, b.img_stride, b.d_diff2, per, b.O, b.T,
-                                  b.N_img, b.P, false, 0, s);
+                                  b.N_img, b.P, false, 0, s, b.score == B200D2_SCORE_CC, 1);
     if (stage == 1) return b200d2::minloc(b.d_diff2, per, b.P, b.d_min, b.d_argmin, s);
     return B200D2_ERR_INVALID;
   }

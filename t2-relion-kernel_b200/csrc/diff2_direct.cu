@@ -20,6 +20,12 @@
 //    whose inner step is 5 FP32 instructions per (o, t, pixel);
 //  * thread (tq, oq) owns translations tq + 16 i and orientations oq + 16 j,
 //    so a warp reads S conflict-free and A as a broadcast.
+//
+// The CC form (cuda_kernel_diff2_CC_coarse, src/diff2.cuh:691-809) runs the
+// same tiles with corr as the weight: the register tile accumulates
+// sum corr Re(conj(A) S) and each thread keeps sum corr |A|^2 of its
+// orientations; the output is -cross / sqrt(norm), written (or added with
+// accumulate).  Pixels outside the projector radius have A = 0 and are skipped.
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -42,6 +48,8 @@ struct DirectArgs {
   int O, T, N_img;
   int o_tiles;
   int filter_img;
+  int cc;          // 1: cross-correlation score
+  int accumulate;  // CC: add onto the output instead of writing it
 };
 
 template <typename R>
@@ -80,7 +88,7 @@ __device__ __forceinline__ double2 shift_pixel<double>(float fx, float fy,
                       c * (double)im + s * (double)re);
 }
 
-template <typename R, int TT, int TO, int KC>
+template <typename R, int TT, int TO, int KC, bool CC>
 __global__ void __launch_bounds__(256) diff2_direct_kernel(const DirectArgs a) {
   using R2 = typename Vec2<R>::type;
   constexpr int BT = 16 * TT, BO = 16 * TO, NT = 256, RAW = 256;
@@ -116,10 +124,13 @@ __global__ void __launch_bounds__(256) diff2_direct_kernel(const DirectArgs a) {
 
   const int tq = tid & 15, oq = tid >> 4;
   R acc[TT][TO];
+  R nrm[TO];
 #pragma unroll
   for (int i = 0; i < TT; ++i)
 #pragma unroll
     for (int j = 0; j < TO; ++j) acc[i][j] = R(0);
+#pragma unroll
+  for (int j = 0; j < TO; ++j) nrm[j] = R(0);
   R out_part = R(0);
 
   for (int base = 0; base < a.N_img; base += RAW) {
@@ -132,14 +143,14 @@ __global__ void __launch_bounds__(256) diff2_direct_kernel(const DirectArgs a) {
       pixel_coor(i, v.imgX, v.imgY, v.maxR, x, y);
       re = g_re[i];
       im = g_im[i];
-      w = g_corr[i] / 2;
+      w = CC ? g_corr[i] : g_corr[i] / 2;
       in = pixel_maybe_inside(x, y, v.padding_factor, v.maxR2_padded);
       if (a.filter_img) {
         // reference filter test (src/diff2.cuh:339-345), in double
         double r2 = (double)(x * x + y * y) * v.padding_factor * v.padding_factor;
         if (r2 > (double)v.maxR2_padded) re = im = 0.f;
       }
-      if (!in) {
+      if (!CC && !in) {
         const R rr = (R)re, ri = (R)im;
         out_part += (rr * rr + ri * ri) * (R)w;
       }
@@ -198,14 +209,24 @@ __global__ void __launch_bounds__(256) diff2_direct_kernel(const DirectArgs a) {
         for (int ii = 0; ii < TT; ++ii) sv[ii] = s_S[k][tq + 16 * ii];
 #pragma unroll
         for (int j = 0; j < TO; ++j) av[j] = s_A[k][oq + 16 * j];
+        if (CC) {
 #pragma unroll
-        for (int ii = 0; ii < TT; ++ii)
+          for (int j = 0; j < TO; ++j) nrm[j] = fma(fma(av[j].x, av[j].x, av[j].y * av[j].y), w, nrm[j]);
 #pragma unroll
-          for (int j = 0; j < TO; ++j) {
-            const R dr = av[j].x - sv[ii].x;
-            const R di = av[j].y - sv[ii].y;
-            acc[ii][j] = fma(fma(dr, dr, di * di), w, acc[ii][j]);
-          }
+          for (int ii = 0; ii < TT; ++ii)
+#pragma unroll
+            for (int j = 0; j < TO; ++j)
+              acc[ii][j] = fma(fma(av[j].x, sv[ii].x, av[j].y * sv[ii].y), w, acc[ii][j]);
+        } else {
+#pragma unroll
+          for (int ii = 0; ii < TT; ++ii)
+#pragma unroll
+            for (int j = 0; j < TO; ++j) {
+              const R dr = av[j].x - sv[ii].x;
+              const R di = av[j].y - sv[ii].y;
+              acc[ii][j] = fma(fma(dr, dr, di * di), w, acc[ii][j]);
+            }
+        }
       }
       __syncthreads();
     }
@@ -230,13 +251,18 @@ __global__ void __launch_bounds__(256) diff2_direct_kernel(const DirectArgs a) {
       const int o = o0 + oq + 16 * j;
       if (o < a.O) {
         R* dst = g_out + (size_t)o * a.T + t;
-        *dst = *dst + (acc[ii][j] + out_total);
+        if (CC) {
+          const R cc = -(acc[ii][j] / sqrt(nrm[j]));
+          *dst = a.accumulate ? *dst + cc : cc;
+        } else {
+          *dst = *dst + (acc[ii][j] + out_total);
+        }
       }
     }
   }
 }
 
-template <typename R, int TT, int TO>
+template <typename R, int TT, int TO, bool CC>
 static int launch_tt_to(const DirectArgs& a0, int P, cudaStream_t s) {
   constexpr int KC = std::is_same<R, double>::value ? 8 : 16;
   DirectArgs a = a0;
@@ -245,16 +271,16 @@ static int launch_tt_to(const DirectArgs& a0, int P, cudaStream_t s) {
   const long long nx = (long long)a.o_tiles * t_tiles;
   if (nx > 0x7fffffffLL || P > 65535) return B200D2_ERR_UNSUPPORTED;
   dim3 grid((unsigned)nx, 1, (unsigned)P);
-  diff2_direct_kernel<R, TT, TO, KC><<<grid, 256, 0, s>>>(a);
+  diff2_direct_kernel<R, TT, TO, KC, CC><<<grid, 256, 0, s>>>(a);
   count_launch();
   return status_from_cuda(cudaGetLastError());
 }
 
-template <typename R, int TT>
+template <typename R, int TT, bool CC>
 static int launch_tt(const DirectArgs& a, int P, int to, cudaStream_t s) {
-  if (to >= 8) return launch_tt_to<R, TT, (std::is_same<R, double>::value ? 4 : 8)>(a, P, s);
-  if (to >= 4) return launch_tt_to<R, TT, 4>(a, P, s);
-  return launch_tt_to<R, TT, 2>(a, P, s);
+  if (to >= 8) return launch_tt_to<R, TT, (std::is_same<R, double>::value ? 4 : 8), CC>(a, P, s);
+  if (to >= 4) return launch_tt_to<R, TT, 4, CC>(a, P, s);
+  return launch_tt_to<R, TT, 2, CC>(a, P, s);
 }
 
 // Tile choice: BT = 16*TT just covers T (up to 128, larger T uses several
@@ -271,11 +297,19 @@ static int launch_direct(const DirectArgs& a, int P, cudaStream_t s) {
   int to = 8;
   while (to > 2 && (long long)P * t_tiles * ((a.O + 16 * to - 1) / (16 * to)) < 2LL * sms)
     to >>= 1;
+  if (a.cc) {
+    switch (tt) {
+      case 1: return launch_tt<R, 1, true>(a, P, to, s);
+      case 2: return launch_tt<R, 2, true>(a, P, to, s);
+      case 4: return launch_tt<R, 4, true>(a, P, to, s);
+      default: return launch_tt<R, 8, true>(a, P, to, s);
+    }
+  }
   switch (tt) {
-    case 1: return launch_tt<R, 1>(a, P, to, s);
-    case 2: return launch_tt<R, 2>(a, P, to, s);
-    case 4: return launch_tt<R, 4>(a, P, to, s);
-    default: return launch_tt<R, 8>(a, P, to, s);
+    case 1: return launch_tt<R, 1, false>(a, P, to, s);
+    case 2: return launch_tt<R, 2, false>(a, P, to, s);
+    case 4: return launch_tt<R, 4, false>(a, P, to, s);
+    default: return launch_tt<R, 8, false>(a, P, to, s);
   }
 }
 
@@ -302,7 +336,7 @@ int direct_batch(const b200d2_view& view, const float* eulers, const float* tx,
                  const float* ty, const float* re, const float* im,
                  const float* corr, long long img_stride, void* out,
                  long long out_stride, int O, int T, int N_img, int P,
-                 bool fp64, int filter_img, cudaStream_t s) {
+                 bool fp64, int filter_img, cudaStream_t s, int cc, int accumulate) {
   DirectArgs a;
   a.view = view;
   a.eulers = eulers;
@@ -319,6 +353,8 @@ int direct_batch(const b200d2_view& view, const float* eulers, const float* tx,
   a.N_img = N_img;
   a.o_tiles = 1;
   a.filter_img = filter_img;
+  a.cc = cc;
+  a.accumulate = accumulate;
   return fp64 ? launch_direct<double>(a, P, s) : launch_direct<float>(a, P, s);
 }
 
@@ -337,7 +373,7 @@ extern "C" int b200d2_diff2_coarse(const b200d2_view* view,
   if (precision != B200D2_PREC_FP32) return B200D2_ERR_UNSUPPORTED;
   return b200d2::direct_batch(*view, d_eulers, d_trans_x, d_trans_y, d_real,
                               d_imag, d_corr, 0, d_diff2s, 0, (int)O, (int)T,
-                              (int)N_img, 1, false, 0, (cudaStream_t)stream);
+                              (int)N_img, 1, false, 0, (cudaStream_t)stream, 0, 1);
 }
 
 extern "C" int b200d2_diff2_coarse_f64(const b200d2_view* view,
@@ -355,5 +391,32 @@ extern "C" int b200d2_diff2_coarse_f64(const b200d2_view* view,
   return b200d2::direct_batch(*view, d_eulers, d_trans_x, d_trans_y, d_real,
                               d_imag, d_corr, 0, d_diff2s, 0, (int)O, (int)T,
                               (int)N_img, 1, true, filter_img,
-                              (cudaStream_t)stream);
+                              (cudaStream_t)stream, 0, 1);
+}
+
+extern "C" int b200d2_diff2_coarse_cc(const b200d2_view* view, const float* d_trans_x,
+                                      const float* d_trans_y, const float* d_corr,
+                                      const float* d_real, const float* d_imag,
+                                      const float* d_eulers, float* d_diff2s, size_t O,
+                                      size_t T, size_t N_img, void* stream, int precision) {
+  int st = b200d2::check_common(view, d_trans_x, d_trans_y, d_corr, d_real,
+                                d_imag, d_eulers, d_diff2s, O, T, N_img);
+  if (st != B200D2_OK) return st;
+  if (precision != B200D2_PREC_FP32) return B200D2_ERR_UNSUPPORTED;
+  return b200d2::direct_batch(*view, d_eulers, d_trans_x, d_trans_y, d_real,
+                              d_imag, d_corr, 0, d_diff2s, 0, (int)O, (int)T,
+                              (int)N_img, 1, false, 0, (cudaStream_t)stream, 1, 0);
+}
+
+extern "C" int b200d2_diff2_coarse_cc_f64(const b200d2_view* view, const float* d_trans_x,
+                                          const float* d_trans_y, const float* d_corr,
+                                          const float* d_real, const float* d_imag,
+                                          const float* d_eulers, double* d_diff2s, size_t O,
+                                          size_t T, size_t N_img, void* stream) {
+  int st = b200d2::check_common(view, d_trans_x, d_trans_y, d_corr, d_real,
+                                d_imag, d_eulers, d_diff2s, O, T, N_img);
+  if (st != B200D2_OK) return st;
+  return b200d2::direct_batch(*view, d_eulers, d_trans_x, d_trans_y, d_real,
+                              d_imag, d_corr, 0, d_diff2s, 0, (int)O, (int)T,
+                              (int)N_img, 1, true, 0, (cudaStream_t)stream, 1, 0);
 }

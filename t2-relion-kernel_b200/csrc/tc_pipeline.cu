@@ -25,6 +25,12 @@
 //   6 gemm       : persistent tcgen05 contraction, TMA-fed, double-buffered TMEM
 //                  accumulators, fused FP64 combine + store + per-particle argmin
 //   7 finalize   : per-particle min / argmin from the packed keys
+//
+// Score CC (cuda_kernel_diff2_CC_coarse, src/diff2.cuh:691-809): the same
+// contraction c = sum (corr/2) Re(S_t conj(A_o)); the norm stage stores
+// k[p][o] = -sqrt(2 / sum (corr/2)|A_o|^2) (FP64, and rounded to FP32) in
+// place of nA, and the combine writes k c = -sum corr Re(conj(A) S) /
+// sqrt(sum corr |A|^2).
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -474,11 +480,12 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
 // CTA tile: (2*8*WM) particles x 64 orientations, 4 warps in a 2 x 2 grid,
 // each warp WM x 4 DMMA tiles of 8 x 8; 16-pixel slabs double-buffered
 // through shared memory with cp.async.
+// cc: store k = -sqrt(2 / sum w|B|^2) (the CC score's factor) instead of nA.
 template <int WM>
 __global__ void __launch_bounds__(128) tc_norma_kernel(const double* __restrict__ wcomp, int Kq,
                                                        const double* __restrict__ q, int O, int P,
                                                        const double* __restrict__ normx, double* na,
-                                                       float2* na_hl) {
+                                                       float2* na_hl, int cc) {
   // Kq: row stride of wcomp and q, a multiple of 16, zero padded.  Shared
   // rows padded to 20 doubles (160 B, 16-byte aligned): the fragment loads
   // of a half-warp (rows g, columns t, g, t < 4) fall on distinct bank pairs
@@ -544,10 +551,16 @@ __global__ void __launch_bounds__(128) tc_norma_kernel(const double* __restrict_
       for (int h = 0; h < 2; ++h) {
         const int o = o0 + wo0 + 8 * j + 2 * tig + h;
         if (o < O) {
-          const double v = normx[p] + acc[i][j][h];
-          na[(size_t)p * O + o] = v;
-          const float hi = (float)v;  // v = hi + lo to 48 bits: the combine's double-float operand
-          na_hl[(size_t)p * O + o] = make_float2(hi, (float)(v - (double)hi));
+          if (cc) {
+            const double k = -sqrt(2.0 / acc[i][j][h]);
+            na[(size_t)p * O + o] = k;
+            na_hl[(size_t)p * O + o] = make_float2((float)k, 0.f);
+          } else {
+            const double v = normx[p] + acc[i][j][h];
+            na[(size_t)p * O + o] = v;
+            const float hi = (float)v;  // v = hi + lo to 48 bits: the combine's double-float operand
+            na_hl[(size_t)p * O + o] = make_float2(hi, (float)(v - (double)hi));
+          }
         }
       }
   }
@@ -667,6 +680,7 @@ struct GemmArgs {
   const double* na;
   const float2* na_hl;  // nA = hi + lo (double-float)
   int combine64;        // 1: FP64 combine; 0: double-float combine
+  int cc;               // 1: CC score k c (na holds k), 0: diff2 nA - 2c
   unsigned long long* keys;
   uint32_t* status;
   const float* inv_sa;  // FP16 forms: [P] 1 / particle scale
@@ -745,11 +759,12 @@ __device__ __forceinline__ void epi_combine(const GemmArgs& g, const EpiRow& x, 
   if (g.combine64) {
     double cr = (double)c;
     if (SCALED) cr *= (double)g.inv_sb[o];
-    f = (float)fma(x.m2s, cr, x.na_row[o]);
+    // CC: k * c with the scales undone (-m2s/2 is the particle's, exact)
+    f = g.cc ? (float)(x.na_row[o] * (cr * (-0.5 * x.m2s))) : (float)fma(x.m2s, cr, x.na_row[o]);
   } else {
     const float2 nh = x.nh_row[o];
     const float sc = SCALED ? x.m2f * g.inv_sb[o] : x.m2f;  // product of powers of two: exact
-    f = __fadd_rn(__fmaf_rn(sc, c, nh.x), nh.y);
+    f = g.cc ? __fmul_rn(nh.x, c * (-0.5f * sc)) : __fadd_rn(__fmaf_rn(sc, c, nh.x), nh.y);
   }
   float* dst = x.out_row + (size_t)lo * x.Tp;
   if (g.accumulate) f += __ldcs(dst);
@@ -775,7 +790,8 @@ __device__ __forceinline__ void epi_drain(const GemmArgs& g, const EpiRow& x, ui
         const int o = oc + j;
         const float2 nh = x.nh_row[o];
         const float sc = SCALED ? x.m2f * g.inv_sb[o] : x.m2f;
-        const float f = __fadd_rn(__fmaf_rn(sc, __uint_as_float(r[j]), nh.x), nh.y);
+        const float c = __uint_as_float(r[j]);
+        const float f = g.cc ? __fmul_rn(nh.x, c * (-0.5f * sc)) : __fadd_rn(__fmaf_rn(sc, c, nh.x), nh.y);
         __stcs(x.out_row + (size_t)o * x.Tp, f);
         if (f < best) {
           best = f;
@@ -1440,6 +1456,7 @@ static int launch_gemm_v(const b200d2_batch& b, const TcGeom& g, void* ws, cudaS
   a.na = ws_at<double>(ws, g.off_na);
   a.na_hl = ws_at<float2>(ws, g.off_nahl);
   a.combine64 = g_combine64.load();
+  a.cc = b.score == B200D2_SCORE_CC ? 1 : 0;
   a.keys = ws_at<unsigned long long>(ws, g.off_keys);
   a.status = ws_at<uint32_t>(ws, g.off_status);
   a.inv_sa = ws_at<float>(ws, g.off_sa);
@@ -1496,6 +1513,7 @@ static int launch_gemm_pair(const b200d2_batch& b, const TcGeom& g, void* ws, cu
   a.na = ws_at<double>(ws, g.off_na);
   a.na_hl = ws_at<float2>(ws, g.off_nahl);
   a.combine64 = g_combine64.load();
+  a.cc = b.score == B200D2_SCORE_CC ? 1 : 0;
   a.keys = ws_at<unsigned long long>(ws, g.off_keys);
   a.status = ws_at<uint32_t>(ws, g.off_status);
   a.inv_sa = ws_at<float>(ws, g.off_sa);
@@ -1601,11 +1619,14 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       const long long otiles = (g.O + 63) / 64;
       const int sms = num_sms();
       if (otiles * ((g.P + 63) / 64) >= sms) {
-        tc_norma_kernel<4><<<dim3(otiles, (g.P + 63) / 64), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl);
+        tc_norma_kernel<4><<<dim3(otiles, (g.P + 63) / 64), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl,
+                                                                                    b.score == B200D2_SCORE_CC);
       } else if (otiles * ((g.P + 31) / 32) >= sms) {
-        tc_norma_kernel<2><<<dim3(otiles, (g.P + 31) / 32), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl);
+        tc_norma_kernel<2><<<dim3(otiles, (g.P + 31) / 32), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl,
+                                                                                    b.score == B200D2_SCORE_CC);
       } else {
-        tc_norma_kernel<1><<<dim3(otiles, (g.P + 15) / 16), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl);
+        tc_norma_kernel<1><<<dim3(otiles, (g.P + 15) / 16), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl,
+                                                                                    b.score == B200D2_SCORE_CC);
       }
       break;
     }

@@ -108,21 +108,34 @@ int main(int argc, char** argv) {
     uint32_t* d_ws = nullptr;
     if (cudaMalloc(&d_ws, wsb) != cudaSuccess) throw std::runtime_error("workspace");
     fn.run(d_eul, d_trans, d_trans + T, d_fre, d_fim, k, d_fco, d_outtc, d_outtc, stream, d_cxy, d_ws);
+    // do_CC: the cross-correlation score, against its FP64 sum
+    float* d_cc = to_device(diff2s);
+    std::vector<double> zero64((size_t)O * T, 0.0);
+    double* d_cc64 = to_device(zero64);
+    runDiff2KernelCoarse(k, d_trans, d_trans + T, nullptr, d_corr, d_fimg, d_fimg + N, d_eul, d_cc, 1.f, O, T, N,
+                         stream, true, false);
+    if (b200d2_diff2_coarse_cc_f64(&k.view, d_trans, d_trans + T, d_corr, d_fimg, d_fimg + N, d_eul, d_cc64, O, T,
+                                   N, stream) != B200D2_OK)
+      throw std::runtime_error("cc_f64");
     if (cudaStreamSynchronize(stream) != cudaSuccess) throw std::runtime_error("stream");
 
     const size_t n = (size_t)O * T;
     const auto o32 = to_host(d_out32, n);
     const auto o64 = to_host(d_out64, n);
     const auto otc = to_host(d_outtc, n);
-    const double e32 = max_rel(o32, o64), etc = max_rel(otc, o64);
+    const auto occ = to_host(d_cc, n);
+    const auto occ64 = to_host(d_cc64, n);
+    const double e32 = max_rel(o32, o64), etc = max_rel(otc, o64), ecc = max_rel(occ, occ64);
     std::printf("{\"O\": %d, \"T\": %d, \"N_img\": %d, \"filtered\": %d, \"workspace_bytes\": %zu, "
-                "\"fp32_vs_fp64_max_rel\": %.3e, \"functor_vs_fp64_max_rel\": %.3e}\n",
-                O, T, N, ps, wsb, e32, etc);
+                "\"fp32_vs_fp64_max_rel\": %.3e, \"functor_vs_fp64_max_rel\": %.3e, "
+                "\"cc_fp32_vs_fp64_max_rel\": %.3e}\n",
+                O, T, N, ps, wsb, e32, etc, ecc);
     for (void* p : {(void*)d_eul, (void*)d_trans, (void*)d_fimg, (void*)d_corr, (void*)d_out32, (void*)d_out64,
-                    (void*)d_fre, (void*)d_fim, (void*)d_fco, (void*)d_cxy, (void*)d_outtc, (void*)d_ws})
+                    (void*)d_fre, (void*)d_fim, (void*)d_fco, (void*)d_cxy, (void*)d_outtc, (void*)d_ws,
+                    (void*)d_cc, (void*)d_cc64})
       cudaFree(p);
     cudaStreamDestroy(stream);
-    return (e32 <= 1e-5 && etc <= 1e-5) ? 0 : 1;
+    return (e32 <= 1e-5 && etc <= 1e-5 && ecc <= 1e-5) ? 0 : 1;
   } catch (const std::exception& e) {
     std::fprintf(stderr, "error: %s\n", e.what());
     return 3;

@@ -150,6 +150,30 @@ def test_significance_oracle_edge_cases(oracle):
     assert (sig, nsig) == (2.0, 1) and passed.tolist() == [0, 0, 1, 0, 1]
 
 
+@pytest.mark.parametrize("case", ["tiny", "c1"])
+def test_cc_restatement_consistent_with_diff2(oracle, synth, case):
+    """sum corr/2 |A - S|^2 = (normA + normX)/2 - cross, so the CC
+    restatement's cross term (-cc sqrt(normA)) must equal the C oracle's FP64
+    diff2 rearranged."""
+    pr = synth.make_problem(case, P=1)
+    proj = oracle.projector_for(pr)
+    cc = oracle.cc_coarse_f64(proj, pr.eulers, pr.trans_x, pr.trans_y, pr.fimg_re[0], pr.fimg_im[0], pr.corr[0])
+    d2 = np.asarray(oracle.diff2_coarse_f64(proj, pr.eulers, pr.trans_x, pr.trans_y, pr.fimg_re[0], pr.fimg_im[0],
+                                            pr.corr[0]), np.float64).reshape(cc.shape)
+    n = pr.N_img
+    x = np.arange(n) % pr.imgX
+    y = np.arange(n) // pr.imgX
+    y = np.where(y > proj.maxR, y - pr.imgY, y)
+    ar, ai = oracle.project_pixels(proj, pr.eulers, x.astype(np.int32), y.astype(np.int32))
+    w = pr.corr[0].astype(np.float64)
+    norm_a = (ar * ar + ai * ai) @ w
+    norm_x = float((pr.fimg_re[0].astype(np.float64) ** 2 + pr.fimg_im[0].astype(np.float64) ** 2) @ w)
+    cross_cc = -cc * np.sqrt(norm_a)[:, None]
+    cross_d2 = 0.5 * (norm_a[:, None] + norm_x) - d2
+    assert np.abs(cross_cc - cross_d2).max() <= 1e-9 * np.abs(cross_d2).max() + 1e-9 * norm_x
+    assert np.unravel_index(cc.argmin(), cc.shape) == np.unravel_index(d2.argmin(), cc.shape)
+
+
 def test_healpix_grid(synth):
     import importlib
     hp = importlib.import_module("relion_b200.healpix")
