@@ -76,6 +76,10 @@ typedef struct b200d2_view {
   const float* lin_re; /* device [mdlZ][mdlY][mdlX], NULL if absent */
   const float* lin_im;
   int interp; /* B200D2_INTERP_* used by kernels taking this view */
+  /* the same volume as one float2 (re, im) texture, 0 if absent: kernels
+   * fetch both channels at once from it (identical values: the filtering
+   * weights are per fetch, not per channel) */
+  unsigned long long tex_c;
 } b200d2_view;
 
 typedef struct b200d2_projector b200d2_projector; /* opaque, owns device memory */

@@ -49,7 +49,7 @@ class View(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("mdlX", "mdlXY", "mdlZ", "imgX", "imgY", "imgZ", "mdlInitY",
                                          "mdlInitZ", "maxR", "maxR2", "maxR2_padded")] + [
         ("padding_factor", C.c_float), ("tex_re", C.c_ulonglong), ("tex_im", C.c_ulonglong),
-        ("lin_re", C.c_void_p), ("lin_im", C.c_void_p), ("interp", C.c_int)]
+        ("lin_re", C.c_void_p), ("lin_im", C.c_void_p), ("interp", C.c_int), ("tex_c", C.c_ulonglong)]
 
 
 class Batch(C.Structure):

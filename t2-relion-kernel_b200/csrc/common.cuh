@@ -111,12 +111,16 @@ __device__ __forceinline__ float2 project_pixel(const b200d2_view& v, float fx,
     if (v.interp == B200D2_INTERP_TEXTURE) {
       yp = __fsub_rn(yp, (float)v.mdlInitY);
       zp = __fsub_rn(zp, (float)v.mdlInitZ);
-      cudaTextureObject_t tre = (cudaTextureObject_t)v.tex_re;
-      cudaTextureObject_t tim = (cudaTextureObject_t)v.tex_im;
       float u = __fadd_rn(xp, 0.5f), w1 = __fadd_rn(yp, 0.5f),
             w2 = __fadd_rn(zp, 0.5f);
-      out.x = tex3D<float>(tre, u, w1, w2);
-      out.y = sgn * tex3D<float>(tim, u, w1, w2);
+      if (v.tex_c) {  // one fetch of both channels
+        const float2 t = tex3D<float2>((cudaTextureObject_t)v.tex_c, u, w1, w2);
+        out.x = t.x;
+        out.y = sgn * t.y;
+      } else {
+        out.x = tex3D<float>((cudaTextureObject_t)v.tex_re, u, w1, w2);
+        out.y = sgn * tex3D<float>((cudaTextureObject_t)v.tex_im, u, w1, w2);
+      }
     } else {
       const int mdlY = v.mdlXY / v.mdlX;
       out.x = trilinear_linear(v.lin_re, xp, yp, zp, v.mdlX, mdlY, v.mdlZ,

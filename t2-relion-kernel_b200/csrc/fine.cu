@@ -16,8 +16,14 @@
 // shuffles and one shared-memory step in a fixed order.  The phase shift
 // e^{i(x tx + y ty)} is the product of two table entries e^{i x tx} and
 // e^{i y ty}, built per pass in shared memory (one sincos per table entry,
-// not per pixel); jobs on images too large for the tables take sincosf per
-// pixel as the reference does.  Pixel coordinates
+// not per pixel).  With the tables the score is taken expanded,
+//   sum w|A - S|^2 = sum w(|A|^2 + |X|^2) - 2 sum Re(q e^{i x tx} e^{i y ty}),
+//   q = w conj(A) X,
+// so a (pixel, translation) pair costs one complex multiply and a real part
+// (the norms are per pixel, in FP64); the per-thread cross sums are combined
+// in FP64 and the final difference is taken in FP64.  Jobs on images too
+// large for the tables take sincosf per pixel and sum w|A - S|^2 directly, as
+// the reference does.  Pixel coordinates
 // follow the fine kernel's mapping (src/diff2.cuh:612-626): rows past maxR
 // wrap to negative y when they lie within maxR of the end, otherwise their x
 // is set to maxR (outside the projector radius).
@@ -58,6 +64,7 @@ __global__ void __launch_bounds__(kFineThreads) diff2_fine_kernel(
   const float* eo = eulers + o * 9;
   float e[6] = {eo[0], eo[1], eo[3], eo[4], eo[6], eo[7]};
   __shared__ float s_part[kFineThreads / 32][NT];
+  __shared__ double s_cross[kFineThreads / 32][NT], s_norm[kFineThreads / 32];
   // TABLES: [NT][exw] e^{i x tx} for x in [0, exw), then [NT][eyw] e^{i y ty}
   // for y in [-maxR, imgY); fine_pixel_coor yields x < max(imgX, maxR + 1)
   // and -maxR <= y < imgY.
@@ -89,43 +96,79 @@ __global__ void __launch_bounds__(kFineThreads) diff2_fine_kernel(
       }
       __syncthreads();
     }
+    double nrm = 0.0;  // TABLES: sum w(|A|^2 + |X|^2) of this thread's pixels
     for (int pixel = threadIdx.x; pixel < image_size; pixel += kFineThreads) {
       int x, y;
       fine_pixel_coor(pixel, v.imgX, v.imgY, v.maxR, x, y);
       const float2 a = project_pixel(v, (float)x, (float)y, e);
       const float xr = re[pixel], xi = im[pixel];
       const float w = 0.5f * corr[pixel];
+      if (TABLES) {
+        const double ad = a.x, bd = a.y, xd = xr, yd = xi;
+        nrm = fma((double)w, fma(ad, ad, fma(bd, bd, fma(xd, xd, yd * yd))), nrm);
+        const float qr = __fmul_rn(w, __fmaf_rn(a.x, xr, __fmul_rn(a.y, xi)));   // w Re(conj(A) X)
+        const float qi = __fmul_rn(w, __fmaf_rn(a.x, xi, -__fmul_rn(a.y, xr)));  // w Im(conj(A) X)
+        const float2* pex = s_ex + x;
+        const float2* pey = s_ey + y + v.maxR;
 #pragma unroll
-      for (int i = 0; i < NT; ++i) {
-        if (i < nt) {
-          float s, c;
-          if (TABLES) {
-            const float2 ex = s_ex[i * exw + x], ey = s_ey[i * eyw + y + v.maxR];
-            c = __fmaf_rn(ex.x, ey.x, -__fmul_rn(ex.y, ey.y));
-            s = __fmaf_rn(ex.x, ey.y, __fmul_rn(ex.y, ey.x));
-          } else {
-            sincosf(__fmaf_rn((float)x, ftx[i], __fmul_rn((float)y, fty[i])), &s, &c);
+        for (int i = 0; i < NT; ++i) {
+          if (i < nt) {
+            const float2 ex = pex[i * exw], ey = pey[i * eyw];
+            const float ur = __fmaf_rn(qr, ex.x, -__fmul_rn(qi, ex.y));
+            const float ui = __fmaf_rn(qr, ex.y, __fmul_rn(qi, ex.x));
+            acc[i] = __fmaf_rn(ur, ey.x, __fmaf_rn(-ui, ey.y, acc[i]));
           }
-          const float dr = a.x - __fmaf_rn(c, xr, -__fmul_rn(s, xi));
-          const float di = a.y - __fmaf_rn(c, xi, __fmul_rn(s, xr));
-          acc[i] = __fmaf_rn(__fmaf_rn(dr, dr, __fmul_rn(di, di)), w, acc[i]);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < NT; ++i) {
+          if (i < nt) {
+            float s, c;
+            sincosf(__fmaf_rn((float)x, ftx[i], __fmul_rn((float)y, fty[i])), &s, &c);
+            const float dr = a.x - __fmaf_rn(c, xr, -__fmul_rn(s, xi));
+            const float di = a.y - __fmaf_rn(c, xi, __fmul_rn(s, xr));
+            acc[i] = __fmaf_rn(__fmaf_rn(dr, dr, __fmul_rn(di, di)), w, acc[i]);
+          }
         }
       }
     }
     // fixed-order reduction: shuffle tree inside each warp, then warps in order
+    if (TABLES) {
 #pragma unroll
-    for (int i = 0; i < NT; ++i) {
-      float vsum = acc[i];
+      for (int i = 0; i < NT; ++i) {
+        double vsum = (double)acc[i];
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) vsum += __shfl_xor_sync(0xffffffffu, vsum, off);
-      if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5][i] = vsum;
+        for (int off = 16; off > 0; off >>= 1) vsum += __shfl_xor_sync(0xffffffffu, vsum, off);
+        if ((threadIdx.x & 31) == 0) s_cross[threadIdx.x >> 5][i] = vsum;
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, off);
+      if ((threadIdx.x & 31) == 0) s_norm[threadIdx.x >> 5] = nrm;
+    } else {
+#pragma unroll
+      for (int i = 0; i < NT; ++i) {
+        float vsum = acc[i];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) vsum += __shfl_xor_sync(0xffffffffu, vsum, off);
+        if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5][i] = vsum;
+      }
     }
     __syncthreads();
     if (threadIdx.x < nt) {
-      float tot = 0.f;
+      if (TABLES) {
+        double cr = 0.0, nt2 = 0.0;
 #pragma unroll
-      for (int w = 0; w < kFineThreads / 32; ++w) tot += s_part[w][threadIdx.x];
-      diff2s[jb + base + threadIdx.x] = tot + sum_init;
+        for (int w = 0; w < kFineThreads / 32; ++w) {
+          cr += s_cross[w][threadIdx.x];
+          nt2 += s_norm[w];
+        }
+        diff2s[jb + base + threadIdx.x] = (float)(fma(-2.0, cr, nt2) + (double)sum_init);
+      } else {
+        float tot = 0.f;
+#pragma unroll
+        for (int w = 0; w < kFineThreads / 32; ++w) tot += s_part[w][threadIdx.x];
+        diff2s[jb + base + threadIdx.x] = tot + sum_init;
+      }
     }
     __syncthreads();
   }

@@ -23,8 +23,8 @@
 struct b200d2_projector {
   int mdlX = 0, mdlY = 0, mdlZ = 0, mdlInitY = 0, mdlInitZ = 0, mdlMaxR = 0;
   float padding_factor = 0.f;
-  cudaArray_t arr_re = nullptr, arr_im = nullptr;
-  cudaTextureObject_t tex_re = 0, tex_im = 0;
+  cudaArray_t arr_re = nullptr, arr_im = nullptr, arr_c = nullptr;
+  cudaTextureObject_t tex_re = 0, tex_im = 0, tex_c = 0;
   float* lin_re = nullptr;
   float* lin_im = nullptr;
   int device = 0;
@@ -36,6 +36,10 @@ void release(b200d2_projector* p) {
   if (!p) return;
   if (p->tex_re) cudaDestroyTextureObject(p->tex_re);
   if (p->tex_im) cudaDestroyTextureObject(p->tex_im);
+  if (p->tex_c) cudaDestroyTextureObject(p->tex_c);
+  if (p->arr_c) cudaFreeArray(p->arr_c);
+  p->tex_c = 0;
+  p->arr_c = nullptr;
   if (p->arr_re) cudaFreeArray(p->arr_re);
   if (p->arr_im) cudaFreeArray(p->arr_im);
   if (p->lin_re) cudaFree(p->lin_re);
@@ -57,6 +61,39 @@ int upload_array(cudaArray_t* arr, cudaTextureObject_t* tex, const float* h,
   cp.kind = cudaMemcpyHostToDevice;
   cp.dstArray = *arr;
   cp.srcPtr = make_cudaPitchedPtr(const_cast<float*>(h), X * sizeof(float), X, Y);
+  B200D2_CUDA_TRY(cudaMemcpy3D(&cp));
+  cudaResourceDesc rd;
+  memset(&rd, 0, sizeof(rd));
+  rd.resType = cudaResourceTypeArray;
+  rd.res.array.array = *arr;
+  cudaTextureDesc td;
+  memset(&td, 0, sizeof(td));
+  td.filterMode = cudaFilterModeLinear;
+  td.readMode = cudaReadModeElementType;
+  td.normalizedCoords = 0;
+  for (int i = 0; i < 3; ++i) td.addressMode[i] = cudaAddressModeClamp;
+  B200D2_CUDA_TRY(cudaCreateTextureObject(tex, &rd, &td, nullptr));
+  return B200D2_OK;
+}
+
+// The same volume as one float2 (re, im) array: a projection sample is one
+// texture fetch instead of two.  The filtering hardware applies the same
+// weights to both channels, so each channel equals the single-channel
+// texture's value.
+int upload_array2(cudaArray_t* arr, cudaTextureObject_t* tex, const float* h_re, const float* h_im, int X, int Y,
+                  int Z) {
+  const size_t n = (size_t)X * Y * Z;
+  std::vector<float2> h(n);
+  for (size_t i = 0; i < n; ++i) h[i] = make_float2(h_re[i], h_im[i]);
+  cudaChannelFormatDesc desc = cudaCreateChannelDesc(32, 32, 0, 0, cudaChannelFormatKindFloat);
+  cudaExtent ext = make_cudaExtent(X, Y, Z);
+  B200D2_CUDA_TRY(cudaMalloc3DArray(arr, &desc, ext));
+  cudaMemcpy3DParms cp;
+  memset(&cp, 0, sizeof(cp));
+  cp.extent = ext;
+  cp.kind = cudaMemcpyHostToDevice;
+  cp.dstArray = *arr;
+  cp.srcPtr = make_cudaPitchedPtr(h.data(), X * sizeof(float2), X, Y);
   B200D2_CUDA_TRY(cudaMemcpy3D(&cp));
   cudaResourceDesc rd;
   memset(&rd, 0, sizeof(rd));
@@ -104,6 +141,8 @@ extern "C" int b200d2_projector_create(int mdlX, int mdlY, int mdlZ,
     st = upload_array(&p->arr_re, &p->tex_re, h_real, mdlX, mdlY, mdlZ);
     if (st == B200D2_OK)
       st = upload_array(&p->arr_im, &p->tex_im, h_imag, mdlX, mdlY, mdlZ);
+    if (st == B200D2_OK)
+      st = upload_array2(&p->arr_c, &p->tex_c, h_real, h_imag, mdlX, mdlY, mdlZ);
   }
   if (st == B200D2_OK && (use_texture == 0 || use_texture == 2)) {
     size_t n = (size_t)mdlX * mdlY * mdlZ;
@@ -228,6 +267,7 @@ extern "C" int b200d2_projector_view(const b200d2_projector* p, int imgX,
   v.padding_factor = p->padding_factor;
   v.tex_re = (unsigned long long)p->tex_re;
   v.tex_im = (unsigned long long)p->tex_im;
+  v.tex_c = (unsigned long long)p->tex_c;
   v.lin_re = p->lin_re;
   v.lin_im = p->lin_im;
   v.interp = interp;

@@ -1720,7 +1720,7 @@ int tc_run_stage(const b200d2_view& v, const b200d2_batch& b, int precision, int
 struct SidePair {
   int device;
   cudaStream_t user, side;
-  cudaEvent_t fork, join;
+  cudaEvent_t fork, mid, join;
 };
 
 static std::mutex g_side_mu;
@@ -1740,6 +1740,7 @@ static int side_for(cudaStream_t user, SidePair* out) {
   sp.user = user;
   B200D2_CUDA_TRY(cudaStreamCreateWithFlags(&sp.side, cudaStreamNonBlocking));
   B200D2_CUDA_TRY(cudaEventCreateWithFlags(&sp.fork, cudaEventDisableTiming));
+  B200D2_CUDA_TRY(cudaEventCreateWithFlags(&sp.mid, cudaEventDisableTiming));
   B200D2_CUDA_TRY(cudaEventCreateWithFlags(&sp.join, cudaEventDisableTiming));
   g_side.push_back(sp);
   *out = sp;
@@ -1755,21 +1756,26 @@ int tc_run(const b200d2_view& v, const b200d2_batch& b, int precision, void* ws,
   SidePair sp;
   st = side_for(s, &sp);
   if (st != B200D2_OK) return st;
-  // caller stream: pixel list -> projections -> normX -> normA ; side stream:
-  // phase tables -> operand generation; join before the contraction.
+  // caller stream: pixel list -> projections -> (normX) -> normA; side
+  // stream: phase tables -> normX -> operand generation; normA waits for
+  // normX, the contraction for both streams.
   st = dispatch_stage(v, b, precision, g, ws, 0, s);
   if (st != B200D2_OK) return st;
   B200D2_CUDA_TRY(cudaEventRecord(sp.fork, s));
   B200D2_CUDA_TRY(cudaStreamWaitEvent(sp.side, sp.fork, 0));
   st = dispatch_stage(v, b, precision, g, ws, 1, sp.side);
+  if (st == B200D2_OK) st = dispatch_stage(v, b, precision, g, ws, 3, sp.side);
+  const cudaError_t rm = cudaEventRecord(sp.mid, sp.side);
   if (st == B200D2_OK) st = dispatch_stage(v, b, precision, g, ws, 5, sp.side);
   const cudaError_t rj = cudaEventRecord(sp.join, sp.side);
   if (st != B200D2_OK) return st;
+  if (rm != cudaSuccess) return status_from_cuda(rm);
   if (rj != cudaSuccess) return status_from_cuda(rj);
-  for (int i : {2, 3, 4}) {
-    st = dispatch_stage(v, b, precision, g, ws, i, s);
-    if (st != B200D2_OK) return st;
-  }
+  st = dispatch_stage(v, b, precision, g, ws, 2, s);
+  if (st != B200D2_OK) return st;
+  B200D2_CUDA_TRY(cudaStreamWaitEvent(s, sp.mid, 0));
+  st = dispatch_stage(v, b, precision, g, ws, 4, s);
+  if (st != B200D2_OK) return st;
   B200D2_CUDA_TRY(cudaStreamWaitEvent(s, sp.join, 0));
   st = dispatch_stage(v, b, precision, g, ws, 6, s);
   if (st == B200D2_OK) st = dispatch_stage(v, b, precision, g, ws, 7, s);

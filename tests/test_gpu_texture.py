@@ -98,3 +98,30 @@ def test_texture_filtering_samples(pkg, cuda, oracle):
     assert err[:3072].max() < 1e-6  # single-axis sweeps: exact 1/256 weights
     assert err.max() < 2e-2  # 3D: joint corner-weight rounding, |values| <= 1
     proj.close()
+
+
+def test_float2_texture_equals_two_textures(pkg, synth, cuda):
+    """The interleaved (re, im) texture gives bit-identical projections to the
+    two single-channel textures the reference uses (one fetch instead of
+    two; the filtering weights belong to the fetch, not the channel)."""
+    torch = cuda
+    pr = synth.make_problem("c1", P=1)
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    both = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    assert both.tex_c != 0
+    split = pkg.View.from_buffer_copy(both)
+    split.tex_c = 0
+    x, y = synth.pixel_coords(pr.imgX, pr.imgY, both.maxR)
+    px = torch.as_tensor(np.asarray(x, np.int32), device="cuda")
+    py = torch.as_tensor(np.asarray(y, np.int32), device="cuda")
+    eul = torch.as_tensor(pr.eulers.reshape(-1), device="cuda")
+    outs = []
+    for v in (both, split):
+        re = torch.empty(pr.O * pr.N_img, device="cuda")
+        im = torch.empty(pr.O * pr.N_img, device="cuda")
+        pkg.project_pixels(v, eul, px, py, re, im, pr.O, pr.N_img)
+        outs.append((re, im))
+    torch.cuda.synchronize()
+    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+    assert float(outs[0][0].abs().max()) > 0
+    proj.close()
