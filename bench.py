@@ -635,8 +635,9 @@ def precision_study(args):
 
 def fine_study(args):
     """Fine pass over job lists (one JSON line): this library's
-    b200d2_diff2_fine against the reference's cuda_kernel_diff2_fine on the
-    same device buffers.  Workload: C2 particles (image 64, 2112 pixels), a
+    b200d2_diff2_fine and b200d2_diff2_fine_cc against the reference's
+    cuda_kernel_diff2_fine and cuda_kernel_diff2_CC_fine on the same device
+    buffers.  Workload: C2 particles (image 64, 2112 pixels), a
     job list per particle of 2048 jobs, each one orientation of the 4608 and a
     run of 16 consecutive translations of the 113 (32768 samples per
     particle, the order of RELION's significant samples after the coarse
@@ -697,15 +698,32 @@ def fine_study(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps
 
+    def ours_cc():
+        for p in range(pr.P):
+            pkg.diff2_fine_cc(view, eul, re[p], im[p], tx, ty, co[p], out[p], rot_idx=d["rot"],
+                              trans_idx=d["trans"], job_idx=d["jidx"], job_num=d["jnum"], image_size=pr.N_img)
+
+    def ref_cc():
+        for p in range(pr.P):
+            L.refshim_diff2_fine_cc(h, pr.imgX, pr.imgY, 1, pr.imgMaxR, eul.data_ptr(), re[p].data_ptr(),
+                                    im[p].data_ptr(), tx.data_ptr(), ty.data_ptr(), co[p].data_ptr(),
+                                    rout[p].data_ptr(), pr.N_img, pr.O, pr.T, n_jobs, d["rot"].data_ptr(),
+                                    d["trans"].data_ptr(), d["jidx"].data_ptr(), d["jnum"].data_ptr(), None)
+
     ms_ours, ms_ref = timed(ours), timed(ref)
     rel = float(((out - rout).abs() / rout.abs().clamp_min(1e-30)).max())
+    ms_ours_cc, ms_ref_cc = timed(ours_cc), timed(ref_cc)
+    # CC scores change sign: error relative to the largest magnitude
+    rel_cc = float((out - rout).abs().max() / rout.abs().max())
     L.refshim_projector_destroy(h)
     evals = pr.P * n_out
     line = {"study": "fine", "workload": f"16 C2 particles (image 64, {pr.N_img} px) x {n_jobs} jobs x {chunk} "
                                          f"translations ({evals} samples)",
             "ours_ms": ms_ours, "reference_ms": ms_ref, "ours_evals_per_s": evals / (ms_ours / 1e3),
             "reference_evals_per_s": evals / (ms_ref / 1e3), "speedup": ms_ref / ms_ours,
-            "max_rel_diff_vs_reference": rel}
+            "max_rel_diff_vs_reference": rel,
+            "cc": {"ours_ms": ms_ours_cc, "reference_ms": ms_ref_cc, "speedup": ms_ref_cc / ms_ours_cc,
+                   "max_diff_vs_reference_over_max_score": rel_cc}}
     print(json.dumps(line), flush=True)
     proj.close()
     return 0

@@ -187,6 +187,21 @@ int b200d2_diff2_fine(const b200d2_view* view, const float* d_eulers,
                       const uint64_t* d_job_idx, const uint64_t* d_job_num,
                       void* stream);
 
+/* CC form of the fine pass (replaces cuda_kernel_diff2_CC_fine,
+ * src/diff2.cuh:811-960): same job list, writes
+ *   d_diff2s[d_job_idx[j] + i] = -sum_px corr Re(conj(proj) shift_i(img))
+ *                                / sqrt(sum_px corr |proj|^2)
+ * (full corr, no sum_init; the reference passes sum_init and
+ * exp_local_sqrtXi2 but does not read them).  FP32 cross sums, FP64 norm and
+ * quotient. */
+int b200d2_diff2_fine_cc(const b200d2_view* view, const float* d_eulers,
+                         const float* d_real, const float* d_imag,
+                         const float* d_trans_x, const float* d_trans_y,
+                         const float* d_corr, float* d_diff2s, size_t image_size,
+                         size_t todo_blocks, const uint64_t* d_rot_idx,
+                         const uint64_t* d_trans_idx, const uint64_t* d_job_idx,
+                         const uint64_t* d_job_num, void* stream);
+
 /* ------------------------------------------------------------------------
  * Batched coarse pass (layout diff2[p][o][t]).  The reference
  * launches one runDiff2KernelCoarse per particle (src/main.cu:483-503); this

@@ -297,6 +297,8 @@ def ref_lib():
         if hasattr(L, "refshim_diff2_fine"):
             L.refshim_diff2_fine.argtypes = ([P] + [C.c_int] * 4 + [P] * 7 + [C.c_long, C.c_float] + [C.c_long] * 3 +
                                              [P] * 4 + [P])
+        if hasattr(L, "refshim_diff2_fine_cc"):
+            L.refshim_diff2_fine_cc.argtypes = ([P] + [C.c_int] * 4 + [P] * 7 + [C.c_long] * 4 + [P] * 4 + [P])
         _ref = L
     return _ref
 

@@ -15,6 +15,7 @@
 //   runDiff2KernelCoarseDouble                src/acc_helper_functions_impl.h:503-854
 //   CoarseMatrixKernel*::run (5 variants)     src/coarse_splitImg_*.cuh
 //   cuda_kernel_diff2_fine (no host wrapper)  src/diff2.cuh:540-682
+//   cuda_kernel_diff2_CC_fine (no host wrapper) src/diff2.cuh:811-960
 //   runDiff2KernelCoarse with do_CC           src/acc_helper_functions_impl.h:441-498
 //   cuda_kernel_find_threshold_idx_in_cumulative,
 //   cuda_kernel_array_over_threshold          src/cuda_device_utils.cuh:238-266
@@ -55,7 +56,7 @@ AccProjectorKernel make_view(RefProjector* p, int imgX, int imgY, int imgZ,
 
 extern "C" {
 
-int refshim_abi_version(void) { return 5; }
+int refshim_abi_version(void) { return 6; }
 
 void* refshim_projector_create(int mdlX, int mdlY, int mdlZ, int initY,
                                int initZ, int maxR, float pf, const float* re,
@@ -190,6 +191,20 @@ int refshim_diff2_fine(void* h, int imgX, int imgY, int imgZ, int imgMaxR, float
   AccProjectorKernel k = make_view(p, imgX, imgY, imgZ, imgMaxR);
   cuda_kernel_diff2_fine<true, false, 128, 16><<<(unsigned)todo_blocks, 128, 0, (cudaStream_t)stream>>>(
       d_eulers, d_re, d_im, d_tx, d_ty, nullptr, k, d_corr, d_diff2s, (unsigned)image_size, sum_init,
+      (unsigned long)O, (unsigned long)T, (unsigned long)todo_blocks, d_rot_idx, d_trans_idx, d_job_idx, d_job_num);
+  return (int)cudaGetLastError();
+}
+
+// The CC form, launched the same way (sum_init and exp_local_sqrtXi2 are not
+// read by the kernel).
+int refshim_diff2_fine_cc(void* h, int imgX, int imgY, int imgZ, int imgMaxR, float* d_eulers, float* d_re,
+                          float* d_im, float* d_tx, float* d_ty, float* d_corr, float* d_diff2s, long image_size,
+                          long O, long T, long todo_blocks, unsigned long* d_rot_idx, unsigned long* d_trans_idx,
+                          unsigned long* d_job_idx, unsigned long* d_job_num, void* stream) {
+  RefProjector* p = reinterpret_cast<RefProjector*>(h);
+  AccProjectorKernel k = make_view(p, imgX, imgY, imgZ, imgMaxR);
+  cuda_kernel_diff2_CC_fine<true, false, 128, 16><<<(unsigned)todo_blocks, 128, 0, (cudaStream_t)stream>>>(
+      d_eulers, d_re, d_im, d_tx, d_ty, nullptr, k, d_corr, d_diff2s, (unsigned)image_size, 0.f, 1.f,
       (unsigned long)O, (unsigned long)T, (unsigned long)todo_blocks, d_rot_idx, d_trans_idx, d_job_idx, d_job_num);
   return (int)cudaGetLastError();
 }

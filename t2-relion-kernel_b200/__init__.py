@@ -164,6 +164,7 @@ def _declare(L):
         "b200d2_set_gemm_variant": [I, I, I, I],
         "b200d2_set_combine": [I],
         "b200d2_diff2_fine": [C.POINTER(View), P, P, P, P, P, P, P, Z, F, Z, P, P, P, P, P],
+        "b200d2_diff2_fine_cc": [C.POINTER(View), P, P, P, P, P, P, P, Z, Z, P, P, P, P, P],
         "b200d2_ctf_fold": [P, P, C.c_longlong, I, I, I, I, I, I, F, P, P, C.c_longlong, P, P, P, P],
     }
     for name, args in sig.items():
@@ -490,6 +491,16 @@ def diff2_fine(view: View, eulers, real, imag, trans_x, trans_y, corr, diff2s, *
                                    _ptr(trans_y), _ptr(corr), _ptr(diff2s), image_size, sum_init,
                                    int(job_idx.numel()), _ptr(rot_idx), _ptr(trans_idx), _ptr(job_idx),
                                    _ptr(job_num), _stream(stream)), "diff2_fine")
+
+
+def diff2_fine_cc(view: View, eulers, real, imag, trans_x, trans_y, corr, diff2s, *, rot_idx, trans_idx, job_idx,
+                  job_num, image_size: int, stream=None):
+    """CC form of the fine pass (b200d2_diff2_fine_cc): -cross / sqrt(norm)
+    per (job, translation), written."""
+    _check(lib().b200d2_diff2_fine_cc(C.byref(view), _ptr(eulers), _ptr(real), _ptr(imag), _ptr(trans_x),
+                                      _ptr(trans_y), _ptr(corr), _ptr(diff2s), image_size, int(job_idx.numel()),
+                                      _ptr(rot_idx), _ptr(trans_idx), _ptr(job_idx), _ptr(job_num),
+                                      _stream(stream)), "diff2_fine_cc")
 
 
 def coarse_weights(diff2, P: int, O: int, T: int, out_min=None, pdf_orient=None, pdf_offset=None,

@@ -27,6 +27,13 @@
 // follow the fine kernel's mapping (src/diff2.cuh:612-626): rows past maxR
 // wrap to negative y when they lie within maxR of the end, otherwise their x
 // is set to maxR (outside the projector radius).
+//
+// The same kernel with CC = true replaces cuda_kernel_diff2_CC_fine
+// (src/diff2.cuh:811-960): per (job, translation) it writes
+//   diff2s[job_idx[j] + i] = -sum_px corr Re(conj(proj) shift_i(img)) / sqrt(sum_px corr |proj|^2)
+// (full corr, no sum_init, written).  The cross sums are taken as above with
+// q = corr conj(A) X; the norm is summed in FP64 and the quotient taken in
+// FP64.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -50,7 +57,7 @@ __device__ __forceinline__ void fine_pixel_coor(int pixel, int imgX, int imgY, i
   }
 }
 
-template <int NT, bool TABLES>
+template <int NT, bool TABLES, bool CC>
 __global__ void __launch_bounds__(kFineThreads) diff2_fine_kernel(
     b200d2_view v, const float* __restrict__ eulers, const float* __restrict__ re, const float* __restrict__ im,
     const float* __restrict__ tx, const float* __restrict__ ty, const float* __restrict__ corr,
@@ -96,16 +103,20 @@ __global__ void __launch_bounds__(kFineThreads) diff2_fine_kernel(
       }
       __syncthreads();
     }
-    double nrm = 0.0;  // TABLES: sum w(|A|^2 + |X|^2) of this thread's pixels
+    double nrm = 0.0;  // this thread's sum w(|A|^2 + |X|^2) (tables) or sum corr |A|^2 (CC)
     for (int pixel = threadIdx.x; pixel < image_size; pixel += kFineThreads) {
       int x, y;
       fine_pixel_coor(pixel, v.imgX, v.imgY, v.maxR, x, y);
       const float2 a = project_pixel(v, (float)x, (float)y, e);
       const float xr = re[pixel], xi = im[pixel];
-      const float w = 0.5f * corr[pixel];
+      const float w = CC ? corr[pixel] : 0.5f * corr[pixel];
+      if (CC) {  // the CC denominator: sum corr |A|^2
+        const double ad = a.x, bd = a.y;
+        nrm = fma((double)w, fma(ad, ad, bd * bd), nrm);
+      }
       if (TABLES) {
         const double ad = a.x, bd = a.y, xd = xr, yd = xi;
-        nrm = fma((double)w, fma(ad, ad, fma(bd, bd, fma(xd, xd, yd * yd))), nrm);
+        if (!CC) nrm = fma((double)w, fma(ad, ad, fma(bd, bd, fma(xd, xd, yd * yd))), nrm);
         const float qr = __fmul_rn(w, __fmaf_rn(a.x, xr, __fmul_rn(a.y, xi)));   // w Re(conj(A) X)
         const float qi = __fmul_rn(w, __fmaf_rn(a.x, xi, -__fmul_rn(a.y, xr)));  // w Im(conj(A) X)
         const float2* pex = s_ex + x;
@@ -125,6 +136,12 @@ __global__ void __launch_bounds__(kFineThreads) diff2_fine_kernel(
           if (i < nt) {
             float s, c;
             sincosf(__fmaf_rn((float)x, ftx[i], __fmul_rn((float)y, fty[i])), &s, &c);
+            if (CC) {  // corr Re(conj(A) S), S = X e^{i(x tx + y ty)}
+              const float sr = __fmaf_rn(c, xr, -__fmul_rn(s, xi));
+              const float si = __fmaf_rn(c, xi, __fmul_rn(s, xr));
+              acc[i] = __fmaf_rn(__fmaf_rn(a.x, sr, __fmul_rn(a.y, si)), w, acc[i]);
+              continue;
+            }
             const float dr = a.x - __fmaf_rn(c, xr, -__fmul_rn(s, xi));
             const float di = a.y - __fmaf_rn(c, xi, __fmul_rn(s, xr));
             acc[i] = __fmaf_rn(__fmaf_rn(dr, dr, __fmul_rn(di, di)), w, acc[i]);
@@ -133,7 +150,7 @@ __global__ void __launch_bounds__(kFineThreads) diff2_fine_kernel(
       }
     }
     // fixed-order reduction: shuffle tree inside each warp, then warps in order
-    if (TABLES) {
+    if (TABLES || CC) {
 #pragma unroll
       for (int i = 0; i < NT; ++i) {
         double vsum = (double)acc[i];
@@ -155,14 +172,14 @@ __global__ void __launch_bounds__(kFineThreads) diff2_fine_kernel(
     }
     __syncthreads();
     if (threadIdx.x < nt) {
-      if (TABLES) {
+      if (TABLES || CC) {
         double cr = 0.0, nt2 = 0.0;
 #pragma unroll
         for (int w = 0; w < kFineThreads / 32; ++w) {
           cr += s_cross[w][threadIdx.x];
           nt2 += s_norm[w];
         }
-        diff2s[jb + base + threadIdx.x] = (float)(fma(-2.0, cr, nt2) + (double)sum_init);
+        diff2s[jb + base + threadIdx.x] = CC ? (float)(-cr / sqrt(nt2)) : (float)(fma(-2.0, cr, nt2) + (double)sum_init);
       } else {
         float tot = 0.f;
 #pragma unroll
@@ -176,11 +193,13 @@ __global__ void __launch_bounds__(kFineThreads) diff2_fine_kernel(
 
 }  // namespace b200d2
 
-extern "C" int b200d2_diff2_fine(const b200d2_view* view, const float* d_eulers, const float* d_real,
-                                 const float* d_imag, const float* d_trans_x, const float* d_trans_y,
-                                 const float* d_corr, float* d_diff2s, size_t image_size, float sum_init,
-                                 size_t todo_blocks, const uint64_t* d_rot_idx, const uint64_t* d_trans_idx,
-                                 const uint64_t* d_job_idx, const uint64_t* d_job_num, void* stream) {
+namespace {
+
+template <bool CC>
+int launch_fine(const b200d2_view* view, const float* d_eulers, const float* d_real, const float* d_imag,
+                const float* d_trans_x, const float* d_trans_y, const float* d_corr, float* d_diff2s,
+                size_t image_size, float sum_init, size_t todo_blocks, const uint64_t* d_rot_idx,
+                const uint64_t* d_trans_idx, const uint64_t* d_job_idx, const uint64_t* d_job_num, void* stream) {
   using namespace b200d2;
   if (!view) return B200D2_ERR_INVALID;
   if (todo_blocks == 0 || image_size == 0) return B200D2_OK;
@@ -198,18 +217,39 @@ extern "C" int b200d2_diff2_fine(const b200d2_view* view, const float* d_eulers,
   if (view->maxR >= 0 && view->imgX > 0 && view->imgY > 0 && tab_bytes <= kFineTableBytes) {
     static bool attr = false;  // the opt-in above 48 KB of dynamic shared memory
     if (!attr) {
-      B200D2_CUDA_TRY(cudaFuncSetAttribute(diff2_fine_kernel<kFineMaxTrans, true>,
+      B200D2_CUDA_TRY(cudaFuncSetAttribute(diff2_fine_kernel<kFineMaxTrans, true, CC>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFineTableBytes));
       attr = true;
     }
-    diff2_fine_kernel<kFineMaxTrans, true><<<(unsigned)todo_blocks, kFineThreads, tab_bytes, (cudaStream_t)stream>>>(
+    diff2_fine_kernel<kFineMaxTrans, true, CC><<<(unsigned)todo_blocks, kFineThreads, tab_bytes,
+                                                 (cudaStream_t)stream>>>(
         *view, d_eulers, d_real, d_imag, d_trans_x, d_trans_y, d_corr, d_diff2s, (int)image_size, sum_init,
         d_rot_idx, d_trans_idx, d_job_idx, d_job_num);
   } else {
-    diff2_fine_kernel<kFineMaxTrans, false><<<(unsigned)todo_blocks, kFineThreads, 0, (cudaStream_t)stream>>>(
+    diff2_fine_kernel<kFineMaxTrans, false, CC><<<(unsigned)todo_blocks, kFineThreads, 0, (cudaStream_t)stream>>>(
         *view, d_eulers, d_real, d_imag, d_trans_x, d_trans_y, d_corr, d_diff2s, (int)image_size, sum_init,
         d_rot_idx, d_trans_idx, d_job_idx, d_job_num);
   }
   count_launch();
   return status_from_cuda(cudaGetLastError());
+}
+
+}  // namespace
+
+extern "C" int b200d2_diff2_fine(const b200d2_view* view, const float* d_eulers, const float* d_real,
+                                 const float* d_imag, const float* d_trans_x, const float* d_trans_y,
+                                 const float* d_corr, float* d_diff2s, size_t image_size, float sum_init,
+                                 size_t todo_blocks, const uint64_t* d_rot_idx, const uint64_t* d_trans_idx,
+                                 const uint64_t* d_job_idx, const uint64_t* d_job_num, void* stream) {
+  return launch_fine<false>(view, d_eulers, d_real, d_imag, d_trans_x, d_trans_y, d_corr, d_diff2s, image_size,
+                            sum_init, todo_blocks, d_rot_idx, d_trans_idx, d_job_idx, d_job_num, stream);
+}
+
+extern "C" int b200d2_diff2_fine_cc(const b200d2_view* view, const float* d_eulers, const float* d_real,
+                                    const float* d_imag, const float* d_trans_x, const float* d_trans_y,
+                                    const float* d_corr, float* d_diff2s, size_t image_size, size_t todo_blocks,
+                                    const uint64_t* d_rot_idx, const uint64_t* d_trans_idx,
+                                    const uint64_t* d_job_idx, const uint64_t* d_job_num, void* stream) {
+  return launch_fine<true>(view, d_eulers, d_real, d_imag, d_trans_x, d_trans_y, d_corr, d_diff2s, image_size,
+                           0.f, todo_blocks, d_rot_idx, d_trans_idx, d_job_idx, d_job_num, stream);
 }

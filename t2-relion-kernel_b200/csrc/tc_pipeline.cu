@@ -56,7 +56,7 @@ struct TcGeom {
   int P, O, T, N_img, K_c, Kpad, Mrows, Mpad, Opad, maxR, exw, eyw;
   int elem, BK, terms;
   int Kq;  // row stride (doubles) of |B|^2 and of the compacted weights: Kpad / 2, zero padded
-  size_t off_status, off_xy, off_idx, off_ex, off_ey, off_bhi, off_blo, off_q, off_w, off_normx, off_na, off_nahl,
+  size_t off_status, off_xy, off_idx, off_ex, off_ey, off_ph, off_bhi, off_blo, off_q, off_w, off_normx, off_na, off_nahl,
       off_ahi, off_alo, off_keys, off_sa, off_sb, off_part, off_cnt, total;
   int split_max;  // largest k-split the workspace holds partial sums for
   int n_cnt;      // split arrival counters
@@ -124,6 +124,7 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, i
   g.off_idx = take(sizeof(int) * (size_t)std::max(g.K_c, 1));
   g.off_ex = take(sizeof(float2) * (size_t)g.T * g.exw);
   g.off_ey = take(sizeof(float2) * (size_t)g.T * g.eyw);
+  g.off_ph = take(sizeof(float2) * (size_t)g.T * (g.Kpad / 2));  // phase of every (table, listed pixel)
   g.off_bhi = take((size_t)g.Opad * g.Kpad * g.elem);
   g.off_blo = planes == 2 ? take((size_t)g.Opad * g.Kpad * g.elem) : g.off_bhi;
   g.Kq = g.Kpad / 2;  // a multiple of 16
@@ -267,6 +268,27 @@ __global__ void tc_phase_kernel(const float* __restrict__ tx, const float* __res
   }
 }
 
+// Phase of every (table, listed pixel) as the product of the separable
+// tables, ph[t][kp] = e^{i x tx} e^{i y ty} (zero past K_c), so that stage 5
+// reads one coalesced 8-byte value per element of A.
+__global__ void tc_phase2d_kernel(const float2* __restrict__ ex, const float2* __restrict__ ey,
+                                  const int2* __restrict__ xy, int K_c, int Kh, int T, int maxR, float2* ph) {
+  const int kp = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kp >= Kh) return;
+  const int exw = maxR + 1, eyw = 2 * maxR + 1;
+  int2 c = make_int2(0, 0);
+  if (kp < K_c) c = xy[kp];
+  for (int t = blockIdx.y; t < T; t += gridDim.y) {
+    float2 v = make_float2(0.f, 0.f);
+    if (kp < K_c) {
+      const float2 fx = ex[t * exw + c.x];
+      const float2 fy = ey[t * eyw + c.y + maxR];
+      v = make_float2(__fmaf_rn(fx.x, fy.x, -__fmul_rn(fx.y, fy.y)), __fmaf_rn(fx.x, fy.y, __fmul_rn(fx.y, fy.x)));
+    }
+    ph[(size_t)t * Kh + kp] = v;
+  }
+}
+
 // ------------------------------------------------------------------ splits
 __device__ __forceinline__ float tf32_round(float v) {
   uint32_t r;
@@ -296,6 +318,52 @@ __device__ __forceinline__ void store_split(void* hi, void* lo, size_t at, float
     reinterpret_cast<float2*>(lo)[at] = make_float2(tf32_round(re - hr), tf32_round(im - hm));
   } else {
     reinterpret_cast<float2*>(hi)[at] = make_float2(tf32_round(re), tf32_round(im));
+  }
+}
+
+// Four consecutive complex values at element `at` (a multiple of 4): the
+// same values as four store_split calls, written as 16-byte stores.
+template <int PREC>
+__device__ __forceinline__ void store_split4(void* hi, void* lo, size_t at, const float (&re)[4],
+                                             const float (&im)[4]) {
+  if constexpr (PREC == B200D2_PREC_BF16X3 || PREC == B200D2_PREC_FP16X3 || PREC == B200D2_PREC_FP16) {
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if constexpr (PREC == B200D2_PREC_BF16X3) {
+        const __nv_bfloat162 hv = __floats2bfloat162_rn(re[j], im[j]);
+        const float2 hf = __bfloat1622float2(hv);
+        const __nv_bfloat162 lv = __floats2bfloat162_rn(re[j] - hf.x, im[j] - hf.y);
+        h[j] = *reinterpret_cast<const uint32_t*>(&hv);
+        l[j] = *reinterpret_cast<const uint32_t*>(&lv);
+      } else {
+        const __half2 hv = __floats2half2_rn(re[j], im[j]);
+        const float2 hf = __half22float2(hv);
+        const __half2 lv = __floats2half2_rn(re[j] - hf.x, im[j] - hf.y);
+        h[j] = *reinterpret_cast<const uint32_t*>(&hv);
+        l[j] = *reinterpret_cast<const uint32_t*>(&lv);
+      }
+    }
+    reinterpret_cast<uint4*>(reinterpret_cast<uint32_t*>(hi) + at)[0] = make_uint4(h[0], h[1], h[2], h[3]);
+    if constexpr (PREC != B200D2_PREC_FP16)
+      reinterpret_cast<uint4*>(reinterpret_cast<uint32_t*>(lo) + at)[0] = make_uint4(l[0], l[1], l[2], l[3]);
+  } else {
+    float hr[4], hm[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      hr[j] = tf32_round(re[j]);
+      hm[j] = tf32_round(im[j]);
+    }
+    float4* ph = reinterpret_cast<float4*>(reinterpret_cast<float2*>(hi) + at);
+    ph[0] = make_float4(hr[0], hm[0], hr[1], hm[1]);
+    ph[1] = make_float4(hr[2], hm[2], hr[3], hm[3]);
+    if constexpr (PREC == B200D2_PREC_TF32X3) {
+      float4* pl = reinterpret_cast<float4*>(reinterpret_cast<float2*>(lo) + at);
+      pl[0] = make_float4(tf32_round(re[0] - hr[0]), tf32_round(im[0] - hm[0]), tf32_round(re[1] - hr[1]),
+                          tf32_round(im[1] - hm[1]));
+      pl[1] = make_float4(tf32_round(re[2] - hr[2]), tf32_round(im[2] - hm[2]), tf32_round(re[3] - hr[3]),
+                          tf32_round(im[3] - hm[3]));
+    }
   }
 }
 
@@ -472,27 +540,38 @@ __device__ __forceinline__ void cp_async_wait() {
 // FP64 tensor-core MMA (DMMA): D[8x8] += A[8x4] * B[4x8], all FP64.  Lane l
 // holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) + {0,1}].
 __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-               : "+d"(d[0]), "+d"(d[1])
-               : "d"(a), "d"(b));
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
 }
 
 // CTA tile: (2*8*WM) particles x 64 orientations, 4 warps in a 2 x 2 grid,
-// each warp WM x 4 DMMA tiles of 8 x 8; 16-pixel slabs double-buffered
-// through shared memory with cp.async.
+// each warp WM x 4 DMMA tiles of 8 x 8; 32-pixel slabs in a three-stage
+// cp.async ring (one barrier per slab, two slabs in flight).  (Splitting each
+// slab's pixels over two groups of 4 warps, with the two sums added at the
+// end, measured slower: 94.9 against 86.3 us at 128 particles.)
 // cc: store k = -sqrt(2 / sum w|B|^2) (the CC score's factor) instead of nA.
+constexpr int kNormaKC = 32, kNormaLD = kNormaKC + 4, kNormaStages = 3, kNormaCO = 64;
 template <int WM>
-__global__ void __launch_bounds__(128) tc_norma_kernel(const double* __restrict__ wcomp, int Kq,
+constexpr size_t norma_smem_bytes() {
+  return sizeof(double) * kNormaStages * (16 * WM + kNormaCO) * kNormaLD;
+}
+
+constexpr int kNormaThreads = 128;
+template <int WM>
+__global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* __restrict__ wcomp, int Kq,
                                                        const double* __restrict__ q, int O, int P,
                                                        const double* __restrict__ normx, double* na,
                                                        float2* na_hl, int cc) {
-  // Kq: row stride of wcomp and q, a multiple of 16, zero padded.  Shared
-  // rows padded to 20 doubles (160 B, 16-byte aligned): the fragment loads
-  // of a half-warp (rows g, columns t, g, t < 4) fall on distinct bank pairs
-  // 8g + 2t.
-  constexpr int KC = 16, LD = KC + 4, CP = 16 * WM, CO = 64;
-  __shared__ __align__(16) double sw[2][CP][LD];
-  __shared__ __align__(16) double sq[2][CO][LD];
+  // Kq: row stride of wcomp and q, a multiple of 16, zero padded; the last
+  // slab is zero-filled past Kq.  Shared rows padded to 36 doubles (288 B,
+  // 16-byte aligned): the fragment loads of a half-warp (rows g, columns t,
+  // g, t < 4) fall on distinct bank pairs 4g + t (mod 16).
+  constexpr int KC = kNormaKC, LD = kNormaLD, NST = kNormaStages, CP = 16 * WM, CO = kNormaCO;
+  extern __shared__ __align__(16) double norma_smem[];
+  double* sw = norma_smem;                   // [NST][CP][LD]
+  double* sq = norma_smem + NST * CP * LD;   // [NST][CO][LD]
+  constexpr int NT = kNormaThreads;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gid = lane >> 2, tig = lane & 3;
   const int wp0 = (warp >> 1) * 8 * WM, wo0 = (warp & 1) * 32;
@@ -503,44 +582,49 @@ __global__ void __launch_bounds__(128) tc_norma_kernel(const double* __restrict_
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   auto stage = [&](int buf, int k0) {
-    // 16-byte pieces (two doubles); rows past P or O are zero-filled
-    for (int e = tid; e < CP * (KC / 2); e += 128) {
+    // 16-byte pieces (two doubles); rows past P or O and columns past Kq are zero-filled
+    double* dw = sw + buf * CP * LD;
+    double* dq = sq + buf * CO * LD;
+    for (int e = tid; e < CP * (KC / 2); e += NT) {
       const int pp = e / (KC / 2), k = 2 * (e % (KC / 2));
-      const bool ok = p0 + pp < P;
-      cp_async16(&sw[buf][pp][k], ok ? wcomp + (size_t)(p0 + pp) * Kq + k0 + k : wcomp, ok);
+      const bool ok = p0 + pp < P && k0 + k < Kq;
+      cp_async16(dw + pp * LD + k, ok ? wcomp + (size_t)(p0 + pp) * Kq + k0 + k : wcomp, ok);
     }
-    for (int e = tid; e < CO * (KC / 2); e += 128) {
+    for (int e = tid; e < CO * (KC / 2); e += NT) {
       const int oo = e / (KC / 2), k = 2 * (e % (KC / 2));
-      const bool ok = o0 + oo < O;
-      cp_async16(&sq[buf][oo][k], ok ? q + (size_t)(o0 + oo) * Kq + k0 + k : q, ok);
+      const bool ok = o0 + oo < O && k0 + k < Kq;
+      cp_async16(dq + oo * LD + k, ok ? q + (size_t)(o0 + oo) * Kq + k0 + k : q, ok);
     }
-    cp_async_commit();
   };
-  const int nslab = Kq / KC;
-  if (nslab > 0) stage(0, 0);
+  const int nslab = (Kq + KC - 1) / KC;
+  // one commit group per slab (empty past the end), so wait<NST-2> leaves
+  // exactly the current slab complete
+#pragma unroll
+  for (int sl = 0; sl < NST - 1; ++sl) {
+    if (sl < nslab) stage(sl, sl * KC);
+    cp_async_commit();
+  }
   for (int sl = 0; sl < nslab; ++sl) {
-    const int buf = sl & 1;
-    if (sl + 1 < nslab) {
-      stage(buf ^ 1, (sl + 1) * KC);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncthreads();
+    cp_async_wait<NST - 2>();
+    __syncthreads();  // slab sl visible to all; every warp is done with slab sl - 1
+    if (sl + NST - 1 < nslab) stage((sl + NST - 1) % NST, (sl + NST - 1) * KC);
+    cp_async_commit();
+    const double* cw = sw + (sl % NST) * CP * LD;
+    const double* cq = sq + (sl % NST) * CO * LD;
 #pragma unroll
     for (int k4 = 0; k4 < KC; k4 += 4) {
       double a[WM], bq[4];
 #pragma unroll
-      for (int i = 0; i < WM; ++i) a[i] = sw[buf][wp0 + 8 * i + gid][k4 + tig];
+      for (int i = 0; i < WM; ++i) a[i] = cw[(wp0 + 8 * i + gid) * LD + k4 + tig];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bq[j] = sq[buf][wo0 + 8 * j + gid][k4 + tig];
+      for (int j = 0; j < 4; ++j) bq[j] = cq[(wo0 + 8 * j + gid) * LD + k4 + tig];
 #pragma unroll
       for (int i = 0; i < WM; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j], a[i], bq[j]);
     }
-    __syncthreads();
   }
+  cp_async_wait<0>();
 #pragma unroll
   for (int i = 0; i < WM; ++i) {
     const int p = p0 + wp0 + 8 * i + gid;
@@ -566,85 +650,123 @@ __global__ void __launch_bounds__(128) tc_norma_kernel(const double* __restrict_
   }
 }
 
+template <int WM>
+static void launch_norma(dim3 grid, cudaStream_t s, const double* wcomp, int Kq, const double* q, int O, int P,
+                         const double* normx, double* na, float2* na_hl, int cc) {
+  static bool attr = false;  // above 48 KB of dynamic shared memory
+  if (!attr) {
+    cudaFuncSetAttribute(tc_norma_kernel<WM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)norma_smem_bytes<WM>());
+    attr = true;
+  }
+  tc_norma_kernel<WM><<<grid, kNormaThreads, norma_smem_bytes<WM>(), s>>>(wcomp, Kq, q, O, P, normx, na, na_hl, cc);
+}
+
 // ------------------------------------------------------------------ stage 5
-// Row m = p*T + t of the translated, weighted image: a = (corr/2) X e^{i(x tx + y ty)}.
-template <int PREC>
+// Row m = p*T + t of the translated, weighted image: a = (corr/2) X e^{i(x tx + y ty)},
+// the phase read from the (table, pixel) product ph.  A thread writes four
+// consecutive complex values of kGenRows consecutive rows with 16-byte
+// stores; rows past Mrows are zero.
+constexpr int kGenV = 4, kGenRows = 16;
+template <int PREC, bool UNEVEN>
 __global__ void __launch_bounds__(256) tc_gen_a_kernel(
     const float* __restrict__ re, const float* __restrict__ im, const float* __restrict__ corr,
-    long long stride, const int2* __restrict__ xy, const int* __restrict__ idx, int K_c, int Kpad,
-    const float2* __restrict__ ex, const float2* __restrict__ ey, int T, int maxR, int Mrows,
-    void* ahi, void* alo, const PartDev* __restrict__ parts, const int4* __restrict__ rows,
+    long long stride, const int* __restrict__ idx, int K_c, int Kh, const float2* __restrict__ ph, int T,
+    int Mrows, void* ahi, void* alo, const PartDev* __restrict__ parts, const int4* __restrict__ rows,
     const float* __restrict__ inv_sa) {
-  constexpr int ROWS = 32;
-  const int kp = blockIdx.x * blockDim.x + threadIdx.x;
-  if (kp >= Kpad / 2) return;
-  const bool has = kp < K_c;
-  int x = 0, y = 0, pix = 0;
-  if (has) {
-    const int2 c = xy[kp];
-    x = c.x;
-    y = c.y;
-    pix = idx[kp];
-  }
-  const int exw = maxR + 1, eyw = 2 * maxR + 1;
-  const int m0 = blockIdx.y * ROWS;
-  int p = rows ? 0 : m0 / T;
-  int t = rows ? 0 : m0 - p * T;
+  const int kp0 = (blockIdx.x * blockDim.x + threadIdx.x) * kGenV;
+  if (kp0 >= Kh) return;
+  int pix[kGenV];
+#pragma unroll
+  for (int j = 0; j < kGenV; ++j) pix[j] = kp0 + j < K_c ? idx[kp0 + j] : -1;
+  const int m0 = blockIdx.y * kGenRows;
+  int p = UNEVEN ? 0 : m0 / T;
+  int t = UNEVEN ? 0 : m0 - p * T;
   int cur_p = -1;
-  float wr = 0.f, wi = 0.f;
-  for (int r = 0; r < ROWS; ++r) {
-    const int m = m0 + r;
-    float ar = 0.f, ai = 0.f;
-    if (has && m < Mrows) {
-      int tab = t;
-      if (rows) {  // uneven batch: (particle, translation, phase table) from the row table
-        const int4 rw = rows[m];
-        p = rw.x;
-        tab = rw.z;
-      }
-      if (p != cur_p) {
-        float w, xr, xi;
-        if (parts) {
-          const PartDev& pd = parts[p];
-          w = pd.corr[pix] / 2;
-          xr = pd.re[pix];
-          xi = pd.im[pix];
-        } else {
-          const long long at = (long long)p * stride + pix;
-          w = corr[at] / 2;
-          xr = re[at];
-          xi = im[at];
+  float wr[kGenV], wi[kGenV];
+#pragma unroll
+  for (int j = 0; j < kGenV; ++j) wr[j] = wi[j] = 0.f;
+  // groups of kGenQ rows: the rows' phase loads are issued together, then
+  // the rows are combined and stored
+  constexpr int kGenQ = 4;
+  static_assert(kGenRows % kGenQ == 0, "row groups");
+  for (int r0 = 0; r0 < kGenRows; r0 += kGenQ) {
+    int prow[kGenQ], tab[kGenQ];
+#pragma unroll
+    for (int q = 0; q < kGenQ; ++q) {
+      const int m = m0 + r0 + q;
+      if (UNEVEN) {  // (particle, translation, phase table) from the row table
+        const int4 rw = m < Mrows ? rows[m] : make_int4(0, 0, 0, 0);
+        prow[q] = rw.x;
+        tab[q] = rw.z;
+      } else {
+        prow[q] = p;
+        tab[q] = t;
+        if (++t == T) {
+          t = 0;
+          ++p;
         }
-        wr = w * xr;
-        wi = w * xi;
-        if (inv_sa) {  // FP16 forms: exact power-of-two scale of the particle's rows
-          const float sc = __frcp_rn(inv_sa[p]);
-          wr *= sc;
-          wi *= sc;
-        }
-        cur_p = p;
       }
-      const float2 fx = ex[tab * exw + x];
-      const float2 fy = ey[tab * eyw + y + maxR];
-      const float pr = __fmaf_rn(fx.x, fy.x, -__fmul_rn(fx.y, fy.y));
-      const float pi = __fmaf_rn(fx.x, fy.y, __fmul_rn(fx.y, fy.x));
-      ar = __fmaf_rn(wr, pr, -__fmul_rn(wi, pi));
-      ai = __fmaf_rn(wr, pi, __fmul_rn(wi, pr));
     }
-    store_split<PREC>(ahi, alo, (size_t)m * (Kpad / 2) + kp, ar, ai);
-    if (++t == T) {
-      t = 0;
-      ++p;
+    float4 f[kGenQ][2];
+#pragma unroll
+    for (int q = 0; q < kGenQ; ++q) {
+      if (m0 + r0 + q < Mrows) {
+        const float4* pp = reinterpret_cast<const float4*>(ph + (size_t)tab[q] * Kh + kp0);
+        f[q][0] = pp[0];
+        f[q][1] = pp[1];
+      } else {
+        f[q][0] = f[q][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kGenQ; ++q) {
+      const int m = m0 + r0 + q;
+      float ar[kGenV], ai[kGenV];
+#pragma unroll
+      for (int j = 0; j < kGenV; ++j) ar[j] = ai[j] = 0.f;
+      if (m < Mrows) {
+        if (prow[q] != cur_p) {
+          const int pq = prow[q];
+          const float sc = inv_sa ? __frcp_rn(inv_sa[pq]) : 1.f;  // FP16 forms: exact power-of-two scale
+#pragma unroll
+          for (int j = 0; j < kGenV; ++j) {
+            float w = 0.f, xr = 0.f, xi = 0.f;
+            if (pix[j] >= 0) {
+              if (parts) {
+                const PartDev& pd = parts[pq];
+                w = pd.corr[pix[j]] / 2;
+                xr = pd.re[pix[j]];
+                xi = pd.im[pix[j]];
+              } else {
+                const long long at = (long long)pq * stride + pix[j];
+                w = corr[at] / 2;
+                xr = re[at];
+                xi = im[at];
+              }
+            }
+            wr[j] = w * xr;
+            wi[j] = w * xi;
+            if (inv_sa) {
+              wr[j] *= sc;
+              wi[j] *= sc;
+            }
+          }
+          cur_p = pq;
+        }
+        const float pr[kGenV] = {f[q][0].x, f[q][0].z, f[q][1].x, f[q][1].z};
+        const float pi[kGenV] = {f[q][0].y, f[q][0].w, f[q][1].y, f[q][1].w};
+#pragma unroll
+        for (int j = 0; j < kGenV; ++j) {
+          ar[j] = __fmaf_rn(wr[j], pr[j], -__fmul_rn(wi[j], pi[j]));
+          ai[j] = __fmaf_rn(wr[j], pi[j], __fmul_rn(wi[j], pr[j]));
+        }
+      }
+      store_split4<PREC>(ahi, alo, (size_t)m * Kh + kp0, ar, ai);
     }
   }
 }
 
-// ------------------------------------------------------------------ stage 6
-// ROWB: bytes of one k-block row of an operand tile (128 -> 128-byte swizzle,
-// 64 -> 64-byte swizzle).  Narrower k-blocks give more pipeline stages in the
-// same shared memory, i.e. more TMA latency hidden behind the tensor pipe.
-// BN: orientations per tile (256 or 128; the accumulator is double-buffered
-// in TMEM, 2 x BN columns).
 template <int PREC, int ROWB, int BN>
 struct GemmCfg {
   static constexpr bool kTf32 = (PREC == B200D2_PREC_TF32 || PREC == B200D2_PREC_TF32X3);
@@ -1571,6 +1693,7 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
   int* idx = ws_at<int>(ws, g.off_idx);
   float2* ex = ws_at<float2>(ws, g.off_ex);
   float2* ey = ws_at<float2>(ws, g.off_ey);
+  float2* ph = ws_at<float2>(ws, g.off_ph);
   void* bhi = ws_at<void>(ws, g.off_bhi);
   void* blo = ws_at<void>(ws, g.off_blo);
   double* q = ws_at<double>(ws, g.off_q);
@@ -1593,6 +1716,9 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       const int n = g.T * (g.exw + g.eyw);
       tc_phase_kernel<<<std::max(1, std::min((n + 255) / 256, 1024)), 256, 0, s>>>(
           b.d_trans_x, b.d_trans_y, g.T, g.maxR, ex, ey, U ? U->tab_txy : nullptr);
+      count_launch();
+      tc_phase2d_kernel<<<dim3((g.Kpad / 2 + 255) / 256, std::min(g.T, 65535)), 256, 0, s>>>(
+          ex, ey, xy, g.K_c, g.Kpad / 2, g.T, g.maxR, ph);
       if (kScaled) {  // the particle scales, needed by stage 5 on the same stream
         count_launch();
         tc_scale_a_kernel<<<g.P, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, parts, idx, g.K_c,
@@ -1618,23 +1744,29 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       // the largest particle tile (64, 32, 16) that still gives every SM a CTA
       const long long otiles = (g.O + 63) / 64;
       const int sms = num_sms();
-      if (otiles * ((g.P + 63) / 64) >= sms) {
-        tc_norma_kernel<4><<<dim3(otiles, (g.P + 63) / 64), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl,
-                                                                                    b.score == B200D2_SCORE_CC);
-      } else if (otiles * ((g.P + 31) / 32) >= sms) {
-        tc_norma_kernel<2><<<dim3(otiles, (g.P + 31) / 32), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl,
-                                                                                    b.score == B200D2_SCORE_CC);
-      } else {
-        tc_norma_kernel<1><<<dim3(otiles, (g.P + 15) / 16), 128, 0, s>>>(wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl,
-                                                                                    b.score == B200D2_SCORE_CC);
-      }
+      const int cc = b.score == B200D2_SCORE_CC;
+      if (otiles * ((g.P + 63) / 64) >= sms)
+        launch_norma<4>(dim3(otiles, (g.P + 63) / 64), s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc);
+      else if (otiles * ((g.P + 31) / 32) >= sms)
+        launch_norma<2>(dim3(otiles, (g.P + 31) / 32), s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc);
+      else
+        launch_norma<1>(dim3(otiles, (g.P + 15) / 16), s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc);
       break;
     }
     case 5: {
-      dim3 grid((g.Kpad / 2 + 255) / 256, g.Mpad / 32);
-      tc_gen_a_kernel<PREC><<<grid, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, xy, idx, g.K_c,
-                                                 g.Kpad, ex, ey, g.T, g.maxR, g.Mrows, ahi, alo, parts,
-                                                 U ? U->rows : nullptr, kScaled ? inv_sa : nullptr);
+      // one thread per four complex pixels of a row; warps spread evenly over
+      // at most 8-warp blocks; kGenRows rows per block (Mpad is a multiple of 128)
+      const int Kh = g.Kpad / 2, warps = (Kh / kGenV + 31) / 32;
+      const int nblk = (warps + 7) / 8, bw = (warps + nblk - 1) / nblk;
+      const dim3 grid(nblk, g.Mpad / kGenRows);
+      const float* isa = kScaled ? inv_sa : nullptr;
+      if (U)
+        tc_gen_a_kernel<PREC, true><<<grid, 32 * bw, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, idx, g.K_c,
+                                                             Kh, ph, g.T, g.Mrows, ahi, alo, parts, U->rows, isa);
+      else
+        tc_gen_a_kernel<PREC, false><<<grid, 32 * bw, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, idx,
+                                                              g.K_c, Kh, ph, g.T, g.Mrows, ahi, alo, parts, nullptr,
+                                                              isa);
       break;
     }
     case 6:
@@ -1678,8 +1810,9 @@ const char* tc_stage_name(int precision, int stage) {
   static const char* tf1[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_kernel<tf32>",
                               "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<tf32>",
                               "tc_gemm[_pair]_kernel<tf32>", "tc_finalize_kernel"};
-  // FP16 forms: stage 1 also launches tc_scale_a_kernel, stage 2 is the
-  // two-pass tc_project_scaled_kernel
+  // stage 1 also launches tc_phase2d_kernel (and, in the FP16 forms,
+  // tc_scale_a_kernel); in the FP16 forms stage 2 is the two-pass
+  // tc_project_scaled_kernel
   static const char* h3[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_scaled_kernel<fp16x3>",
                              "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<fp16x3>",
                              "tc_gemm[_pair]_kernel<fp16x3>", "tc_finalize_kernel"};
