@@ -440,6 +440,8 @@ def ours_arm(args):
     h_am = torch.empty(P, dtype=torch.int64).pin_memory()
     e2e_steps = max(3, min(args.steps, 10))
     torch.cuda.synchronize()
+    e2e_clocks = ClockSampler(local)
+    e2e_clocks.start()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     if plan is None:
@@ -482,6 +484,7 @@ def ours_arm(args):
             h_am.copy_(am, non_blocking=True)
         e1.record(stream)
     torch.cuda.synchronize()
+    e2e_clk = e2e_clocks.stop()
     e2e_val = replicas.job_rate(evals_step * e2e_steps, e0.elapsed_time(e1), dist, dev)
     h2d = 3 * P * N * 4
     d2h = P * (8 + 8)
@@ -538,7 +541,7 @@ def ours_arm(args):
                            "parallelism": f"replicas x{world}", **plan_extra},
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_val, "unit": "diff2 evals/s", "h2d_bytes_per_step": h2d,
-                        "d2h_bytes_per_step": d2h,
+                        "d2h_bytes_per_step": d2h, "clocks": e2e_clk,
                         "note": ("H2D of images+corr from pinned memory, batch call, D2H of per-particle min/argmin, every "
                           "step; uniform batches double-buffer the images so that step k+1's copy overlaps step k")},
                 "clocks": clk, "gpu_launches": int(l1 - l0), "kernels": kern.get("per_kernel_ms")}
