@@ -190,6 +190,18 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU baseline (oracle FP32 port), bounded sample
 # ---------------------------------------------------------------------------
+def cpu_model() -> str | None:
+    """The host CPU's model name (Linux /proc/cpuinfo), for the baseline record."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_sample(pr, budget_s: float, max_particles: int | None = None) -> dict:
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # the oracle's C restatement; measured here as the CPU baseline only
@@ -208,6 +220,7 @@ def cpu_sample(pr, budget_s: float, max_particles: int | None = None) -> dict:
         if el >= budget_s or (max_particles is not None and done >= max_particles):
             break
     return {"value": evals / el, "unit": "diff2 evals/s", "cores": nthreads, "kind": "port", "particles": done,
+            "nproc": os.cpu_count(), "cpu_model": cpu_model(),
             "sample": f"{done} particle(s) x {pr.O} orientations x {pr.T} translations of the same "
                       f"workload, FP32 C restatement of cuda_kernel_diff2_coarse, {nthreads} threads, "
                       f"{el:.1f} s"}
@@ -278,7 +291,7 @@ def reference_arm(args):
                                    f"image {pr.img_size} ({pr.N_img} px); each step = {per_step_particles} "
                                    f"particles (bounded CPU sample)", "particles_per_step": per_step_particles},
             "cpu_baseline": {"value": v, "unit": "diff2 evals/s", "cores": cores, "kind": "port",
-                             "sample": s["sample"]},
+                             "nproc": os.cpu_count(), "cpu_model": cpu_model(), "sample": s["sample"]},
             "e2e": {"value": v, "unit": "diff2 evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
