@@ -10,7 +10,7 @@
 // its input and output buffers.  For them this file keeps a fixed scratch
 // area in the library's own device image and runs the same pipeline on it.
 //
-// The scratch is a file-scope __device__ array of B200D2_STATIC_SCRATCH_BYTES
+// The scratch is a file-scope static __device__ array of B200D2_STATIC_SCRATCH_BYTES
 // (64 MiB): every GPU that loads the library holds it until the process
 // exits.  Host code cannot use the array's name as a device address (on the
 // host it names a stand-in object), so the device address is looked up once
@@ -43,7 +43,7 @@ const char* tc_stage_name(int precision, int stage);
 
 namespace {
 
-__device__ __align__(256) unsigned char g_static_scratch[B200D2_STATIC_SCRATCH_BYTES];
+static __device__ __align__(256) unsigned char g_static_scratch[B200D2_STATIC_SCRATCH_BYTES];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
