@@ -116,13 +116,14 @@ def test_fine_matches_reference_and_fp64(pkg, synth, oracle, cuda, case, max_chu
 
 
 @pytest.mark.parametrize("cc", [False, True], ids=["diff2", "cc"])
-@pytest.mark.parametrize("imgX,imgY,imgMaxR", [(65, 128, 64), (257, 512, 256)])
+@pytest.mark.parametrize("imgX,imgY,imgMaxR", [(65, 128, 64), (129, 256, 128), (257, 512, 256)])
 def test_fine_images_beyond_projector_radius(pkg, synth, oracle, cuda, imgX, imgY, imgMaxR, cc):
     """Images larger than the c1 projector's radius (16): the view's maxR is
     the projector's, so rows between maxR and imgY - maxR take the fine
-    kernel's x = maxR mapping.  At 128 pixels the phase tables fit; at 512
-    (257 x 512 half-transform) they would exceed the shared-memory area and
-    the kernel takes sincos per pixel.  Random image data; pixels beyond the
+    kernel's x = maxR mapping.  At 128 pixels the column form runs (tables
+    and the shared q fit); at 256 only the tables fit and the per-pixel table
+    form runs; at 512 (257 x 512 half-transform) the tables would exceed the
+    shared-memory area and the kernel takes sincos per pixel.  Random image data; pixels beyond the
     projector's radius score against a zero projection."""
     torch = cuda
     pr = synth.make_problem("c1", P=1, orient_limit=64)
