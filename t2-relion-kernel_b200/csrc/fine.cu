@@ -212,7 +212,7 @@ __host__ __device__ inline int fine_cols_eyw(int imgY, int maxR) { return maxR +
 constexpr size_t kFineColsSmem = 160 * 1024;  // tables + q, per CTA
 
 template <int NT, bool CC>
-__global__ void __launch_bounds__(kFineColsMaxThreads, 2) diff2_fine_cols_kernel(
+__global__ void __launch_bounds__(kFineColsMaxThreads, 3) diff2_fine_cols_kernel(
     b200d2_view v, const float* __restrict__ eulers, const float* __restrict__ re, const float* __restrict__ im,
     const float* __restrict__ tx, const float* __restrict__ ty, const float* __restrict__ corr,
     float* __restrict__ diff2s, int image_size, float sum_init, int groups, const uint64_t* __restrict__ rot_idx,
