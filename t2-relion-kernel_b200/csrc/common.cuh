@@ -11,6 +11,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "../../include/b200d2.h"
 
 namespace b200d2 {
@@ -23,6 +25,21 @@ namespace b200d2 {
 
 // Process-wide count of kernel launches made by this library.
 void count_launch(unsigned n = 1);
+
+// Opts `kernel` in to `bytes` of dynamic shared memory on the current device,
+// once per device (the attribute belongs to each device's context); `done`
+// holds one bit per device ordinal (mod 64).
+template <typename K>
+inline cudaError_t smem_opt_in(K* kernel, int bytes, std::atomic<unsigned long long>& done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load() & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done.fetch_or(bit);
+  return e;
+}
 
 inline int status_from_cuda(cudaError_t e) {
   if (e == cudaSuccess) return B200D2_OK;

@@ -401,22 +401,14 @@ int launch_fine(const b200d2_view* view, const float* d_eulers, const float* d_r
     const int groups = std::max(1, std::min(view->imgY, std::min((256 + view->imgX / 2) / view->imgX,
                                                                   kFineColsMaxThreads / view->imgX)));
     const int threads = (view->imgX * groups + 31) / 32 * 32;
-    static bool attr = false;  // the opt-in above 48 KB of dynamic shared memory
-    if (!attr) {
-      B200D2_CUDA_TRY(cudaFuncSetAttribute(diff2_fine_cols_kernel<kFineMaxTrans, CC>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFineColsSmem));
-      attr = true;
-    }
+    static std::atomic<unsigned long long> opted{0};  // above 48 KB of dynamic shared memory
+    B200D2_CUDA_TRY(smem_opt_in(diff2_fine_cols_kernel<kFineMaxTrans, CC>, (int)kFineColsSmem, opted));
     diff2_fine_cols_kernel<kFineMaxTrans, CC><<<(unsigned)todo_blocks, threads, cols_bytes, (cudaStream_t)stream>>>(
         *view, d_eulers, d_real, d_imag, d_trans_x, d_trans_y, d_corr, d_diff2s, (int)image_size, sum_init, groups,
         d_rot_idx, d_trans_idx, d_job_idx, d_job_num);
   } else if (view->maxR >= 0 && view->imgX > 0 && view->imgY > 0 && tab_bytes <= kFineTableBytes) {
-    static bool attr = false;  // the opt-in above 48 KB of dynamic shared memory
-    if (!attr) {
-      B200D2_CUDA_TRY(cudaFuncSetAttribute(diff2_fine_kernel<kFineMaxTrans, true, CC>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFineTableBytes));
-      attr = true;
-    }
+    static std::atomic<unsigned long long> opted{0};  // above 48 KB of dynamic shared memory
+    B200D2_CUDA_TRY(smem_opt_in(diff2_fine_kernel<kFineMaxTrans, true, CC>, (int)kFineTableBytes, opted));
     diff2_fine_kernel<kFineMaxTrans, true, CC><<<(unsigned)todo_blocks, kFineThreads, tab_bytes,
                                                  (cudaStream_t)stream>>>(
         *view, d_eulers, d_real, d_imag, d_trans_x, d_trans_y, d_corr, d_diff2s, (int)image_size, sum_init,

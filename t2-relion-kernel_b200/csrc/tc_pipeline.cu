@@ -651,15 +651,13 @@ __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* _
 }
 
 template <int WM>
-static void launch_norma(dim3 grid, cudaStream_t s, const double* wcomp, int Kq, const double* q, int O, int P,
-                         const double* normx, double* na, float2* na_hl, int cc) {
-  static bool attr = false;  // above 48 KB of dynamic shared memory
-  if (!attr) {
-    cudaFuncSetAttribute(tc_norma_kernel<WM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)norma_smem_bytes<WM>());
-    attr = true;
-  }
+static cudaError_t launch_norma(dim3 grid, cudaStream_t s, const double* wcomp, int Kq, const double* q, int O,
+                                int P, const double* normx, double* na, float2* na_hl, int cc) {
+  static std::atomic<unsigned long long> opted{0};  // above 48 KB of dynamic shared memory
+  const cudaError_t e = smem_opt_in(tc_norma_kernel<WM>, (int)norma_smem_bytes<WM>(), opted);
+  if (e != cudaSuccess) return e;
   tc_norma_kernel<WM><<<grid, kNormaThreads, norma_smem_bytes<WM>(), s>>>(wcomp, Kq, q, O, P, normx, na, na_hl, cc);
+  return cudaSuccess;
 }
 
 // ------------------------------------------------------------------ stage 5
@@ -1746,11 +1744,11 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       const int sms = num_sms();
       const int cc = b.score == B200D2_SCORE_CC;
       if (otiles * ((g.P + 63) / 64) >= sms)
-        launch_norma<4>(dim3(otiles, (g.P + 63) / 64), s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc);
+        B200D2_CUDA_TRY(launch_norma<4>(dim3(otiles, (g.P + 63) / 64), s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc));
       else if (otiles * ((g.P + 31) / 32) >= sms)
-        launch_norma<2>(dim3(otiles, (g.P + 31) / 32), s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc);
+        B200D2_CUDA_TRY(launch_norma<2>(dim3(otiles, (g.P + 31) / 32), s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc));
       else
-        launch_norma<1>(dim3(otiles, (g.P + 15) / 16), s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc);
+        B200D2_CUDA_TRY(launch_norma<1>(dim3(otiles, (g.P + 15) / 16), s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc));
       break;
     }
     case 5: {
