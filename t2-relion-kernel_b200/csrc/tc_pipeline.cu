@@ -2051,6 +2051,49 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
       mid[i] = c[d.O / 2];
     }
     std::stable_sort(ord.begin(), ord.end(), [&](int a, int c) { return mid[a] < mid[c]; });
+    // then a nearest-neighbour chain over the particles' sets of 128-column
+    // blocks (Hamming distance, ties by distance in the median order), so that
+    // particles sharing an m-tile need similar column blocks: on C4 (1024
+    // particles) 5427 instead of 6034 CTA-pair tiles.  Quadratic in P, so
+    // larger plans keep the median order.
+    constexpr int kChainMaxParticles = 4096;
+    if (P > 2 && P <= kChainMaxParticles) {
+      const int nb = (O_all + 127) / 128, W = (nb + 63) / 64;
+      std::vector<uint64_t> bits((size_t)P * W, 0ull);
+      for (int i = 0; i < P; ++i) {
+        const b200d2_particle_desc& d = parts[i];
+        for (int k = 0; k < d.O; ++k) {
+          const int blk = pos[d.h_orient ? d.h_orient[k] : k] / 128;
+          bits[(size_t)i * W + blk / 64] |= 1ull << (blk % 64);
+        }
+      }
+      std::vector<int> rank(P);
+      for (int r = 0; r < P; ++r) rank[ord[r]] = r;
+      std::vector<char> used(P, 0);
+      std::vector<int> chain;
+      chain.reserve(P);
+      int cur = ord[0];
+      used[cur] = 1;
+      chain.push_back(cur);
+      for (int step = 1; step < P; ++step) {
+        int best = -1;
+        long long best_key = 0;
+        for (int j = 0; j < P; ++j) {
+          if (used[j]) continue;
+          int dist = 0;
+          for (int w = 0; w < W; ++w) dist += __builtin_popcountll(bits[(size_t)cur * W + w] ^ bits[(size_t)j * W + w]);
+          const long long k = ((long long)dist << 32) + std::abs(rank[j] - rank[cur]);
+          if (best < 0 || k < best_key) {
+            best = j;
+            best_key = k;
+          }
+        }
+        used[best] = 1;
+        chain.push_back(best);
+        cur = best;
+      }
+      ord.swap(chain);
+    }
   }
 
   // distinct translation sets -> phase tables; rows (particle, t, table)
