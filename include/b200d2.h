@@ -279,9 +279,10 @@ enum {
   B200D2_PLAN_AUTOTUNE = 1,   /* time the contraction variants, keep the fastest */
   B200D2_PLAN_GRAPH = 2,      /* capture the whole pipeline in a CUDA graph */
   B200D2_PLAN_ACCUMULATE = 4, /* add onto d_diff2 instead of overwriting */
-  /* order orientations by viewing direction (Morton code of the projection
-   * normal) and particles by where their subsets fall, so that local
-   * orientation subsets touch few output tiles; outputs are unchanged */
+  /* order orientations by viewing direction (Hilbert curve over the
+   * projection normal's z and azimuth) and particles by the column blocks
+   * their subsets touch, so that local orientation subsets touch few output
+   * tiles; outputs are unchanged */
   B200D2_PLAN_REORDER = 8
 };
 
