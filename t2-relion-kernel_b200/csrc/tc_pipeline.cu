@@ -52,6 +52,8 @@
 namespace b200d2 {
 
 // ------------------------------------------------------------------ geometry
+constexpr int kMaxSplit = 8;  // largest k-split of the single-CTA contraction
+
 struct TcGeom {
   int P, O, T, N_img, K_c, Kpad, Mrows, Mpad, Opad, maxR, exw, eyw;
   int elem, BK, terms;
@@ -146,7 +148,7 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, i
     g.split_max = 1;
     const int sms = num_sms();
     if (allow_split && tiles256 < sms)
-      while (g.split_max * 2 <= 8 && (long long)tiles256 * g.split_max * 2 <= 2LL * sms && kb / (g.split_max * 2) >= 2)
+      while (g.split_max * 2 <= kMaxSplit && (long long)tiles256 * g.split_max * 2 <= 2LL * sms && kb / (g.split_max * 2) >= 2)
         g.split_max *= 2;
     g.off_part = take(g.split_max > 1 ? (size_t)g.split_max * tiles256 * 256 * 128 * sizeof(float) : 0);
     g.n_cnt = 8 * mt * (g.Opad / 128);  // per (tile, column half, lane quadrant) of 128-wide tiles
@@ -870,20 +872,48 @@ struct EpiRow {
 // bits (FP64 norms); the default double-float form rounds nA_hi - 2c once
 // (FMA) and adds nA_lo, within 2 ulp of the FP64 combine rounded to FP32, at
 // about a tenth of its cost on this GPU.
+//
+// EpiCol: the per-column operands of the combine, loaded ahead of it: the
+// local column (-1: not stored), nA in FP64 or as a double-float, and the
+// FP16 orientation scale.
+struct EpiCol {
+  int lo;
+  double na;
+  float2 nh;
+  float isb;
+};
+
 template <bool SCALED>
-__device__ __forceinline__ void epi_combine(const GemmArgs& g, const EpiRow& x, int o, float c, float& best,
-                                            int& best_lo) {
-  const int lo = (o < g.O) ? (x.inv ? x.inv[o] : o) : -1;
+__device__ __forceinline__ EpiCol epi_col(const GemmArgs& g, const EpiRow& x, int o) {
+  EpiCol k;
+  k.lo = (o < g.O) ? (x.inv ? x.inv[o] : o) : -1;
+  k.na = 0.0;
+  k.nh = make_float2(0.f, 0.f);
+  k.isb = 1.f;
+  if (k.lo >= 0) {
+    if (g.combine64)
+      k.na = x.na_row[o];
+    else
+      k.nh = x.nh_row[o];
+    if (SCALED) k.isb = g.inv_sb[o];
+  }
+  return k;
+}
+
+template <bool SCALED>
+__device__ __forceinline__ void epi_combine_col(const GemmArgs& g, const EpiRow& x, const EpiCol& k, float c,
+                                                float& best, int& best_lo) {
+  const int lo = k.lo;
   if (lo < 0) return;
   float f;
   if (g.combine64) {
     double cr = (double)c;
-    if (SCALED) cr *= (double)g.inv_sb[o];
+    if (SCALED) cr *= (double)k.isb;
     // CC: k * c with the scales undone (-m2s/2 is the particle's, exact)
-    f = g.cc ? (float)(x.na_row[o] * (cr * (-0.5 * x.m2s))) : (float)fma(x.m2s, cr, x.na_row[o]);
+    f = g.cc ? (float)(k.na * (cr * (-0.5 * x.m2s))) : (float)fma(x.m2s, cr, k.na);
   } else {
-    const float2 nh = x.nh_row[o];
-    const float sc = SCALED ? x.m2f * g.inv_sb[o] : x.m2f;  // product of powers of two: exact
+    const float2 nh = k.nh;
+    const float sc = SCALED ? x.m2f * k.isb : x.m2f;  // product of powers of two: exact
     f = g.cc ? __fmul_rn(nh.x, c * (-0.5f * sc)) : __fadd_rn(__fmaf_rn(sc, c, nh.x), nh.y);
   }
   float* dst = x.out_row + (size_t)lo * x.Tp;
@@ -893,6 +923,12 @@ __device__ __forceinline__ void epi_combine(const GemmArgs& g, const EpiRow& x, 
     best = f;
     best_lo = lo;
   }
+}
+
+template <bool SCALED>
+__device__ __forceinline__ void epi_combine(const GemmArgs& g, const EpiRow& x, int o, float c, float& best,
+                                            int& best_lo) {
+  epi_combine_col<SCALED>(g, x, epi_col<SCALED>(g, x, o), c, best, best_lo);
 }
 
 // Drain NCH 32-column chunks of one TMEM lane quadrant starting at `taddr`
@@ -1167,11 +1203,29 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const __grid_c
           __threadfence();
           const float* base = g.part + (size_t)tile * g.split * C::kBN * 128 + row;
           if (vrow) {
+            // the partials of kSumCols columns are loaded together (their
+            // loads overlap), then added in split order in FP64
+            constexpr int kSumCols = 4;
+            static_assert(kCols % kSumCols == 0, "column chunks");
 #pragma unroll 1
-            for (int col = half * kCols; col < (half + 1) * kCols; ++col) {
-              double acc = 0.0;
-              for (int s2 = 0; s2 < g.split; ++s2) acc += (double)__ldcg(base + ((size_t)s2 * C::kBN + col) * 128);
-              epi_combine<C::kScaled>(g, x, n0 + col, (float)acc, best, best_lo);
+            for (int col0 = half * kCols; col0 < (half + 1) * kCols; col0 += kSumCols) {
+              float v[kSumCols][kMaxSplit];
+              EpiCol kc[kSumCols];
+#pragma unroll
+              for (int c = 0; c < kSumCols; ++c) {
+                kc[c] = epi_col<C::kScaled>(g, x, n0 + col0 + c);
+#pragma unroll
+                for (int s2 = 0; s2 < kMaxSplit; ++s2)
+                  v[c][s2] = s2 < g.split ? __ldcg(base + ((size_t)s2 * C::kBN + col0 + c) * 128) : 0.f;
+              }
+#pragma unroll
+              for (int c = 0; c < kSumCols; ++c) {
+                double acc = 0.0;
+#pragma unroll
+                for (int s2 = 0; s2 < kMaxSplit; ++s2)
+                  if (s2 < g.split) acc += (double)v[c][s2];
+                epi_combine_col<C::kScaled>(g, x, kc[c], (float)acc, best, best_lo);
+              }
             }
           }
           __syncwarp();
@@ -1571,7 +1625,7 @@ static int launch_gemm_v(const b200d2_batch& b, const TcGeom& g, void* ws, cudaS
   const int tiles = U ? U->ntiles[wl] : a.Mtiles * a.Ntiles;
   if (tiles == 0) return B200D2_OK;
   a.split = split > 0 ? std::min(split, g.split_max) : auto_split(tiles, a.KB, g.split_max);
-  a.split = std::max(1, std::min(a.split, a.KB));
+  a.split = std::max(1, std::min(std::min(a.split, a.KB), kMaxSplit));  // the epilogue sums at most kMaxSplit
   a.out = b.d_diff2;
   a.na = ws_at<double>(ws, g.off_na);
   a.na_hl = ws_at<float2>(ws, g.off_nahl);
