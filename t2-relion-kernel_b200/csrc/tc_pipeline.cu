@@ -1580,11 +1580,16 @@ static std::atomic<int> g_combine64{0};  // b200d2_set_combine
 // k-splits for `tiles` tiles of KB k-blocks: 1 when the tiles fill the GPU,
 // else the largest power of two (<= cap) keeping two work items per SM at
 // most and at least two k-blocks per split.
+// A k-split stores every split's partial tile and has the last split add
+// them (about 30 us at C1), so it pays only for long k-loops: each split
+// keeps at least kSplitMinKB k-blocks (at C1, 28 k-blocks, splitting 4 ways
+// took the contraction from 41 to 70 us).
+constexpr int kSplitMinKB = 64;
 static int auto_split(int tiles, int KB, int cap) {
   const int sms = num_sms();
   int sp = 1;
   if (tiles >= sms) return 1;
-  while (sp * 2 <= cap && (long long)tiles * sp * 2 <= 2LL * sms && KB / (sp * 2) >= 2) sp *= 2;
+  while (sp * 2 <= cap && (long long)tiles * sp * 2 <= 2LL * sms && KB / (sp * 2) >= kSplitMinKB) sp *= 2;
   return sp;
 }
 
@@ -1729,6 +1734,9 @@ static int launch_gemm(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStr
     return prb == 128 ? launch_gemm_pair<PREC, 128>(b, g, ws, s, U) : launch_gemm_pair<PREC, 64>(b, g, ws, s, U);
   }
   const int rb = var.row_bytes > 0 ? var.row_bytes : gemm_row_bytes();
+  // uniform batches too small for CTA pairs: 128-wide tiles while they still
+  // fit in one wave (twice the CTAs; at C1 31 instead of 41 us)
+  if (var.bn <= 0 && !U && (long long)(g.Mpad / 128) * ((g.Opad + 127) / 128) <= num_sms()) var.bn = 128;
   if (var.bn == 128)
     return rb == 128 ? launch_gemm_v<PREC, 128, 128>(b, g, ws, s, U, var.split)
                      : launch_gemm_v<PREC, 64, 128>(b, g, ws, s, U, var.split);

@@ -183,11 +183,13 @@ def test_tc_pair_tiles_c2_subset(pkg, synth, oracle, cuda, name):
     proj.close()
 
 
-@pytest.mark.parametrize("case,variant", [("c1", (0, 0, 0, 0)), ("c1", (64, 256, 1, 2)), ("c2", (0, 0, 1, 1))])
+@pytest.mark.parametrize("case,variant", [("c1", (0, 0, 0, 0)), ("c1", (64, 256, 4, 2)), ("c1", (64, 256, 1, 2)),
+                                          ("c2", (0, 0, 1, 1))])
 def test_combine_df32_matches_fp64_combine(pkg, synth, oracle, cuda, case, variant):
     """The double-float combine (nA as hi + lo floats, one FMA and one add)
-    stays within 2 ulp of the FP64 combine rounded to FP32, on the split-K,
-    single-CTA and CTA-pair contractions."""
+    stays within 2 ulp of the FP64 combine rounded to FP32, on the default
+    small-batch choice (128-wide tiles), a 4-way k-split, single-CTA
+    256-wide and CTA-pair contractions."""
     pr = synth.make_problem(case, P=5 if case == "c2" else None, orient_limit=700 if case == "c2" else None)
     proj = pkg.Projector(pr.projector, use_texture=1)
     view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
