@@ -547,20 +547,21 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
       : "d"(a), "d"(b));
 }
 
-// CTA tile: (2*8*WM) particles x 64 orientations, 4 warps in a 2 x 2 grid,
-// each warp WM x 4 DMMA tiles of 8 x 8; 32-pixel slabs in a three-stage
+// CTA tile: (2*8*WM) particles x (2*8*WN) orientations, 4 warps in a 2 x 2
+// grid, each warp WM x WN DMMA tiles of 8 x 8 (WN = 4 unless the batch is too
+// small to give every SM a CTA); 32-pixel slabs in a three-stage
 // cp.async ring (one barrier per slab, two slabs in flight).  (Splitting each
 // slab's pixels over two groups of 4 warps, with the two sums added at the
 // end, measured slower: 94.9 against 86.3 us at 128 particles.)
 // cc: store k = -sqrt(2 / sum w|B|^2) (the CC score's factor) instead of nA.
-constexpr int kNormaKC = 32, kNormaLD = kNormaKC + 4, kNormaStages = 3, kNormaCO = 64;
-template <int WM>
+constexpr int kNormaKC = 32, kNormaLD = kNormaKC + 4, kNormaStages = 3;
+template <int WM, int WN>
 constexpr size_t norma_smem_bytes() {
-  return sizeof(double) * kNormaStages * (16 * WM + kNormaCO) * kNormaLD;
+  return sizeof(double) * kNormaStages * (16 * WM + 16 * WN) * kNormaLD;
 }
 
 constexpr int kNormaThreads = 128;
-template <int WM>
+template <int WM, int WN>
 __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* __restrict__ wcomp, int Kq,
                                                        const double* __restrict__ q, int O, int P,
                                                        const double* __restrict__ normx, double* na,
@@ -569,20 +570,20 @@ __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* _
   // slab is zero-filled past Kq.  Shared rows padded to 36 doubles (288 B,
   // 16-byte aligned): the fragment loads of a half-warp (rows g, columns t,
   // g, t < 4) fall on distinct bank pairs 4g + t (mod 16).
-  constexpr int KC = kNormaKC, LD = kNormaLD, NST = kNormaStages, CP = 16 * WM, CO = kNormaCO;
+  constexpr int KC = kNormaKC, LD = kNormaLD, NST = kNormaStages, CP = 16 * WM, CO = 16 * WN;
   extern __shared__ __align__(16) double norma_smem[];
   double* sw = norma_smem;                   // [NST][CP][LD]
   double* sq = norma_smem + NST * CP * LD;   // [NST][CO][LD]
   constexpr int NT = kNormaThreads;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gid = lane >> 2, tig = lane & 3;
-  const int wp0 = (warp >> 1) * 8 * WM, wo0 = (warp & 1) * 32;
+  const int wp0 = (warp >> 1) * 8 * WM, wo0 = (warp & 1) * 8 * WN;
   const int p0 = blockIdx.y * CP, o0 = blockIdx.x * CO;
-  double acc[WM][4][2];
+  double acc[WM][WN][2];
 #pragma unroll
   for (int i = 0; i < WM; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int j = 0; j < WN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   auto stage = [&](int buf, int k0) {
     // 16-byte pieces (two doubles); rows past P or O and columns past Kq are zero-filled
     double* dw = sw + buf * CP * LD;
@@ -615,15 +616,15 @@ __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* _
     const double* cq = sq + (sl % NST) * CO * LD;
 #pragma unroll
     for (int k4 = 0; k4 < KC; k4 += 4) {
-      double a[WM], bq[4];
+      double a[WM], bq[WN];
 #pragma unroll
       for (int i = 0; i < WM; ++i) a[i] = cw[(wp0 + 8 * i + gid) * LD + k4 + tig];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bq[j] = cq[(wo0 + 8 * j + gid) * LD + k4 + tig];
+      for (int j = 0; j < WN; ++j) bq[j] = cq[(wo0 + 8 * j + gid) * LD + k4 + tig];
 #pragma unroll
       for (int i = 0; i < WM; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j], a[i], bq[j]);
+        for (int j = 0; j < WN; ++j) dmma_8x8x4(acc[i][j], a[i], bq[j]);
     }
   }
   cp_async_wait<0>();
@@ -632,7 +633,7 @@ __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* _
     const int p = p0 + wp0 + 8 * i + gid;
     if (p >= P) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < WN; ++j)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int o = o0 + wo0 + 8 * j + 2 * tig + h;
@@ -652,13 +653,15 @@ __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* _
   }
 }
 
-template <int WM>
-static cudaError_t launch_norma(dim3 grid, cudaStream_t s, const double* wcomp, int Kq, const double* q, int O,
-                                int P, const double* normx, double* na, float2* na_hl, int cc) {
+template <int WM, int WN>
+static cudaError_t launch_norma(cudaStream_t s, const double* wcomp, int Kq, const double* q, int O, int P,
+                                const double* normx, double* na, float2* na_hl, int cc) {
   static std::atomic<unsigned long long> opted{0};  // above 48 KB of dynamic shared memory
-  const cudaError_t e = smem_opt_in(tc_norma_kernel<WM>, (int)norma_smem_bytes<WM>(), opted);
+  const cudaError_t e = smem_opt_in(tc_norma_kernel<WM, WN>, (int)norma_smem_bytes<WM, WN>(), opted);
   if (e != cudaSuccess) return e;
-  tc_norma_kernel<WM><<<grid, kNormaThreads, norma_smem_bytes<WM>(), s>>>(wcomp, Kq, q, O, P, normx, na, na_hl, cc);
+  const dim3 grid((O + 16 * WN - 1) / (16 * WN), (P + 16 * WM - 1) / (16 * WM));
+  tc_norma_kernel<WM, WN><<<grid, kNormaThreads, norma_smem_bytes<WM, WN>(), s>>>(wcomp, Kq, q, O, P, normx, na,
+                                                                                 na_hl, cc);
   return cudaSuccess;
 }
 
@@ -1801,16 +1804,21 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
                                           idx, g.K_c, g.Kq, wcomp);
       break;
     case 4: {
-      // the largest particle tile (64, 32, 16) that still gives every SM a CTA
-      const long long otiles = (g.O + 63) / 64;
+      // the largest tile (particles x orientations: 64 x 64, 32 x 64, 16 x 64,
+      // 16 x 32, 16 x 16) that still gives every SM a CTA
       const int sms = num_sms();
       const int cc = b.score == B200D2_SCORE_CC;
-      if (otiles * ((g.P + 63) / 64) >= sms)
-        B200D2_CUDA_TRY(launch_norma<4>(dim3(otiles, (g.P + 63) / 64), s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc));
-      else if (otiles * ((g.P + 31) / 32) >= sms)
-        B200D2_CUDA_TRY(launch_norma<2>(dim3(otiles, (g.P + 31) / 32), s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc));
+      auto ctas = [&](int cp, int co) { return (long long)((g.O + co - 1) / co) * ((g.P + cp - 1) / cp); };
+      if (ctas(64, 64) >= sms)
+        B200D2_CUDA_TRY((launch_norma<4, 4>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc)));
+      else if (ctas(32, 64) >= sms)
+        B200D2_CUDA_TRY((launch_norma<2, 4>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc)));
+      else if (ctas(16, 64) >= sms)
+        B200D2_CUDA_TRY((launch_norma<1, 4>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc)));
+      else if (ctas(16, 32) >= sms)
+        B200D2_CUDA_TRY((launch_norma<1, 2>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc)));
       else
-        B200D2_CUDA_TRY(launch_norma<1>(dim3(otiles, (g.P + 15) / 16), s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc));
+        B200D2_CUDA_TRY((launch_norma<1, 1>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc)));
       break;
     }
     case 5: {
