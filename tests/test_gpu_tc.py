@@ -96,6 +96,27 @@ def test_tc_c1(pkg, oracle, cuda, c1, name):
     _check(pkg, oracle, cuda, c1, name)
 
 
+@pytest.mark.parametrize("P", [32, 40, 128])
+def test_tc_norm_tile_shapes(pkg, synth, oracle, cuda, P):
+    """The FP64 norm kernel picks its particle x orientation tile by batch
+    size: with 4608 orientations, 32 particles take 16 x 32 tiles, 40 take
+    16 x 64 and 128 take 32 x 64 (C2's 256 take 64 x 64, C1 16 x 16).  Every
+    shape gives the same diff2, min and argmin as the FP64 kernel within the
+    BF16x3 tolerance.  Five of the 113 translations keep the FP64 reference
+    short; the tile choice depends only on particles and orientations."""
+    import dataclasses
+    pr = synth.make_problem("c2", P=P)
+    pr = dataclasses.replace(pr, trans_x=pr.trans_x[:5].copy(), trans_y=pr.trans_y[:5].copy(),
+                             shifts=pr.shifts[:5].copy())
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dp = DeviceProblem(cuda, pr)
+    try:
+        _check(pkg, oracle, cuda, (pr, view, dp, fp64_all(pkg, view, dp)), "bf16x3")
+    finally:
+        proj.close()
+
+
 def test_tc_c2_subset(pkg, synth, oracle, cuda):
     pr = synth.make_problem("c2", P=6)
     proj = pkg.Projector(pr.projector, use_texture=1)
