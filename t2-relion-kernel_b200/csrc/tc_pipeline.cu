@@ -370,29 +370,36 @@ __device__ __forceinline__ void store_split4(void* hi, void* lo, size_t at, cons
 }
 
 // ------------------------------------------------------------------ stage 2
+// A CTA takes kProjOrients consecutive orientations of one block of pixels,
+// one orientation after the other: consecutive orientations are usually
+// in-plane rotations of one viewing direction, which sample the same slice of
+// the volume, so the block's texels are reused from L1.
+constexpr int kProjOrients = 8;  // divides Opad (a multiple of 256)
 template <int PREC>
 __global__ void __launch_bounds__(128) tc_project_kernel(b200d2_view v, const float* __restrict__ eulers,
                                                          int O, const int2* __restrict__ xy, int K_c,
                                                          int Kpad, void* bhi, void* blo, double* q) {
   const int kp = blockIdx.x * blockDim.x + threadIdx.x;  // complex pixel slot
-  const int o = blockIdx.y;
   if (kp >= Kpad / 2) return;
-  float2 b = make_float2(0.f, 0.f);
-  if (o < O && kp >= K_c) q[(size_t)o * (Kpad / 2) + kp] = 0.0;  // zero padding of the |B|^2 row
-  if (o < O && kp < K_c) {
-    float e[6];
-    const float* eo = eulers + (size_t)o * 9;
-    e[0] = eo[0];
-    e[1] = eo[1];
-    e[2] = eo[3];
-    e[3] = eo[4];
-    e[4] = eo[6];
-    e[5] = eo[7];
-    const int2 c = xy[kp];
-    b = project_pixel(v, (float)c.x, (float)c.y, e);
-    q[(size_t)o * (Kpad / 2) + kp] = (double)b.x * (double)b.x + (double)b.y * (double)b.y;
+  const int2 c = kp < K_c ? xy[kp] : make_int2(0, 0);
+  for (int j = 0; j < kProjOrients; ++j) {
+    const int o = blockIdx.y * kProjOrients + j;
+    float2 b = make_float2(0.f, 0.f);
+    if (o < O && kp >= K_c) q[(size_t)o * (Kpad / 2) + kp] = 0.0;  // zero padding of the |B|^2 row
+    if (o < O && kp < K_c) {
+      float e[6];
+      const float* eo = eulers + (size_t)o * 9;
+      e[0] = eo[0];
+      e[1] = eo[1];
+      e[2] = eo[3];
+      e[3] = eo[4];
+      e[4] = eo[6];
+      e[5] = eo[7];
+      b = project_pixel(v, (float)c.x, (float)c.y, e);
+      q[(size_t)o * (Kpad / 2) + kp] = (double)b.x * (double)b.x + (double)b.y * (double)b.y;
+    }
+    store_split<PREC>(bhi, blo, (size_t)o * (Kpad / 2) + kp, b.x, b.y);
   }
-  store_split<PREC>(bhi, blo, (size_t)o * (Kpad / 2) + kp, b.x, b.y);
 }
 
 // ------------------------------------------------------------------ FP16 scales
@@ -1794,7 +1801,8 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
         tc_project_scaled_kernel<PREC><<<g.Opad, 256, 0, s>>>(v, b.d_eulers, g.O, xy, g.K_c, g.Kpad, bhi, blo, q,
                                                               inv_sb);
       } else {
-        dim3 grid((g.Kpad / 2 + 127) / 128, g.Opad);
+        static_assert(256 % kProjOrients == 0, "orientation groups divide Opad");
+        dim3 grid((g.Kpad / 2 + 127) / 128, g.Opad / kProjOrients);
         tc_project_kernel<PREC><<<grid, 128, 0, s>>>(v, b.d_eulers, g.O, xy, g.K_c, g.Kpad, bhi, blo, q);
       }
       break;
