@@ -487,15 +487,36 @@ def ours_arm(args):
             h_am.copy_(am, non_blocking=True)
         e1.record(stream)
     else:
+        # the same double buffering for the uneven batch: a second plan over a
+        # second set of input buffers (the autotuner's choice is cached)
+        plan2, bufs2, _ = build_plan_case(pkg, pr, dev, prec,
+                                          pkg.PLAN_AUTOTUNE | pkg.PLAN_GRAPH | pkg.PLAN_REORDER)
+        sets = [(re, im, corr, mn, am, plan), (bufs2[1], bufs2[2], bufs2[3], bufs2[5], bufs2[6], plan2)]
+        plan2.run(stream)  # warm-up of the second plan's graph, outside the timed region
+        torch.cuda.synchronize()
+        copy_stream = torch.cuda.Stream(device=dev)
+        ready = [torch.cuda.Event() for _ in range(2)]
+        free = [torch.cuda.Event() for _ in range(2)]
         e0.record(stream)
-        for _ in range(e2e_steps):
-            re.copy_(h_re, non_blocking=True)
-            im.copy_(h_im, non_blocking=True)
-            corr.copy_(h_corr, non_blocking=True)
-            step()
-            h_mn.copy_(mn, non_blocking=True)
-            h_am.copy_(am, non_blocking=True)
+        copy_stream.wait_event(e0)
+        for k in range(e2e_steps):
+            d_re, d_im, d_corr, mk, ak, pk = sets[k % 2]
+            with torch.cuda.stream(copy_stream):
+                if k >= 2:
+                    copy_stream.wait_event(free[k % 2])
+                d_re.copy_(h_re, non_blocking=True)
+                d_im.copy_(h_im, non_blocking=True)
+                d_corr.copy_(h_corr, non_blocking=True)
+                ready[k % 2].record(copy_stream)
+            stream.wait_event(ready[k % 2])
+            pk.run(stream)
+            free[k % 2].record(stream)
+            h_mn.copy_(mk, non_blocking=True)
+            h_am.copy_(ak, non_blocking=True)
         e1.record(stream)
+        torch.cuda.synchronize()
+        plan2.close()
+        del bufs2
     torch.cuda.synchronize()
     e2e_clk = e2e_clocks.stop()
     e2e_val = replicas.job_rate(evals_step * e2e_steps, e0.elapsed_time(e1), dist, dev)
@@ -556,7 +577,8 @@ def ours_arm(args):
                 "e2e": {"value": e2e_val, "unit": "diff2 evals/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "clocks": e2e_clk,
                         "note": ("H2D of images+corr from pinned memory, batch call, D2H of per-particle min/argmin, every "
-                          "step; uniform batches double-buffer the images so that step k+1's copy overlaps step k")},
+                          "step; the images are double-buffered (uneven batches: two plans) so that step k+1's "
+                          "copy overlaps step k")},
                 "clocks": clk, "gpu_launches": int(l1 - l0), "kernels": kern.get("per_kernel_ms")}
         print(json.dumps(line), flush=True)
     proj.close()
