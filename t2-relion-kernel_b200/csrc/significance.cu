@@ -290,7 +290,10 @@ __global__ void __launch_bounds__(kSThreads) sig_scan_kernel(const u64* __restri
   const long long lo = (long long)blockIdx.x * kScanChunk, hi = min(n, lo + kScanChunk);
   const u64* row = keys + (long long)p * n;
   double tsum = 0.0;
-  u64 maxnot = 0ull, amaxnot = 0ull;
+  u64 maxnot = 0ull;
+  // above the window only the exponent of the smallest key is used later, so
+  // the minimum of the keys' high words is kept (32-bit)
+  unsigned amin_hi = 0xFFFFFFFFu;
   unsigned tcnt = 0u, acnt = 0u;
   for (long long i0 = lo; i0 < hi; i0 += kPerThread * kSThreads) {
     u64 kv[kPerThread];
@@ -311,7 +314,7 @@ __global__ void __launch_bounds__(kSThreads) sig_scan_kernel(const u64* __restri
       }
       if (pf && !tail && !win) {
         ++acnt;
-        amaxnot = max(amaxnot, ~key);
+        amin_hi = min(amin_hi, khw);
       }
       if (win) {
         if (run_n && b == run_b) {
@@ -331,7 +334,7 @@ __global__ void __launch_bounds__(kSThreads) sig_scan_kernel(const u64* __restri
     tcnt += __shfl_xor_sync(0xffffffffu, tcnt, o);
     acnt += __shfl_xor_sync(0xffffffffu, acnt, o);
     maxnot = max(maxnot, __shfl_xor_sync(0xffffffffu, maxnot, o));
-    amaxnot = max(amaxnot, __shfl_xor_sync(0xffffffffu, amaxnot, o));
+    amin_hi = min(amin_hi, __shfl_xor_sync(0xffffffffu, amin_hi, o));
   }
   if (lane == 0) {
     if (tcnt) {
@@ -342,7 +345,7 @@ __global__ void __launch_bounds__(kSThreads) sig_scan_kernel(const u64* __restri
     }
     if (acnt) {
       atomicAdd(&S.above_cnt, (u64)acnt);
-      atomicMax(&S.above_maxnot, amaxnot);
+      atomicMax(&S.above_maxnot, ~((u64)amin_hi << 32));  // (~above_maxnot) >> 52: that key's exponent
     }
     if (maxnot) atomicMax(&S.maxnot, maxnot);
   }
