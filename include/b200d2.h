@@ -229,7 +229,11 @@ typedef struct b200d2_batch {
    * NULL the first n_listed image entries are the pixels at integer-valued
    * coordinates (d_coor_xy[2i], d_coor_xy[2i+1]), |x|,|y| <= 512, shared by
    * all particles, and entries n_listed .. N_img-1 lie outside the projector
-   * radius (they add only corr/2 |X|^2).  Tensor-core precisions only. */
+   * radius (they add only corr/2 |X|^2).  Tensor-core precisions only.  The
+   * coordinates are device data, checked on the device: x outside [0, 512],
+   * y outside [-512, 512] or a value that is not an integer sets the
+   * workspace status word to B200D2_ERR_INVALID (b200d2_workspace_status),
+   * and the scores of that call are not to be used. */
   const float* d_coor_xy;
   int n_listed;
   /* B200D2_SCORE_DIFF2 (0): diff2 as above.  B200D2_SCORE_CC (1): the
@@ -383,13 +387,16 @@ int b200d2_server_destroy(b200d2_server* s);
  * buffers.  Same semantics and outputs as b200d2_diff2_coarse_batch with a
  * tensor-core precision, but the workspace is a fixed scratch area of
  * B200D2_STATIC_SCRATCH_BYTES inside the library's device image, held by
- * every GPU that loads the library until the process exits.  A batch whose
- * b200d2_diff2_coarse_batch_workspace exceeds that size is rejected with
- * B200D2_ERR_TOO_LARGE before anything runs (64 MiB holds, for example, 8
- * particles x 576 orientations x 21 translations at image 32, or 16
- * particles x 1024 orientations x 113 translations at image 64).  The
- * scratch address is looked up on the first call on each device: make that
- * call before any stream capture.  Calls share the scratch, so calls that
+ * every GPU that loads the library until the process exits.  This entry
+ * point never splits the contraction over k, so it needs the batch's
+ * workspace without the split-K partial-sum buffer, which can be less than
+ * b200d2_diff2_coarse_batch_workspace reports; a batch whose need exceeds
+ * the scratch is rejected with B200D2_ERR_TOO_LARGE before anything runs
+ * (64 MiB holds, for example, 8 particles x 576 orientations x 21
+ * translations at image 32, or 16 particles x 1024 orientations x 113
+ * translations at image 64).  The scratch address is looked up on the first
+ * call on each device, and again after the device's context is recreated
+ * (cudaDeviceReset): make those calls before any stream capture.  Calls share the scratch, so calls that
  * overlap on the GPU race; serialise them.  Runs all stages on `stream`. */
 #define B200D2_STATIC_SCRATCH_BYTES (64ull << 20)
 int b200d2_diff2_coarse_batch_static(const b200d2_view* view,
@@ -508,11 +515,26 @@ int b200d2_diff2_coarse_batch_stage(const b200d2_view* view,
                                     size_t workspace_bytes, void* stream);
 const char* b200d2_stage_name(int precision, int stage);
 
-/* Status word of the last tensor-core batch run in this workspace: 0, or
- * B200D2_ERR_TIMEOUT when a bounded device-side wait gave up (the outputs of
- * that run are then incomplete).  Synchronises `stream`. */
+/* Status word of the last tensor-core batch run in this workspace: 0,
+ * B200D2_ERR_INVALID when caller-listed pixel coordinates were out of range
+ * or not integers, or B200D2_ERR_TIMEOUT when a bounded device-side wait gave
+ * up (the outputs of that run are then incomplete).  Synchronises `stream`. */
 int b200d2_workspace_status(const void* d_workspace, void* stream,
                             int* status);
+
+/* Test hook for the give-up path of the bounded device-side waits (no
+ * counterpart in the reference, whose waits cannot hang: it recomputes instead
+ * of spinning, src/translation_matrix_handler.cuh:145-206).  Sets, process
+ * wide, the limit in nanoseconds of the single-CTA contraction's pipeline
+ * waits (its shared-memory stage ring and accumulator hand-over); 0 restores
+ * the default of 4 s.  When a wait runs out the kernel raises an abort flag
+ * that its other roles see, lets its copies and MMAs in flight finish (those
+ * drain waits keep the 4 s limit), frees its tensor memory and returns, and
+ * b200d2_workspace_status reports B200D2_ERR_TIMEOUT.  The CTA-pair
+ * contraction keeps the default limit.  Read when a contraction is launched
+ * (plans capture it in their graph).  For tests only: a short limit makes
+ * correct runs fail. */
+int b200d2_set_wait_limit_ns(unsigned long long ns);
 
 /* Number of kernels this library has launched in the process so far (all
  * entry points, all devices).  Lets a caller count launches in a region. */

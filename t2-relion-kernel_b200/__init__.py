@@ -163,6 +163,7 @@ def _declare(L):
         "b200d2_significance": [P, I, C.c_longlong, P, C.c_double, C.c_longlong, P, P, P, P, Z, P],
         "b200d2_set_gemm_variant": [I, I, I, I],
         "b200d2_set_combine": [I],
+        "b200d2_set_wait_limit_ns": [C.c_ulonglong],
         "b200d2_diff2_fine": [C.POINTER(View), P, P, P, P, P, P, P, Z, F, Z, P, P, P, P, P],
         "b200d2_diff2_fine_cc": [C.POINTER(View), P, P, P, P, P, P, P, Z, Z, P, P, P, P, P],
         "b200d2_ctf_fold": [P, P, C.c_longlong, I, I, I, I, I, I, F, P, P, C.c_longlong, P, P, P, P],
@@ -472,9 +473,12 @@ class Server:
 def diff2_coarse_batch_static(view: View, batch: Batch, precision: int = PREC_BF16X3, stream=None):
     """The tensor-core batch on the library's fixed scratch (no device allocation).
 
-    For callers that cannot allocate device memory; rejects batches whose
-    workspace exceeds STATIC_SCRATCH_BYTES (B200D2Error code 7).  Calls share
-    the scratch, so they must not overlap on the GPU."""
+    For callers that cannot allocate device memory.  This path never splits
+    the contraction over k, so it needs the batch's workspace without the
+    split-K partial-sum buffer, which can be less than
+    batch_workspace_bytes() reports; a batch whose need exceeds
+    STATIC_SCRATCH_BYTES is rejected (B200D2Error code 7).  Calls share the
+    scratch, so they must not overlap on the GPU."""
     _check(lib().b200d2_diff2_coarse_batch_static(C.byref(view), C.byref(batch), precision, _stream(stream)),
            "diff2_coarse_batch_static")
 
@@ -588,6 +592,13 @@ def set_combine(mode: int) -> None:
     """Final combination of the tensor-core forms: COMBINE_DF32 (default,
     double-float) or COMBINE_FP64."""
     _check(lib().b200d2_set_combine(mode), "set_combine")
+
+
+def set_wait_limit_ns(ns: int) -> None:
+    """Test hook: limit (ns) of the single-CTA contraction's pipeline waits;
+    0 restores the default (4 s).  A short limit makes correct runs give up
+    with B200D2_ERR_TIMEOUT in the workspace status word."""
+    _check(lib().b200d2_set_wait_limit_ns(int(ns)), "set_wait_limit_ns")
 
 
 def set_gemm_variant(row_bytes: int = 0, tile_n: int = 0, split: int = 0, pair: int = 0) -> None:

@@ -208,16 +208,22 @@ __global__ void __launch_bounds__(1024) tc_pixel_list_kernel(b200d2_view v, int 
   }
   for (int p = tid; p < P; p += blockDim.x) keys[p] = ~0ull;
   for (int i = tid; i < n_cnt; i += blockDim.x) cnt[i] = 0u;  // split-K arrival counters
+  __syncthreads();  // the status reset above precedes any report below
   if (coor_xy) {  // caller-listed pixels, in the caller's order
+    bool bad = false;
     for (int k = tid; k < n_listed; k += blockDim.x) {
-      const int x = clampi(__float2int_rn(coor_xy[2 * k]), 0, ext);
-      const int y = clampi(__float2int_rn(coor_xy[2 * k + 1]), -ext, ext);
+      const float fx = coor_xy[2 * k], fy = coor_xy[2 * k + 1];
+      const int x = clampi(__float2int_rn(fx), 0, ext);
+      const int y = clampi(__float2int_rn(fy), -ext, ext);
+      // outside the documented range, or not integer-valued: report it (the
+      // scores of this call are then not those of the listed pixels)
+      bad |= (float)x != fx || (float)y != fy;
       xy[k] = make_int2(x, y);
       idx[k] = k;
     }
+    if (__syncthreads_or(bad) && tid == 0) atomicCAS(status, 0u, (uint32_t)B200D2_ERR_INVALID);
     return;
   }
-  __syncthreads();
   for (int base = 0; base < N_img; base += 1024) {
     const int i = base + tid;
     int x = 0, y = 0;
@@ -820,6 +826,9 @@ struct GemmArgs {
   float* part;          // split > 1: [tiles * split][BN][128] FP32 partial sums
   unsigned* cnt;        // split > 1: [tiles][8] arrivals per (tile, column half, TMEM lane quadrant)
   Layout L;  // uneven batch tables (all null for a uniform batch)
+  // limit (ns) of the single-CTA kernel's pipeline waits (stage ring and
+  // accumulator hand-over); its drain waits keep kWaitLimitNs
+  unsigned long long wait_ns;
 };
 
 // (m0, n0) of the tile-th tile: the work list of an uneven batch, or the
@@ -859,6 +868,10 @@ __device__ __forceinline__ float from_ordered(uint32_t k) {
 }
 
 constexpr uint64_t kWaitLimitNs = 4000000000ull;  // 4 s
+
+// Pipeline-wait limit of the single-CTA contraction, set by
+// b200d2_set_wait_limit_ns for tests of the give-up path (0: kWaitLimitNs).
+static std::atomic<unsigned long long> g_wait_ns{0};
 
 // Epilogue warps of the contraction kernels: two per TMEM lane quadrant, each
 // draining half of the accumulator's columns.
@@ -1057,7 +1070,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const __grid_c
         for (int kb = kb0; kb < kb1; ++kb, ++gk) {
           const int s = gk % C::kStages;
           const uint32_t u = gk / C::kStages;
-          if (u > 0 && !sm100::mbar_wait_bounded(&empty[s], (u - 1) & 1, s_abort, kWaitLimitNs)) {
+          if (u > 0 && !sm100::mbar_wait_bounded(&empty[s], (u - 1) & 1, s_abort, g.wait_ns)) {
             raise_abort();
             ok = false;
             break;
@@ -1086,7 +1099,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const __grid_c
       for (int item = blockIdx.x; item < num_items && ok; item += gridDim.x, ++i) {
         const int b = i & 1;
         const uint32_t v = (uint32_t)(i >> 1);
-        if (v > 0 && !sm100::mbar_wait_bounded(&acce[b], (v - 1) & 1, s_abort, kWaitLimitNs)) {
+        if (v > 0 && !sm100::mbar_wait_bounded(&acce[b], (v - 1) & 1, s_abort, g.wait_ns)) {
           raise_abort();
           break;
         }
@@ -1097,7 +1110,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const __grid_c
         for (int kb = kb0; kb < kb1; ++kb, ++gk) {
           const int s = gk % C::kStages;
           const uint32_t u = gk / C::kStages;
-          if (!sm100::mbar_wait_bounded(&full[s], u & 1, s_abort, kWaitLimitNs)) {
+          if (!sm100::mbar_wait_bounded(&full[s], u & 1, s_abort, g.wait_ns)) {
             raise_abort();
             ok = false;
             break;
@@ -1139,7 +1152,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const __grid_c
       const int b = i & 1;
       const uint32_t v = (uint32_t)(i >> 1);
       int ok = 1;
-      if (lane == 0) ok = sm100::mbar_wait_bounded(&accf[b], v & 1, s_abort, kWaitLimitNs) ? 1 : 0;
+      if (lane == 0) ok = sm100::mbar_wait_bounded(&accf[b], v & 1, s_abort, g.wait_ns) ? 1 : 0;
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) {
         if (lane == 0) raise_abort();
@@ -1653,6 +1666,7 @@ static int launch_gemm_v(const b200d2_batch& b, const TcGeom& g, void* ws, cudaS
   a.part = ws_at<float>(ws, g.off_part);
   a.cnt = ws_at<unsigned>(ws, g.off_cnt);
   a.L = Layout{U ? U->parts : nullptr, U ? U->rows : nullptr, U ? U->tiles[wl] : nullptr, U ? U->ntiles[wl] : 0};
+  a.wait_ns = g_wait_ns.load() ? g_wait_ns.load() : kWaitLimitNs;
   // the shared-memory opt-in is a per-device function attribute
   static std::atomic<unsigned long long> attr_dev{0};
   int dev = 0;
@@ -1708,6 +1722,7 @@ static int launch_gemm_pair(const b200d2_batch& b, const TcGeom& g, void* ws, cu
   a.inv_sa = ws_at<float>(ws, g.off_sa);
   a.inv_sb = ws_at<float>(ws, g.off_sb);
   a.L = Layout{U ? U->parts : nullptr, U ? U->rows : nullptr, U ? U->tiles[2] : nullptr, U ? U->ntiles[2] : 0};
+  a.wait_ns = kWaitLimitNs;  // the pair kernel's waits are not shortened (see b200d2_set_wait_limit_ns)
   static std::atomic<unsigned long long> attr_dev{0};
   int dev = 0;
   B200D2_CUDA_TRY(cudaGetDevice(&dev));
@@ -1905,9 +1920,6 @@ const char* tc_stage_name(int precision, int stage) {
 }
 
 static int check_tc(const b200d2_view& v, const b200d2_batch& b) {
-  if (b.accumulate == 0) {
-    // fine: the epilogue overwrites
-  }
   if ((long long)b.O * b.T >= 0xffffffffLL) return B200D2_ERR_UNSUPPORTED;  // argmin index is 32-bit
   if (v.maxR > 4096) return B200D2_ERR_UNSUPPORTED;
   return B200D2_OK;
@@ -2477,5 +2489,10 @@ extern "C" int b200d2_set_gemm_variant(int row_bytes, int tile_n, int split, int
 extern "C" int b200d2_set_combine(int mode) {
   if (mode != B200D2_COMBINE_DF32 && mode != B200D2_COMBINE_FP64) return B200D2_ERR_INVALID;
   b200d2::g_combine64.store(mode == B200D2_COMBINE_FP64 ? 1 : 0);
+  return B200D2_OK;
+}
+
+extern "C" int b200d2_set_wait_limit_ns(unsigned long long ns) {
+  b200d2::g_wait_ns.store(ns);
   return B200D2_OK;
 }

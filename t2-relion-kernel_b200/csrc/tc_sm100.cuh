@@ -62,17 +62,17 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 
 // Bounded wait: gives up after `limit_ns` of wall time or when another role
 // has raised *abort; returns false in that case (the caller stops its loop).
+// The slow path is entered only when the phase has not completed; each of its
+// try_wait rounds (which may suspend the thread for a while) is followed by
+// the abort and clock checks, so a short limit is honoured.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
                                                   volatile uint32_t* abort, uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
-  uint32_t spins = 0;
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((++spins & 255u) == 0u) {
-      if (*abort) return false;
-      if (globaltimer_ns() - t0 > limit_ns) return false;
-    }
+    if (*abort) return false;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
   }
 }
 

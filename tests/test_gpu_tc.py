@@ -230,3 +230,73 @@ def test_combine_df32_matches_fp64_combine(pkg, synth, oracle, cuda, case, varia
     assert oracle.error_stats(d32, ref)["max_rel"] <= TOL["bf16x3"]
     proj.close()
 
+
+
+@pytest.mark.parametrize("bad", [(600.0, 0.0), (-1.0, 3.0), (2.0, -513.0), (2.5, 1.0)])
+def test_listed_coordinate_out_of_range_reported(pkg, synth, oracle, cuda, bad):
+    """Caller-listed pixel coordinates are device data: one that lies outside
+    x in [0, 512], y in [-512, 512], or is not an integer, sets the workspace
+    status word to B200D2_ERR_INVALID; the same batch with valid coordinates
+    reports 0."""
+    torch = cuda
+    pr = synth.make_problem("tiny")
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dp = DeviceProblem(torch, pr)
+    op = oracle.projector_for(pr)
+    cols = [oracle.filter_image(op, pr.fimg_re[p], pr.fimg_im[p], pr.corr[p]) for p in range(pr.P)]
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(np.stack(a)), device="cuda")  # noqa: E731
+    re, im, corr = t([c[0] for c in cols]), t([c[1] for c in cols]), t([c[2] for c in cols])
+    n_listed = cols[0][4]
+    for corrupt in (False, True):
+        xy = cols[0][3].copy()
+        if corrupt:
+            xy[2 * (n_listed // 2)], xy[2 * (n_listed // 2) + 1] = bad
+        coor = torch.as_tensor(xy, device="cuda")
+        out = torch.zeros(pr.P * pr.O * pr.T, device="cuda")
+        b = pkg.make_batch(dp.eulers, dp.tx, dp.ty, re, im, corr, out, O=pr.O, T=pr.T, P=pr.P, N_img=pr.N_img,
+                           coor_xy=coor, n_listed=n_listed)
+        ws = torch.empty(pkg.batch_workspace_bytes(view, b, pkg.PREC_BF16X3), device="cuda", dtype=torch.uint8)
+        pkg.diff2_coarse_batch(view, b, pkg.PREC_BF16X3, ws)
+        torch.cuda.synchronize()
+        assert pkg.workspace_status(ws) == (1 if corrupt else 0)
+    proj.close()
+
+
+def test_bounded_wait_gives_up_and_context_stays_usable(pkg, synth, oracle, cuda):
+    """The contraction's device-side waits are bounded.  With the pipeline-wait
+    limit of the single-CTA contraction cut to 1 us (a test hook), its waits
+    for an accumulator run out before the first tile's MMAs finish: the kernel
+    raises its abort flag, lets its copies and MMAs in flight finish, frees
+    its tensor memory and returns, and the workspace status reads
+    B200D2_ERR_TIMEOUT.  The call returns, the context stays usable, and the
+    next call with the default limit gives correct results in the same
+    workspace."""
+    torch = cuda
+    pr = synth.make_problem("c1")
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dp = DeviceProblem(torch, pr)
+    ref = fp64_all(pkg, view, dp)
+    out = torch.zeros(pr.P * pr.O * pr.T, device="cuda")
+    b = pkg.make_batch(dp.eulers, dp.tx, dp.ty, dp.re, dp.im, dp.corr, out, O=pr.O, T=pr.T, P=pr.P,
+                       N_img=pr.N_img)
+    ws = torch.empty(pkg.batch_workspace_bytes(view, b, pkg.PREC_BF16X3), device="cuda", dtype=torch.uint8)
+    pkg.set_gemm_variant(64, 256, 1, 2)  # single-CTA tiles: the kernel the hook applies to
+    try:
+        pkg.set_wait_limit_ns(1000)
+        try:
+            pkg.diff2_coarse_batch(view, b, pkg.PREC_BF16X3, ws)
+            torch.cuda.synchronize()
+        finally:
+            pkg.set_wait_limit_ns(0)
+        assert pkg.workspace_status(ws) == 5  # B200D2_ERR_TIMEOUT
+        out.zero_()
+        pkg.diff2_coarse_batch(view, b, pkg.PREC_BF16X3, ws)
+        torch.cuda.synchronize()
+        assert pkg.workspace_status(ws) == 0
+    finally:
+        pkg.set_gemm_variant(0, 0, 0, 0)
+    got = out.cpu().numpy().reshape(pr.P, pr.O, pr.T)
+    assert oracle.error_stats(got, ref)["max_rel"] <= TOL["bf16x3"]
+    proj.close()

@@ -200,11 +200,14 @@ def test_config_shapes(synth):
 
 
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "ref_*.npz"))))
-def test_oracle_against_reference_golden(oracle, path):
+def test_oracle_against_reference_golden(oracle, synth, path):
     """Golden vectors written by the reference's own kernels (runDiff2KernelCoarse
     and runDiff2KernelCoarseDouble, compiled from the reference sources and run
     on a B200 by tests/golden/make_golden.py), with the texture unit's
-    projections at every pixel stored beside them.
+    projections at every pixel stored beside them: the box-16 problem g0 and
+    a C1-sized slice (image 32, radius 16, 21 translations, every 9th of the
+    576 orientations, 2 particles) whose inputs are rebuilt from the seeded
+    generator and checked by digest.
 
     * Given the hardware projections, the oracle's FP64 arithmetic (phase
       shift, corr/2 weighting, sum, accumulation) reproduces the reference's
@@ -212,20 +215,16 @@ def test_oracle_against_reference_golden(oracle, path):
     * With its own texture-weight model the oracle is within 5e-4: the B200
       texture unit rounds the eight corner weights jointly to 1/256 in a way
       the model approximates but does not reproduce exactly."""
-    g = np.load(path)
-    from types import SimpleNamespace
-    pv = SimpleNamespace(re=g["vol_re"], im=g["vol_im"], **{k: int(g[k]) for k in
-                         ("mdlX", "mdlY", "mdlZ", "mdlInitY", "mdlInitZ", "mdlMaxR")},
-                         padding_factor=float(g["pf"]))
-    op = oracle.Projector(pv, int(g["imgX"]), int(g["imgY"]), int(g["imgMaxR"]))
-    for p in range(g["fimg_re"].shape[0]):
-        if "prj_re" in g.files:
-            d = oracle.diff2_from_projections(op, g["prj_re"], g["prj_im"], g["trans_x"], g["trans_y"],
-                                              g["fimg_re"][p], g["fimg_im"][p], g["corr"][p])
-            s_d = oracle.error_stats(d, g["ref_f64"][p])
-            s_f = oracle.error_stats(d, g["ref_f32"][p])
-            assert s_d["max_rel"] < 1e-9, s_d
-            assert s_f["max_rel"] < 1e-5, s_f
-        d = oracle.diff2_coarse_f64(op, g["eulers"], g["trans_x"], g["trans_y"], g["fimg_re"][p],
-                                    g["fimg_im"][p], g["corr"][p], mode=oracle.INTERP_TEX_ROUND)
-        assert oracle.error_stats(d, g["ref_f64"][p])["max_rel"] < 5e-4
+    import golden_util
+    g = golden_util.load(path, synth)
+    op = oracle.Projector(g.pv, g.imgX, g.imgY, g.imgMaxR)
+    for p in range(g.P):
+        d = oracle.diff2_from_projections(op, g.prj_re, g.prj_im, g.trans_x, g.trans_y, g.fimg_re[p], g.fimg_im[p],
+                                          g.corr[p])
+        s_d = oracle.error_stats(d, g.ref_f64[p])
+        s_f = oracle.error_stats(d, g.ref_f32[p])
+        assert s_d["max_rel"] < 1e-9, s_d
+        assert s_f["max_rel"] < 1e-5, s_f
+        d = oracle.diff2_coarse_f64(op, g.eulers, g.trans_x, g.trans_y, g.fimg_re[p], g.fimg_im[p], g.corr[p],
+                                    mode=oracle.INTERP_TEX_ROUND)
+        assert oracle.error_stats(d, g.ref_f64[p])["max_rel"] < 5e-4

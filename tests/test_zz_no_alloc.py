@@ -28,17 +28,45 @@ def _outputs(torch, pr):
     return d, mn, am
 
 
-def test_static_scratch_matches_allocating_entry_point(pkg, synth, oracle, cuda):
+def _listed_inputs(torch, oracle, pr):
+    """The reference's filtered layout (FilterCoarseParamImage): in-radius
+    pixels first with their coordinates, shared by all particles."""
+    op = oracle.projector_for(pr)
+    cols = [oracle.filter_image(op, pr.fimg_re[p], pr.fimg_im[p], pr.corr[p]) for p in range(pr.P)]
+    n = cols[0][4]
+    assert all(c[4] == n for c in cols)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(np.stack(a)), device="cuda")  # noqa: E731
+    return t([c[0] for c in cols]), t([c[1] for c in cols]), t([c[2] for c in cols]), \
+        torch.as_tensor(cols[0][3], device="cuda"), n
+
+
+@pytest.mark.parametrize("form", ["diff2", "listed", "cc", "accumulate"])
+def test_static_scratch_matches_allocating_entry_point(pkg, synth, oracle, cuda, form):
+    """Two calls in a row on the fixed scratch give the allocating entry
+    point's outputs, for the plain diff2 batch, caller-listed pixels (whose
+    first stage takes another branch), the CC score and accumulation onto the
+    caller's buffer.  Between the two calls a batch of another shape runs on
+    the same scratch, so the second call starts from different leftovers."""
     torch = cuda
     pr = synth.make_problem("c1")
     proj = pkg.Projector(pr.projector, use_texture=1)
     view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
     dp = DeviceProblem(torch, pr)
+    re, im, corr = dp.re, dp.im, dp.corr
+    coor, n_listed = None, 0
+    if form == "listed":
+        re, im, corr, coor, n_listed = _listed_inputs(torch, oracle, pr)
+    score = pkg.SCORE_CC if form == "cc" else pkg.SCORE_DIFF2
+    accumulate = form == "accumulate"
+    init = np.random.default_rng(7).uniform(0, 50, pr.P * pr.O * pr.T).astype(np.float32)
 
     def batch(out):
         d, mn, am = out
-        return pkg.make_batch(dp.eulers, dp.tx, dp.ty, dp.re, dp.im, dp.corr, d, O=pr.O, T=pr.T, P=pr.P,
-                              N_img=pr.N_img, out_min=mn, out_argmin=am)
+        if accumulate:
+            d.copy_(torch.as_tensor(init, device="cuda"))
+        return pkg.make_batch(dp.eulers, dp.tx, dp.ty, re, im, corr, d, O=pr.O, T=pr.T, P=pr.P,
+                              N_img=pr.N_img, out_min=mn, out_argmin=am, coor_xy=coor, n_listed=n_listed,
+                              score=score, accumulate=accumulate)
 
     ref = _outputs(torch, pr)
     b = batch(ref)
@@ -47,17 +75,34 @@ def test_static_scratch_matches_allocating_entry_point(pkg, synth, oracle, cuda)
     ws = torch.empty(need, device="cuda", dtype=torch.uint8)
     pkg.diff2_coarse_batch(view, b, pkg.PREC_BF16X3, ws)
     torch.cuda.synchronize()
+    assert pkg.workspace_status(ws) == 0
     r_d, r_mn, r_am = (t.cpu().numpy() for t in ref)
+    if form == "cc":  # CC scores pass through zero: errors relative to the largest magnitude
+        scale = np.abs(r_d).max()
 
+    other = synth.make_problem("tiny")
+    oproj = pkg.Projector(other.projector, use_texture=1)
+    oview = oproj.view(other.imgX, other.imgY, other.imgMaxR)
+    odp = DeviceProblem(torch, other)
     for call in range(2):
         out = _outputs(torch, pr)
         pkg.diff2_coarse_batch_static(view, batch(out), pkg.PREC_BF16X3)
         torch.cuda.synchronize()
         d, mn, am = (t.cpu().numpy() for t in out)
-        s = oracle.error_stats(d, r_d)
-        assert s["max_rel"] <= TOL, (call, s)
-        np.testing.assert_allclose(mn, r_mn, rtol=TOL)
+        if form == "cc":
+            assert np.abs(d.astype(np.float64) - r_d).max() <= TOL * scale, call
+        else:
+            s = oracle.error_stats(d, r_d)
+            assert s["max_rel"] <= TOL, (call, s)
+        np.testing.assert_allclose(mn, r_mn, rtol=TOL, atol=TOL * abs(r_mn).max())
         np.testing.assert_array_equal(am, r_am)
+        if call == 0:  # another shape on the same scratch before the second call
+            od = _outputs(torch, other)
+            pkg.diff2_coarse_batch_static(oview, pkg.make_batch(
+                odp.eulers, odp.tx, odp.ty, odp.re, odp.im, odp.corr, od[0], O=other.O, T=other.T, P=other.P,
+                N_img=other.N_img, out_min=od[1], out_argmin=od[2]), pkg.PREC_BF16X3)
+            torch.cuda.synchronize()
+    oproj.close()
     proj.close()
 
 
