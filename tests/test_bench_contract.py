@@ -17,7 +17,7 @@ def _run(env_extra=None):
     env = dict(os.environ)
     env.update(env_extra or {})
     return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "2",
-                           "--warmup", "1", "--config", "c1"], cwd=ROOT, env=env, capture_output=True, text=True,
+                           "--warmup", "1", "--config", "c1", "--cpu-budget", "2"], cwd=ROOT, env=env, capture_output=True, text=True,
                           timeout=300)
 
 
