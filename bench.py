@@ -1233,7 +1233,7 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
         view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
         pin = [torch.as_tensor(a).pin_memory() for a in (pr.fimg_re, pr.fimg_im, pr.corr)]
         refs.append(dict(pr=pr, proj=proj, view=view, pin=pin))
-    rate, horizon = 200.0, args.serve_seconds
+    rate = 200.0
     trace, t = [], 0.0
     while True:
         t += rng.exponential(1.0 / rate)
