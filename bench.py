@@ -245,6 +245,8 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving trace of the default line")
     ap.add_argument("--serve-fp32-seconds", type=float, default=0.5,
                     help="c5: part of the trace replayed through the FP32 baseline")
+    ap.add_argument("--operand-gen", type=int, default=0, choices=[0, 1],
+                    help="0: A operand materialised by its own kernel (default); 1: generated inside the contraction")
     ap.add_argument("--combine", default="df32", choices=["df32", "fp64"],
                     help="final combination nA - 2 cross: double-float (default) or FP64")
     ap.add_argument("--gemm-variant", default=None,
@@ -495,6 +497,7 @@ def ours_arm(args):
     if args.gemm_variant:
         pkg.set_gemm_variant(*[int(x) for x in args.gemm_variant.split(",")])
     pkg.set_combine(pkg.COMBINE_FP64 if args.combine == "fp64" else pkg.COMBINE_DF32)
+    pkg.set_operand_gen(args.operand_gen)
     stream = torch.cuda.current_stream()
 
     proj = pkg.Projector(pr.projector, use_texture=1)
@@ -620,6 +623,67 @@ def ours_arm(args):
         kern = {"per_kernel_ms": {name: tuned}, "dominant": name, "dominant_ms": tuned or None, "traffic": None}
     else:
         kern = pkg.kernel_breakdown(view, batch, prec, ws, stream, reps=3)
+
+    # ---- one particle per call, as RELION's per-particle caller makes it ----
+    # (the reference's runDiff2KernelCoarse signature; its best kernel is timed
+    # per particle in the reference arm's reference_gpu field)
+    single = None
+    if not uneven and prec != 0:
+        o1 = torch.empty(O * T, device=dev)
+        m1 = torch.empty(1, device=dev, dtype=torch.float64)
+        a1 = torch.empty(1, device=dev, dtype=torch.int64)
+        b1 = pkg.make_batch(eul, tx, ty, re[0:1], im[0:1], corr[0:1], o1, O=O, T=T, P=1, N_img=N, out_min=m1,
+                            out_argmin=a1)
+        ws1 = torch.empty(max(pkg.batch_workspace_bytes(view, b1, prec), 16), device=dev, dtype=torch.uint8)
+        o32 = torch.zeros(O * T, device=dev)
+
+        def per_call(fn, reps=20):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(reps):
+                fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            return a.elapsed_time(b) / reps
+
+        ms_tc = per_call(lambda: pkg.diff2_coarse_batch(view, b1, prec, ws1, stream))
+        ms_fp32 = per_call(lambda: pkg.run_diff2_kernel_coarse(view, tx, ty, corr[0], re[0], im[0], eul, o32, O, T, N,
+                                                               stream=stream))
+        single = {"batch_api_ms_per_particle": ms_tc, "fp32_dropin_ms_per_particle": ms_fp32,
+                  "evals_per_particle": O * T,
+                  "note": f"one particle per call, {args.precision} batch entry point (all stages: projection, "
+                          "norms, contraction) and the FP32 runDiff2KernelCoarse drop-in; back-to-back calls, "
+                          "CUDA events"}
+        del ws1, o1, o32
+
+    # ---- the same batch with the A operand generated inside the contraction ----
+    gen_leg = None
+    if not uneven and prec != 0 and args.operand_gen == 0:
+        pkg.set_operand_gen(1)
+        try:
+            ws_g = torch.empty(max(pkg.batch_workspace_bytes(view, batch, prec), 16), device=dev, dtype=torch.uint8)
+            for _ in range(2):
+                pkg.diff2_coarse_batch(view, batch, prec, ws_g, stream)
+            torch.cuda.synchronize()
+            g_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(5)]
+            for ga, gb in g_evs:
+                flush.zero_()
+                ga.record(stream)
+                pkg.diff2_coarse_batch(view, batch, prec, ws_g, stream)
+                gb.record(stream)
+            torch.cuda.synchronize()
+            kg = pkg.kernel_breakdown(view, batch, prec, ws_g, stream, reps=2)
+            gen_leg = {"ms_per_step": statistics.median(a.elapsed_time(b) for a, b in g_evs),
+                       "contraction_ms": kg["dominant_ms"], "workspace_bytes": int(ws_g.numel()),
+                       "workspace_bytes_materialised": int(ws.numel()),
+                       "note": "b200d2_set_operand_gen(1): generator warps write A into shared memory inside the "
+                               "contraction (bit-identical scores, no A planes); L2 flushed before each step"}
+            del ws_g
+        finally:
+            pkg.set_operand_gen(0)
 
     # ---- end to end through the public API with host buffers ----
     h_re = torch.empty_like(re, device="cpu").pin_memory()
@@ -828,6 +892,7 @@ def ours_arm(args):
                                        (f"{args.config}: {P} particles x {O} orientations x {T} translations, "
                                         f"image {pr.img_size} ({N} px, {K_c} in radius)"),
                            "precision": args.precision, "combine": args.combine,
+                           "operand": "generated in the contraction" if args.operand_gen else "materialised",
                            "particles": P, "orientations": O, "translations": T,
                            "pixels_in_radius": K_c, "l2": "flushed (256 MB write) before every timed step",
                            "parallelism": f"replicas x{world}", **plan_extra},
@@ -840,7 +905,9 @@ def ours_arm(args):
                           f"({4 * evals_step / 1e6:.0f} MB per step) stays on the device, where the weights and "
                           "significance steps read it; e2e_significance reads their product back")},
                 "e2e_significance": e2e_sig,
-                "parity": parity, "fp32_cuda_core": fp32_leg, "serving": serving,
+                "parity": parity, "fp32_cuda_core": fp32_leg, "operand_generated_in_contraction": gen_leg,
+                "single_particle_call": single,
+                "serving": serving,
                 "clocks": clk, "gpu_launches": int(l1 - l0), "kernels": kern.get("per_kernel_ms"),
                 "kernels_note": "each stage timed alone (CUDA events, 3 launches); stages 1, 3 and 5 overlap "
                                 "stages 2 and 4 on a side stream inside a step, so their sum exceeds ms_per_step"}

@@ -522,6 +522,20 @@ const char* b200d2_stage_name(int precision, int stage);
 int b200d2_workspace_status(const void* d_workspace, void* stream,
                             int* status);
 
+/* How the tensor-core contraction gets its A operand (the weighted,
+ * phase-shifted images; the reference builds it per output tile in shared
+ * memory, src/translation_matrix_handler.cuh:279-369,432-511).  0 (default):
+ * A is written to the workspace by its own kernel and read back by TMA.  1:
+ * generator warps of the contraction write each k-block of A into shared
+ * memory from the weighted image and the translation's separable phase rows,
+ * so A never goes through device memory (no operand-generation stage, no A
+ * planes in the workspace: 385 MB less at 256 x 4608 x 113 at image 64), at
+ * the cost of shared-memory bandwidth (that contraction is 1.3x slower).
+ * Both give bit-identical scores.  Process-wide; read when a workspace size
+ * is queried, a batch runs or a plan is created, so query, run and plan
+ * creation must see the same mode. */
+int b200d2_set_operand_gen(int mode);
+
 /* Test hook for the give-up path of the bounded device-side waits (no
  * counterpart in the reference, whose waits cannot hang: it recomputes instead
  * of spinning, src/translation_matrix_handler.cuh:145-206).  Sets, process

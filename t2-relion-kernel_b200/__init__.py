@@ -164,6 +164,7 @@ def _declare(L):
         "b200d2_set_gemm_variant": [I, I, I, I],
         "b200d2_set_combine": [I],
         "b200d2_set_wait_limit_ns": [C.c_ulonglong],
+        "b200d2_set_operand_gen": [I],
         "b200d2_diff2_fine": [C.POINTER(View), P, P, P, P, P, P, P, Z, F, Z, P, P, P, P, P],
         "b200d2_diff2_fine_cc": [C.POINTER(View), P, P, P, P, P, P, P, Z, Z, P, P, P, P, P],
         "b200d2_ctf_fold": [P, P, C.c_longlong, I, I, I, I, I, I, F, P, P, C.c_longlong, P, P, P, P],
@@ -592,6 +593,13 @@ def set_combine(mode: int) -> None:
     """Final combination of the tensor-core forms: COMBINE_DF32 (default,
     double-float) or COMBINE_FP64."""
     _check(lib().b200d2_set_combine(mode), "set_combine")
+
+
+def set_operand_gen(mode: int) -> None:
+    """A operand of the contraction: 0 (default) materialised in the workspace
+    by its own kernel, 1 generated in shared memory inside the contraction
+    (bit-identical results).  Query workspace sizes after setting it."""
+    _check(lib().b200d2_set_operand_gen(int(mode)), "set_operand_gen")
 
 
 def set_wait_limit_ns(ns: int) -> None:

@@ -13,6 +13,8 @@
 
 #include <atomic>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/b200d2.h"
 
 namespace b200d2 {
@@ -25,6 +27,16 @@ namespace b200d2 {
 
 // Process-wide count of kernel launches made by this library.
 void count_launch(unsigned n = 1);
+
+// NVTX range over a host scope (a batch call, a pipeline stage, a served
+// request), so that a timeline profiler labels the library's launches; without
+// a profiler attached the push and pop cost a few nanoseconds.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Opts `kernel` in to `bytes` of dynamic shared memory on the current device,
 // once per device (the attribute belongs to each device's context); `done`

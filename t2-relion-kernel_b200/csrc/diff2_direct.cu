@@ -367,6 +367,7 @@ extern "C" int b200d2_diff2_coarse(const b200d2_view* view,
                                    const float* d_eulers, float* d_diff2s,
                                    size_t O, size_t T, size_t N_img,
                                    void* stream, int precision) {
+  b200d2::NvtxRange range("b200d2_diff2_coarse");
   int st = b200d2::check_common(view, d_trans_x, d_trans_y, d_corr, d_real,
                                 d_imag, d_eulers, d_diff2s, O, T, N_img);
   if (st != B200D2_OK) return st;

@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cstdio>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -87,6 +88,9 @@ void CUDART_CB on_done(void* arg) {
 
 // Launch a request's work on its slot stream (called with the lock held).
 int admit(b200d2_server* s, Req& q) {
+  char label[64];
+  snprintf(label, sizeof(label), "b200d2 request %lld (ref %d, %d particles)", q.ticket, q.r.ref, q.r.P);
+  b200d2::NvtxRange range(label);
   const Ref& ref = s->refs[q.r.ref];
   cudaStream_t st = s->streams[q.slot];
   const b200d2_request& r = q.r;

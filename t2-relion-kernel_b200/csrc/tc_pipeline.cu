@@ -58,13 +58,26 @@ struct TcGeom {
   int P, O, T, N_img, K_c, Kpad, Mrows, Mpad, Opad, maxR, exw, eyw;
   int elem, BK, terms;
   int Kq;  // row stride (doubles) of |B|^2 and of the compacted weights: Kpad / 2, zero padded
+  // 1: the contraction generates the A operand in shared memory (no A planes
+  // in the workspace, no operand-generation stage); 0: A is written to the
+  // workspace by tc_gen_a_kernel and read by TMA
+  int gen;
   size_t off_status, off_xy, off_idx, off_ex, off_ey, off_ph, off_bhi, off_blo, off_q, off_w, off_normx, off_na, off_nahl,
-      off_ahi, off_alo, off_keys, off_sa, off_sb, off_part, off_cnt, total;
+      off_ahi, off_alo, off_keys, off_sa, off_sb, off_part, off_cnt, off_wx, off_cxy, off_thdr, off_exc, off_eyc, total;
   int split_max;  // largest k-split the workspace holds partial sums for
   int n_cnt;      // split arrival counters
 };
 
 static int num_sms();
+
+// Operand mode of the contraction (b200d2_set_operand_gen): 0 (default) = A
+// materialised in the workspace by tc_gen_a_kernel and read by TMA, 1 = A
+// generated inside the contraction.  At C2 (BF16x3, CTA pairs) the
+// generating contraction takes 2.19 ms against 1.67 ms plus 0.09 ms for the
+// materialising kernel: its generator warps' shared-memory loads and stores
+// add to the tensor cores' operand reads, and shared-memory bandwidth bounds
+// it, where TMA writes A without loads.
+static std::atomic<int> g_operand_gen{0};
 
 static inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -135,8 +148,22 @@ static TcGeom make_geom(const b200d2_view& v, const b200d2_batch& b, int prec, i
   g.off_normx = take(sizeof(double) * (size_t)g.P);
   g.off_na = take(sizeof(double) * (size_t)g.P * g.O);
   g.off_nahl = take(sizeof(float2) * (size_t)g.P * g.O);  // nA as an unevaluated sum hi + lo of two floats
-  g.off_ahi = take((size_t)g.Mpad * g.Kpad * g.elem);
-  g.off_alo = planes == 2 ? take((size_t)g.Mpad * g.Kpad * g.elem) : g.off_ahi;
+  g.gen = g_operand_gen.load();
+  if (g.gen) {  // no A planes: the contraction writes A into shared memory
+    g.off_ahi = g.off_alo = 0;
+  } else {
+    g.off_ahi = take((size_t)g.Mpad * g.Kpad * g.elem);
+    g.off_alo = planes == 2 ? take((size_t)g.Mpad * g.Kpad * g.elem) : g.off_ahi;
+  }
+  // weighted images w X of the listed pixels [P][Kpad / 2] (FP16 forms: times
+  // the particle scale), read by the contraction's operand generation
+  g.off_wx = take(sizeof(float2) * (size_t)(g.P + 1) * (g.Kpad / 2));  // + an all-zero row (rows past the batch)
+  // phase tables deduplicated by translation value: table -> (x row, y row),
+  // a header {rows x, rows y, extent, fits}, and the compact rows
+  g.off_cxy = take(sizeof(int2) * (size_t)std::max(g.T, 1));
+  g.off_thdr = take(4 * sizeof(int));
+  g.off_exc = take(sizeof(float2) * (size_t)g.T * g.exw);
+  g.off_eyc = take(sizeof(float2) * (size_t)g.T * g.eyw);
   g.off_keys = take(sizeof(unsigned long long) * (size_t)g.P);
   g.off_sa = take(sizeof(float) * (size_t)g.P);     // FP16 forms: 1 / particle scale
   g.off_sb = take(sizeof(float) * (size_t)g.Opad);  // FP16 forms: 1 / orientation scale
@@ -294,6 +321,130 @@ __global__ void tc_phase2d_kernel(const float2* __restrict__ ex, const float2* _
       v = make_float2(__fmaf_rn(fx.x, fy.x, -__fmul_rn(fx.y, fy.y)), __fmaf_rn(fx.x, fy.y, __fmul_rn(fx.y, fy.x)));
     }
     ph[(size_t)t * Kh + kp] = v;
+  }
+}
+
+// Phase tables deduplicated by translation value, for the contraction's
+// operand generation.  e^{i x tx} depends only on tx and e^{i y ty} only on
+// ty, and translation grids repeat few values (a disc of radius 6 px has 113
+// translations but 13 distinct tx and 13 distinct ty), so the rows of the
+// per-table tables ex / ey that belong to equal values (bit for bit) are kept
+// once: cxy[t] = (x row, y row) of table t, exc [rows x][ext + 1] and
+// eyc [rows y][2 ext + 1], with ext the largest |x| or |y| of the listed
+// pixels.  hdr = {rows x, rows y, ext, fits}: fits = 1 when the compact rows
+// take at most `cap` entries (they then fit the contraction's shared-memory
+// table; otherwise it reads the (table, pixel) products ph from global
+// memory).  The values are copies of ex / ey, so both give bit-identical
+// operands.  One CTA of kCompactThreads threads; up to kCompactMaxT tables.
+constexpr int kCompactThreads = 1024, kCompactMaxT = 4096;
+__global__ void __launch_bounds__(kCompactThreads) tc_phase_compact_kernel(
+    const float* __restrict__ tx, const float* __restrict__ ty, const float2* __restrict__ txy, int T,
+    const int2* __restrict__ xy, int K_c, const float2* __restrict__ ex, const float2* __restrict__ ey, int maxR,
+    int2* __restrict__ cxy, int* __restrict__ hdr, float2* __restrict__ exc, float2* __restrict__ eyc, int cap) {
+  __shared__ int s_fx[kCompactMaxT], s_fy[kCompactMaxT];  // first table with the same value; then its row
+  __shared__ int s_part[2][kCompactThreads / 32];
+  __shared__ int s_ext, s_n[2];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_ext = 0;
+  __syncthreads();
+  int e = 0;
+  for (int k = tid; k < K_c; k += kCompactThreads) {
+    const int2 c = xy[k];
+    e = max(e, max(abs(c.x), abs(c.y)));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
+  if (lane == 0) atomicMax(&s_ext, e);
+  __syncthreads();
+  const int ext = min(s_ext, maxR);
+  if (T > kCompactMaxT) {  // too many tables to deduplicate here: global products
+    if (tid == 0) {
+      hdr[0] = hdr[1] = 0;
+      hdr[2] = ext;
+      hdr[3] = 0;
+    }
+    return;
+  }
+  auto val = [&](int t, int axis) -> uint32_t {
+    const float v = txy ? (axis ? txy[t].y : txy[t].x) : (axis ? ty[t] : tx[t]);
+    return __float_as_uint(v);
+  };
+  for (int t = tid; t < T; t += kCompactThreads) {
+    const uint32_t vx = val(t, 0), vy = val(t, 1);
+    int fx = t, fy = t;
+    for (int u = 0; u < t && (fx == t || fy == t); ++u) {
+      if (fx == t && val(u, 0) == vx) fx = u;
+      if (fy == t && val(u, 1) == vy) fy = u;
+    }
+    s_fx[t] = fx;
+    s_fy[t] = fy;
+  }
+  __syncthreads();
+  // rank of every first occurrence among the first occurrences: each thread
+  // counts a contiguous chunk of tables, then an exclusive scan over threads
+  const int chunk = (T + kCompactThreads - 1) / kCompactThreads;
+  const int t0 = min(T, tid * chunk), t1 = min(T, t0 + chunk);
+  int nx = 0, ny = 0;
+  for (int t = t0; t < t1; ++t) {
+    nx += s_fx[t] == t;
+    ny += s_fy[t] == t;
+  }
+  int ix = nx, iy = ny;  // inclusive scan within the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int ax = __shfl_up_sync(0xffffffffu, ix, o), ay = __shfl_up_sync(0xffffffffu, iy, o);
+    if (lane >= o) {
+      ix += ax;
+      iy += ay;
+    }
+  }
+  if (lane == 31) {
+    s_part[0][warp] = ix;
+    s_part[1][warp] = iy;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int ax = 0, ay = 0;
+    for (int w = 0; w < kCompactThreads / 32; ++w) {
+      const int bx = s_part[0][w], by = s_part[1][w];
+      s_part[0][w] = ax;
+      s_part[1][w] = ay;
+      ax += bx;
+      ay += by;
+    }
+    s_n[0] = ax;
+    s_n[1] = ay;
+  }
+  __syncthreads();
+  int rx = s_part[0][warp] + ix - nx, ry = s_part[1][warp] + iy - ny;  // exclusive
+  // turn first occurrences into their row numbers (other entries keep the
+  // index of their first occurrence, which is below them)
+  for (int t = t0; t < t1; ++t) {
+    if (s_fx[t] == t) s_fx[t] = -1 - rx++;
+    if (s_fy[t] == t) s_fy[t] = -1 - ry++;
+  }
+  __syncthreads();
+  const int nrx = s_n[0], nry = s_n[1];
+  const int ew = ext + 1, yw = 2 * ext + 1;
+  const bool fits = (long long)nrx * ew + (long long)nry * yw <= cap;
+  const int exw = maxR + 1, eyw = 2 * maxR + 1;
+  for (int t = tid; t < T; t += kCompactThreads) {
+    const int fx = s_fx[t], fy = s_fy[t];
+    const int rxt = fx < 0 ? -1 - fx : -1 - s_fx[fx];
+    const int ryt = fy < 0 ? -1 - fy : -1 - s_fy[fy];
+    cxy[t] = make_int2(rxt, ryt);
+    if (fits) {
+      if (fx < 0)
+        for (int x = 0; x <= ext; ++x) exc[rxt * ew + x] = ex[(size_t)t * exw + x];
+      if (fy < 0)
+        for (int y = -ext; y <= ext; ++y) eyc[ryt * yw + y + ext] = ey[(size_t)t * eyw + y + maxR];
+    }
+  }
+  if (tid == 0) {
+    hdr[0] = nrx;
+    hdr[1] = nry;
+    hdr[2] = ext;
+    hdr[3] = fits ? 1 : 0;
   }
 }
 
@@ -505,13 +656,34 @@ __global__ void __launch_bounds__(256) tc_normx_kernel(const float* __restrict__
                                                        long long stride, int N_img, double* normx,
                                                        const PartDev* __restrict__ parts,
                                                        const int* __restrict__ idx, int K_c, int Kq,
-                                                       double* wcomp) {
+                                                       double* wcomp, float2* wx, const float* __restrict__ inv_sa) {
   const long long p = blockIdx.x;
   const float* pre = parts ? parts[p].re : re + p * stride;
   const float* pim = parts ? parts[p].im : im + p * stride;
   const float* pco = parts ? parts[p].corr : corr + p * stride;
   // the weights of the listed pixels, compacted for the normA contraction
-  for (int k = threadIdx.x; k < Kq; k += blockDim.x) wcomp[p * Kq + k] = k < K_c ? (double)pco[idx[k]] / 2.0 : 0.0;
+  // (Kq = Kpad / 2 entries per particle), and the weighted image w X of the
+  // listed pixels for the contraction's operand generation: w = corr / 2,
+  // (w re, w im), then times the FP16 forms' particle scale, rounded as the
+  // materialised operand's generation rounds them
+  const float sc = inv_sa ? __frcp_rn(inv_sa[p]) : 1.f;
+  for (int k = threadIdx.x; k < Kq; k += blockDim.x) {
+    double wd = 0.0;
+    float2 v = make_float2(0.f, 0.f);
+    if (k < K_c) {
+      const int pix = idx[k];
+      const float w = pco[pix] / 2;
+      wd = (double)pco[pix] / 2.0;
+      v = make_float2(w * pre[pix], w * pim[pix]);
+      if (inv_sa) {
+        v.x *= sc;
+        v.y *= sc;
+      }
+    }
+    wcomp[p * Kq + k] = wd;
+    wx[p * Kq + k] = v;
+    if (p == 0) wx[(long long)gridDim.x * Kq + k] = make_float2(0.f, 0.f);  // the zero row after the last particle
+  }
   double acc = 0.0;
   for (int i = threadIdx.x; i < N_img; i += blockDim.x) {
     const double r = pre[i], m = pim[i];
@@ -806,7 +978,7 @@ struct GemmCfg {
   static constexpr int kBarBytes = 256;
   static constexpr int kSmem = kStages * kStageBytes + kBarBytes + 1024;
   static_assert(kStages >= 2, "at least two pipeline stages");
-  static_assert(2 * kStages * 8 + 5 * 8 + 8 <= kBarBytes, "barrier area");
+  static_assert(3 * kStages * 8 + 5 * 8 + 8 <= kBarBytes, "barrier area");
   static_assert(BN == 128 || BN == 256, "tile width");
 };
 
@@ -829,6 +1001,16 @@ struct GemmArgs {
   // limit (ns) of the single-CTA kernel's pipeline waits (stage ring and
   // accumulator hand-over); its drain waits keep kWaitLimitNs
   unsigned long long wait_ns;
+  // operand generation in the contraction (GEN kernels)
+  const float2* wx;    // [P][Kh] weighted images of the listed pixels
+  const int2* xy;      // [K_c] listed pixel coordinates
+  const float2* ph;    // [tables][Kh] phase products (when the shared rows do not fit)
+  const int2* cxy;     // [tables] rows of the compact phase tables
+  const int* thdr;     // {rows x, rows y, extent, fits}
+  const float2* exc;   // compact e^{i x tx} rows
+  const float2* eyc;   // compact e^{i y ty} rows
+  int Kh, K_c;
+  int P;               // particles (row P of wx is all zero)
 };
 
 // (m0, n0) of the tile-th tile: the work list of an uneven batch, or the
@@ -991,6 +1173,301 @@ __device__ __forceinline__ void epi_drain(const GemmArgs& g, const EpiRow& x, ui
   }
 }
 
+// ------------------------------------------------------------ A in shared memory
+// Operand generation inside the contraction: kGenWarps extra warps write each
+// k-block of A (128 rows of the weighted, phase-shifted images, split into
+// hi/lo planes) straight into the stage ring, in the layout TMA would have
+// written (K-major rows of ROWB bytes, 128- or 64-byte swizzle), so A never
+// goes through global memory.  Element (row m = (p, t), listed pixel k):
+//   a = wx[p][k] * ph,  ph = ex[x(k)] * ey[y(k)] of translation t
+// with the products rounded exactly as tc_phase2d_kernel and tc_gen_a_kernel
+// round them: the operands are bit-identical to the materialised ones.  The
+// deduplicated phase rows (tc_phase_compact_kernel) sit in shared memory; when
+// they do not fit, ph is read from the (table, pixel) products in global
+// memory instead (same values).
+// The generating kernels have 4 epilogue warps (one per TMEM lane quadrant,
+// all columns; with the double-float combine they need a few thousand cycles
+// of a tile's tens of thousands) and 8 generator warps in two groups that
+// take alternate k-blocks: 448 threads, the most that 128 registers per
+// thread allow (four warps per SM sub-partition).
+constexpr int kEpiWarpsGen = 4;
+constexpr int kGenWarps = 8;
+constexpr int kGenFirstWarp = 2 + kEpiWarpsGen;
+constexpr int kGemmThreadsGen = 64 + 32 * (kEpiWarpsGen + kGenWarps);
+constexpr int kGenTabEntries = 1920;                   // float2 entries of the shared phase rows
+constexpr int kGenTabBytes = kGenTabEntries * 8;       // 15 KB
+// per generator warp: a k-block's pixel coordinates and the weighted images
+// of up to 8 particle runs (32 pixels each, 33 entries apart)
+constexpr int kGenSlotBytes = kGenWarps * (32 * 8 + 8 * 33 * 8);
+constexpr int kSmemLimit = 227 * 1024;
+
+// Byte offset of byte b of row R in a K-major tile of ROWB-byte rows written
+// with TMA's 128-byte (ROWB 128) or 64-byte (ROWB 64) swizzle: the 16-byte
+// chunk index is XORed with address bits 7-9 (7-8); tiles are 1024-byte aligned.
+template <int ROWB>
+__device__ __forceinline__ uint32_t swz_off(int R, int b) {
+  if constexpr (ROWB == 128)
+    return (uint32_t)(R * 128 + ((((b >> 4) ^ (R & 7)) << 4) | (b & 15)));
+  else
+    return (uint32_t)(R * 64 + ((((b >> 4) ^ ((R >> 1) & 3)) << 4) | (b & 15)));
+}
+
+// Split of the element pair (re, im) of one pixel into the hi and lo words of
+// the 2-byte forms (the same values as store_split): bf16x2 / half2 bits.
+template <int PREC>
+__device__ __forceinline__ void split_words(float re, float im, uint32_t& hi, uint32_t& lo) {
+  if constexpr (PREC == B200D2_PREC_BF16X3) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(re, im);
+    const float2 hf = __bfloat1622float2(h);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(re - hf.x, im - hf.y);
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+  } else if constexpr (PREC == B200D2_PREC_FP16X3) {
+    const __half2 h = __floats2half2_rn(re, im);
+    const float2 hf = __half22float2(h);
+    const __half2 l = __floats2half2_rn(re - hf.x, im - hf.y);
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+  } else {  // FP16 (one plane)
+    const __half2 h = __floats2half2_rn(re, im);
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = 0u;
+  }
+}
+
+// (the phase rows are written once, before the named barrier that precedes
+// every read, so the loads need no ordering against other memory operations)
+__device__ __forceinline__ float2 lds_f2(uint32_t addr) {
+  float2 v;
+  asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+  return v;
+}
+
+// (no memory clobber: nothing this thread loads aliases the operand tiles, and
+// volatile asm keeps the stores ordered with the barrier waits and the proxy
+// fence around them)
+__device__ __forceinline__ void sts_u4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d));
+}
+
+// 8-byte asynchronous copy global -> shared (zero-filled when !pred; the
+// source is then not read)
+__device__ __forceinline__ void cp_async8_u32(uint32_t smem, const void* gmem, bool pred) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem), "l"(gmem), "r"(pred ? 8 : 0) : "memory");
+}
+
+// One generator warp.  The generator warps form two groups of four, which
+// take the k-blocks of this CTA in turns (group gw / 4 the k-blocks of that
+// parity in the CTA's sequence), so consecutive stages are written at the
+// same time; within a group warp gw owns rows (gw % 4) * 32 .. + 31 of the
+// CTA's 128-row tile.  Lane i keeps its row's particle, translation and
+// phase rows in registers for the whole tile and writes the row's k-block a
+// 16-byte chunk (VPC pixels) at a time: within a warp the chunks of eight
+// consecutive rows fall on distinct banks under the swizzle, so the stores
+// are conflict-free.  A row's particle is one of few: a particle's rows are
+// contiguous, so the warp's 32 rows form runs.  The k-block's pixel
+// coordinates and the weighted images of the first kGenRuns runs are copied
+// into the warp's shared slots with cp.async as soon as the warp has handed
+// over its previous k-block (they land while the other group writes), so the
+// element loop reads shared memory only; rows of later runs (batches with
+// fewer than about four translations per particle) read their weighted image
+// from global memory.
+constexpr int kGenRuns = 8;
+template <int PREC, int ROWB>
+struct GenWarp {
+  static constexpr bool kTf32 = (PREC == B200D2_PREC_TF32 || PREC == B200D2_PREC_TF32X3);
+  static constexpr int kElem = kTf32 ? 4 : 2;
+  static constexpr int PPR = ROWB / (2 * kElem);  // complex pixels per row of a k-block
+  static constexpr int VPC = 16 / (2 * kElem);    // pixels per 16-byte chunk
+  static constexpr int NCH = ROWB / 16;           // chunks per row
+  static constexpr int RPW = 32 / PPR;            // runs staged per warp-wide copy
+  static constexpr int kCoordSlot = 32 * 8;       // bytes of a warp's coordinate slots
+  // runs PPR + 1 entries apart (odd word-pair stride): rows of different runs
+  // read distinct banks
+  static constexpr int kRunStride = PPR + 1;
+  static constexpr int kWSlot = kGenRuns * 33 * 8;
+  const GemmArgs& g;
+  int lane;
+  uint32_t s_ex, s_ey;  // shared addresses of the phase rows (when fits)
+  uint32_t s_coord;     // this warp's coordinate slots [PPR] int2
+  uint32_t s_w;         // this warp's weighted-image slots [kGenRuns][PPR] float2
+  int ext, fits;
+  // this lane's row
+  bool valid;
+  uint32_t ex_row, ey_row;  // shared addresses of the row's e^{i x tx} and e^{i y ty} rows
+  const float2* wx_row;     // weighted image of the row's particle (global)
+  const float2* ph_row;     // (translation, pixel) products of the row's table (when the rows do not fit)
+  int R;                    // row within the CTA's tile
+  int run, nruns;           // this row's run and the runs staged in shared memory
+  int run_p;                // lane r < runs: particle row of run r
+
+  __device__ __forceinline__ GenWarp(const GemmArgs& g_, int gw, int lane_, uint32_t s_ex_, uint32_t s_ey_,
+                                     uint32_t s_slots, int ext_, int fits_)
+      : g(g_), lane(lane_), s_ex(s_ex_), s_ey(s_ey_), ext(ext_), fits(fits_) {
+    R = (gw % 4) * 32 + lane;
+    s_coord = s_slots + (uint32_t)gw * kCoordSlot;
+    s_w = s_slots + (uint32_t)kGenWarps * kCoordSlot + (uint32_t)gw * kWSlot;
+  }
+
+  __device__ __forceinline__ void begin_tile(int m0) {
+    const int m = m0 + R;
+    valid = m < g.Mrows;
+    int p = 0, t = 0;
+    if (valid) {
+      if (g.L.rows) {
+        const int4 rw = g.L.rows[m];
+        p = rw.x;
+        t = rw.z;
+      } else {
+        p = m / g.T;
+        t = m - p * g.T;
+      }
+    }
+    // rows past the batch read the all-zero row after the last particle, so
+    // their elements come out zero without a branch
+    const int pe = valid ? p : g.P;
+    wx_row = g.wx + (size_t)pe * g.Kh;
+    ph_row = g.ph + (size_t)t * g.Kh;
+    int2 cx = make_int2(0, 0);
+    if (fits && valid) cx = g.cxy[t];
+    ex_row = s_ex + (uint32_t)(cx.x * (ext + 1)) * 8u;
+    ey_row = s_ey + (uint32_t)(cx.y * (2 * ext + 1) + ext) * 8u;
+    // runs of equal particle rows
+    const int prev = __shfl_up_sync(0xffffffffu, pe, 1);
+    const unsigned runs = __ballot_sync(0xffffffffu, lane == 0 || pe != prev);
+    run = __popc(runs & ((2u << lane) - 1u)) - 1;
+    const int n = __popc(runs);
+    nruns = n < kGenRuns ? n : kGenRuns;
+    run_p = __shfl_sync(0xffffffffu, pe, lane < n ? (int)__fns(runs, 0, lane + 1) : 0);
+  }
+
+  // copy k-block kb's coordinates and the staged runs' weighted images into
+  // the slots (one cp.async group; the slots' previous contents have been read)
+  __device__ __forceinline__ void stage(int kb) {
+    const int k0 = kb * PPR;
+    if (lane < PPR) {
+      const int kp = k0 + lane;
+      const bool ok = kp < g.K_c;
+      cp_async8_u32(s_coord + (uint32_t)lane * 8u, ok ? (const void*)(g.xy + kp) : (const void*)g.xy, ok);
+    }
+    const int px = lane % PPR;
+#pragma unroll
+    for (int i = 0; i < (kGenRuns + RPW - 1) / RPW; ++i) {
+      const int r = i * RPW + lane / PPR;
+      const int pr = __shfl_sync(0xffffffffu, run_p, r < 32 ? r : 31);
+      if (r < nruns)
+        cp_async8_u32(s_w + (uint32_t)(r * kRunStride + px) * 8u, g.wx + (size_t)pr * g.Kh + k0 + px, true);
+    }
+    cp_async_commit();
+  }
+
+  // element (re, im) of this row at pixel j (w_sh: the row's staged weighted
+  // image in shared memory, or wk the global one; pk: phase products)
+  template <bool FITS, bool SHARED_W>
+  __device__ __forceinline__ float2 element(uint32_t w_sh, const float2* wk, const float2* pk, int j) {
+    float pr, pi;
+    if constexpr (FITS) {
+      int xs, ys;
+      asm("ld.shared.v2.b32 {%0, %1}, [%2];" : "=r"(xs), "=r"(ys) : "r"(s_coord + 8u * (uint32_t)j));
+      const float2 fx = lds_f2(ex_row + (uint32_t)xs * 8u);
+      const float2 fy = lds_f2(ey_row + (uint32_t)ys * 8u);
+      pr = __fmaf_rn(fx.x, fy.x, -__fmul_rn(fx.y, fy.y));
+      pi = __fmaf_rn(fx.x, fy.y, __fmul_rn(fx.y, fy.x));
+    } else {
+      const float2 v = pk[j];
+      pr = v.x;
+      pi = v.y;
+    }
+    const float2 w = SHARED_W ? lds_f2(w_sh + 8u * (uint32_t)j) : wk[j];
+    return make_float2(__fmaf_rn(w.x, pr, -__fmul_rn(w.y, pi)), __fmaf_rn(w.x, pi, __fmul_rn(w.y, pr)));
+  }
+
+  // write k-block kb (staged in the slots) into the tiles at shared addresses
+  // hi / lo (FITS: the phase rows are in shared memory)
+  template <bool FITS, bool SHARED_W>
+  __device__ __forceinline__ void write_rows(int kb, uint32_t hi, uint32_t lo) {
+    const uint32_t w_sh = s_w + (uint32_t)((run < kGenRuns ? run : 0) * kRunStride) * 8u;
+    const float2* wk = wx_row + kb * PPR;
+    const float2* pk = ph_row + kb * PPR;
+    // half a row's chunks in flight (4 for 128-byte rows, 2 for 64-byte ones):
+    // enough independent work to cover the loads' and the arithmetic chains'
+    // latency within the 128-register budget
+    constexpr int kUnroll = NCH / 2;
+#pragma unroll kUnroll
+    for (int q = 0; q < NCH; ++q) {
+      const uint32_t off = swz_off<ROWB>(R, q * 16);
+      if constexpr (kTf32) {
+        float v[4];
+#pragma unroll
+        for (int j = 0; j < VPC; ++j) {
+          const float2 a = element<FITS, SHARED_W>(w_sh, wk, pk, q * VPC + j);
+          v[2 * j] = a.x;
+          v[2 * j + 1] = a.y;
+        }
+        float h[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) h[e] = tf32_round(v[e]);
+        sts_u4(hi + off, __float_as_uint(h[0]), __float_as_uint(h[1]), __float_as_uint(h[2]), __float_as_uint(h[3]));
+        if constexpr (PREC == B200D2_PREC_TF32X3)
+          sts_u4(lo + off, __float_as_uint(tf32_round(v[0] - h[0])), __float_as_uint(tf32_round(v[1] - h[1])),
+                 __float_as_uint(tf32_round(v[2] - h[2])), __float_as_uint(tf32_round(v[3] - h[3])));
+      } else {
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int j = 0; j < VPC; ++j) {
+          const float2 a = element<FITS, SHARED_W>(w_sh, wk, pk, q * VPC + j);
+          split_words<PREC>(a.x, a.y, h[j], l[j]);
+        }
+        sts_u4(hi + off, h[0], h[1], h[2], h[3]);
+        if constexpr (PREC != B200D2_PREC_FP16) sts_u4(lo + off, l[0], l[1], l[2], l[3]);
+      }
+    }
+  }
+
+  // k-block kb, its slots complete (cp.async.wait_group + __syncwarp by the caller)
+  __device__ __forceinline__ void write(int kb, uint32_t hi, uint32_t lo) {
+    const bool all_shared = __all_sync(0xffffffffu, run < kGenRuns);
+    if (fits) {
+      if (all_shared)
+        write_rows<true, true>(kb, hi, lo);
+      else
+        write_rows<true, false>(kb, hi, lo);
+    } else {
+      if (all_shared)
+        write_rows<false, true>(kb, hi, lo);
+      else
+        write_rows<false, false>(kb, hi, lo);
+    }
+  }
+};
+
+// Shared phase rows: copied from the compact tables by the generator warps
+// (a named barrier over those warps alone) when they fit; s_ex / s_ey are
+// their shared addresses.
+__device__ __forceinline__ void gen_load_tables(const GemmArgs& g, float2* s_tab, int& ext, int& fits,
+                                                uint32_t& s_ex, uint32_t& s_ey) {
+  const int nrx = g.thdr[0], nry = g.thdr[1];
+  ext = g.thdr[2];
+  fits = g.thdr[3];
+  const int ew = ext + 1, yw = 2 * ext + 1;
+  s_ex = sm100::smem_u32(s_tab);
+  s_ey = s_ex + (uint32_t)(nrx * ew) * 8u;
+  if (fits) {
+    const int tid = threadIdx.x - 32 * kGenFirstWarp;
+    for (int i = tid; i < nrx * ew; i += 32 * kGenWarps) s_tab[i] = g.exc[i];
+    for (int i = tid; i < nry * yw; i += 32 * kGenWarps) s_tab[nrx * ew + i] = g.eyc[i];
+  }
+  asm volatile("bar.sync 1, %0;" ::"n"(32 * kGenWarps) : "memory");
+}
+
+// Dynamic shared memory of a contraction configuration: the stage ring, the
+// barriers, 1024 bytes of alignment slack and, when the kernel generates A,
+// the shared phase rows and the generator warps' slots.
+template <class C, bool GEN>
+constexpr int gemm_smem_bytes() {
+  return C::kStages * C::kStageBytes + C::kBarBytes + 1024 + (GEN ? kGenTabBytes + kGenSlotBytes : 0);
+}
+
 // Persistent contraction.  Work items are (tile, k-split) pairs, item =
 // tile * split + s, handed out round-robin over the grid.  Warp 0 streams the
 // operand k-blocks with TMA into a ring of shared-memory stages, warp 1 issues
@@ -999,32 +1476,37 @@ __device__ __forceinline__ void epi_drain(const GemmArgs& g, const EpiRow& x, ui
 // combines directly; with split > 1 each split stores its FP32 partial and the
 // last split to arrive for a (tile, quadrant) adds all partials in split order
 // (FP64) and combines, so the result does not depend on arrival order.
-template <int PREC, int ROWB, int BN>
-__global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap mAhi,
-                                                         const __grid_constant__ CUtensorMap mAlo,
-                                                         const __grid_constant__ CUtensorMap mBhi,
-                                                         const __grid_constant__ CUtensorMap mBlo,
-                                                         const GemmArgs g) {
+template <int PREC, int ROWB, int BN, bool GEN>
+__global__ void __launch_bounds__(GEN ? kGemmThreadsGen : kGemmThreads, 1)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
+                   const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo,
+                   const __grid_constant__ GemmArgs g) {
   using C = GemmCfg<PREC, ROWB, BN>;
+  static_assert(gemm_smem_bytes<C, GEN>() <= kSmemLimit, "shared memory");
+  constexpr int EPI = GEN ? kEpiWarpsGen : kEpiWarps;  // epilogue warps
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::kStages * C::kStageBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::kStages * C::kStageBytes);  // TMA bytes
   uint64_t* empty = full + C::kStages;
-  uint64_t* accf = empty + C::kStages;
+  uint64_t* gfull = empty + C::kStages;  // GEN: generator warps' arrivals
+  uint64_t* accf = gfull + C::kStages;
   uint64_t* acce = accf + 2;
   uint64_t* drain = acce + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile uint32_t* s_abort = tmem_slot + 1;
+  // GEN: shared phase rows
+  float2* s_tab = reinterpret_cast<float2*>(smem + C::kStages * C::kStageBytes + C::kBarBytes);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < C::kStages; ++s) {
-      sm100::mbar_init(&full[s], 1);
+      sm100::mbar_init(&full[s], 1);             // the TMA warp's arrival and its bytes
       sm100::mbar_init(&empty[s], 1);
+      sm100::mbar_init(&gfull[s], kGenWarps / 2);  // GEN: one arrival per warp of the group writing it
     }
     for (int b = 0; b < 2; ++b) {
       sm100::mbar_init(&accf[b], 1);
-      sm100::mbar_init(&acce[b], 32 * kEpiWarps);
+      sm100::mbar_init(&acce[b], 32 * EPI);
     }
     sm100::mbar_init(drain, 1);
     *s_abort = 0;
@@ -1032,10 +1514,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const __grid_c
     sm100::fence_proxy_async_smem();
   }
   if (warp == 0 && lane == 0) {
-    sm100::prefetch_tensormap(&mAhi);
+    if (!GEN) sm100::prefetch_tensormap(&mAhi);
     sm100::prefetch_tensormap(&mBhi);
     if (C::kPlanes == 2) {
-      sm100::prefetch_tensormap(&mAlo);
+      if (!GEN) sm100::prefetch_tensormap(&mAlo);
       sm100::prefetch_tensormap(&mBlo);
     }
   }
@@ -1075,20 +1557,23 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const __grid_c
             ok = false;
             break;
           }
-          sm100::mbar_arrive_expect_tx(&full[s], C::kStageBytes);
+          sm100::mbar_arrive_expect_tx(&full[s], GEN ? C::kPlanes * C::kBTile : C::kStageBytes);
           uint8_t* st = smem + s * C::kStageBytes;
           const int kc = kb * C::kBK;
-          sm100::tma_load_2d(st, &mAhi, &full[s], kc, m0);
-          if (C::kPlanes == 2) sm100::tma_load_2d(st + C::kATile, &mAlo, &full[s], kc, m0);
+          if (!GEN) {
+            sm100::tma_load_2d(st, &mAhi, &full[s], kc, m0);
+            if (C::kPlanes == 2) sm100::tma_load_2d(st + C::kATile, &mAlo, &full[s], kc, m0);
+          }
           uint8_t* sb = st + C::kPlanes * C::kATile;
           sm100::tma_load_2d_hint(sb, &mBhi, &full[s], kc, n0, keep);
           if (C::kPlanes == 2) sm100::tma_load_2d_hint(sb + C::kBTile, &mBlo, &full[s], kc, n0, keep);
         }
       }
-      // let the copies in flight land before the CTA can exit
+      // let the copies in flight land before the CTA can exit (full[] counts
+      // the TMA bytes alone, so this completes also after a give-up)
       const uint32_t issued = gk;
       for (uint32_t j = (issued > (uint32_t)C::kStages ? issued - C::kStages : 0); j < issued; ++j)
-        sm100::mbar_wait_bounded(&full[j % C::kStages], (j / C::kStages) & 1, s_abort, kWaitLimitNs);
+        sm100::mbar_wait_drain(&full[j % C::kStages], (j / C::kStages) & 1, kWaitLimitNs);
     }
   } else if (warp == 1) {
     // ------------------------------------------------ MMA issuer
@@ -1110,7 +1595,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const __grid_c
         for (int kb = kb0; kb < kb1; ++kb, ++gk) {
           const int s = gk % C::kStages;
           const uint32_t u = gk / C::kStages;
-          if (!sm100::mbar_wait_bounded(&full[s], u & 1, s_abort, g.wait_ns)) {
+          if (!sm100::mbar_wait_bounded(&full[s], u & 1, s_abort, g.wait_ns) ||
+              (GEN && !sm100::mbar_wait_bounded(&gfull[s], u & 1, s_abort, g.wait_ns))) {
             raise_abort();
             ok = false;
             break;
@@ -1135,18 +1621,63 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const __grid_c
         }
         if (ok) sm100::mma_commit(&accf[b]);
       }
-      // every MMA issued by this thread has retired once `drain` fires
+      // every MMA issued by this thread has retired once `drain` fires (the
+      // tensor memory is released after it)
       sm100::mma_commit(drain);
-      if (!sm100::mbar_wait_bounded(drain, 0, s_abort, kWaitLimitNs)) raise_abort();
+      if (!sm100::mbar_wait_drain(drain, 0, kWaitLimitNs)) raise_abort();
     }
+  } else if (GEN && warp >= kGenFirstWarp) {
+    // ------------------------------------------------ A generators (warps 10..13)
+    int ext, fits;
+    uint32_t s_ex, s_ey;
+    gen_load_tables(g, s_tab, ext, fits, s_ex, s_ey);
+    const int gw = warp - kGenFirstWarp;
+    GenWarp<PREC, ROWB> gen(g, gw, lane, s_ex, s_ey, sm100::smem_u32(s_tab) + kGenTabBytes, ext, fits);
+    const uint32_t par = (uint32_t)(gw / 4);  // this warp's group takes the k-blocks gk with gk % 2 == par
+    uint32_t gk = 0;
+    bool ok = true;
+    for (int item = blockIdx.x; item < num_items && ok; item += gridDim.x) {
+      const int tile = item / g.split;
+      int m0, n0, kb0, kb1;
+      tile_origin(g, tile, C::kBM, C::kBN, m0, n0);
+      split_range(g, item - tile * g.split, kb0, kb1);
+      gen.begin_tile(m0);
+      bool pending = false;  // the next own k-block is already staged
+      for (int kb = kb0; kb < kb1; ++kb, ++gk) {
+        if ((gk & 1u) != par) continue;
+        if (!pending) gen.stage(kb);
+        const int s = gk % C::kStages;
+        const uint32_t u = gk / C::kStages;
+        int w = 1;
+        if (u > 0 && lane == 0) w = sm100::mbar_wait_bounded(&empty[s], (u - 1) & 1, s_abort, g.wait_ns) ? 1 : 0;
+        w = __shfl_sync(0xffffffffu, w, 0);
+        if (!w) {
+          if (lane == 0) raise_abort();
+          ok = false;
+          break;
+        }
+        cp_async_wait<0>();  // this k-block's slots have landed
+        __syncwarp();
+        const uint32_t st = sm100::smem_u32(smem + s * C::kStageBytes);
+        gen.write(kb, st, st + C::kATile);
+        sm100::fence_proxy_async_smem();  // the tensor cores read these tiles through the async proxy
+        __syncwarp();
+        if (lane == 0) sm100::mbar_arrive(&gfull[s]);
+        // the next own k-block of this tile lands while the other group writes
+        pending = kb + 2 < kb1;
+        if (pending) gen.stage(kb + 2);
+      }
+    }
+    cp_async_wait<0>();  // no copy into shared memory outlives the loop
   } else {
-    // ------------------------------------------------ epilogue (warps 2..9)
-    // warp w may read TMEM lanes 32 (w % 4) .. +31; warps 2-5 drain the
-    // first half of the columns, warps 6-9 the second half
+    // ------------------------------------------------ epilogue (warps 2 .. 2 + EPI - 1)
+    // warp w may read TMEM lanes 32 (w % 4) .. +31; with 8 epilogue warps
+    // warps 2-5 drain the first half of the columns and warps 6-9 the second,
+    // with 4 each warp drains all columns of its quadrant
     const int qd = warp & 3;
     const int half = (warp - 2) >> 2;
     const int row = qd * 32 + lane;
-    constexpr int kCols = C::kBN / 2;  // columns per epilogue warp
+    constexpr int kCols = C::kBN / (EPI / 4);  // columns per epilogue warp
     int i = 0;
     for (int item = blockIdx.x; item < num_items; item += gridDim.x, ++i) {
       const int b = i & 1;
@@ -1306,36 +1837,42 @@ struct GemmCfgPair {
   static constexpr int kBarBytes = 256;
   static constexpr int kSmem = kStages * kStageBytes + kBarBytes + 1024;
   static_assert(kStages >= 2, "at least two pipeline stages");
-  static_assert(2 * kStages * 8 + 5 * 8 + 8 <= kBarBytes, "barrier area");
+  static_assert(3 * kStages * 8 + 5 * 8 + 8 <= kBarBytes, "barrier area");
 };
 
-template <int PREC, int ROWB>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
+template <int PREC, int ROWB, bool GEN>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEN ? kGemmThreadsGen : kGemmThreads, 1)
     tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
                         const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo,
-                        const GemmArgs g) {
+                        const __grid_constant__ GemmArgs g) {
   using C = GemmCfgPair<PREC, ROWB>;
+  static_assert(gemm_smem_bytes<C, GEN>() <= kSmemLimit, "shared memory");
+  constexpr int EPI = GEN ? kEpiWarpsGen : kEpiWarps;  // epilogue warps
+  constexpr int kCols = 256 / (EPI / 4);                // columns per epilogue warp
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::kStages * C::kStageBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::kStages * C::kStageBytes);  // TMA bytes
   uint64_t* empty = full + C::kStages;
-  uint64_t* accf = empty + C::kStages;
+  uint64_t* gfull = empty + C::kStages;  // GEN: generator warps' arrivals
+  uint64_t* accf = gfull + C::kStages;
   uint64_t* acce = accf + 2;
   uint64_t* drain = acce + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile uint32_t* s_abort = tmem_slot + 1;
+  float2* s_tab = reinterpret_cast<float2*>(smem + C::kStages * C::kStageBytes + C::kBarBytes);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t rank = sm100::cluster_ctarank();  // 0 issues the MMAs
   const bool lead = rank == 0;
   if (threadIdx.x == 0) {
     for (int s = 0; s < C::kStages; ++s) {
-      sm100::mbar_init(&full[s], 1);   // used in the even CTA: its own arrive + both CTAs' bytes
-      sm100::mbar_init(&empty[s], 1);  // one multicast commit per use
+      sm100::mbar_init(&full[s], 1);                  // used in the even CTA: its own arrive + both CTAs' bytes
+      sm100::mbar_init(&empty[s], 1);                 // one multicast commit per use
+      sm100::mbar_init(&gfull[s], kGenWarps);         // GEN, even CTA: the writing group's warps of both CTAs
     }
     for (int b = 0; b < 2; ++b) {
       sm100::mbar_init(&accf[b], 1);
-      sm100::mbar_init(&acce[b], 2 * 32 * kEpiWarps);  // even CTA: the epilogue threads of both CTAs
+      sm100::mbar_init(&acce[b], 2 * 32 * EPI);  // even CTA: the epilogue threads of both CTAs
     }
     sm100::mbar_init(drain, 1);
     *s_abort = 0;
@@ -1343,10 +1880,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
     sm100::fence_proxy_async_smem();
   }
   if (warp == 0 && lane == 0) {
-    sm100::prefetch_tensormap(&mAhi);
+    if (!GEN) sm100::prefetch_tensormap(&mAhi);
     sm100::prefetch_tensormap(&mBhi);
     if (C::kPlanes == 2) {
-      sm100::prefetch_tensormap(&mAlo);
+      if (!GEN) sm100::prefetch_tensormap(&mAlo);
       sm100::prefetch_tensormap(&mBlo);
     }
   }
@@ -1362,6 +1899,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
   const int num_tiles = g.L.tiles ? g.L.ntiles : g.Mtiles * g.Ntiles;
   const int cl = blockIdx.x >> 1, ncl = gridDim.x >> 1;
   const uint32_t full0 = sm100::map_to_rank(full, 0);  // the even CTA's full[0]
+  const uint32_t gfull0 = sm100::map_to_rank(gfull, 0);
   const uint32_t acce0 = sm100::map_to_rank(acce, 0);
 
   auto raise_abort = [&]() {
@@ -1386,12 +1924,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
             ok = false;
             break;
           }
-          if (lead) sm100::mbar_arrive_expect_tx(&full[s], 2 * C::kStageBytes);
+          if (lead) sm100::mbar_arrive_expect_tx(&full[s], GEN ? 2 * C::kPlanes * C::kBTile : 2 * C::kStageBytes);
           uint8_t* st = smem + s * C::kStageBytes;
           const uint32_t fb = full0 + 8u * (uint32_t)s;
           const int kc = kb * C::kBK;
-          sm100::tma_load_2d_pair(st, &mAhi, fb, kc, m0 + 128 * (int)rank);
-          if (C::kPlanes == 2) sm100::tma_load_2d_pair(st + C::kATile, &mAlo, fb, kc, m0 + 128 * (int)rank);
+          if (!GEN) {
+            sm100::tma_load_2d_pair(st, &mAhi, fb, kc, m0 + 128 * (int)rank);
+            if (C::kPlanes == 2) sm100::tma_load_2d_pair(st + C::kATile, &mAlo, fb, kc, m0 + 128 * (int)rank);
+          }
           uint8_t* sb = st + C::kPlanes * C::kATile;
           sm100::tma_load_2d_pair_hint(sb, &mBhi, fb, kc, n0 + 128 * (int)rank, keep);
           if (C::kPlanes == 2) sm100::tma_load_2d_pair_hint(sb + C::kBTile, &mBlo, fb, kc, n0 + 128 * (int)rank, keep);
@@ -1403,7 +1943,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
       if (lead) {
         const uint32_t issued = gk;
         for (uint32_t j = (issued > (uint32_t)C::kStages ? issued - C::kStages : 0); j < issued; ++j)
-          sm100::mbar_wait_bounded(&full[j % C::kStages], (j / C::kStages) & 1, s_abort, kWaitLimitNs);
+          sm100::mbar_wait_drain(&full[j % C::kStages], (j / C::kStages) & 1, kWaitLimitNs);
       }
     }
   } else if (warp == 1) {
@@ -1424,7 +1964,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
         for (int kb = 0; kb < g.KB; ++kb, ++gk) {
           const int s = gk % C::kStages;
           const uint32_t u = gk / C::kStages;
-          if (!sm100::mbar_wait_bounded(&full[s], u & 1, s_abort, kWaitLimitNs)) {
+          if (!sm100::mbar_wait_bounded(&full[s], u & 1, s_abort, kWaitLimitNs) ||
+              (GEN && !sm100::mbar_wait_bounded(&gfull[s], u & 1, s_abort, kWaitLimitNs))) {
             raise_abort();
             ok = false;
             break;
@@ -1450,12 +1991,55 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
         if (ok) sm100::mma_commit_pair(&accf[b], (uint16_t)3);
       }
       sm100::mma_commit_pair(drain, (uint16_t)1);
-      if (!sm100::mbar_wait_bounded(drain, 0, s_abort, kWaitLimitNs)) raise_abort();
+      if (!sm100::mbar_wait_drain(drain, 0, kWaitLimitNs)) raise_abort();
     }
+  } else if (GEN && warp >= kGenFirstWarp) {
+    // ------------------------------------------------ A generators (warps 10..13, both CTAs)
+    // each CTA writes its own 128 rows; the stage completes on the even
+    // CTA's barrier
+    int ext, fits;
+    uint32_t s_ex, s_ey;
+    gen_load_tables(g, s_tab, ext, fits, s_ex, s_ey);
+    const int gw = warp - kGenFirstWarp;
+    GenWarp<PREC, ROWB> gen(g, gw, lane, s_ex, s_ey, sm100::smem_u32(s_tab) + kGenTabBytes, ext, fits);
+    const uint32_t par = (uint32_t)(gw / 4);  // this warp's group takes the k-blocks gk with gk % 2 == par
+    uint32_t gk = 0;
+    bool ok = true;
+    for (int tile = cl; tile < num_tiles && ok; tile += ncl) {
+      int m0, n0;
+      tile_origin(g, tile, 256, 256, m0, n0);
+      gen.begin_tile(m0 + 128 * (int)rank);
+      bool pending = false;  // the next own k-block is already staged
+      for (int kb = 0; kb < g.KB; ++kb, ++gk) {
+        if ((gk & 1u) != par) continue;
+        if (!pending) gen.stage(kb);
+        const int s = gk % C::kStages;
+        const uint32_t u = gk / C::kStages;
+        int w = 1;
+        if (u > 0 && lane == 0) w = sm100::mbar_wait_bounded(&empty[s], (u - 1) & 1, s_abort, kWaitLimitNs) ? 1 : 0;
+        w = __shfl_sync(0xffffffffu, w, 0);
+        if (!w) {
+          if (lane == 0) raise_abort();
+          ok = false;
+          break;
+        }
+        cp_async_wait<0>();  // this k-block's slots have landed
+        __syncwarp();
+        const uint32_t st = sm100::smem_u32(smem + s * C::kStageBytes);
+        gen.write(kb, st, st + C::kATile);
+        sm100::fence_proxy_async_smem();  // the tensor cores read these tiles through the async proxy
+        __syncwarp();
+        if (lane == 0) sm100::mbar_arrive_cluster(gfull0 + 8u * (uint32_t)s);
+        // the next own k-block of this tile lands while the other group writes
+        pending = kb + 2 < g.KB;
+        if (pending) gen.stage(kb + 2);
+      }
+    }
+    cp_async_wait<0>();  // no copy into shared memory outlives the loop
   } else {
-    // ------------------------------------------------ epilogue (warps 2..9, both CTAs)
+    // ------------------------------------------------ epilogue (warps 2 .. 2 + EPI - 1, both CTAs)
     const int qd = warp & 3;            // TMEM lane quadrant this warp may access
-    const int half = (warp - 2) >> 2;  // column half of the 256-wide tile
+    const int half = (warp - 2) >> 2;  // column half of the 256-wide tile (8 epilogue warps)
     const int row = qd * 32 + lane;
     int i = 0;
     for (int tile = cl; tile < num_tiles; tile += ncl, ++i) {
@@ -1499,12 +2083,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmThreads, 1)
       x.nh_row = g.na_hl + (size_t)p * g.O;
       x.m2s = C::kScaled ? -2.0 * (double)g.inv_sa[p] : -2.0;
       x.m2f = (float)x.m2s;
-      const int o0 = n0 + half * 128;
-      const bool fast = !x.inv && !g.accumulate && !g.combine64 && o0 + 128 <= g.O;
+      const int o0 = n0 + half * kCols;
+      const bool fast = !x.inv && !g.accumulate && !g.combine64 && o0 + kCols <= g.O;
       float best = __int_as_float(0x7f800000);
       int best_lo = -1;
-      epi_drain<C::kScaled, 4>(g, x, tmem + (uint32_t)(b * 256 + half * 128) + ((uint32_t)(qd * 32) << 16), o0,
-                               vrow, fast, best, best_lo);
+      epi_drain<C::kScaled, kCols / 32>(g, x, tmem + (uint32_t)(b * 256 + half * kCols) + ((uint32_t)(qd * 32) << 16),
+                                        o0, vrow, fast, best, best_lo);
       sm100::tc_fence_before();
       sm100::mbar_arrive_cluster(acce0 + 8u * (uint32_t)b);  // the even CTA may reuse buffer b
       unsigned long long key =
@@ -1616,22 +2200,42 @@ static int auto_split(int tiles, int KB, int cap) {
   return sp;
 }
 
-template <int PREC, int ROWB, int BN>
+// The operand-generation fields of the contraction's arguments.
+static void set_gen_args(GemmArgs& a, const TcGeom& g, void* ws) {
+  a.wx = ws_at<float2>(ws, g.off_wx);
+  a.xy = ws_at<int2>(ws, g.off_xy);
+  a.ph = ws_at<float2>(ws, g.off_ph);
+  a.cxy = ws_at<int2>(ws, g.off_cxy);
+  a.thdr = ws_at<int>(ws, g.off_thdr);
+  a.exc = ws_at<float2>(ws, g.off_exc);
+  a.eyc = ws_at<float2>(ws, g.off_eyc);
+  a.Kh = g.Kpad / 2;
+  a.K_c = g.K_c;
+  a.P = g.P;
+}
+
+template <int PREC, int ROWB, int BN, bool GEN>
 static int launch_gemm_v(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s,
                          const UnevenTabs* U, int split) {
   using C = GemmCfg<PREC, ROWB, BN>;
   void* bhi = ws_at<void>(ws, g.off_bhi);
   void* blo = ws_at<void>(ws, g.off_blo);
-  void* ahi = ws_at<void>(ws, g.off_ahi);
-  void* alo = ws_at<void>(ws, g.off_alo);
   CUtensorMap mAhi, mAlo, mBhi, mBlo;
-  int st = make_map(&mAhi, ahi, g.elem, g.Kpad, g.Mpad, C::kBM, ROWB, C::kScaled);
-  if (st == B200D2_OK) st = make_map(&mAlo, alo, g.elem, g.Kpad, g.Mpad, C::kBM, ROWB, C::kScaled);
-  if (st == B200D2_OK) st = make_map(&mBhi, bhi, g.elem, g.Kpad, g.Opad, C::kBN, ROWB, C::kScaled);
+  int st = make_map(&mBhi, bhi, g.elem, g.Kpad, g.Opad, C::kBN, ROWB, C::kScaled);
   if (st == B200D2_OK) st = make_map(&mBlo, blo, g.elem, g.Kpad, g.Opad, C::kBN, ROWB, C::kScaled);
+  if (GEN) {  // no A planes; the kernel does not read these maps
+    mAhi = mBhi;
+    mAlo = mBlo;
+  } else {
+    if (st == B200D2_OK)
+      st = make_map(&mAhi, ws_at<void>(ws, g.off_ahi), g.elem, g.Kpad, g.Mpad, C::kBM, ROWB, C::kScaled);
+    if (st == B200D2_OK)
+      st = make_map(&mAlo, ws_at<void>(ws, g.off_alo), g.elem, g.Kpad, g.Mpad, C::kBM, ROWB, C::kScaled);
+  }
   if (st != B200D2_OK) return st;
   const int wl = BN == 256 ? 0 : 1;  // work list of this tile width
   GemmArgs a;
+  memset(&a, 0, sizeof(a));
   a.Mrows = g.Mrows;
   a.Mtiles = g.Mpad / C::kBM;
   a.Ntiles = g.Opad / C::kBN;
@@ -1667,32 +2271,42 @@ static int launch_gemm_v(const b200d2_batch& b, const TcGeom& g, void* ws, cudaS
   a.cnt = ws_at<unsigned>(ws, g.off_cnt);
   a.L = Layout{U ? U->parts : nullptr, U ? U->rows : nullptr, U ? U->tiles[wl] : nullptr, U ? U->ntiles[wl] : 0};
   a.wait_ns = g_wait_ns.load() ? g_wait_ns.load() : kWaitLimitNs;
+  set_gen_args(a, g, ws);
+  constexpr int kSmem = gemm_smem_bytes<C, GEN>();
   // the shared-memory opt-in is a per-device function attribute
   static std::atomic<unsigned long long> attr_dev{0};
   int dev = 0;
   B200D2_CUDA_TRY(cudaGetDevice(&dev));
   const unsigned long long bit = 1ull << (dev & 63);
   if (!(attr_dev.load() & bit)) {
-    B200D2_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<PREC, ROWB, BN>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, C::kSmem));
+    B200D2_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<PREC, ROWB, BN, GEN>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
     attr_dev.fetch_or(bit);
   }
   const long long items = (long long)tiles * a.split;
   const int grid = (int)std::max(1LL, std::min(items, (long long)num_sms()));
-  tc_gemm_kernel<PREC, ROWB, BN><<<grid, kGemmThreads, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
+  tc_gemm_kernel<PREC, ROWB, BN, GEN><<<grid, GEN ? kGemmThreadsGen : kGemmThreads, kSmem, s>>>(mAhi, mAlo, mBhi,
+                                                                                                  mBlo, a);
   count_launch();
   return status_from_cuda(cudaGetLastError());
 }
 
-template <int PREC, int ROWB>
+template <int PREC, int ROWB, bool GEN>
 static int launch_gemm_pair(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStream_t s,
                             const UnevenTabs* U) {
   using C = GemmCfgPair<PREC, ROWB>;
   CUtensorMap mAhi, mAlo, mBhi, mBlo;
-  int st = make_map(&mAhi, ws_at<void>(ws, g.off_ahi), g.elem, g.Kpad, g.Mpad, 128, ROWB, C::kScaled);
-  if (st == B200D2_OK) st = make_map(&mAlo, ws_at<void>(ws, g.off_alo), g.elem, g.Kpad, g.Mpad, 128, ROWB, C::kScaled);
-  if (st == B200D2_OK) st = make_map(&mBhi, ws_at<void>(ws, g.off_bhi), g.elem, g.Kpad, g.Opad, 128, ROWB, C::kScaled);
+  int st = make_map(&mBhi, ws_at<void>(ws, g.off_bhi), g.elem, g.Kpad, g.Opad, 128, ROWB, C::kScaled);
   if (st == B200D2_OK) st = make_map(&mBlo, ws_at<void>(ws, g.off_blo), g.elem, g.Kpad, g.Opad, 128, ROWB, C::kScaled);
+  if (GEN) {  // no A planes; the kernel does not read these maps
+    mAhi = mBhi;
+    mAlo = mBlo;
+  } else {
+    if (st == B200D2_OK)
+      st = make_map(&mAhi, ws_at<void>(ws, g.off_ahi), g.elem, g.Kpad, g.Mpad, 128, ROWB, C::kScaled);
+    if (st == B200D2_OK)
+      st = make_map(&mAlo, ws_at<void>(ws, g.off_alo), g.elem, g.Kpad, g.Mpad, 128, ROWB, C::kScaled);
+  }
   if (st != B200D2_OK) return st;
   GemmArgs a;
   memset(&a, 0, sizeof(a));
@@ -1723,19 +2337,22 @@ static int launch_gemm_pair(const b200d2_batch& b, const TcGeom& g, void* ws, cu
   a.inv_sb = ws_at<float>(ws, g.off_sb);
   a.L = Layout{U ? U->parts : nullptr, U ? U->rows : nullptr, U ? U->tiles[2] : nullptr, U ? U->ntiles[2] : 0};
   a.wait_ns = kWaitLimitNs;  // the pair kernel's waits are not shortened (see b200d2_set_wait_limit_ns)
+  set_gen_args(a, g, ws);
+  constexpr int kSmem = gemm_smem_bytes<C, GEN>();
   static std::atomic<unsigned long long> attr_dev{0};
   int dev = 0;
   B200D2_CUDA_TRY(cudaGetDevice(&dev));
   const unsigned long long bit = 1ull << (dev & 63);
   if (!(attr_dev.load() & bit)) {
-    B200D2_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_pair_kernel<PREC, ROWB>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, C::kSmem));
+    B200D2_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_pair_kernel<PREC, ROWB, GEN>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
     attr_dev.fetch_or(bit);
   }
   const int tiles = U ? U->ntiles[2] : a.Mtiles * a.Ntiles;
   if (tiles == 0) return B200D2_OK;
   const int pairs = std::max(1, std::min(tiles, num_sms() / 2));
-  tc_gemm_pair_kernel<PREC, ROWB><<<2 * pairs, kGemmThreads, C::kSmem, s>>>(mAhi, mAlo, mBhi, mBlo, a);
+  tc_gemm_pair_kernel<PREC, ROWB, GEN><<<2 * pairs, GEN ? kGemmThreadsGen : kGemmThreads, kSmem, s>>>(
+      mAhi, mAlo, mBhi, mBlo, a);
   count_launch();
   return status_from_cuda(cudaGetLastError());
 }
@@ -1756,17 +2373,28 @@ static int launch_gemm(const b200d2_batch& b, const TcGeom& g, void* ws, cudaStr
     pair = (long long)((g.Mpad + 255) / 256) * (g.Opad / 256) >= num_sms() / 2;
   if (pair && (var.bn <= 0 || var.bn == 256) && var.split <= 1) {
     const int prb = var.row_bytes > 0 ? var.row_bytes : 128;
-    return prb == 128 ? launch_gemm_pair<PREC, 128>(b, g, ws, s, U) : launch_gemm_pair<PREC, 64>(b, g, ws, s, U);
+    if (g.gen)
+      return prb == 128 ? launch_gemm_pair<PREC, 128, true>(b, g, ws, s, U)
+                        : launch_gemm_pair<PREC, 64, true>(b, g, ws, s, U);
+    return prb == 128 ? launch_gemm_pair<PREC, 128, false>(b, g, ws, s, U)
+                      : launch_gemm_pair<PREC, 64, false>(b, g, ws, s, U);
   }
   const int rb = var.row_bytes > 0 ? var.row_bytes : gemm_row_bytes();
   // uniform batches too small for CTA pairs: 128-wide tiles while they still
   // fit in one wave (twice the CTAs; at C1 31 instead of 41 us)
   if (var.bn <= 0 && !U && (long long)(g.Mpad / 128) * ((g.Opad + 127) / 128) <= num_sms()) var.bn = 128;
+  if (g.gen) {
+    if (var.bn == 128)
+      return rb == 128 ? launch_gemm_v<PREC, 128, 128, true>(b, g, ws, s, U, var.split)
+                       : launch_gemm_v<PREC, 64, 128, true>(b, g, ws, s, U, var.split);
+    return rb == 128 ? launch_gemm_v<PREC, 128, 256, true>(b, g, ws, s, U, var.split)
+                     : launch_gemm_v<PREC, 64, 256, true>(b, g, ws, s, U, var.split);
+  }
   if (var.bn == 128)
-    return rb == 128 ? launch_gemm_v<PREC, 128, 128>(b, g, ws, s, U, var.split)
-                     : launch_gemm_v<PREC, 64, 128>(b, g, ws, s, U, var.split);
-  return rb == 128 ? launch_gemm_v<PREC, 128, 256>(b, g, ws, s, U, var.split)
-                   : launch_gemm_v<PREC, 64, 256>(b, g, ws, s, U, var.split);
+    return rb == 128 ? launch_gemm_v<PREC, 128, 128, false>(b, g, ws, s, U, var.split)
+                     : launch_gemm_v<PREC, 64, 128, false>(b, g, ws, s, U, var.split);
+  return rb == 128 ? launch_gemm_v<PREC, 128, 256, false>(b, g, ws, s, U, var.split)
+                   : launch_gemm_v<PREC, 64, 256, false>(b, g, ws, s, U, var.split);
 }
 
 template <int PREC>
@@ -1804,6 +2432,13 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       count_launch();
       tc_phase2d_kernel<<<dim3((g.Kpad / 2 + 255) / 256, std::min(g.T, 65535)), 256, 0, s>>>(
           ex, ey, xy, g.K_c, g.Kpad / 2, g.T, g.maxR, ph);
+      if (g.gen) {
+        count_launch();
+        tc_phase_compact_kernel<<<1, kCompactThreads, 0, s>>>(
+            b.d_trans_x, b.d_trans_y, U ? U->tab_txy : nullptr, g.T, xy, g.K_c, ex, ey, g.maxR,
+            ws_at<int2>(ws, g.off_cxy), ws_at<int>(ws, g.off_thdr), ws_at<float2>(ws, g.off_exc),
+            ws_at<float2>(ws, g.off_eyc), kGenTabEntries);
+      }
       if (kScaled) {  // the particle scales, needed by stage 5 on the same stream
         count_launch();
         tc_scale_a_kernel<<<g.P, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, parts, idx, g.K_c,
@@ -1824,7 +2459,8 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
     }
     case 3:
       tc_normx_kernel<<<g.P, 256, 0, s>>>(b.d_real, b.d_imag, b.d_corr, b.img_stride, g.N_img, normx, parts,
-                                          idx, g.K_c, g.Kq, wcomp);
+                                          idx, g.K_c, g.Kq, wcomp, ws_at<float2>(ws, g.off_wx),
+                                          kScaled ? inv_sa : nullptr);
       break;
     case 4: {
       // the largest tile (particles x orientations: 64 x 64, 32 x 64, 16 x 64,
@@ -1845,6 +2481,7 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       break;
     }
     case 5: {
+      if (g.gen) return B200D2_OK;  // A is generated inside the contraction
       // one thread per four complex pixels of a row; warps spread evenly over
       // at most 8-warp blocks; kGenRows rows per block (Mpad is a multiple of 128)
       const int Kh = g.Kpad / 2, warps = (Kh / kGenV + 31) / 32;
@@ -1872,9 +2509,13 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
   return status_from_cuda(cudaGetLastError());
 }
 
+const char* tc_stage_name(int precision, int stage);
+
 static int dispatch_stage(const b200d2_view& v, const b200d2_batch& b, int prec, const TcGeom& g, void* ws,
                           int stage, cudaStream_t s, const UnevenTabs* U = nullptr,
                           GemmVariant var = GemmVariant()) {
+  const char* name = tc_stage_name(prec, stage);
+  NvtxRange range(name ? name : "b200d2 stage");
   switch (prec) {
     case B200D2_PREC_BF16X3: return launch_stage<B200D2_PREC_BF16X3>(v, b, g, ws, stage, s, U, var);
     case B200D2_PREC_TF32X3: return launch_stage<B200D2_PREC_TF32X3>(v, b, g, ws, stage, s, U, var);
@@ -1901,9 +2542,9 @@ const char* tc_stage_name(int precision, int stage) {
   static const char* tf1[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_kernel<tf32>",
                               "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<tf32>",
                               "tc_gemm[_pair]_kernel<tf32>", "tc_finalize_kernel"};
-  // stage 1 also launches tc_phase2d_kernel (and, in the FP16 forms,
-  // tc_scale_a_kernel); in the FP16 forms stage 2 is the two-pass
-  // tc_project_scaled_kernel
+  // stage 1 also launches tc_phase2d_kernel, tc_phase_compact_kernel (when
+  // the contraction generates A) and, in the FP16 forms, tc_scale_a_kernel;
+  // in the FP16 forms stage 2 is the two-pass tc_project_scaled_kernel
   static const char* h3[] = {"tc_pixel_list_kernel", "tc_phase_kernel", "tc_project_scaled_kernel<fp16x3>",
                              "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<fp16x3>",
                              "tc_gemm[_pair]_kernel<fp16x3>", "tc_finalize_kernel"};
@@ -1911,6 +2552,8 @@ const char* tc_stage_name(int precision, int stage) {
                              "tc_normx_kernel", "tc_norma_kernel", "tc_gen_a_kernel<fp16>",
                              "tc_gemm[_pair]_kernel<fp16>", "tc_finalize_kernel"};
   if (stage < 0 || stage >= kNumStages) return nullptr;
+  // with the operand generated inside the contraction, stage 5 launches nothing
+  if (stage == 5 && is_tc_precision(precision) && g_operand_gen.load()) return "(A operand: generated in the contraction)";
   if (precision == B200D2_PREC_BF16X3) return bf16[stage];
   if (precision == B200D2_PREC_TF32X3) return tf3[stage];
   if (precision == B200D2_PREC_TF32) return tf1[stage];
@@ -1970,6 +2613,7 @@ static int side_for(cudaStream_t user, SidePair* out) {
 
 int tc_run(const b200d2_view& v, const b200d2_batch& b, int precision, void* ws, size_t ws_bytes,
            cudaStream_t s) {
+  NvtxRange range("b200d2_diff2_coarse_batch");
   int st = check_tc(v, b);
   if (st != B200D2_OK) return st;
   const TcGeom g = make_geom(v, b, precision);
@@ -2443,6 +3087,7 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
 
 extern "C" int b200d2_plan_run(b200d2_plan* p, void* stream) {
   if (!p) return B200D2_ERR_INVALID;
+  b200d2::NvtxRange range("b200d2_plan_run");
   cudaStream_t s = (cudaStream_t)stream;
   if (p->exec) {
     B200D2_CUDA_TRY(cudaGraphLaunch(p->exec, s));
@@ -2494,5 +3139,11 @@ extern "C" int b200d2_set_combine(int mode) {
 
 extern "C" int b200d2_set_wait_limit_ns(unsigned long long ns) {
   b200d2::g_wait_ns.store(ns);
+  return B200D2_OK;
+}
+
+extern "C" int b200d2_set_operand_gen(int mode) {
+  if (mode != 0 && mode != 1) return B200D2_ERR_INVALID;
+  b200d2::g_operand_gen.store(mode);
   return B200D2_OK;
 }

@@ -54,6 +54,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+// try_wait that may suspend the thread for up to `hint_ns` (instead of the
+// system-dependent limit) until the phase completes: a waiting warp then
+// leaves its scheduler's issue slots to the warps that work.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
+// Suspend hint of the slow path of the bounded waits (ns); short against
+// the 4 s limit, long against a k-block.
+constexpr uint32_t kWaitSleepNs = 20000;
+
 __device__ __forceinline__ uint64_t globaltimer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -69,9 +88,24 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
                                                   volatile uint32_t* abort, uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
+  const uint32_t hint = limit_ns < kWaitSleepNs ? (uint32_t)limit_ns : kWaitSleepNs;
   while (true) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait_sleep(bar, parity, hint)) return true;
     if (*abort) return false;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
+  }
+}
+
+// Drain wait: for work this thread itself started (copies or MMAs in flight)
+// that must finish before shared or tensor memory is released.  Unlike
+// mbar_wait_bounded it ignores the abort flag, so that a give-up elsewhere
+// cannot release memory that is still being written; it returns false only
+// after `limit_ns`.
+__device__ __forceinline__ bool mbar_wait_drain(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  while (true) {
+    if (mbar_try_wait_sleep(bar, parity, kWaitSleepNs)) return true;
     if (globaltimer_ns() - t0 > limit_ns) return false;
   }
 }
