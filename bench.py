@@ -650,13 +650,16 @@ def ours_arm(args):
             return a.elapsed_time(b) / reps
 
         ms_tc = per_call(lambda: pkg.diff2_coarse_batch(view, b1, prec, ws1, stream))
+        ms_drop_tc = per_call(lambda: pkg.run_diff2_kernel_coarse(view, tx, ty, corr[0], re[0], im[0], eul, o32, O, T,
+                                                                  N, stream=stream, precision=prec))
         ms_fp32 = per_call(lambda: pkg.run_diff2_kernel_coarse(view, tx, ty, corr[0], re[0], im[0], eul, o32, O, T, N,
                                                                stream=stream))
-        single = {"batch_api_ms_per_particle": ms_tc, "fp32_dropin_ms_per_particle": ms_fp32,
-                  "evals_per_particle": O * T,
-                  "note": f"one particle per call, {args.precision} batch entry point (all stages: projection, "
-                          "norms, contraction) and the FP32 runDiff2KernelCoarse drop-in; back-to-back calls, "
-                          "CUDA events"}
+        single = {"batch_api_ms_per_particle": ms_tc, "dropin_tensor_core_ms_per_particle": ms_drop_tc,
+                  "fp32_dropin_ms_per_particle": ms_fp32, "evals_per_particle": O * T,
+                  "note": f"one particle per call: the {args.precision} batch entry point and the "
+                          f"runDiff2KernelCoarse signature (b200d2_diff2_coarse) with {args.precision} (all stages: "
+                          "projection, norms, contraction; library-owned workspace) or FP32 CUDA cores; "
+                          "back-to-back calls, CUDA events"}
         del ws1, o1, o32
 
     # ---- the same batch with the A operand generated inside the contraction ----

@@ -130,7 +130,14 @@ int b200d2_project_pixels(const b200d2_view* view, const float* d_eulers,
  * exactly as the reference does (src/diff2.cuh:533-536).  d_eulers holds 9
  * floats per orientation (row-major 3x3); image arrays hold N_img half-plane
  * pixels in pixel_index2coor order.  corr must be >= 0.
- * precision: B200D2_PREC_FP32 (FP32 CUDA cores).
+ * precision: B200D2_PREC_FP32 (FP32 CUDA cores, within 1e-5 of the
+ * reference's own kernel), or a tensor-core precision: the particle then runs
+ * through the batch pipeline (projection, FP64 norms, tcgen05 contraction)
+ * on a workspace the library owns, one per (device, stream), allocated with
+ * cudaMallocAsync on `stream` when first needed and grown the same way (the
+ * first call per stream, and a larger problem, allocate).  At C2 sizes (4608
+ * orientations x 113 translations, image 64) BF16x3 takes 0.18 ms per
+ * particle against 0.45 ms for the FP32 kernel.
  * ---------------------------------------------------------------------- */
 int b200d2_diff2_coarse(const b200d2_view* view, const float* d_trans_x,
                         const float* d_trans_y, const float* d_corr,

@@ -158,9 +158,25 @@ class AccProjectorKernel {
   }
 };
 
-// diff2s[o*T + t] += diff2(o, t)  (FP32 CUDA cores, asynchronous on `stream`);
-// with do_CC, diff2s[o*T + t] = -cross / sqrt(norm) as cuda_kernel_diff2_CC_coarse
-// (src/diff2.cuh:691-809) writes it.
+// Precision of runDiff2KernelCoarse's non-CC branch, process-wide:
+// B200D2_PREC_FP32 (default: FP32 CUDA cores, within 1e-5 of the reference's
+// own kernel) or a tensor-core precision (the one-particle tensor-core
+// pipeline on a library-owned workspace; B200D2_PREC_BF16X3 stays within 1e-5
+// of the FP64 kernel).  Returns the previous setting.
+inline int setCoarsePrecision(int precision) {
+  static int p = B200D2_PREC_FP32;
+  const int old = p;
+  if (precision >= 0) p = precision;
+  return old;
+}
+inline int coarsePrecision() {
+  const int p = setCoarsePrecision(-1);
+  return p;
+}
+
+// diff2s[o*T + t] += diff2(o, t)  (asynchronous on `stream`, in the precision
+// set by setCoarsePrecision); with do_CC, diff2s[o*T + t] = -cross / sqrt(norm)
+// as cuda_kernel_diff2_CC_coarse (src/diff2.cuh:691-809) writes it.
 inline void runDiff2KernelCoarse(AccProjectorKernel& projector, XFLOAT* trans_x, XFLOAT* trans_y,
                                  XFLOAT* /*trans_z*/, XFLOAT* corr_img, XFLOAT* Fimg_real, XFLOAT* Fimg_imag,
                                  XFLOAT* d_eulers, XFLOAT* diff2s, XFLOAT /*local_sqrtXi2*/,
@@ -176,7 +192,7 @@ inline void runDiff2KernelCoarse(AccProjectorKernel& projector, XFLOAT* trans_x,
   }
   b200d2_relion_detail::check(
       b200d2_diff2_coarse(&projector.view, trans_x, trans_y, corr_img, Fimg_real, Fimg_imag, d_eulers, diff2s,
-                          orientation_num, translation_num, image_size, stream, B200D2_PREC_FP32),
+                          orientation_num, translation_num, image_size, stream, coarsePrecision()),
       "runDiff2KernelCoarse");
 }
 

@@ -5,6 +5,10 @@
 // its harness loops runDiff2KernelCoarse over particles (src/main.cu:483-503).
 #include <cuda_runtime.h>
 
+#include <cstring>
+#include <mutex>
+#include <vector>
+
 #include "common.cuh"
 
 namespace b200d2 {
@@ -39,6 +43,73 @@ static int validate(const b200d2_view* v, const b200d2_batch* b) {
 
 static unsigned long long g_launches = 0;
 void count_launch(unsigned n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
+
+// Workspaces owned by the library for the single-particle entry point with a
+// tensor-core precision, whose signature (runDiff2KernelCoarse's) carries
+// none: one per (device, stream), allocated and grown stream-ordered
+// (cudaMallocAsync / cudaFreeAsync on that stream, so calls queued on the
+// stream before the growth finish with the old buffer), kept until the
+// process exits.
+struct OwnedWorkspace {
+  int device;
+  cudaStream_t stream;
+  void* ptr;
+  size_t bytes;
+};
+static std::mutex g_owned_mu;
+static std::vector<OwnedWorkspace> g_owned;
+
+static int owned_workspace(cudaStream_t s, size_t need, void** out) {
+  int dev = 0;
+  B200D2_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_owned_mu);
+  for (OwnedWorkspace& w : g_owned)
+    if (w.device == dev && w.stream == s) {
+      if (w.bytes < need) {
+        B200D2_CUDA_TRY(cudaFreeAsync(w.ptr, s));
+        w.ptr = nullptr;
+        w.bytes = 0;
+        B200D2_CUDA_TRY(cudaMallocAsync(&w.ptr, need, s));
+        w.bytes = need;
+      }
+      *out = w.ptr;
+      return B200D2_OK;
+    }
+  OwnedWorkspace w{dev, s, nullptr, need};
+  B200D2_CUDA_TRY(cudaMallocAsync(&w.ptr, need, s));
+  g_owned.push_back(w);
+  *out = w.ptr;
+  return B200D2_OK;
+}
+
+// One particle through the tensor-core pipeline, accumulating onto diff2s as
+// the reference's runDiff2KernelCoarse does.
+int single_particle_tc(const b200d2_view& v, const float* tx, const float* ty, const float* corr, const float* re,
+                       const float* im, const float* eulers, float* diff2s, int O, int T, int N_img, int precision,
+                       cudaStream_t s) {
+  b200d2_batch b;
+  memset(&b, 0, sizeof(b));
+  b.d_eulers = eulers;
+  b.O = O;
+  b.d_trans_x = tx;
+  b.d_trans_y = ty;
+  b.T = T;
+  b.P = 1;
+  b.N_img = N_img;
+  b.d_real = re;
+  b.d_imag = im;
+  b.d_corr = corr;
+  b.img_stride = N_img;
+  b.d_diff2 = diff2s;
+  b.accumulate = 1;
+  int st = validate(&v, &b);
+  if (st != B200D2_OK) return st;
+  const size_t need = tc_workspace_bytes(v, b, precision);
+  void* ws = nullptr;
+  st = owned_workspace(s, need, &ws);
+  if (st != B200D2_OK) return st;
+  return tc_run(v, b, precision, ws, need, s);
+}
 
 }  // namespace b200d2
 

@@ -360,6 +360,12 @@ int direct_batch(const b200d2_view& view, const float* eulers, const float* tx,
 
 }  // namespace b200d2
 
+namespace b200d2 {
+int single_particle_tc(const b200d2_view& v, const float* tx, const float* ty, const float* corr, const float* re,
+                       const float* im, const float* eulers, float* diff2s, int O, int T, int N_img, int precision,
+                       cudaStream_t s);
+}  // namespace b200d2
+
 extern "C" int b200d2_diff2_coarse(const b200d2_view* view,
                                    const float* d_trans_x,
                                    const float* d_trans_y, const float* d_corr,
@@ -371,6 +377,11 @@ extern "C" int b200d2_diff2_coarse(const b200d2_view* view,
   int st = b200d2::check_common(view, d_trans_x, d_trans_y, d_corr, d_real,
                                 d_imag, d_eulers, d_diff2s, O, T, N_img);
   if (st != B200D2_OK) return st;
+  if (b200d2::is_tc_precision(precision)) {
+    if (O > 0x7fffffff || T > 0x7fffffff || N_img > 0x7fffffff) return B200D2_ERR_UNSUPPORTED;
+    return b200d2::single_particle_tc(*view, d_trans_x, d_trans_y, d_corr, d_real, d_imag, d_eulers, d_diff2s,
+                                      (int)O, (int)T, (int)N_img, precision, (cudaStream_t)stream);
+  }
   if (precision != B200D2_PREC_FP32) return B200D2_ERR_UNSUPPORTED;
   return b200d2::direct_batch(*view, d_eulers, d_trans_x, d_trans_y, d_real,
                               d_imag, d_corr, 0, d_diff2s, 0, (int)O, (int)T,

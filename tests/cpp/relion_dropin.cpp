@@ -80,6 +80,12 @@ int main(int argc, char** argv) {
 
     runDiff2KernelCoarse(k, d_trans, d_trans + T, nullptr, d_corr, d_fimg, d_fimg + N, d_eul, d_out32, 1.f, O, T,
                          N, stream, false, false);
+    // the same call with the tensor-core pipeline behind it (BF16x3)
+    float* d_outbf = to_device(diff2s);
+    const int prev = setCoarsePrecision(B200D2_PREC_BF16X3);
+    runDiff2KernelCoarse(k, d_trans, d_trans + T, nullptr, d_corr, d_fimg, d_fimg + N, d_eul, d_outbf, 1.f, O, T,
+                         N, stream, false, false);
+    setCoarsePrecision(prev);
     runDiff2KernelCoarseDouble(k, d_trans, d_trans + T, nullptr, d_corr, d_fimg, d_fimg + N, d_eul, d_out64, 1.f,
                                O, T, N, stream, false, false);
 
@@ -123,19 +129,21 @@ int main(int argc, char** argv) {
     const auto o32 = to_host(d_out32, n);
     const auto o64 = to_host(d_out64, n);
     const auto otc = to_host(d_outtc, n);
+    const auto obf = to_host(d_outbf, n);
     const auto occ = to_host(d_cc, n);
     const auto occ64 = to_host(d_cc64, n);
-    const double e32 = max_rel(o32, o64), etc = max_rel(otc, o64), ecc = max_rel(occ, occ64);
+    const double e32 = max_rel(o32, o64), etc = max_rel(otc, o64), ecc = max_rel(occ, occ64),
+                 ebf = max_rel(obf, o64);
     std::printf("{\"O\": %d, \"T\": %d, \"N_img\": %d, \"filtered\": %d, \"workspace_bytes\": %zu, "
                 "\"fp32_vs_fp64_max_rel\": %.3e, \"functor_vs_fp64_max_rel\": %.3e, "
-                "\"cc_fp32_vs_fp64_max_rel\": %.3e}\n",
-                O, T, N, ps, wsb, e32, etc, ecc);
+                "\"cc_fp32_vs_fp64_max_rel\": %.3e, \"bf16x3_dropin_vs_fp64_max_rel\": %.3e}\n",
+                O, T, N, ps, wsb, e32, etc, ecc, ebf);
     for (void* p : {(void*)d_eul, (void*)d_trans, (void*)d_fimg, (void*)d_corr, (void*)d_out32, (void*)d_out64,
                     (void*)d_fre, (void*)d_fim, (void*)d_fco, (void*)d_cxy, (void*)d_outtc, (void*)d_ws,
-                    (void*)d_cc, (void*)d_cc64})
+                    (void*)d_cc, (void*)d_cc64, (void*)d_outbf})
       cudaFree(p);
     cudaStreamDestroy(stream);
-    return (e32 <= 1e-5 && etc <= 1e-5 && ecc <= 1e-5) ? 0 : 1;
+    return (e32 <= 1e-5 && etc <= 1e-5 && ecc <= 1e-5 && ebf <= 1e-5) ? 0 : 1;
   } catch (const std::exception& e) {
     std::fprintf(stderr, "error: %s\n", e.what());
     return 3;

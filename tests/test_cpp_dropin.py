@@ -48,4 +48,5 @@ def test_cpp_caller_runs_on_dat_files(pkg, synth, cuda, tmp_path):
     res = json.loads(r.stdout.strip().splitlines()[-1])
     assert res["fp32_vs_fp64_max_rel"] <= 1e-5
     assert res["functor_vs_fp64_max_rel"] <= 1e-5
+    assert res["bf16x3_dropin_vs_fp64_max_rel"] <= 1e-5  # runDiff2KernelCoarse on the tensor cores
     assert res["cc_fp32_vs_fp64_max_rel"] <= 1e-5  # runDiff2KernelCoarse with do_CC

@@ -150,3 +150,32 @@ def test_empty_problem_is_noop(pkg, cuda, c1):
                                 pr.N_img)
     cuda.cuda.synchronize()
     assert out.cpu().tolist() == [7.0] * 4
+
+
+@pytest.mark.parametrize("prec_name", ["bf16x3", "tf32x3"])
+def test_single_particle_entry_point_on_tensor_cores(pkg, synth, oracle, cuda, prec_name):
+    """runDiff2KernelCoarse's signature (b200d2_diff2_coarse) with a
+    tensor-core precision: the particle runs through the batch pipeline on a
+    library-owned workspace (one per device and stream, allocated and grown
+    stream-ordered) and accumulates onto the caller's buffer like the
+    reference.  A C1 particle, then a larger C2 particle on the same stream
+    (the workspace grows), then the C1 particle on a second stream: each
+    within 1e-5 of the FP64 kernel."""
+    torch = cuda
+    prec = {"bf16x3": pkg.PREC_BF16X3, "tf32x3": pkg.PREC_TF32X3}[prec_name]
+    s2 = torch.cuda.Stream()
+    for name, stream in (("c1", None), ("c2", None), ("c1", s2)):
+        pr = synth.make_problem(name, P=1)
+        proj = pkg.Projector(pr.projector, use_texture=1)
+        view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+        dp = DeviceProblem(torch, pr)
+        init = np.random.default_rng(5).uniform(0, 100, (pr.O, pr.T)).astype(np.float32)
+        out = torch.as_tensor(init.reshape(-1), device="cuda").clone()
+        torch.cuda.synchronize()
+        pkg.run_diff2_kernel_coarse(view, dp.tx, dp.ty, dp.corr[0], dp.re[0], dp.im[0], dp.eulers, out, pr.O, pr.T,
+                                    pr.N_img, stream=stream, precision=prec)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy().reshape(pr.O, pr.T).astype(np.float64) - init
+        ref = ours_f64(pkg, view, dp, 0)
+        assert oracle.error_stats(got, ref)["max_rel"] <= 2e-5, (name, prec_name)
+        proj.close()
