@@ -708,29 +708,45 @@ def ours_arm(args):
         # images cross PCIe on a copy stream while step k computes; every
         # step's inputs are copied from pinned memory and its min/argmin read
         # back inside the timed region
-        re2, im2, corr2 = torch.empty_like(re), torch.empty_like(im), torch.empty_like(corr)
-        batch2 = pkg.make_batch(eul, tx, ty, re2, im2, corr2, out, O=O, T=T, P=P, N_img=N, out_min=mn,
-                                out_argmin=am)
-        sets = [(re, im, corr, batch), (re2, im2, corr2, batch2)]
+        # a step's images, imaginary parts and weights travel in one copy
+        # (one pinned buffer [3][P][N]) and its minimum and argmin come back in
+        # one (one device buffer [2][P] of 8-byte words), as a caller that
+        # packs its transfers would run it
+        h_pack = torch.empty((3, P, N), dtype=torch.float32).pin_memory()
+        h_pack[0].copy_(h_re)
+        h_pack[1].copy_(h_im)
+        h_pack[2].copy_(h_corr)
+        h_res = torch.empty(2 * P, dtype=torch.float64).pin_memory()
+        packs, res, sets = [], [], []
+        for _ in range(2):
+            d_pack = torch.empty((3, P, N), device=dev, dtype=torch.float32)
+            d_res = torch.empty(2 * P, device=dev, dtype=torch.float64)
+            bk = pkg.make_batch(eul, tx, ty, d_pack[0], d_pack[1], d_pack[2], out, O=O, T=T, P=P, N_img=N,
+                                out_min=d_res[:P], out_argmin=d_res[P:].view(torch.int64))
+            packs.append(d_pack)
+            res.append(d_res)
+            sets.append((d_pack, d_res, bk))
         copy_stream = torch.cuda.Stream(device=dev)
         ready = [torch.cuda.Event() for _ in range(2)]
         free = [torch.cuda.Event() for _ in range(2)]
+        for _ in range(2):  # each signature's first call and graph capture happen outside the timed region
+            for d_pack, d_res, bk in sets:
+                d_pack.copy_(h_pack)
+                pkg.diff2_coarse_batch(view, bk, prec, ws, stream)
+        torch.cuda.synchronize()
         e0.record(stream)
         copy_stream.wait_event(e0)
         for k in range(e2e_steps):
-            d_re, d_im, d_corr, bk = sets[k % 2]
+            d_pack, d_res, bk = sets[k % 2]
             with torch.cuda.stream(copy_stream):
                 if k >= 2:
                     copy_stream.wait_event(free[k % 2])
-                d_re.copy_(h_re, non_blocking=True)
-                d_im.copy_(h_im, non_blocking=True)
-                d_corr.copy_(h_corr, non_blocking=True)
+                d_pack.copy_(h_pack, non_blocking=True)
                 ready[k % 2].record(copy_stream)
             stream.wait_event(ready[k % 2])
             pkg.diff2_coarse_batch(view, bk, prec, ws, stream)
             free[k % 2].record(stream)
-            h_mn.copy_(mn, non_blocking=True)
-            h_am.copy_(am, non_blocking=True)
+            h_res.copy_(d_res, non_blocking=True)
         e1.record(stream)
     else:
         # the same double buffering for the uneven batch: a second plan over a
@@ -796,8 +812,8 @@ def ours_arm(args):
         def sig_step(k, bk):
             pkg.diff2_coarse_batch(view, bk, prec, ws, stream)
             in_free[k % 2].record(stream)
-            pkg.coarse_weights(out, P, O, T, out_min=mn, normalize=False, weights=W, sums=S, workspace=WW,
-                               stream=stream)
+            pkg.coarse_weights(out, P, O, T, out_min=sets[k % 2][1][:P], normalize=False, weights=W, sums=S,
+                               workspace=WW, stream=stream)
             if k >= 2:
                 stream.wait_event(out_free[k % 2])
             pkg.significance(W.view(P, n), S, frac, 0, passed=masks[k % 2], sig_weight=sigs[k % 2],
@@ -810,7 +826,7 @@ def ours_arm(args):
                 h_nsig[k % 2].copy_(nsigs[k % 2], non_blocking=True)
                 out_free[k % 2].record(out_stream)
 
-        sig_step(0, batch)  # warm-up (weights and significance kernels, pinned buffers)
+        sig_step(0, sets[0][2])  # warm-up (weights and significance kernels, pinned buffers)
         torch.cuda.synchronize()
         s_clocks = ClockSampler(local)
         s_clocks.start()
@@ -818,13 +834,11 @@ def ours_arm(args):
         s0.record(stream)
         copy_stream.wait_event(s0)
         for k in range(e2e_steps):
-            d_re, d_im, d_corr, bk = sets[k % 2]
+            d_pack, d_res, bk = sets[k % 2]
             with torch.cuda.stream(copy_stream):
                 if k >= 2:
                     copy_stream.wait_event(in_free[k % 2])
-                d_re.copy_(h_re, non_blocking=True)
-                d_im.copy_(h_im, non_blocking=True)
-                d_corr.copy_(h_corr, non_blocking=True)
+                d_pack.copy_(h_pack, non_blocking=True)
                 ready[k % 2].record(copy_stream)
             stream.wait_event(ready[k % 2])
             sig_step(k, bk)
@@ -902,9 +916,9 @@ def ours_arm(args):
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_val, "unit": "diff2 evals/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "clocks": e2e_clk,
-                        "note": ("H2D of images+corr from pinned memory, batch call, D2H of per-particle min/argmin, every "
-                          "step; the images are double-buffered (uneven batches: two plans) so that step k+1's "
-                          "copy overlaps step k.  The diff2 block itself "
+                        "note": ("H2D of images+corr from pinned memory (one packed copy), batch call, D2H of per-particle "
+                          "min/argmin (one packed copy), every step; the images are double-buffered (uneven "
+                          "batches: two plans) so that step k+1's copy overlaps step k.  The diff2 block itself "
                           f"({4 * evals_step / 1e6:.0f} MB per step) stays on the device, where the weights and "
                           "significance steps read it; e2e_significance reads their product back")},
                 "e2e_significance": e2e_sig,

@@ -511,6 +511,19 @@ int b200d2_set_combine(int mode);
  * this setting at creation (single-CTA 256-wide tiles when it is 0). */
 int b200d2_set_gemm_variant(int row_bytes, int tile_n, int split, int pair);
 
+/* CUDA graphs of the batch entry point (b200d2_diff2_coarse_batch with a
+ * tensor-core precision), process-wide, on by default: a call's launches are
+ * fixed by its arguments (view, batch fields and device pointers, precision,
+ * workspace, stream, device) and the process-wide settings above, so the
+ * second call with the same arguments captures the pipeline into a graph and
+ * later calls launch that graph, which takes about a tenth of the host time
+ * of the dozen launches and stream waits it replaces.  Input contents may
+ * change between calls; the pointers may not, without making a new
+ * signature.  Up to 32 signatures are kept (least recently used evicted).
+ * Calls made while the caller captures `stream` into its own graph launch
+ * directly.  enable: 1 on, 0 off (every call launches directly). */
+int b200d2_set_batch_graphs(int enable);
+
 /* Run a single stage of the batch pipeline, so that a caller can time one
  * kernel with events on its stream.  Stages are numbered in pipeline order
  * from 0; b200d2_stage_name returns NULL past the last stage of `precision`.

@@ -165,6 +165,7 @@ def _declare(L):
         "b200d2_set_combine": [I],
         "b200d2_set_wait_limit_ns": [C.c_ulonglong],
         "b200d2_set_operand_gen": [I],
+        "b200d2_set_batch_graphs": [I],
         "b200d2_diff2_fine": [C.POINTER(View), P, P, P, P, P, P, P, Z, F, Z, P, P, P, P, P],
         "b200d2_diff2_fine_cc": [C.POINTER(View), P, P, P, P, P, P, P, Z, Z, P, P, P, P, P],
         "b200d2_ctf_fold": [P, P, C.c_longlong, I, I, I, I, I, I, F, P, P, C.c_longlong, P, P, P, P],
@@ -593,6 +594,12 @@ def set_combine(mode: int) -> None:
     """Final combination of the tensor-core forms: COMBINE_DF32 (default,
     double-float) or COMBINE_FP64."""
     _check(lib().b200d2_set_combine(mode), "set_combine")
+
+
+def set_batch_graphs(enable: bool) -> None:
+    """CUDA graphs of the batch entry point (on by default): the second call
+    with the same arguments captures the pipeline, later ones launch it."""
+    _check(lib().b200d2_set_batch_graphs(1 if enable else 0), "set_batch_graphs")
 
 
 def set_operand_gen(mode: int) -> None:

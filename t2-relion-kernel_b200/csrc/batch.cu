@@ -43,6 +43,8 @@ static int validate(const b200d2_view* v, const b200d2_batch* b) {
 
 static unsigned long long g_launches = 0;
 void count_launch(unsigned n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
+unsigned long long launch_counter() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+void uncount_launch(unsigned n) { __atomic_fetch_sub(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
 
 // Workspaces owned by the library for the single-particle entry point with a
 // tensor-core precision, whose signature (runDiff2KernelCoarse's) carries

@@ -2611,13 +2611,11 @@ static int side_for(cudaStream_t user, SidePair* out) {
   return B200D2_OK;
 }
 
-int tc_run(const b200d2_view& v, const b200d2_batch& b, int precision, void* ws, size_t ws_bytes,
-           cudaStream_t s) {
-  NvtxRange range("b200d2_diff2_coarse_batch");
-  int st = check_tc(v, b);
-  if (st != B200D2_OK) return st;
-  const TcGeom g = make_geom(v, b, precision);
-  if (ws_bytes < g.total) return B200D2_ERR_INVALID;
+// The whole pipeline of one batch on stream s (forking to the side stream
+// paired with s and joining back).
+static int tc_launch_pipeline(const b200d2_view& v, const b200d2_batch& b, int precision, const TcGeom& g, void* ws,
+                              cudaStream_t s) {
+  int st = B200D2_OK;
   SidePair sp;
   st = side_for(s, &sp);
   if (st != B200D2_OK) return st;
@@ -2645,6 +2643,147 @@ int tc_run(const b200d2_view& v, const b200d2_batch& b, int precision, void* ws,
   st = dispatch_stage(v, b, precision, g, ws, 6, s);
   if (st == B200D2_OK) st = dispatch_stage(v, b, precision, g, ws, 7, s);
   return st;
+}
+
+// Cached CUDA graphs of the batch pipeline.  A call's launches are fixed by
+// its arguments (view, batch fields and pointers, precision, workspace) and
+// the process-wide settings (contraction variant, combine, operand mode,
+// wait limit) on a given device and stream: the second call with the same
+// signature captures the pipeline once into a graph, later ones launch that
+// graph (one host call instead of about a dozen launches, event records and
+// waits).  Calls whose stream is being captured by the caller run the
+// launches directly, so that they become part of the caller's graph.
+static std::atomic<int> g_batch_graphs{1};  // b200d2_set_batch_graphs
+
+struct BatchGraph {
+  std::vector<uint64_t> key;
+  int seen = 0;
+  unsigned long long last = 0;
+  unsigned launches = 0;  // kernels in the graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+static std::mutex g_graph_mu;
+static std::vector<BatchGraph> g_graphs;
+static unsigned long long g_graph_clock = 0;
+constexpr size_t kMaxBatchGraphs = 32;
+
+static std::vector<uint64_t> batch_key(const b200d2_view& v, const b200d2_batch& b, int precision, const void* ws,
+                                       size_t ws_bytes, cudaStream_t s, int dev) {
+  auto u = [](const void* p) { return (uint64_t)(uintptr_t)p; };
+  auto f = [](float x) {
+    uint32_t r;
+    memcpy(&r, &x, 4);
+    return (uint64_t)r;
+  };
+  return {(uint64_t)dev, u(s), u(ws), (uint64_t)ws_bytes, (uint64_t)precision,
+          // view
+          (uint64_t)v.mdlX, (uint64_t)v.mdlXY, (uint64_t)v.mdlZ, (uint64_t)v.imgX, (uint64_t)v.imgY,
+          (uint64_t)v.imgZ, (uint64_t)(uint32_t)v.mdlInitY, (uint64_t)(uint32_t)v.mdlInitZ, (uint64_t)v.maxR,
+          (uint64_t)v.maxR2, (uint64_t)v.maxR2_padded, f(v.padding_factor), v.tex_re, v.tex_im, u(v.lin_re),
+          u(v.lin_im), (uint64_t)v.interp, v.tex_c,
+          // batch
+          u(b.d_eulers), (uint64_t)b.O, u(b.d_trans_x), u(b.d_trans_y), (uint64_t)b.T, (uint64_t)b.P,
+          (uint64_t)b.N_img, u(b.d_real), u(b.d_imag), u(b.d_corr), (uint64_t)b.img_stride, u(b.d_diff2),
+          (uint64_t)b.accumulate, u(b.d_min), u(b.d_argmin), u(b.d_coor_xy), (uint64_t)b.n_listed,
+          (uint64_t)b.score,
+          // process-wide settings read by the launches
+          (uint64_t)g_var_rb.load(), (uint64_t)g_var_bn.load(), (uint64_t)g_var_split.load(),
+          (uint64_t)g_var_pair.load(), (uint64_t)g_combine64.load(), (uint64_t)g_operand_gen.load(),
+          (uint64_t)g_wait_ns.load()};
+}
+
+// A private capture stream per device.
+static cudaStream_t capture_stream(int dev) {
+  static std::mutex mu;
+  static std::map<int, cudaStream_t> streams;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = streams.find(dev);
+  if (it != streams.end()) return it->second;
+  cudaStream_t cs = nullptr;
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  streams[dev] = cs;
+  return cs;
+}
+
+unsigned long long launch_counter();
+void uncount_launch(unsigned n);
+
+int tc_run(const b200d2_view& v, const b200d2_batch& b, int precision, void* ws, size_t ws_bytes,
+           cudaStream_t s) {
+  NvtxRange range("b200d2_diff2_coarse_batch");
+  int st = check_tc(v, b);
+  if (st != B200D2_OK) return st;
+  const TcGeom g = make_geom(v, b, precision);
+  if (ws_bytes < g.total) return B200D2_ERR_INVALID;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (!g_batch_graphs.load() || cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
+    return tc_launch_pipeline(v, b, precision, g, ws, s);
+  int dev = 0;
+  B200D2_CUDA_TRY(cudaGetDevice(&dev));
+  const std::vector<uint64_t> key = batch_key(v, b, precision, ws, ws_bytes, s, dev);
+  std::unique_lock<std::mutex> lk(g_graph_mu);
+  BatchGraph* e = nullptr;
+  for (BatchGraph& x : g_graphs)
+    if (x.key == key) {
+      e = &x;
+      break;
+    }
+  if (!e) {
+    if (g_graphs.size() >= kMaxBatchGraphs) {  // evict the least recently used signature
+      size_t lru = 0;
+      for (size_t i = 1; i < g_graphs.size(); ++i)
+        if (g_graphs[i].last < g_graphs[lru].last) lru = i;
+      if (g_graphs[lru].exec) cudaGraphExecDestroy(g_graphs[lru].exec);
+      if (g_graphs[lru].graph) cudaGraphDestroy(g_graphs[lru].graph);
+      g_graphs.erase(g_graphs.begin() + (long)lru);
+    }
+    g_graphs.push_back(BatchGraph());
+    e = &g_graphs.back();
+    e->key = key;
+  }
+  e->last = ++g_graph_clock;
+  if (!e->exec && e->seen == 0) {  // first call with this signature: launch directly
+    e->seen = 1;
+    lk.unlock();
+    return tc_launch_pipeline(v, b, precision, g, ws, s);
+  }
+  if (!e->exec) {  // second call: capture once
+    cudaStream_t cs = capture_stream(dev);
+    if (!cs) {
+      lk.unlock();
+      return tc_launch_pipeline(v, b, precision, g, ws, s);
+    }
+    const unsigned long long l0 = launch_counter();
+    st = status_from_cuda(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    if (st == B200D2_OK) {
+      const int st2 = tc_launch_pipeline(v, b, precision, g, ws, cs);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(cs, &graph);
+      st = st2 != B200D2_OK ? st2 : status_from_cuda(ce);
+      if (st == B200D2_OK) st = status_from_cuda(cudaGraphInstantiate(&e->exec, graph, 0));
+      if (st == B200D2_OK) {
+        e->graph = graph;
+      } else if (graph) {
+        cudaGraphDestroy(graph);
+      }
+    }
+    // the launches were counted while capturing; the graph launch below counts them
+    e->launches = (unsigned)(launch_counter() - l0);
+    uncount_launch(e->launches);
+    if (st != B200D2_OK || !e->exec) {  // capture not possible: stay with direct launches
+      e->exec = nullptr;
+      e->seen = 1;
+      lk.unlock();
+      return tc_launch_pipeline(v, b, precision, g, ws, s);
+    }
+  }
+  const cudaError_t le = cudaGraphLaunch(e->exec, s);
+  const unsigned n = e->launches;
+  lk.unlock();
+  if (le != cudaSuccess) return status_from_cuda(le);
+  count_launch(n);
+  return B200D2_OK;
 }
 
 // ------------------------------------------------------------------ plans
@@ -3145,5 +3284,11 @@ extern "C" int b200d2_set_wait_limit_ns(unsigned long long ns) {
 extern "C" int b200d2_set_operand_gen(int mode) {
   if (mode != 0 && mode != 1) return B200D2_ERR_INVALID;
   b200d2::g_operand_gen.store(mode);
+  return B200D2_OK;
+}
+
+extern "C" int b200d2_set_batch_graphs(int enable) {
+  if (enable != 0 && enable != 1) return B200D2_ERR_INVALID;
+  b200d2::g_batch_graphs.store(enable);
   return B200D2_OK;
 }

@@ -300,3 +300,82 @@ def test_bounded_wait_gives_up_and_context_stays_usable(pkg, synth, oracle, cuda
     got = out.cpu().numpy().reshape(pr.P, pr.O, pr.T)
     assert oracle.error_stats(got, ref)["max_rel"] <= TOL["bf16x3"]
     proj.close()
+
+
+def test_batch_graphs_match_direct_launches(pkg, oracle, cuda, c1):
+    """The batch entry point's cached graphs: calls 2.. with the same
+    arguments launch a captured graph of the pipeline.  Outputs are bit
+    identical to direct launches, inputs refilled in place are picked up, a
+    different output buffer is a new signature, the launch count stays the
+    number of kernels, and a caller's own capture of the call still works."""
+    torch = cuda
+    pr, view, dp, ref = c1
+    prec = pkg.PREC_BF16X3
+
+    def run(out, mn, am, stream=None):
+        b = pkg.make_batch(dp.eulers, dp.tx, dp.ty, dp.re, dp.im, dp.corr, out, O=pr.O, T=pr.T, P=pr.P,
+                           N_img=pr.N_img, out_min=mn, out_argmin=am)
+        pkg.diff2_coarse_batch(view, b, prec, ws, stream)
+
+    mk = lambda: (torch.zeros(pr.P * pr.O * pr.T, device="cuda"),  # noqa: E731
+                  torch.empty(pr.P, device="cuda", dtype=torch.float64),
+                  torch.empty(pr.P, device="cuda", dtype=torch.int64))
+    o = mk()
+    b0 = pkg.make_batch(dp.eulers, dp.tx, dp.ty, dp.re, dp.im, dp.corr, o[0], O=pr.O, T=pr.T, P=pr.P, N_img=pr.N_img)
+    ws = torch.empty(pkg.batch_workspace_bytes(view, b0, prec), device="cuda", dtype=torch.uint8)
+    pkg.set_batch_graphs(False)
+    try:
+        run(*o)
+        torch.cuda.synchronize()
+        direct = [t.clone() for t in o]
+        n0 = pkg.launch_count()
+        run(*o)
+        torch.cuda.synchronize()
+        per_call = pkg.launch_count() - n0
+    finally:
+        pkg.set_batch_graphs(True)
+    outs = []
+    for k in range(4):  # direct, capture + launch, launch, launch
+        n0 = pkg.launch_count()
+        o[0].fill_(-1.0)
+        run(*o)
+        torch.cuda.synchronize()
+        assert pkg.launch_count() - n0 == per_call
+        outs.append(o[0].clone())
+        for a, b in zip(o, direct):
+            assert torch.equal(a, b), k
+    # inputs refilled in place: the graph reads the new values
+    saved = dp.re.clone()
+    dp.re.mul_(0.5)
+    run(*o)
+    torch.cuda.synchronize()
+    changed = o[0].clone()
+    pkg.set_batch_graphs(False)
+    try:
+        run(*o)
+        torch.cuda.synchronize()
+        assert torch.equal(o[0], changed)
+    finally:
+        pkg.set_batch_graphs(True)
+        dp.re.copy_(saved)
+    assert not torch.equal(changed, direct[0])
+    # a new output buffer is a new signature
+    o2 = mk()
+    for _ in range(3):
+        run(*o2)
+    torch.cuda.synchronize()
+    assert torch.equal(o2[0], direct[0])
+    # the caller captures the call into its own graph
+    o3 = mk()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        run(*o3, stream=s)  # warm (attributes set outside the capture)
+    torch.cuda.synchronize()
+    o3[0].fill_(-1.0)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        run(*o3, stream=s)
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(o3[0], direct[0])
+    del g
