@@ -345,7 +345,9 @@ typedef struct b200d2_server b200d2_server;
 typedef struct b200d2_request {
   int ref;              /* reference id from b200d2_server_add_reference */
   int P;                /* particles */
-  const float* h_real;  /* host [P][N_img] (page-locked memory overlaps best) */
+  const float* h_real;  /* host [P][N_img]; pageable host buffers (inputs and
+                           outputs) go through the server's page-locked staging
+                           buffers, page-locked ones are copied directly */
   const float* h_imag;
   const float* h_corr;
   const int* h_orient;  /* host [O]: indices into the reference's orientations */
@@ -362,10 +364,15 @@ typedef struct b200d2_server_stats {
   long long submitted, completed, rejected, evals;
   int in_flight, queued, max_in_flight;
   size_t bytes_in_use, peak_bytes;
+  double admit_host_s; /* scheduler-thread time spent issuing admitted requests' work */
 } b200d2_server_stats;
 
 /* slots: concurrent streams; hbm_budget_bytes: device bytes the in-flight
- * requests may hold; precision: tensor-core precision or B200D2_PREC_FP32. */
+ * requests may hold; precision: tensor-core precision or B200D2_PREC_FP32.
+ * Each slot keeps a device buffer between requests (powers of two from
+ * 32 MiB, released for idle slots when a growth would pass the budget), from
+ * a memory pool of the server's own; creation maps min(budget, 8 GiB) of it.
+ * The default memory pool of the process is not touched. */
 int b200d2_server_create(int slots, size_t hbm_budget_bytes, int precision,
                          b200d2_server** out);
 /* Register a resident reference: a projector view and its host orientation

@@ -106,7 +106,7 @@ class Request(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("rejected", C.c_longlong),
                 ("evals", C.c_longlong), ("in_flight", C.c_int), ("queued", C.c_int), ("max_in_flight", C.c_int),
-                ("bytes_in_use", C.c_size_t), ("peak_bytes", C.c_size_t)]
+                ("bytes_in_use", C.c_size_t), ("peak_bytes", C.c_size_t), ("admit_host_s", C.c_double)]
 
 
 PLAN_AUTOTUNE = 1

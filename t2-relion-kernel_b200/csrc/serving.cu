@@ -6,11 +6,15 @@
 // request starts as soon as a stream slot is free and its device footprint
 // (inputs, outputs, workspace) fits the HBM budget, in arrival order with
 // later requests allowed past one that does not fit yet.  An admitted request
-// runs entirely on its slot's stream: stream-ordered allocation
-// (cudaMallocAsync), host-to-device copies, the batch pipeline, device-to-
-// host copies, stream-ordered free, and a host callback that timestamps the
-// completion and wakes the scheduler.  Requests on different slots overlap on
-// the GPU.
+// runs entirely on its slot's stream, in the slot's device buffer (kept
+// between requests, grown in the slot stream's order): host-to-device copies,
+// the batch pipeline, device-to-host copies, and a host callback that
+// timestamps the completion and wakes the scheduler.  Requests on different slots overlap on
+// the GPU.  The scheduler thread never waits for the GPU: host buffers that
+// are not page-locked (a copy to or from them would block the issuing thread
+// until the stream reaches it) go through the slot's page-locked staging
+// buffer, inputs copied into it on the host before the upload, outputs
+// copied out of it by the completion callback.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -42,10 +46,19 @@ struct Ref {
   int O_all, N_img;
 };
 
+// A host-to-host copy the completion callback makes (staged output -> the
+// caller's buffer).
+struct HostCopy {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+
 struct Req {
   long long ticket = 0;
   b200d2_request r{};
   std::vector<float> eul;  // gathered [O][9]
+  std::vector<HostCopy> out_copies;
   size_t ws_bytes = 0, footprint = 0;
   int status = -1;  // -1 pending, else a b200d2_status
   double t_submit = 0, t_done = 0, device_s = 0;
@@ -66,6 +79,11 @@ struct b200d2_server {
   std::vector<Ref> refs;
   std::vector<cudaStream_t> streams;
   std::vector<int> slot_busy;
+  cudaMemPool_t pool = nullptr;    // device memory of the slots
+  std::vector<void*> dev;          // per slot: device buffer of its request, grown on its own stream
+  std::vector<size_t> dev_bytes;
+  std::vector<void*> pin;          // per slot: page-locked staging buffer
+  std::vector<size_t> pin_bytes;
   std::deque<std::shared_ptr<Req>> queue;
   std::vector<std::shared_ptr<Req>> inflight;
   std::map<long long, std::shared_ptr<Req>> all;
@@ -81,9 +99,74 @@ namespace {
 
 void CUDART_CB on_done(void* arg) {
   Req* q = static_cast<Req*>(arg);
+  for (const HostCopy& c : q->out_copies) memcpy(c.dst, c.src, c.bytes);
   q->t_done = now_s();
   q->finished.store(1);
   q->srv->cv_sched.notify_all();
+}
+
+// True when host memory at p is page-locked (or registered), so that an
+// asynchronous copy from or to it does not block the calling thread.
+bool page_locked(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // unregistered memory on older runtimes: clear the error
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// The slot's staging buffer, at least `need` bytes.  Called for an idle slot
+// (its previous request's copies and callback have completed).
+void* slot_staging(b200d2_server* s, int slot, size_t need) {
+  if (need == 0) return nullptr;
+  if (s->pin_bytes[slot] < need) {
+    if (s->pin[slot]) cudaFreeHost(s->pin[slot]);
+    s->pin[slot] = nullptr;
+    s->pin_bytes[slot] = 0;
+    const size_t bytes = std::max(need + need / 2, (size_t)1 << 20);
+    if (cudaHostAlloc(&s->pin[slot], bytes, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      s->pin[slot] = nullptr;
+      return nullptr;
+    }
+    s->pin_bytes[slot] = bytes;
+  }
+  return s->pin[slot];
+}
+
+// The slot's device buffer, at least `need` bytes.  Called for an idle slot
+// before its next request's work is issued on its stream, so a replacement
+// is freed and allocated in that stream's order (no other stream ever waits
+// on it).  Sizes are powers of two from 32 MiB (within the budget), so a slot
+// grows a few times at most; when growing would take the slots' buffers past
+// the budget, the buffers of idle slots are released first.
+void* slot_device(b200d2_server* s, int slot, size_t need) {
+  if (s->dev_bytes[slot] >= need) return s->dev[slot];
+  size_t want = (size_t)32 << 20;
+  while (want < need) want <<= 1;
+  if (want > s->budget) want = need;
+  need = want;
+  cudaStream_t st = s->streams[slot];
+  if (s->dev[slot]) cudaFreeAsync(s->dev[slot], st);
+  s->dev[slot] = nullptr;
+  s->dev_bytes[slot] = 0;
+  size_t held = 0;
+  for (size_t b : s->dev_bytes) held += b;
+  for (int k = 0; k < s->slots && held + need > s->budget; ++k)
+    if (k != slot && !s->slot_busy[k] && s->dev[k]) {
+      cudaFreeAsync(s->dev[k], s->streams[k]);
+      held -= s->dev_bytes[k];
+      s->dev[k] = nullptr;
+      s->dev_bytes[k] = 0;
+    }
+  if (cudaMallocFromPoolAsync(&s->dev[slot], need, s->pool, st) != cudaSuccess) {
+    cudaGetLastError();
+    s->dev[slot] = nullptr;
+    return nullptr;
+  }
+  s->dev_bytes[slot] = need;
+  return s->dev[slot];
 }
 
 // Launch a request's work on its slot stream (called with the lock held).
@@ -107,15 +190,60 @@ int admit(b200d2_server* s, Req& q) {
                o_out = take(out), o_mn = take((size_t)r.P * sizeof(double)),
                o_am = take((size_t)r.P * sizeof(long long)), o_ws = take(q.ws_bytes);
   (void)o_ws;
-  if (cudaMallocAsync(&q.dbuf, q.footprint, st) != cudaSuccess) return B200D2_ERR_OOM;
+  // host side: which buffers go through the staging buffer, and where
+  struct Up {
+    size_t dev_off;
+    const void* src;
+    size_t bytes;
+    bool staged;
+    size_t pin_off;
+  };
+  struct Down {
+    void* dst;
+    size_t dev_off;
+    size_t bytes;
+    bool staged;
+    size_t pin_off;
+  };
+  size_t pin_need = 0;
+  auto stage_at = [&](size_t bytes) {
+    size_t a = pin_need;
+    pin_need += up256(bytes);
+    return a;
+  };
+  Up ups[6] = {{o_re, r.h_real, img, false, 0},
+               {o_im, r.h_imag, img, false, 0},
+               {o_co, r.h_corr, img, false, 0},
+               {o_eu, q.eul.data(), q.eul.size() * sizeof(float), true, 0},
+               {o_tx, r.h_trans_x, (size_t)r.T * sizeof(float), false, 0},
+               {o_ty, r.h_trans_y, (size_t)r.T * sizeof(float), false, 0}};
+  for (Up& u : ups) {
+    if (!u.staged) u.staged = !page_locked(u.src);
+    if (u.staged) u.pin_off = stage_at(u.bytes);
+  }
+  Down downs[3] = {{r.h_diff2, o_out, out, false, 0},
+                   {r.h_min, o_mn, (size_t)r.P * sizeof(double), false, 0},
+                   {r.h_argmin, o_am, (size_t)r.P * sizeof(long long), false, 0}};
+  for (Down& w : downs) {
+    if (!w.dst) continue;
+    w.staged = !page_locked(w.dst);
+    if (w.staged) w.pin_off = stage_at(w.bytes);
+  }
+  uint8_t* pin = static_cast<uint8_t*>(slot_staging(s, q.slot, pin_need));
+  if (pin_need && !pin) return B200D2_ERR_OOM;
+  q.out_copies.clear();
+  q.dbuf = slot_device(s, q.slot, q.footprint);
+  if (!q.dbuf) return B200D2_ERR_OOM;
   uint8_t* d = static_cast<uint8_t*>(q.dbuf);
   cudaEventRecord(q.ev0, st);
-  cudaMemcpyAsync(d + o_re, r.h_real, img, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(d + o_im, r.h_imag, img, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(d + o_co, r.h_corr, img, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(d + o_eu, q.eul.data(), q.eul.size() * sizeof(float), cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(d + o_tx, r.h_trans_x, (size_t)r.T * sizeof(float), cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(d + o_ty, r.h_trans_y, (size_t)r.T * sizeof(float), cudaMemcpyHostToDevice, st);
+  for (const Up& u : ups) {
+    const void* src = u.src;
+    if (u.staged) {
+      memcpy(pin + u.pin_off, u.src, u.bytes);
+      src = pin + u.pin_off;
+    }
+    cudaMemcpyAsync(d + u.dev_off, src, u.bytes, cudaMemcpyHostToDevice, st);
+  }
   b200d2_batch b;
   memset(&b, 0, sizeof(b));
   b.d_eulers = reinterpret_cast<const float*>(d + o_eu);
@@ -134,11 +262,15 @@ int admit(b200d2_server* s, Req& q) {
   b.d_min = reinterpret_cast<double*>(d + o_mn);
   b.d_argmin = reinterpret_cast<long long*>(d + o_am);
   int rc = b200d2_diff2_coarse_batch(&ref.view, &b, s->prec, q.ws_bytes ? d + o_ws : nullptr, q.ws_bytes, st);
-  if (r.h_diff2) cudaMemcpyAsync(r.h_diff2, d + o_out, out, cudaMemcpyDeviceToHost, st);
-  if (r.h_min) cudaMemcpyAsync(r.h_min, d + o_mn, (size_t)r.P * sizeof(double), cudaMemcpyDeviceToHost, st);
-  if (r.h_argmin)
-    cudaMemcpyAsync(r.h_argmin, d + o_am, (size_t)r.P * sizeof(long long), cudaMemcpyDeviceToHost, st);
-  cudaFreeAsync(q.dbuf, st);
+  for (const Down& w : downs) {
+    if (!w.dst) continue;
+    if (w.staged) {
+      cudaMemcpyAsync(pin + w.pin_off, d + w.dev_off, w.bytes, cudaMemcpyDeviceToHost, st);
+      q.out_copies.push_back(HostCopy{w.dst, pin + w.pin_off, w.bytes});
+    } else {
+      cudaMemcpyAsync(w.dst, d + w.dev_off, w.bytes, cudaMemcpyDeviceToHost, st);
+    }
+  }
   cudaEventRecord(q.ev1, st);
   q.status = rc;  // final status once finished
   const cudaError_t e = cudaLaunchHostFunc(st, on_done, &q);
@@ -185,7 +317,9 @@ void sched_loop(b200d2_server* s) {
       s->slot_busy[slot] = 1;
       s->st.bytes_in_use += q.footprint;
       s->st.peak_bytes = std::max(s->st.peak_bytes, s->st.bytes_in_use);
+      const double t_admit = now_s();
       const int rc = admit(s, q);
+      s->st.admit_host_s += now_s() - t_admit;
       if (rc != B200D2_OK && !q.finished.load()) {
         // nothing was left on the stream that would signal completion
         q.status = rc;
@@ -217,6 +351,10 @@ extern "C" int b200d2_server_create(int slots, size_t hbm_budget_bytes, int prec
   s->prec = precision;
   cudaGetDevice(&s->device);
   s->slot_busy.assign(slots, 0);
+  s->pin.assign(slots, nullptr);
+  s->pin_bytes.assign(slots, 0);
+  s->dev.assign(slots, nullptr);
+  s->dev_bytes.assign(slots, 0);
   for (int k = 0; k < slots; ++k) {
     cudaStream_t st;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
@@ -226,11 +364,36 @@ extern "C" int b200d2_server_create(int slots, size_t hbm_budget_bytes, int prec
     }
     s->streams.push_back(st);
   }
-  // keep freed request memory cached in the process's pool up to the budget
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
-    uint64_t thr = hbm_budget_bytes;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  // the server's own memory pool for the slots' buffers: no internal
+  // dependencies, so memory released by one slot never makes another slot's
+  // stream wait (it is reused once its free has completed)
+  cudaMemPoolProps props;
+  memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = s->device;
+  if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess) {
+    for (cudaStream_t x : s->streams) cudaStreamDestroy(x);
+    delete s;
+    return B200D2_ERR_CUDA;
+  }
+  uint64_t thr = hbm_budget_bytes;
+  int no = 0, yes = 1;
+  cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  cudaMemPoolSetAttribute(s->pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+  cudaMemPoolSetAttribute(s->pool, cudaMemPoolReuseAllowOpportunistic, &yes);
+  // map the first part of the budget (up to 8 GiB) now, so that the slots'
+  // buffers are carved from memory the pool already holds instead of mapping
+  // new memory (milliseconds per growth) while requests wait
+  {
+    void* warm = nullptr;
+    const size_t reserve = std::min(hbm_budget_bytes, (size_t)8 << 30);
+    if (cudaMallocFromPoolAsync(&warm, reserve, s->pool, s->streams[0]) == cudaSuccess) {
+      cudaFreeAsync(warm, s->streams[0]);
+      cudaStreamSynchronize(s->streams[0]);
+    } else {
+      cudaGetLastError();
+    }
   }
   s->sched = std::thread(sched_loop, s);
   *out = s;
@@ -344,6 +507,11 @@ extern "C" int b200d2_server_destroy(b200d2_server* s) {
     cudaStreamSynchronize(x);
     cudaStreamDestroy(x);
   }
+  for (void* p : s->pin)
+    if (p) cudaFreeHost(p);
+  for (void* p : s->dev)
+    if (p) cudaFree(p);
+  if (s->pool) cudaMemPoolDestroy(s->pool);
   for (auto& kv : s->all) {
     if (kv.second->ev0) cudaEventDestroy(kv.second->ev0);
     if (kv.second->ev1) cudaEventDestroy(kv.second->ev1);

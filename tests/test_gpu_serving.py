@@ -108,3 +108,41 @@ def test_serving_admission_by_budget(pkg, synth, cuda):
     assert st["max_in_flight"] == 1  # the budget, not the two slots, limited concurrency
     srv.close()
     proj.close()
+
+
+def test_serving_page_locked_and_pageable_buffers(pkg, synth, cuda):
+    """Host buffers that are not page-locked go through the server's staging
+    buffers (so the scheduler thread never waits for the GPU); page-locked
+    ones are copied directly.  Every combination gives the same results, and
+    the staging buffers are reused across requests of different sizes."""
+    torch = cuda
+    rng = np.random.default_rng(23)
+    prob = synth.make_problem("c1", P=6)
+    proj = pkg.Projector(prob.projector, use_texture=1)
+    view = proj.view(prob.imgX, prob.imgY, prob.imgMaxR)
+    srv = pkg.Server(slots=2, hbm_budget=2 << 30, precision=pkg.PREC_BF16X3)
+    ref = srv.add_reference(view, prob.eulers, prob.N_img)
+    reqs = _requests(synth, rng, prob, ref, 4)
+
+    def run(rq, pinned_in, pinned_out):
+        n, O, T = len(rq["ps"]), rq["orient"].size, rq["tx"].size
+        host = (lambda a: torch.as_tensor(a).pin_memory()) if pinned_in else (lambda a: a)  # noqa: E731
+        mk = (lambda *s, dt: torch.zeros(s, dtype=dt).pin_memory()) if pinned_out else \
+            (lambda *s, dt: torch.zeros(s, dtype=dt))  # noqa: E731
+        out, mn, am = mk(n, O, T, dt=torch.float32), mk(n, dt=torch.float64), mk(n, dt=torch.int64)
+        if not pinned_out:
+            assert not out.is_pinned()
+        t = srv.submit(ref, host(rq["real"]), host(rq["imag"]), host(rq["corr"]), rq["orient"], rq["tx"], rq["ty"],
+                       out, mn, am)
+        assert srv.wait(t)[0] == 0
+        return out.numpy().copy(), mn.numpy().copy(), am.numpy().copy()
+
+    for rq in reqs:
+        base = run(rq, False, False)
+        for pin_in, pin_out in ((True, True), (True, False), (False, True)):
+            got = run(rq, pin_in, pin_out)
+            for a, b in zip(got, base):
+                np.testing.assert_array_equal(a, b)
+        assert np.all(base[1] == base[0].reshape(len(rq["ps"]), -1).min(axis=1))
+    srv.close()
+    proj.close()
