@@ -832,7 +832,7 @@ def ours_arm(args):
     # the significance threshold on the device, D2H of the significance mask
     # (one byte per sample) with each particle's threshold weight and count;
     # double-buffered on both copy directions
-    e2e_sig = None
+    e2e_sig = e2e_sig_packed = None
     if not uneven:
         n = O * T
         frac = 0.999
@@ -851,51 +851,72 @@ def ours_arm(args):
         out_free = [torch.cuda.Event() for _ in range(2)]
         in_free = [torch.cuda.Event() for _ in range(2)]
 
-        def sig_step(k, bk):
-            pkg.diff2_coarse_batch(view, bk, prec, ws, stream)
-            in_free[k % 2].record(stream)
-            pkg.coarse_weights(out, P, O, T, out_min=sets[k % 2][1][:P], normalize=False, weights=W, sums=S,
-                               workspace=WW, stream=stream)
-            if k >= 2:
-                stream.wait_event(out_free[k % 2])
-            pkg.significance(W.view(P, n), S, frac, 0, passed=masks[k % 2], sig_weight=sigs[k % 2],
-                             nsig=nsigs[k % 2], workspace=SW, stream=stream)
-            done[k % 2].record(stream)
-            with torch.cuda.stream(out_stream):
-                out_stream.wait_event(done[k % 2])
-                h_mask[k % 2].copy_(masks[k % 2], non_blocking=True)
-                h_sig[k % 2].copy_(sigs[k % 2], non_blocking=True)
-                h_nsig[k % 2].copy_(nsigs[k % 2], non_blocking=True)
-                out_free[k % 2].record(out_stream)
+        W_ = (P + 0) * ((n + 31) // 32)
+        bitss = [torch.empty((P, (n + 31) // 32), dtype=torch.int32, device=dev) for _ in range(2)]
+        h_bits = [torch.empty((P, (n + 31) // 32), dtype=torch.int32).pin_memory() for _ in range(2)]
 
-        sig_step(0, sets[0][2])  # warm-up (weights and significance kernels, pinned buffers)
-        torch.cuda.synchronize()
-        s_clocks = ClockSampler(local)
-        s_clocks.start()
-        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s0.record(stream)
-        copy_stream.wait_event(s0)
-        for k in range(e2e_steps):
-            d_pack, d_res, bk = sets[k % 2]
-            with torch.cuda.stream(copy_stream):
+        def sig_leg(packed):
+            def sig_step(k, bk):
+                pkg.diff2_coarse_batch(view, bk, prec, ws, stream)
+                in_free[k % 2].record(stream)
+                pkg.coarse_weights(out, P, O, T, out_min=sets[k % 2][1][:P], normalize=False, weights=W, sums=S,
+                                   workspace=WW, stream=stream)
                 if k >= 2:
-                    copy_stream.wait_event(in_free[k % 2])
-                d_pack.copy_(h_pack, non_blocking=True)
-                ready[k % 2].record(copy_stream)
-            stream.wait_event(ready[k % 2])
-            sig_step(k, bk)
-        stream.wait_stream(out_stream)
-        s1.record(stream)
-        torch.cuda.synchronize()
-        sig_clk = s_clocks.stop()
-        e2e_sig = {"value": replicas.job_rate(evals_step * e2e_steps, s0.elapsed_time(s1), dist, dev),
-                   "unit": "diff2 evals/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": P * n + 16 * P,
-                   "clocks": sig_clk, "adaptive_fraction": frac,
-                   "median_significant_per_particle": float(np.median(h_nsig[(e2e_steps - 1) % 2].numpy())),
-                   "note": ("every step: H2D of images+corr, the batch call, b200d2_coarse_weights (FP64) and "
-                            "b200d2_significance on the device, D2H of the significance mask (1 byte per sample) "
-                            "and each particle's threshold weight and count; inputs and outputs double-buffered")}
-        del W, WW, SW, masks
+                    stream.wait_event(out_free[k % 2])
+                pkg.significance(W.view(P, n), S, frac, 0, passed=masks[k % 2], sig_weight=sigs[k % 2],
+                                 nsig=nsigs[k % 2], workspace=SW, stream=stream)
+                if packed:
+                    pkg.pack_mask(masks[k % 2], out=bitss[k % 2], stream=stream)
+                done[k % 2].record(stream)
+                with torch.cuda.stream(out_stream):
+                    out_stream.wait_event(done[k % 2])
+                    if packed:
+                        h_bits[k % 2].copy_(bitss[k % 2], non_blocking=True)
+                    else:
+                        h_mask[k % 2].copy_(masks[k % 2], non_blocking=True)
+                    h_sig[k % 2].copy_(sigs[k % 2], non_blocking=True)
+                    h_nsig[k % 2].copy_(nsigs[k % 2], non_blocking=True)
+                    out_free[k % 2].record(out_stream)
+
+            sig_step(0, sets[0][2])  # warm-up (weights and significance kernels, pinned buffers)
+            torch.cuda.synchronize()
+            s_clocks = ClockSampler(local)
+            s_clocks.start()
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            copy_stream.wait_event(s0)
+            for k in range(e2e_steps):
+                d_pack, d_res, bk = sets[k % 2]
+                with torch.cuda.stream(copy_stream):
+                    if k >= 2:
+                        copy_stream.wait_event(in_free[k % 2])
+                    d_pack.copy_(h_pack, non_blocking=True)
+                    ready[k % 2].record(copy_stream)
+                stream.wait_event(ready[k % 2])
+                sig_step(k, bk)
+            stream.wait_stream(out_stream)
+            s1.record(stream)
+            torch.cuda.synchronize()
+            sig_clk = s_clocks.stop()
+            last = (e2e_steps - 1) % 2
+            if packed:  # the packed mask of the last step sets the bits its byte mask sets
+                cnt = np.unpackbits(h_bits[last].numpy().view(np.uint8), axis=1).sum(axis=1)
+                ref = masks[last].to(torch.int64).sum(dim=1).cpu().numpy()
+                assert cnt.tolist() == ref.tolist(), "packed mask disagrees with the byte mask"
+            return {"value": replicas.job_rate(evals_step * e2e_steps, s0.elapsed_time(s1), dist, dev),
+                    "unit": "diff2 evals/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": (4 * W_ if packed else P * n) + 16 * P,
+                    "clocks": sig_clk, "adaptive_fraction": frac,
+                    "median_significant_per_particle": float(np.median(h_nsig[last].numpy())),
+                    "note": ("every step: H2D of images+corr, the batch call, b200d2_coarse_weights (FP64) and "
+                             "b200d2_significance on the device, D2H of the significance mask " +
+                             ("packed to one bit per sample by b200d2_pack_mask " if packed else
+                              "(1 byte per sample) ") +
+                             "and each particle's threshold weight and count; inputs and outputs double-buffered")}
+
+        e2e_sig = sig_leg(False)
+        e2e_sig_packed = sig_leg(True)
+        del W, WW, SW, masks, bitss
 
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
@@ -970,6 +991,7 @@ def ours_arm(args):
                           f"({4 * evals_step / 1e6:.0f} MB per step) stays on the device, where the weights and "
                           "significance steps read it; e2e_significance reads their product back")},
                 "e2e_significance": e2e_sig,
+                "e2e_significance_packed": e2e_sig_packed,
                 "parity": parity, "fp32_cuda_core": fp32_leg, "operand_generated_in_contraction": gen_leg,
                 "single_particle_call": single,
                 "serving": serving,

@@ -495,6 +495,15 @@ int b200d2_significance(const double* d_weights, int P, long long n,
                         void* d_workspace, size_t workspace_bytes,
                         void* stream);
 
+/* A significance mask (or any byte mask) d_mask[P][n] packed to bits for a
+ * copy to the host, eight times smaller: d_bits[P][(n + 31) / 32] words, word
+ * j of particle p holding samples 32 j .. 32 j + 31, sample 32 j + i in bit i
+ * (set when the byte is non-zero; bits past n zero).  No counterpart in the
+ * reference, whose mask stays one byte per sample.  Asynchronous on
+ * `stream`. */
+int b200d2_pack_mask(const unsigned char* d_mask, int P, long long n,
+                     unsigned int* d_bits, void* stream);
+
 /* Final combination diff2 = nA - 2 cross of the tensor-core forms, where nA =
  * sum w|X|^2 + sum w|A|^2 is accumulated in FP64 and cross comes from the
  * FP32 tensor-core accumulator.  B200D2_COMBINE_DF32 (default): nA is kept as

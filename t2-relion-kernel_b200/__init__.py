@@ -161,6 +161,7 @@ def _declare(L):
         "b200d2_server_destroy": [P],
         "b200d2_coarse_weights": [P, I, I, I, P, P, P, I, P, P, P, Z, P],
         "b200d2_significance": [P, I, C.c_longlong, P, C.c_double, C.c_longlong, P, P, P, P, Z, P],
+        "b200d2_pack_mask": [P, I, C.c_longlong, P, P],
         "b200d2_set_gemm_variant": [I, I, I, I],
         "b200d2_set_combine": [I],
         "b200d2_set_wait_limit_ns": [C.c_ulonglong],
@@ -557,6 +558,19 @@ def significance(weights, sums, adaptive_fraction: float, max_significants: int 
                                      _ptr(sig_weight), _ptr(nsig), _ptr(mask), _ptr(workspace), nb, _stream(stream)),
            "significance")
     return sig_weight, nsig, mask
+
+
+def pack_mask(mask, out=None, stream=None):
+    """Byte mask [P, n] (CUDA uint8) packed to bits (b200d2_pack_mask):
+    returns CUDA int32 [P, (n + 31) // 32], sample 32 j + i of a row in bit i
+    of its word j."""
+    import torch
+    P = int(mask.shape[0])
+    n = int(mask.numel() // max(P, 1))
+    if out is None:
+        out = torch.empty((P, (n + 31) // 32), dtype=torch.int32, device=mask.device)
+    _check(lib().b200d2_pack_mask(_ptr(mask), P, n, _ptr(out), _stream(stream)), "pack_mask")
+    return out
 
 
 def ctf_fold(real, imag, ctf_params: list, minvsigma2, *, imgX: int, imgY: int, maxR: int, ori_size: int,

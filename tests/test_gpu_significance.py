@@ -187,3 +187,47 @@ def test_significance_matches_reference_kernels(pkg, oracle, cuda):
                 continue  # the FP64 scan's rounding reaches the threshold
             assert sig[p].item() == ref_sig and nsig[p].item() == ref_nsig
             assert torch.equal(passed[p].bool(), ref_mask)
+
+
+def _packbits_ref(m):
+    """numpy reference of b200d2_pack_mask: rows of bits, little-endian words."""
+    P, n = m.shape
+    w = (n + 31) // 32
+    out = np.zeros((P, w * 4), np.uint8)
+    for p in range(P):
+        b = np.packbits(m[p] != 0, bitorder="little")
+        out[p, :b.size] = b
+    return out.view("<u4")
+
+
+@pytest.mark.parametrize("P,n,offset", [(3, 100, 0), (2, 64, 0), (4, 1000, 1), (1, 1, 0), (5, 4096, 0),
+                                        (2, 4096, 3), (3, 31, 0)])
+def test_pack_mask(pkg, cuda, P, n, offset):
+    """Byte masks packed to bits: aligned rows (16-byte loads), unaligned
+    bases and ragged rows (byte loads), arbitrary non-zero bytes."""
+    torch = cuda
+    rng = np.random.default_rng(P * 1000 + n + offset)
+    m = (rng.integers(0, 2, (P, n)) * rng.integers(1, 256, (P, n))).astype(np.uint8)
+    flat = torch.zeros(P * n + offset, dtype=torch.uint8, device="cuda")
+    flat[offset:] = torch.as_tensor(m.reshape(-1), device="cuda")
+    got = pkg.pack_mask(flat[offset:].view(P, n))
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(got.cpu().numpy().view(np.uint32), _packbits_ref(m))
+
+
+def test_pack_mask_of_significance(pkg, oracle, cuda):
+    """The packed form of a significance mask unpacks to the byte mask (with
+    no tied weights, as here, it holds exactly nsig set bits per particle;
+    weights equal to the threshold weight all pass)."""
+    torch = cuda
+    rng = np.random.default_rng(5)
+    P, n = 4, 20000
+    w = torch.as_tensor(rng.exponential(1.0, (P, n)) ** 4, device="cuda")
+    sums = w.sum(dim=1)
+    _, nsig, mask = pkg.significance(w, sums, 0.999)
+    bits = pkg.pack_mask(mask)
+    torch.cuda.synchronize()
+    b = bits.cpu().numpy().view(np.uint32)
+    unpacked = np.unpackbits(b.view(np.uint8), axis=1, bitorder="little")[:, :n]
+    np.testing.assert_array_equal(unpacked, mask.cpu().numpy())
+    assert [int(np.unpackbits(b[p].view(np.uint8)).sum()) for p in range(P)] == nsig.cpu().tolist()
