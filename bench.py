@@ -655,12 +655,22 @@ def ours_arm(args):
                                                                   N, stream=stream, precision=prec))
         ms_fp32 = per_call(lambda: pkg.run_diff2_kernel_coarse(view, tx, ty, corr[0], re[0], im[0], eul, o32, O, T, N,
                                                                stream=stream))
+        pkg.set_projection_cache(False)
+        try:
+            ms_drop_tc_nocache = per_call(lambda: pkg.run_diff2_kernel_coarse(view, tx, ty, corr[0], re[0], im[0], eul,
+                                                                              o1, O, T, N, stream=stream,
+                                                                              precision=prec))
+        finally:
+            pkg.set_projection_cache(True)
         single = {"batch_api_ms_per_particle": ms_tc, "dropin_tensor_core_ms_per_particle": ms_drop_tc,
+                  "dropin_tensor_core_ms_per_particle_projecting": ms_drop_tc_nocache,
                   "fp32_dropin_ms_per_particle": ms_fp32, "evals_per_particle": O * T,
                   "note": f"one particle per call: the {args.precision} batch entry point and the "
                           f"runDiff2KernelCoarse signature (b200d2_diff2_coarse) with {args.precision} (all stages: "
                           "projection, norms, contraction; library-owned workspace) or FP32 CUDA cores; "
-                          "back-to-back calls, CUDA events"}
+                          "back-to-back calls on the same orientations, CUDA events; the signature's calls reuse "
+                          "the projections of the previous call (Euler matrices compared on the device), "
+                          "'_projecting' with that cache off"}
         del ws1, o1, o32
 
     # ---- the same batch with the A operand generated inside the contraction ----

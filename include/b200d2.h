@@ -572,6 +572,15 @@ int b200d2_workspace_status(const void* d_workspace, void* stream,
  * creation must see the same mode. */
 int b200d2_set_operand_gen(int mode);
 
+/* Projection cache of b200d2_diff2_coarse with a tensor-core precision (on by
+ * default).  The library-owned workspace keeps the last call's projections;
+ * a call skips its projection stage when its Euler matrices equal, bit for
+ * bit, those that were projected (compared on the device) and nothing else
+ * they depend on has changed: the view, the precision, the workspace layout,
+ * and no projector created or destroyed since.  Scores are bit-identical
+ * either way.  The FP16 forms always project.  0 turns it off. */
+int b200d2_set_projection_cache(int enable);
+
 /* Test hook for the give-up path of the bounded device-side waits (no
  * counterpart in the reference, whose waits cannot hang: it recomputes instead
  * of spinning, src/translation_matrix_handler.cuh:145-206).  Sets, process

@@ -166,6 +166,7 @@ def _declare(L):
         "b200d2_set_combine": [I],
         "b200d2_set_wait_limit_ns": [C.c_ulonglong],
         "b200d2_set_operand_gen": [I],
+        "b200d2_set_projection_cache": [I],
         "b200d2_set_batch_graphs": [I],
         "b200d2_diff2_fine": [C.POINTER(View), P, P, P, P, P, P, P, Z, F, Z, P, P, P, P, P],
         "b200d2_diff2_fine_cc": [C.POINTER(View), P, P, P, P, P, P, P, Z, Z, P, P, P, P, P],
@@ -621,6 +622,13 @@ def set_operand_gen(mode: int) -> None:
     by its own kernel, 1 generated in shared memory inside the contraction
     (bit-identical results).  Query workspace sizes after setting it."""
     _check(lib().b200d2_set_operand_gen(int(mode)), "set_operand_gen")
+
+
+def set_projection_cache(enable: bool) -> None:
+    """Projection cache of the single-particle tensor-core call (on by
+    default): calls whose Euler matrices equal the last projected ones (bit
+    for bit, checked on the device) reuse those projections."""
+    _check(lib().b200d2_set_projection_cache(1 if enable else 0), "set_projection_cache")
 
 
 def set_wait_limit_ns(ns: int) -> None:

@@ -5,6 +5,7 @@
 // its harness loops runDiff2KernelCoarse over particles (src/main.cu:483-503).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -21,7 +22,8 @@ int minloc(const float* d, long long n, int P, double* mn, long long* arg, cudaS
 size_t tc_workspace_bytes(const b200d2_view& view, const b200d2_batch& b, int precision,
                           bool allow_split = true);
 int tc_run(const b200d2_view& view, const b200d2_batch& b, int precision, void* ws,
-           size_t ws_bytes, cudaStream_t s);
+           size_t ws_bytes, cudaStream_t s, const int* d_proj_need = nullptr);
+bool tc_projection_layout(const b200d2_view& v, const b200d2_batch& b, int precision, std::vector<uint64_t>& key);
 
 static int validate(const b200d2_view* v, const b200d2_batch* b) {
   if (!v || !b) return B200D2_ERR_INVALID;
@@ -52,36 +54,71 @@ void uncount_launch(unsigned n) { __atomic_fetch_sub(&g_launches, (unsigned long
 // (cudaMallocAsync / cudaFreeAsync on that stream, so calls queued on the
 // stream before the growth finish with the old buffer), kept until the
 // process exits.
+//
+// Projection cache.  A caller of the single-particle signature scores one
+// particle after another against the same orientations (the reference's
+// harness loops runDiff2KernelCoarse over particles with one Euler array,
+// src/main.cu:483-503), and the projections of those orientations are most
+// of a call's work.  The workspace keeps the last call's projections; the
+// next call skips its projection stage when
+//   - everything the projections and their place in the workspace depend on,
+//     other than the Euler matrices, is unchanged (host key: the view, the
+//     workspace address and layout, the precision, the projector epoch,
+//     which advances whenever any projector is created or destroyed), and
+//   - its Euler matrices equal, bit for bit, those of the call that projected
+//     (compared on the device against a copy kept with the workspace, so the
+//     check needs no host synchronisation and sees contents changed in place).
+// Otherwise it projects and the copy is refreshed.  Skipped or not, the
+// scores are bit-identical.  The FP16 forms, whose projection stage rescales
+// per call, always project.
 struct OwnedWorkspace {
   int device;
   cudaStream_t stream;
   void* ptr;
   size_t bytes;
+  float* eul;                 // device copy of the Euler matrices last projected, then the flag
+  size_t eul_cap;             // floats
+  int* need;                  // device flag: nonzero = project this call
+  std::vector<uint64_t> key;  // host key of the cached projections; empty = none
 };
 static std::mutex g_owned_mu;
 static std::vector<OwnedWorkspace> g_owned;
+static std::atomic<int> g_proj_cache{1};  // b200d2_set_projection_cache
 
-static int owned_workspace(cudaStream_t s, size_t need, void** out) {
+// (with g_owned_mu held)
+static int owned_workspace(cudaStream_t s, size_t need, OwnedWorkspace** out) {
   int dev = 0;
   B200D2_CUDA_TRY(cudaGetDevice(&dev));
-  std::lock_guard<std::mutex> lk(g_owned_mu);
   for (OwnedWorkspace& w : g_owned)
     if (w.device == dev && w.stream == s) {
       if (w.bytes < need) {
+        w.key.clear();
         B200D2_CUDA_TRY(cudaFreeAsync(w.ptr, s));
         w.ptr = nullptr;
         w.bytes = 0;
         B200D2_CUDA_TRY(cudaMallocAsync(&w.ptr, need, s));
         w.bytes = need;
       }
-      *out = w.ptr;
+      *out = &w;
       return B200D2_OK;
     }
-  OwnedWorkspace w{dev, s, nullptr, need};
+  OwnedWorkspace w{dev, s, nullptr, need, nullptr, 0, nullptr, {}};
   B200D2_CUDA_TRY(cudaMallocAsync(&w.ptr, need, s));
   g_owned.push_back(w);
-  *out = w.ptr;
+  *out = &g_owned.back();
   return B200D2_OK;
+}
+
+__global__ void eul_compare_kernel(const float* __restrict__ a, const float* __restrict__ cached, int n,
+                                   int* need) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (__float_as_uint(a[i]) != __float_as_uint(cached[i])) *need = 1;  // every writer stores 1
+}
+
+__global__ void eul_update_kernel(const float* __restrict__ a, float* __restrict__ cached, int n,
+                                  const int* __restrict__ need) {
+  if (*need == 0) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) cached[i] = a[i];
 }
 
 // One particle through the tensor-core pipeline, accumulating onto diff2s as
@@ -107,13 +144,60 @@ int single_particle_tc(const b200d2_view& v, const float* tx, const float* ty, c
   int st = validate(&v, &b);
   if (st != B200D2_OK) return st;
   const size_t need = tc_workspace_bytes(v, b, precision);
-  void* ws = nullptr;
-  st = owned_workspace(s, need, &ws);
+  std::vector<uint64_t> key;
+  const bool cacheable = g_proj_cache.load() != 0 && tc_projection_layout(v, b, precision, key);
+  std::lock_guard<std::mutex> lk(g_owned_mu);
+  OwnedWorkspace* w = nullptr;
+  st = owned_workspace(s, need, &w);
   if (st != B200D2_OK) return st;
-  return tc_run(v, b, precision, ws, need, s);
+  if (!cacheable) {
+    w->key.clear();
+    return tc_run(v, b, precision, w->ptr, need, s);
+  }
+  uint32_t pf;
+  memcpy(&pf, &v.padding_factor, 4);
+  key.insert(key.end(), {(uint64_t)v.mdlX, (uint64_t)v.mdlXY, (uint64_t)v.mdlZ, (uint64_t)v.imgX, (uint64_t)v.imgY,
+                         (uint64_t)v.imgZ, (uint64_t)(uint32_t)v.mdlInitY, (uint64_t)(uint32_t)v.mdlInitZ,
+                         (uint64_t)v.maxR, (uint64_t)v.maxR2, (uint64_t)v.maxR2_padded, (uint64_t)pf, v.tex_re,
+                         v.tex_im, (uint64_t)(uintptr_t)v.lin_re, (uint64_t)(uintptr_t)v.lin_im,
+                         (uint64_t)v.interp, v.tex_c, projector_epoch(), (uint64_t)(uintptr_t)w->ptr,
+                         (uint64_t)N_img});
+  const int n = O * 9;
+  if (w->eul_cap < (size_t)n) {
+    w->key.clear();
+    if (w->eul) B200D2_CUDA_TRY(cudaFreeAsync(w->eul, s));
+    w->eul = nullptr;
+    w->eul_cap = 0;
+    const size_t at = ((size_t)n * sizeof(float) + 15) / 16 * 16;
+    void* p = nullptr;
+    B200D2_CUDA_TRY(cudaMallocAsync(&p, at + 16, s));
+    w->eul = static_cast<float*>(p);
+    w->need = reinterpret_cast<int*>(static_cast<char*>(p) + at);
+    w->eul_cap = (size_t)n;
+  }
+  const bool force = key != w->key;
+  w->key.clear();  // set again once this call's launches are issued
+  B200D2_CUDA_TRY(cudaMemsetAsync(w->need, force ? 0xff : 0, sizeof(int), s));
+  const int blocks = (n + 255) / 256;
+  if (!force) {
+    eul_compare_kernel<<<blocks, 256, 0, s>>>(eulers, w->eul, n, w->need);
+    count_launch();
+  }
+  eul_update_kernel<<<blocks, 256, 0, s>>>(eulers, w->eul, n, w->need);
+  count_launch();
+  B200D2_CUDA_TRY(cudaGetLastError());
+  st = tc_run(v, b, precision, w->ptr, need, s, w->need);
+  if (st == B200D2_OK) w->key = key;
+  return st;
 }
 
 }  // namespace b200d2
+
+extern "C" int b200d2_set_projection_cache(int enable) {
+  if (enable != 0 && enable != 1) return B200D2_ERR_INVALID;
+  b200d2::g_proj_cache.store(enable);
+  return B200D2_OK;
+}
 
 extern "C" unsigned long long b200d2_launch_count(void) {
   return __atomic_load_n(&b200d2::g_launches, __ATOMIC_RELAXED);

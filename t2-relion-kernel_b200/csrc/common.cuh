@@ -28,6 +28,11 @@ namespace b200d2 {
 // Process-wide count of kernel launches made by this library.
 void count_launch(unsigned n = 1);
 
+// Counter advanced whenever a projector is created or destroyed: state keyed
+// on a projector view (whose texture handles a later projector may reuse) is
+// valid only while it is unchanged.
+unsigned long long projector_epoch();
+
 // NVTX range over a host scope (a batch call, a pipeline stage, a served
 // request), so that a timeline profiler labels the library's launches; without
 // a profiler attached the push and pop cost a few nanoseconds.

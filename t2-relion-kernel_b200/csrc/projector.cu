@@ -14,6 +14,8 @@
 // representation and stays resident in the 126 MB L2 while a batch runs.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -111,6 +113,11 @@ int upload_array2(cudaArray_t* arr, cudaTextureObject_t* tex, const float* h_re,
 
 }  // namespace
 
+namespace b200d2 {
+static std::atomic<unsigned long long> g_projector_epoch{1};
+unsigned long long projector_epoch() { return g_projector_epoch.load(); }
+}  // namespace b200d2
+
 extern "C" int b200d2_projector_create(int mdlX, int mdlY, int mdlZ,
                                        int mdlInitY, int mdlInitZ, int mdlMaxR,
                                        float padding_factor,
@@ -119,6 +126,7 @@ extern "C" int b200d2_projector_create(int mdlX, int mdlY, int mdlZ,
                                        b200d2_projector** out) {
   if (!out || !h_real || !h_imag) return B200D2_ERR_INVALID;
   *out = nullptr;
+  b200d2::g_projector_epoch.fetch_add(1);
   if (mdlZ == 1) mdlZ = 0;  // setMdlDim: zdim 1 means a 2D model
   if (mdlX <= 1 || mdlY <= 1 || mdlZ < 0) return B200D2_ERR_INVALID;
   if (mdlZ == 0) return B200D2_ERR_UNSUPPORTED;  // 2D references: out of scope
@@ -188,6 +196,7 @@ extern "C" int b200d2_projector_load_dat(const char* path, int use_texture,
 
 extern "C" int b200d2_projector_destroy(b200d2_projector* p) {
   if (!p) return B200D2_ERR_INVALID;
+  b200d2::g_projector_epoch.fetch_add(1);
   release(p);
   delete p;
   return B200D2_OK;

@@ -179,3 +179,98 @@ def test_single_particle_entry_point_on_tensor_cores(pkg, synth, oracle, cuda, p
         ref = ours_f64(pkg, view, dp, 0)
         assert oracle.error_stats(got, ref)["max_rel"] <= 2e-5, (name, prec_name)
         proj.close()
+
+
+def test_single_particle_projection_cache(pkg, synth, cuda):
+    """The single-particle signature's projection cache (tensor-core
+    precisions): one scripted sequence of calls is run with the cache off and
+    then on, and every call's scores must be bit-identical.  The sequence
+    covers particles one after another on the same orientations (hits), the
+    same Euler values in another buffer (hit), an Euler value changed in
+    place (the device comparison misses), another translation count (the
+    workspace layout moves), an FP16 form in between (never cached), and the
+    projector destroyed and created again with another volume at the same
+    geometry (the projector epoch)."""
+    torch = cuda
+    pr = synth.make_problem("c1", P=4)
+    pr_b = synth.make_problem("c1", P=4, seed=99)  # same geometry, another volume
+    dp = DeviceProblem(torch, pr)
+
+    def sequence():
+        outs = []
+        proj = pkg.Projector(pr.projector, use_texture=1)
+        view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+        eul2 = dp.eulers.clone()
+
+        def call(v, p, eul, T=pr.T, prec=pkg.PREC_BF16X3):
+            out = torch.zeros(pr.O * T, device="cuda")
+            pkg.run_diff2_kernel_coarse(v, dp.tx[:T], dp.ty[:T], dp.corr[p], dp.re[p], dp.im[p], eul, out, pr.O, T,
+                                        pr.N_img, precision=prec)
+            torch.cuda.synchronize()
+            outs.append(out.cpu().numpy())
+
+        for p in range(3):
+            call(view, p, dp.eulers)
+        call(view, 3, eul2)  # same values, another buffer
+        eul2[5] += 0.01      # changed in place
+        call(view, 0, eul2)
+        call(view, 1, eul2)
+        eul2[7] -= 0.02
+        call(view, 2, eul2)
+        call(view, 3, eul2, T=9)  # another layout
+        call(view, 3, eul2)
+        call(view, 0, eul2, prec=pkg.PREC_FP16X3)
+        call(view, 0, eul2)
+        proj.close()
+        proj_b = pkg.Projector(pr_b.projector, use_texture=1)
+        view_b = proj_b.view(pr.imgX, pr.imgY, pr.imgMaxR)
+        call(view_b, 1, eul2)
+        call(view_b, 2, eul2)
+        proj_b.close()
+        return outs
+
+    pkg.set_projection_cache(False)
+    try:
+        ref = sequence()
+    finally:
+        pkg.set_projection_cache(True)
+    got = sequence()
+    assert len(got) == len(ref)
+    for i, (a, b) in enumerate(zip(got, ref)):
+        np.testing.assert_array_equal(a, b, err_msg=f"call {i}")
+    # calls 6 and 12: the same particle and Euler values against the two volumes
+    assert not np.array_equal(ref[6], ref[12])
+
+
+def test_single_particle_projection_cache_skips_work(pkg, synth, cuda):
+    """At C2 (4608 orientations) a call that reuses the projections takes
+    clearly less time than one that projects (CUDA events, 20 calls each)."""
+    torch = cuda
+    pr = synth.make_problem("c2", P=1)
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dp = DeviceProblem(torch, pr)
+    out = torch.zeros(pr.O * pr.T, device="cuda")
+
+    def timed(enable, reps=20):
+        pkg.set_projection_cache(enable)
+        for _ in range(3):
+            pkg.run_diff2_kernel_coarse(view, dp.tx, dp.ty, dp.corr[0], dp.re[0], dp.im[0], dp.eulers, out, pr.O,
+                                        pr.T, pr.N_img, precision=pkg.PREC_BF16X3)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            pkg.run_diff2_kernel_coarse(view, dp.tx, dp.ty, dp.corr[0], dp.re[0], dp.im[0], dp.eulers, out, pr.O,
+                                        pr.T, pr.N_img, precision=pkg.PREC_BF16X3)
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    try:
+        off = timed(False)
+        on = timed(True)
+    finally:
+        pkg.set_projection_cache(True)
+    print(f"projecting {off:.3f} ms, reusing {on:.3f} ms per call")
+    assert on < 0.8 * off, (on, off)
+    proj.close()
