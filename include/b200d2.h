@@ -578,7 +578,9 @@ int b200d2_set_operand_gen(int mode);
  * bit, those that were projected (compared on the device) and nothing else
  * they depend on has changed: the view, the precision, the workspace layout,
  * and no projector created or destroyed since.  Scores are bit-identical
- * either way.  The FP16 forms always project.  0 turns it off. */
+ * either way.  The FP16 forms, and projections of fewer than 2^20 samples
+ * (orientations x pixels, quicker than the check), always project.  0 turns
+ * it off. */
 int b200d2_set_projection_cache(int enable);
 
 /* Test hook for the give-up path of the bounded device-side waits (no

@@ -22,7 +22,8 @@ int minloc(const float* d, long long n, int P, double* mn, long long* arg, cudaS
 size_t tc_workspace_bytes(const b200d2_view& view, const b200d2_batch& b, int precision,
                           bool allow_split = true);
 int tc_run(const b200d2_view& view, const b200d2_batch& b, int precision, void* ws,
-           size_t ws_bytes, cudaStream_t s, const int* d_proj_need = nullptr);
+           size_t ws_bytes, cudaStream_t s, const int* d_proj_need = nullptr,
+           float* d_eul_cache = nullptr);
 bool tc_projection_layout(const b200d2_view& v, const b200d2_batch& b, int precision, std::vector<uint64_t>& key);
 
 static int validate(const b200d2_view* v, const b200d2_batch* b) {
@@ -68,17 +69,18 @@ void uncount_launch(unsigned n) { __atomic_fetch_sub(&g_launches, (unsigned long
 //   - its Euler matrices equal, bit for bit, those of the call that projected
 //     (compared on the device against a copy kept with the workspace, so the
 //     check needs no host synchronisation and sees contents changed in place).
-// Otherwise it projects and the copy is refreshed.  Skipped or not, the
-// scores are bit-identical.  The FP16 forms, whose projection stage rescales
-// per call, always project.
+// Otherwise it projects and the projection stage refreshes the copy.  Skipped
+// or not, the scores are bit-identical.  The FP16 forms, whose projection
+// stage rescales per call, and projections of fewer than 2^20 samples (faster
+// than the check) always project.
 struct OwnedWorkspace {
   int device;
   cudaStream_t stream;
   void* ptr;
   size_t bytes;
-  float* eul;                 // device copy of the Euler matrices last projected, then the flag
+  float* eul;                 // device copy of the Euler matrices last projected, then the verdict words
   size_t eul_cap;             // floats
-  int* need;                  // device flag: nonzero = project this call
+  int* need;                  // device: kEulCheckBlocks verdict words, any nonzero = project this call
   std::vector<uint64_t> key;  // host key of the cached projections; empty = none
 };
 static std::mutex g_owned_mu;
@@ -109,16 +111,21 @@ static int owned_workspace(cudaStream_t s, size_t need, OwnedWorkspace** out) {
   return B200D2_OK;
 }
 
-__global__ void eul_compare_kernel(const float* __restrict__ a, const float* __restrict__ cached, int n,
-                                   int* need) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    if (__float_as_uint(a[i]) != __float_as_uint(cached[i])) *need = 1;  // every writer stores 1
-}
-
-__global__ void eul_update_kernel(const float* __restrict__ a, float* __restrict__ cached, int n,
-                                  const int* __restrict__ need) {
-  if (*need == 0) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) cached[i] = a[i];
+// need[b] = force, or whether any Euler value of block b's share differs
+// (bit for bit) from the copy of the last projected ones; every word is
+// written each call, so none needs a reset.  The projection stage ORs the
+// kEulCheckBlocks words and, when it projects, refreshes the copy.
+__global__ void __launch_bounds__(256) eul_check_kernel(const float* __restrict__ a,
+                                                        const float* __restrict__ cached, int n, int force,
+                                                        int* need) {
+  const int chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int i0 = blockIdx.x * chunk, i1 = min(n, i0 + chunk);
+  int differ = force;
+  if (!force)
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x)
+      differ |= __float_as_uint(a[i]) != __float_as_uint(cached[i]);
+  differ = __syncthreads_or(differ);
+  if (threadIdx.x == 0) need[blockIdx.x] = differ;
 }
 
 // One particle through the tensor-core pipeline, accumulating onto diff2s as
@@ -170,23 +177,17 @@ int single_particle_tc(const b200d2_view& v, const float* tx, const float* ty, c
     w->eul_cap = 0;
     const size_t at = ((size_t)n * sizeof(float) + 15) / 16 * 16;
     void* p = nullptr;
-    B200D2_CUDA_TRY(cudaMallocAsync(&p, at + 16, s));
+    B200D2_CUDA_TRY(cudaMallocAsync(&p, at + sizeof(int) * kEulCheckBlocks, s));
     w->eul = static_cast<float*>(p);
     w->need = reinterpret_cast<int*>(static_cast<char*>(p) + at);
     w->eul_cap = (size_t)n;
   }
   const bool force = key != w->key;
   w->key.clear();  // set again once this call's launches are issued
-  B200D2_CUDA_TRY(cudaMemsetAsync(w->need, force ? 0xff : 0, sizeof(int), s));
-  const int blocks = (n + 255) / 256;
-  if (!force) {
-    eul_compare_kernel<<<blocks, 256, 0, s>>>(eulers, w->eul, n, w->need);
-    count_launch();
-  }
-  eul_update_kernel<<<blocks, 256, 0, s>>>(eulers, w->eul, n, w->need);
+  eul_check_kernel<<<kEulCheckBlocks, 256, 0, s>>>(eulers, w->eul, n, force ? 1 : 0, w->need);
   count_launch();
   B200D2_CUDA_TRY(cudaGetLastError());
-  st = tc_run(v, b, precision, w->ptr, need, s, w->need);
+  st = tc_run(v, b, precision, w->ptr, need, s, w->need, w->eul);
   if (st == B200D2_OK) w->key = key;
   return st;
 }

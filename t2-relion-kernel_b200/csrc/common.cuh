@@ -33,6 +33,10 @@ void count_launch(unsigned n = 1);
 // valid only while it is unchanged.
 unsigned long long projector_epoch();
 
+// Blocks of the projection cache's check of the Euler matrices: block b
+// writes its verdict to word b, and the projection stage ORs the words.
+constexpr int kEulCheckBlocks = 64;
+
 // NVTX range over a host scope (a batch call, a pipeline stage, a served
 // request), so that a timeline profiler labels the library's launches; without
 // a profiler attached the push and pop cost a few nanoseconds.

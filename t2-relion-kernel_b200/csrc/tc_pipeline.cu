@@ -64,10 +64,13 @@ struct TcGeom {
   int gen;
   size_t off_status, off_xy, off_idx, off_ex, off_ey, off_ph, off_bhi, off_blo, off_q, off_w, off_normx, off_na, off_nahl,
       off_ahi, off_alo, off_keys, off_sa, off_sb, off_part, off_cnt, off_wx, off_cxy, off_thdr, off_exc, off_eyc, total;
-  // device flag read by the projection stage: 0 = the workspace already
-  // holds this call's projections (skip the stage), else project; null =
-  // always project (set by the single-particle entry point's projection cache)
+  // device flags read by the projection stage (kEulCheckBlocks words): all
+  // 0 = the workspace already holds this call's projections (skip the
+  // stage), else project and copy the Euler matrices to d_eul_cache; null =
+  // always project (both set by the single-particle entry point's projection
+  // cache)
   const int* d_proj_need;
+  float* d_eul_cache;
   int split_max;  // largest k-split the workspace holds partial sums for
   int n_cnt;      // split arrival counters
 };
@@ -540,8 +543,16 @@ template <int PREC>
 __global__ void __launch_bounds__(128) tc_project_kernel(b200d2_view v, const float* __restrict__ eulers,
                                                          int O, const int2* __restrict__ xy, int K_c,
                                                          int Kpad, void* bhi, void* blo, double* q,
-                                                         const int* __restrict__ need) {
-  if (need && *need == 0) return;  // the workspace holds these projections already
+                                                         const int* __restrict__ need, float* eul_cache) {
+  if (need) {  // kEulCheckBlocks verdict words of the cache check
+    const int any = __syncthreads_or(threadIdx.x < kEulCheckBlocks ? need[threadIdx.x] : 0);
+    if (!any) return;     // the workspace holds these projections already
+    if (blockIdx.x == 0)  // keep the Euler matrices projected here for the next call's check
+      for (int i = threadIdx.x; i < kProjOrients * 9; i += blockDim.x) {
+        const int o = blockIdx.y * kProjOrients + i / 9;
+        if (o < O) eul_cache[(size_t)o * 9 + i % 9] = eulers[(size_t)o * 9 + i % 9];
+      }
+  }
   const int kp = blockIdx.x * blockDim.x + threadIdx.x;  // complex pixel slot
   if (kp >= Kpad / 2) return;
   const int2 c = kp < K_c ? xy[kp] : make_int2(0, 0);
@@ -2460,7 +2471,7 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
         static_assert(256 % kProjOrients == 0, "orientation groups divide Opad");
         dim3 grid((g.Kpad / 2 + 127) / 128, g.Opad / kProjOrients);
         tc_project_kernel<PREC><<<grid, 128, 0, s>>>(v, b.d_eulers, g.O, xy, g.K_c, g.Kpad, bhi, blo, q,
-                                                     g.d_proj_need);
+                                                     g.d_proj_need, g.d_eul_cache);
       }
       break;
     }
@@ -2541,10 +2552,13 @@ size_t tc_workspace_bytes(const b200d2_view& v, const b200d2_batch& b, int preci
 
 // Where a batch's projections live in its workspace and what they were
 // computed from, for the single-particle entry point's projection cache:
-// false for the FP16 forms (their projection stage also rescales per call).
+// false for the FP16 forms (their projection stage also rescales per call)
+// and for projections of fewer than 2^20 samples, which take less time than
+// the check that would skip them.
 bool tc_projection_layout(const b200d2_view& v, const b200d2_batch& b, int precision, std::vector<uint64_t>& key) {
   if (precision == B200D2_PREC_FP16 || precision == B200D2_PREC_FP16X3) return false;
   const TcGeom g = make_geom(v, b, precision);
+  if ((long long)g.O * g.K_c < (1LL << 20)) return false;
   key.insert(key.end(), {(uint64_t)precision, (uint64_t)g.elem, (uint64_t)g.terms, (uint64_t)g.K_c,
                          (uint64_t)g.Kpad, (uint64_t)g.Kq, (uint64_t)g.O, (uint64_t)g.Opad, (uint64_t)g.maxR,
                          (uint64_t)g.off_xy, (uint64_t)g.off_bhi, (uint64_t)g.off_blo, (uint64_t)g.off_q,
@@ -2730,12 +2744,13 @@ unsigned long long launch_counter();
 void uncount_launch(unsigned n);
 
 int tc_run(const b200d2_view& v, const b200d2_batch& b, int precision, void* ws, size_t ws_bytes,
-           cudaStream_t s, const int* d_proj_need) {
+           cudaStream_t s, const int* d_proj_need, float* d_eul_cache) {
   NvtxRange range("b200d2_diff2_coarse_batch");
   int st = check_tc(v, b);
   if (st != B200D2_OK) return st;
   TcGeom g = make_geom(v, b, precision);
   g.d_proj_need = d_proj_need;
+  g.d_eul_cache = d_eul_cache;
   if (ws_bytes < g.total) return B200D2_ERR_INVALID;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   if (!g_batch_graphs.load() || cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
@@ -2744,6 +2759,7 @@ int tc_run(const b200d2_view& v, const b200d2_batch& b, int precision, void* ws,
   B200D2_CUDA_TRY(cudaGetDevice(&dev));
   std::vector<uint64_t> key = batch_key(v, b, precision, ws, ws_bytes, s, dev);
   key.push_back((uint64_t)(uintptr_t)d_proj_need);
+  key.push_back((uint64_t)(uintptr_t)d_eul_cache);
   std::unique_lock<std::mutex> lk(g_graph_mu);
   BatchGraph* e = nullptr;
   for (BatchGraph& x : g_graphs)

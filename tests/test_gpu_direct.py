@@ -190,10 +190,11 @@ def test_single_particle_projection_cache(pkg, synth, cuda):
     place (the device comparison misses), another translation count (the
     workspace layout moves), an FP16 form in between (never cached), and the
     projector destroyed and created again with another volume at the same
-    geometry (the projector epoch)."""
+    geometry (the projector epoch).  C2 geometry: projections of fewer than
+    2^20 samples are never cached (C1's take less time than the check)."""
     torch = cuda
-    pr = synth.make_problem("c1", P=4)
-    pr_b = synth.make_problem("c1", P=4, seed=99)  # same geometry, another volume
+    pr = synth.make_problem("c2", P=4)
+    pr_b = synth.make_problem("c2", P=4, seed=99)  # same geometry, another volume
     dp = DeviceProblem(torch, pr)
 
     def sequence():
@@ -273,4 +274,31 @@ def test_single_particle_projection_cache_skips_work(pkg, synth, cuda):
         pkg.set_projection_cache(True)
     print(f"projecting {off:.3f} ms, reusing {on:.3f} ms per call")
     assert on < 0.8 * off, (on, off)
+    proj.close()
+
+
+def test_small_projections_are_not_cached(pkg, synth, cuda):
+    """C1 (576 orientations x 544 pixels, under 2^20 samples): the cache is not
+    used, so a call costs no more with it on than off (within noise)."""
+    torch = cuda
+    pr = synth.make_problem("c1", P=1)
+    proj = pkg.Projector(pr.projector, use_texture=1)
+    view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
+    dp = DeviceProblem(torch, pr)
+    out = torch.zeros(pr.O * pr.T, device="cuda")
+    n0 = pkg.launch_count()
+    pkg.run_diff2_kernel_coarse(view, dp.tx, dp.ty, dp.corr[0], dp.re[0], dp.im[0], dp.eulers, out, pr.O, pr.T,
+                                pr.N_img, precision=pkg.PREC_BF16X3)
+    torch.cuda.synchronize()
+    with_cache = pkg.launch_count() - n0
+    pkg.set_projection_cache(False)
+    try:
+        n0 = pkg.launch_count()
+        pkg.run_diff2_kernel_coarse(view, dp.tx, dp.ty, dp.corr[0], dp.re[0], dp.im[0], dp.eulers, out, pr.O, pr.T,
+                                    pr.N_img, precision=pkg.PREC_BF16X3)
+        torch.cuda.synchronize()
+        without = pkg.launch_count() - n0
+    finally:
+        pkg.set_projection_cache(True)
+    assert with_cache == without  # no check kernel
     proj.close()
