@@ -1437,6 +1437,17 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
         big = max(trace, key=lambda q: q["P"] * q["orient"].size * q["tx"].size)
         for tk, _ in [submit(big) for _ in range(slots)]:
             srv.wait(tk)
+        # and each reference's largest request in device bytes (the A operand's
+        # rows x pixels and the output dominate a request's footprint)
+        def nbytes(q):
+            n_img = refs[q["ref"]]["pr"].N_img
+            return q["P"] * q["tx"].size * (2 * n_img * 4 + q["orient"].size * 4)
+        for r in range(len(refs)):
+            mine = [q for q in trace if q["ref"] == r]
+            if mine:
+                heavy = max(mine, key=nbytes)
+                for tk, _ in [submit(heavy) for _ in range(slots)]:
+                    srv.wait(tk)
         admit0 = srv.stats()["admit_host_s"]
         t0 = time.perf_counter()
         sent = []
@@ -1449,11 +1460,13 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
             ts = time.perf_counter()
             tk, keep = submit(q)
             sent.append((tk, ts, q, keep))
-        lats, done_at, ev, dev_s = [], [], 0, 0.0
+        lats, done_at, ev, dev_s, slow = [], [], 0, 0.0, []
         for tk, ts, q, keep in sent:
             st, lat, dev = srv.wait(tk, timeout=600.0)
             if st != 0:
                 raise RuntimeError(f"request failed: status {st}")
+            slow.append((lat * 1e3, dev * 1e3, q["t"], C5_REFS[q["ref"]], q["P"], int(q["orient"].size),
+                         int(q["tx"].size)))
             lats.append(lat)
             done_at.append(ts + lat)
             dev_s += dev
@@ -1467,7 +1480,9 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
                 "evals": ev, "evals_per_s": ev / span, "span_s": span, "max_in_flight": stats["max_in_flight"],
                 "peak_bytes": stats["peak_bytes"], "admit_host_s_per_s": (stats["admit_host_s"] - admit0) / span,
                 # each request's stream time (first copy in to last copy out) summed, per second of the run
-                "device_s_per_s": dev_s / span}
+                "device_s_per_s": dev_s / span,
+                "slowest": [{"latency_ms": round(a, 3), "stream_ms": round(b, 3), "arrival_s": round(c, 4), "ref": r,
+                             "P": p_, "O": o_, "T": t_} for a, b, c, r, p_, o_, t_ in sorted(slow)[-5:]]}
 
     try:
         tc = replay(pkg.PREC_TF32, 4, 48 << 30, horizon)

@@ -301,14 +301,19 @@ void sched_loop(b200d2_server* s) {
     }
     if (progress) s->cv_done.notify_all();
     for (auto it = s->queue.begin(); it != s->queue.end();) {
-      int slot = -1;
-      for (int k = 0; k < s->slots; ++k)
-        if (!s->slot_busy[k]) {
-          slot = k;
-          break;
-        }
-      if (slot < 0) break;
       Req& q = **it;
+      // an idle slot whose buffer already holds the request (the smallest
+      // such), else the idle slot with the largest buffer, which grows: a
+      // growth maps new memory while the scheduler waits, so it is avoided
+      // whenever an idle slot can take the request as it is
+      int slot = -1, fit = -1;
+      for (int k = 0; k < s->slots; ++k) {
+        if (s->slot_busy[k]) continue;
+        if (s->dev_bytes[k] >= q.footprint && (fit < 0 || s->dev_bytes[k] < s->dev_bytes[fit])) fit = k;
+        if (slot < 0 || s->dev_bytes[k] > s->dev_bytes[slot]) slot = k;
+      }
+      if (slot < 0) break;
+      if (fit >= 0) slot = fit;
       if (s->st.bytes_in_use + q.footprint > s->budget) {
         ++it;
         continue;
