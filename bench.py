@@ -1209,7 +1209,7 @@ def significance_study(args):
     synth = load_synth()
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # the reference's own kernels, built from its sources into oracle/_ref
-    pr = synth.make_problem("c2")
+    pr = synth.make_problem("c2", P=args.particles)  # --particles: a smaller batch (profiling)
     proj = pkg.Projector(pr.projector, use_texture=1)
     view = proj.view(pr.imgX, pr.imgY, pr.imgMaxR)
     dev = "cuda"
