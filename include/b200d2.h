@@ -31,7 +31,8 @@ typedef enum b200d2_status {
   B200D2_ERR_OOM = 4,         /* device allocation failed */
   B200D2_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
   B200D2_ERR_NO_DEVICE = 6,   /* no usable sm_100 device */
-  B200D2_ERR_TOO_LARGE = 7    /* request exceeds a fixed capacity */
+  B200D2_ERR_TOO_LARGE = 7,   /* request exceeds a fixed capacity */
+  B200D2_ERR_CANCELLED = 8    /* a served request was cancelled before it ran */
 } b200d2_status;
 
 /* How the projector volume is interpolated. */
@@ -365,6 +366,7 @@ typedef struct b200d2_server_stats {
   int in_flight, queued, max_in_flight;
   size_t bytes_in_use, peak_bytes;
   double admit_host_s; /* scheduler-thread time spent issuing admitted requests' work */
+  long long cancelled;
 } b200d2_server_stats;
 
 /* slots: concurrent streams; hbm_budget_bytes: device bytes the in-flight
@@ -390,6 +392,11 @@ int b200d2_server_submit(b200d2_server* s, const b200d2_request* req,
 int b200d2_server_wait(b200d2_server* s, long long ticket, double timeout_s,
                        double* latency_s, double* device_s);
 int b200d2_server_get_stats(b200d2_server* s, b200d2_server_stats* st);
+/* Cancel a queued request: it will not run, and b200d2_server_wait returns
+ * B200D2_ERR_CANCELLED for it.  B200D2_ERR_UNSUPPORTED when the request has
+ * been admitted already (work on the GPU is not interrupted; wait for it),
+ * B200D2_ERR_INVALID for an unknown ticket. */
+int b200d2_server_cancel(b200d2_server* s, long long ticket);
 /* Drain all requests and free the server. */
 int b200d2_server_destroy(b200d2_server* s);
 

@@ -106,8 +106,12 @@ class Request(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("rejected", C.c_longlong),
                 ("evals", C.c_longlong), ("in_flight", C.c_int), ("queued", C.c_int), ("max_in_flight", C.c_int),
-                ("bytes_in_use", C.c_size_t), ("peak_bytes", C.c_size_t), ("admit_host_s", C.c_double)]
+                ("bytes_in_use", C.c_size_t), ("peak_bytes", C.c_size_t), ("admit_host_s", C.c_double),
+                ("cancelled", C.c_longlong)]
 
+
+# status codes (b200d2_status)
+OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_NO_DEVICE, ERR_TOO_LARGE, ERR_CANCELLED = range(9)
 
 PLAN_AUTOTUNE = 1
 PLAN_GRAPH = 2
@@ -158,6 +162,7 @@ def _declare(L):
         "b200d2_server_submit": [P, C.POINTER(Request), C.POINTER(C.c_longlong)],
         "b200d2_server_wait": [P, C.c_longlong, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)],
         "b200d2_server_get_stats": [P, C.POINTER(ServerStats)],
+        "b200d2_server_cancel": [P, C.c_longlong],
         "b200d2_server_destroy": [P],
         "b200d2_coarse_weights": [P, I, I, I, P, P, P, I, P, P, P, Z, P],
         "b200d2_significance": [P, I, C.c_longlong, P, C.c_double, C.c_longlong, P, P, P, P, Z, P],
@@ -455,6 +460,11 @@ class Server:
         st = lib().b200d2_server_wait(self._h, ticket, timeout, C.byref(lat), C.byref(dev))
         self._keep.pop(ticket, None)
         return st, lat.value, dev.value
+
+    def cancel(self, ticket: int) -> int:
+        """Cancel a queued request (b200d2_server_cancel): 0, or the status code
+        (ERR_UNSUPPORTED once it has been admitted, ERR_INVALID if unknown)."""
+        return int(lib().b200d2_server_cancel(self._h, ticket))
 
     def stats(self) -> dict:
         s = ServerStats()

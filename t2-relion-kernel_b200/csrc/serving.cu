@@ -65,6 +65,7 @@ struct Req {
   int slot = -1;
   void* dbuf = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool timed = false;  // both events recorded on the slot stream
   std::atomic<int> finished{0};
   struct b200d2_server* srv = nullptr;
 };
@@ -229,20 +230,29 @@ int admit(b200d2_server* s, Req& q) {
     w.staged = !page_locked(w.dst);
     if (w.staged) w.pin_off = stage_at(w.bytes);
   }
+  // a failed call leaves its error as this thread's last error, which the
+  // next launch check would report: start every request from a clean state
+  cudaGetLastError();
   uint8_t* pin = static_cast<uint8_t*>(slot_staging(s, q.slot, pin_need));
   if (pin_need && !pin) return B200D2_ERR_OOM;
   q.out_copies.clear();
   q.dbuf = slot_device(s, q.slot, q.footprint);
   if (!q.dbuf) return B200D2_ERR_OOM;
   uint8_t* d = static_cast<uint8_t*>(q.dbuf);
-  cudaEventRecord(q.ev0, st);
+  // the first failure among the copies and event records; the request still
+  // runs to its completion callback and reports it
+  cudaError_t first = cudaSuccess;
+  auto note = [&](cudaError_t e) {
+    if (e != cudaSuccess && first == cudaSuccess) first = e;
+  };
+  note(cudaEventRecord(q.ev0, st));
   for (const Up& u : ups) {
     const void* src = u.src;
     if (u.staged) {
       memcpy(pin + u.pin_off, u.src, u.bytes);
       src = pin + u.pin_off;
     }
-    cudaMemcpyAsync(d + u.dev_off, src, u.bytes, cudaMemcpyHostToDevice, st);
+    note(cudaMemcpyAsync(d + u.dev_off, src, u.bytes, cudaMemcpyHostToDevice, st));
   }
   b200d2_batch b;
   memset(&b, 0, sizeof(b));
@@ -265,13 +275,15 @@ int admit(b200d2_server* s, Req& q) {
   for (const Down& w : downs) {
     if (!w.dst) continue;
     if (w.staged) {
-      cudaMemcpyAsync(pin + w.pin_off, d + w.dev_off, w.bytes, cudaMemcpyDeviceToHost, st);
+      note(cudaMemcpyAsync(pin + w.pin_off, d + w.dev_off, w.bytes, cudaMemcpyDeviceToHost, st));
       q.out_copies.push_back(HostCopy{w.dst, pin + w.pin_off, w.bytes});
     } else {
-      cudaMemcpyAsync(w.dst, d + w.dev_off, w.bytes, cudaMemcpyDeviceToHost, st);
+      note(cudaMemcpyAsync(w.dst, d + w.dev_off, w.bytes, cudaMemcpyDeviceToHost, st));
     }
   }
-  cudaEventRecord(q.ev1, st);
+  note(cudaEventRecord(q.ev1, st));
+  q.timed = first == cudaSuccess;
+  if (rc == B200D2_OK && first != cudaSuccess) rc = b200d2::status_from_cuda(first);
   q.status = rc;  // final status once finished
   const cudaError_t e = cudaLaunchHostFunc(st, on_done, &q);
   if (e != cudaSuccess) return b200d2::status_from_cuda(e);
@@ -286,8 +298,11 @@ void sched_loop(b200d2_server* s) {
     for (size_t i = 0; i < s->inflight.size();) {
       Req& q = *s->inflight[i];
       if (q.finished.load()) {
+        // a request that failed before its work was issued has no recorded
+        // events (asking for their elapsed time would fail and leave an error)
         float ms = 0.f;
-        if (cudaEventElapsedTime(&ms, q.ev0, q.ev1) == cudaSuccess) q.device_s = ms / 1e3;
+        if (q.timed && cudaEventElapsedTime(&ms, q.ev0, q.ev1) == cudaSuccess) q.device_s = ms / 1e3;
+        cudaGetLastError();
         if (q.status == -1) q.status = B200D2_OK;
         s->slot_busy[q.slot] = 0;
         s->st.bytes_in_use -= q.footprint;
@@ -491,6 +506,28 @@ extern "C" int b200d2_server_wait(b200d2_server* s, long long ticket, double tim
   q->ev0 = q->ev1 = nullptr;
   s->all.erase(it);
   return status;
+}
+
+extern "C" int b200d2_server_cancel(b200d2_server* s, long long ticket) {
+  if (!s) return B200D2_ERR_INVALID;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end()) return B200D2_ERR_INVALID;
+    if (it->second->status == B200D2_ERR_CANCELLED) return B200D2_OK;  // cancelled before
+    auto qi = std::find(s->queue.begin(), s->queue.end(), it->second);
+    if (qi == s->queue.end()) return B200D2_ERR_UNSUPPORTED;  // admitted already
+    Req& q = **qi;
+    q.status = B200D2_ERR_CANCELLED;
+    q.t_done = now_s();
+    q.finished.store(1);
+    s->queue.erase(qi);
+    s->st.cancelled++;
+    s->st.queued = (int)s->queue.size();
+  }
+  s->cv_done.notify_all();
+  s->cv_sched.notify_all();
+  return B200D2_OK;
 }
 
 extern "C" int b200d2_server_get_stats(b200d2_server* s, b200d2_server_stats* st) {

@@ -5,6 +5,8 @@ deterministic, so within 1e-6 relative), and agree with the FP64 CUDA-core
 kernel within the TF32 tolerance (1e-3)."""
 from __future__ import annotations
 
+import time
+
 import numpy as np
 import pytest
 
@@ -145,4 +147,73 @@ def test_serving_page_locked_and_pageable_buffers(pkg, synth, cuda):
                 np.testing.assert_array_equal(a, b)
         assert np.all(base[1] == base[0].reshape(len(rq["ps"]), -1).min(axis=1))
     srv.close()
+    proj.close()
+
+
+def test_serving_cancel_queued_request(pkg, synth, cuda):
+    """A queued request can be cancelled: it never runs and its wait returns
+    ERR_CANCELLED; an admitted one cannot (ERR_UNSUPPORTED) and completes; an
+    unknown ticket is ERR_INVALID.  One slot held by a C2 batch of 256
+    particles on the FP32 CUDA cores (about 57 ms) keeps the queue waiting
+    while the test cancels."""
+    prob = synth.make_problem("c2")
+    proj = pkg.Projector(prob.projector, use_texture=1)
+    view = proj.view(prob.imgX, prob.imgY, prob.imgMaxR)
+    srv = pkg.Server(slots=1, hbm_budget=8 << 30, precision=pkg.PREC_FP32)
+    ref = srv.add_reference(view, prob.eulers, prob.N_img)
+    allo = np.arange(prob.O, dtype=np.int32)
+    mn_a, am_a = np.zeros(prob.P), np.zeros(prob.P, np.int64)
+    long_t = srv.submit(ref, prob.fimg_re, prob.fimg_im, prob.corr, allo, prob.trans_x, prob.trans_y, None, mn_a, am_a)
+    t0 = time.monotonic()
+    while srv.stats()["in_flight"] < 1:  # admitted: the slot is busy from here on
+        assert time.monotonic() - t0 < 30.0
+        time.sleep(0.0005)
+    small = [srv.submit(ref, prob.fimg_re[:1].copy(), prob.fimg_im[:1].copy(), prob.corr[:1].copy(), allo[:64],
+                        prob.trans_x, prob.trans_y, None, np.zeros(1), np.zeros(1, np.int64)) for _ in range(3)]
+    assert srv.cancel(long_t) == pkg.ERR_UNSUPPORTED  # running: not interrupted
+    assert srv.cancel(small[1]) == pkg.OK
+    assert srv.cancel(small[1]) == pkg.OK  # again: still cancelled
+    st_long = srv.wait(long_t)[0]
+    assert st_long == pkg.OK and np.isfinite(mn_a).all()
+    assert srv.cancel(long_t) == pkg.ERR_INVALID  # waited for: the ticket is gone
+    assert srv.wait(small[0])[0] == pkg.OK
+    assert srv.wait(small[1])[0] == pkg.ERR_CANCELLED
+    assert srv.wait(small[2])[0] == pkg.OK
+    st = srv.stats()
+    assert st["cancelled"] == 1 and st["completed"] == 3
+    srv.close()
+    proj.close()
+
+
+def test_serving_allocation_failure_is_reported(pkg, synth, cuda):
+    """A request whose device footprint cannot be allocated (its output alone
+    is about 400 GB, more than the GPU holds, within a 1 TB budget) fails with
+    ERR_OOM before anything is launched, and the server goes on serving: the
+    next request's minima and argmins equal those of a server that never saw
+    the failure (the kernels are deterministic)."""
+    prob = synth.make_problem("c1", P=8)
+    proj = pkg.Projector(prob.projector, use_texture=1)
+    view = proj.view(prob.imgX, prob.imgY, prob.imgMaxR)
+    srv = pkg.Server(slots=2, hbm_budget=1 << 40, precision=pkg.PREC_FP32)
+    ref = srv.add_reference(view, prob.eulers, prob.N_img)
+    allo = np.arange(prob.O, dtype=np.int32)
+    T = 22_000_000  # 8 x 576 x 2.2e7 x 4 B = 405 GB of diff2
+    tx = np.zeros(T, np.float32)
+    t_big = srv.submit(ref, prob.fimg_re, prob.fimg_im, prob.corr, allo, tx, tx, None, np.zeros(prob.P),
+                       np.zeros(prob.P, np.int64))
+    assert srv.wait(t_big, timeout=120.0)[0] == pkg.ERR_OOM
+    mn, am = np.zeros(prob.P), np.zeros(prob.P, np.int64)
+    t_ok = srv.submit(ref, prob.fimg_re, prob.fimg_im, prob.corr, allo, prob.trans_x, prob.trans_y, None, mn, am)
+    assert srv.wait(t_ok)[0] == pkg.OK
+    assert np.isfinite(mn).all() and (am >= 0).all()
+    assert srv.stats()["completed"] == 2
+    srv.close()
+    fresh = pkg.Server(slots=2, hbm_budget=1 << 40, precision=pkg.PREC_FP32)
+    ref2 = fresh.add_reference(view, prob.eulers, prob.N_img)
+    mn2, am2 = np.zeros(prob.P), np.zeros(prob.P, np.int64)
+    t2 = fresh.submit(ref2, prob.fimg_re, prob.fimg_im, prob.corr, allo, prob.trans_x, prob.trans_y, None, mn2, am2)
+    assert fresh.wait(t2)[0] == pkg.OK
+    np.testing.assert_array_equal(am, am2)
+    np.testing.assert_array_equal(mn, mn2)
+    fresh.close()
     proj.close()
