@@ -1416,8 +1416,10 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
         trace.append(dict(t=t, ref=r, s0=s0, P=P, orient=orient, tx=tx, ty=ty))
     evals = sum(q["P"] * q["orient"].size * q["tx"].size for q in trace)
 
-    def replay(precision, slots, budget, limit_s, burst=False):
+    def replay(precision, slots, budget, limit_s, burst=False, merge=True):
         srv = pkg.Server(slots=slots, hbm_budget=budget, precision=precision)
+        if not merge:
+            srv.set_merging(1)
         ids = [srv.add_reference(rf["view"], rf["pr"].eulers, rf["pr"].N_img) for rf in refs]
 
         def submit(q):
@@ -1448,7 +1450,8 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
                 heavy = max(mine, key=nbytes)
                 for tk, _ in [submit(heavy) for _ in range(slots)]:
                     srv.wait(tk)
-        admit0 = srv.stats()["admit_host_s"]
+        st0 = srv.stats()
+        admit0, stream0 = st0["admit_host_s"], st0["stream_s"]
         t0 = time.perf_counter()
         sent = []
         for q in trace:
@@ -1460,7 +1463,7 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
             ts = time.perf_counter()
             tk, keep = submit(q)
             sent.append((tk, ts, q, keep))
-        lats, done_at, ev, dev_s, slow = [], [], 0, 0.0, []
+        lats, done_at, ev, slow = [], [], 0, []
         for tk, ts, q, keep in sent:
             st, lat, dev = srv.wait(tk, timeout=600.0)
             if st != 0:
@@ -1469,7 +1472,6 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
                          int(q["tx"].size)))
             lats.append(lat)
             done_at.append(ts + lat)
-            dev_s += dev
             ev += q["P"] * q["orient"].size * q["tx"].size
         stats = srv.stats()
         srv.close()
@@ -1479,8 +1481,11 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
                 "p99_ms": float(np.percentile(lat_ms, 99)), "mean_ms": float(lat_ms.mean()),
                 "evals": ev, "evals_per_s": ev / span, "span_s": span, "max_in_flight": stats["max_in_flight"],
                 "peak_bytes": stats["peak_bytes"], "admit_host_s_per_s": (stats["admit_host_s"] - admit0) / span,
-                # each request's stream time (first copy in to last copy out) summed, per second of the run
-                "device_s_per_s": dev_s / span,
+                # merged admissions over the whole run (warm-up included) and the requests they carried
+                "merged_admissions": stats["merged_admissions"], "merged_requests": stats["merged_requests"],
+                # each admission's stream time (first copy in to last copy out; a merged
+                # admission once) summed, per second of the run
+                "device_s_per_s": (stats["stream_s"] - stream0) / span,
                 "slowest": [{"latency_ms": round(a, 3), "stream_ms": round(b, 3), "arrival_s": round(c, 4), "ref": r,
                              "P": p_, "O": o_, "T": t_} for a, b, c, r, p_, o_, t_ in sorted(slow)[-5:]]}
 
@@ -1490,6 +1495,8 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
         # queue never empties and evals/s measures the server, not the offered
         # load (latencies then include the queueing of the whole burst)
         sat = replay(pkg.PREC_TF32, 4, 48 << 30, horizon, burst=True)
+        # the same burst with one request per admission (merging off)
+        sat1 = replay(pkg.PREC_TF32, 4, 48 << 30, horizon, burst=True, merge=False)
         # the FP32 baseline cannot keep up with 200 requests/s; replay the
         # first part of the same trace so the run stays bounded
         fp32 = replay(pkg.PREC_FP32, 1, 48 << 30, min(horizon, fp32_seconds))
@@ -1501,7 +1508,8 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
                         f"particles per request, 10-100 % orientation subsets, translation radius "
                         f"2-6 px, outputs: per-particle min/argmin",
             "slots": 4, "hbm_budget_gib": 48, "trace_evals": evals,
-            "tensor_core_tf32": tc, "tensor_core_tf32_saturated": sat, "fp32_cuda_core_per_request": fp32,
+            "tensor_core_tf32": tc, "tensor_core_tf32_saturated": sat,
+            "tensor_core_tf32_saturated_unmerged": sat1, "fp32_cuda_core_per_request": fp32,
             "evals_per_s_ratio": tc["evals_per_s"] / fp32["evals_per_s"]}
 
 
@@ -1517,6 +1525,7 @@ def serving_arm(args):
             "n_gpus": 1, "higher_is_better": False, "dtype": "tf32", "data": "synthetic",
             "config": {k: r[k] for k in ("workload", "slots", "hbm_budget_gib", "trace_evals")},
             "tensor_core_tf32": tc, "tensor_core_tf32_saturated": r["tensor_core_tf32_saturated"],
+            "tensor_core_tf32_saturated_unmerged": r["tensor_core_tf32_saturated_unmerged"],
             "fp32_cuda_core_per_request": r["fp32_cuda_core_per_request"],
             "evals_per_s_ratio": r["evals_per_s_ratio"]}
     print(json.dumps(line), flush=True)

@@ -367,6 +367,10 @@ typedef struct b200d2_server_stats {
   size_t bytes_in_use, peak_bytes;
   double admit_host_s; /* scheduler-thread time spent issuing admitted requests' work */
   long long cancelled;
+  /* merged admissions (b200d2_server_set_merging) and the requests they ran */
+  long long merged_admissions, merged_requests;
+  double stream_s; /* slot-stream time of the completed admissions (first copy in to
+                      last copy out; a merged admission counted once) */
 } b200d2_server_stats;
 
 /* slots: concurrent streams; hbm_budget_bytes: device bytes the in-flight
@@ -388,10 +392,23 @@ int b200d2_server_add_reference(b200d2_server* s, const b200d2_view* view,
 int b200d2_server_submit(b200d2_server* s, const b200d2_request* req,
                          long long* ticket);
 /* Wait for a request: status of the request, its latency (submit to
- * completion, seconds) and its device time (seconds). */
+ * completion, seconds) and its device time (seconds: the stream time of the
+ * run that carried it, shared by the requests of a merged admission). */
 int b200d2_server_wait(b200d2_server* s, long long ticket, double timeout_s,
                        double* latency_s, double* device_s);
 int b200d2_server_get_stats(b200d2_server* s, b200d2_server_stats* st);
+/* Merged admissions.  When a slot frees up, the scheduler runs the first
+ * queued request that fits together with later queued requests on the same
+ * reference (arrival order), up to max_requests requests and max_particles
+ * particles in all, as one batch: one copy-in, one pipeline run and one
+ * copy-out on one slot, instead of a pipeline per request.  The batch is
+ * block-diagonal: each request's particles are scored against its own
+ * orientations at its own translations only, so no request pays for
+ * another's, and each result equals the request's result alone (same
+ * kernels, same sums).  The merged requests complete together.  Tensor-core
+ * servers only; max_requests = 1 turns merging off.  Default: 8 requests,
+ * 512 particles. */
+int b200d2_server_set_merging(b200d2_server* s, int max_requests, int max_particles);
 /* Cancel a queued request: it will not run, and b200d2_server_wait returns
  * B200D2_ERR_CANCELLED for it.  B200D2_ERR_UNSUPPORTED when the request has
  * been admitted already (work on the GPU is not interrupted; wait for it),

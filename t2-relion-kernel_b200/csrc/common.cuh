@@ -189,4 +189,37 @@ __host__ __device__ __forceinline__ bool pixel_maybe_inside(int x, int y,
   return r2 < (double)maxR2_padded + 2.0;
 }
 
+// Merged batches: several requests on one reference in one stream-ordered
+// pipeline run, each request's particles against its own orientation columns
+// (tc_pipeline.cu; used by the serving loop).
+struct MergedRequest {
+  int P, O, T;  // particles, orientations, translations
+  int col0;     // first column of its orientations in the merged set: a multiple of 256, increasing
+  const float* h_tx;  // host [T] phase slopes
+  const float* h_ty;
+};
+struct MergedDev {
+  const float* re;  // device [P][N_img]
+  const float* im;
+  const float* corr;
+  float* out;  // device [P][O][T]
+};
+struct MergedBatch;
+// Host-side tables of the batch (no CUDA calls); null with *status set when invalid.
+MergedBatch* merged_create(const b200d2_view& v, int N_img, int precision, const MergedRequest* r, int n,
+                           int O_cols, int* status);
+// Device bytes (workspace and tables) and page-locked staging bytes (tables) of a run.
+size_t merged_device_bytes(const MergedBatch* m);
+size_t merged_host_bytes(const MergedBatch* m);
+// Copy the tables from `hstage` (page-locked, 256-byte aligned, merged_host_bytes)
+// into `dmem` (256-byte aligned, merged_device_bytes) and launch every stage on s.
+// d_eulers: [O_cols][9] device; d_min / d_argmin: device [sum of P] in request order.
+int merged_enqueue(MergedBatch* m, const float* d_eulers, const MergedDev* d, double* d_min, long long* d_argmin,
+                   void* dmem, void* hstage, cudaStream_t s);
+void merged_destroy(MergedBatch* m);
+
+// Load every kernel the tensor-core pipeline of `precision` can launch
+// (instead of at its first launch, which can wait for running work).
+int tc_preload(int precision);
+
 }  // namespace b200d2

@@ -68,6 +68,11 @@ struct Req {
   bool timed = false;  // both events recorded on the slot stream
   std::atomic<int> finished{0};
   struct b200d2_server* srv = nullptr;
+  // a merged admission: the other requests its run carries (this one holds
+  // the slot, the footprint, the events and the completion callback); a
+  // member is finished by the scheduler when its leader is
+  std::vector<std::shared_ptr<Req>> members;
+  bool member = false;
 };
 
 }  // namespace
@@ -85,6 +90,7 @@ struct b200d2_server {
   std::vector<size_t> dev_bytes;
   std::vector<void*> pin;          // per slot: page-locked staging buffer
   std::vector<size_t> pin_bytes;
+  std::vector<void*> pin_retired;  // outgrown staging buffers, freed with the server
   std::deque<std::shared_ptr<Req>> queue;
   std::vector<std::shared_ptr<Req>> inflight;
   std::map<long long, std::shared_ptr<Req>> all;
@@ -94,6 +100,9 @@ struct b200d2_server {
   bool stop = false;
   long long next_ticket = 1;
   b200d2_server_stats st{};
+  // merged admissions (b200d2_server_set_merging): queued requests on one
+  // reference run as one batch, at most this many requests and particles
+  int merge_requests = 8, merge_particles = 512;
 };
 
 namespace {
@@ -122,7 +131,9 @@ bool page_locked(const void* p) {
 void* slot_staging(b200d2_server* s, int slot, size_t need) {
   if (need == 0) return nullptr;
   if (s->pin_bytes[slot] < need) {
-    if (s->pin[slot]) cudaFreeHost(s->pin[slot]);
+    // cudaFreeHost waits for the device to go idle, which would stall every
+    // slot: an outgrown buffer is kept until the server is destroyed
+    if (s->pin[slot]) s->pin_retired.push_back(s->pin[slot]);
     s->pin[slot] = nullptr;
     s->pin_bytes[slot] = 0;
     const size_t bytes = std::max(need + need / 2, (size_t)1 << 20);
@@ -290,6 +301,182 @@ int admit(b200d2_server* s, Req& q) {
   return B200D2_OK;
 }
 
+// A merged admission: requests on one reference (arrival order, the first
+// one the leader) as one block-diagonal batch.  Each request's orientations
+// take columns from a multiple of 256, so that no tile of the contraction
+// holds two requests' columns.
+struct MergedLayout {
+  std::vector<b200d2::MergedRequest> mr;
+  int O_cols = 0, P = 0;
+  b200d2::MergedBatch* mb = nullptr;
+  size_t footprint = 0;
+};
+
+int merged_layout(b200d2_server* s, const std::vector<std::shared_ptr<Req>>& grp, MergedLayout& L) {
+  const Ref& ref = s->refs[grp[0]->r.ref];
+  L.mr.clear();
+  L.P = 0;
+  long long col = 0;
+  for (const auto& q : grp) {
+    b200d2::MergedRequest m;
+    m.P = q->r.P;
+    m.O = q->r.O;
+    m.T = q->r.T;
+    m.col0 = (int)col;
+    m.h_tx = q->r.h_trans_x;
+    m.h_ty = q->r.h_trans_y;
+    L.mr.push_back(m);
+    col = (col + q->r.O + 255) / 256 * 256;
+    L.P += q->r.P;
+  }
+  if (col > (1 << 30)) return B200D2_ERR_TOO_LARGE;
+  L.O_cols = L.mr.back().col0 + L.mr.back().O;
+  int st = B200D2_OK;
+  L.mb = b200d2::merged_create(ref.view, ref.N_img, s->prec, L.mr.data(), (int)L.mr.size(), L.O_cols, &st);
+  if (!L.mb) return st;
+  size_t fp = up256((size_t)L.O_cols * 9 * sizeof(float)) + up256((size_t)L.P * sizeof(double)) +
+              up256((size_t)L.P * sizeof(long long)) + up256(b200d2::merged_device_bytes(L.mb));
+  for (const auto& q : grp)
+    fp += 3 * up256((size_t)q->r.P * ref.N_img * sizeof(float)) +
+          up256((size_t)q->r.P * q->r.O * q->r.T * sizeof(float));
+  L.footprint = fp;
+  return B200D2_OK;
+}
+
+// Launch a merged admission's work on the leader's slot stream (called with
+// the lock held): every request's copies in, one pipeline run, every
+// request's copies out, one completion callback.
+int admit_merged(b200d2_server* s, Req& lead, const std::vector<std::shared_ptr<Req>>& grp, MergedLayout& L) {
+  char label[80];
+  snprintf(label, sizeof(label), "b200d2 merged requests %lld.. (%d requests, ref %d, %d particles)", lead.ticket,
+           (int)grp.size(), lead.r.ref, L.P);
+  b200d2::NvtxRange range(label);
+  const Ref& ref = s->refs[lead.r.ref];
+  cudaStream_t st = s->streams[lead.slot];
+  const int n = (int)grp.size();
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    size_t a = off;
+    off += up256(b);
+    return a;
+  };
+  struct Up {
+    size_t dev_off;
+    const void* src;
+    size_t bytes;
+    bool staged;
+    size_t pin_off;
+  };
+  struct Down {
+    void* dst;
+    size_t dev_off;
+    size_t bytes;
+    bool staged;
+    size_t pin_off;
+  };
+  size_t pin_need = 0;
+  auto stage_at = [&](size_t bytes) {
+    size_t a = pin_need;
+    pin_need += up256(bytes);
+    return a;
+  };
+  // staging: the batch's tables first (256-byte aligned), the merged
+  // orientations, then the host buffers that are not page-locked
+  const size_t p_tab = stage_at(b200d2::merged_host_bytes(L.mb));
+  const size_t eu_bytes = (size_t)L.O_cols * 9 * sizeof(float);
+  const size_t p_eu = stage_at(eu_bytes);
+  const size_t o_eu = take(eu_bytes), o_mn = take((size_t)L.P * sizeof(double)),
+               o_am = take((size_t)L.P * sizeof(long long));
+  std::vector<b200d2::MergedDev> md(n);
+  std::vector<size_t> o_in(n), o_out(n);
+  std::vector<Up> ups;
+  std::vector<Down> downs;
+  int part0 = 0;
+  for (int k = 0; k < n; ++k) {
+    const b200d2_request& r = grp[k]->r;
+    const size_t img = (size_t)r.P * ref.N_img * sizeof(float);
+    const size_t out = (size_t)r.P * r.O * r.T * sizeof(float);
+    o_in[k] = take(img);
+    take(img);
+    take(img);
+    o_out[k] = take(out);
+    ups.push_back({o_in[k], r.h_real, img, false, 0});
+    ups.push_back({o_in[k] + up256(img), r.h_imag, img, false, 0});
+    ups.push_back({o_in[k] + 2 * up256(img), r.h_corr, img, false, 0});
+    if (r.h_diff2) downs.push_back({r.h_diff2, o_out[k], out, false, 0});
+    if (r.h_min) downs.push_back({r.h_min, o_mn + (size_t)part0 * sizeof(double), (size_t)r.P * sizeof(double), false, 0});
+    if (r.h_argmin)
+      downs.push_back({r.h_argmin, o_am + (size_t)part0 * sizeof(long long), (size_t)r.P * sizeof(long long), false, 0});
+    part0 += r.P;
+  }
+  const size_t o_mb = take(b200d2::merged_device_bytes(L.mb));
+  for (Up& u : ups) {
+    u.staged = !page_locked(u.src);
+    if (u.staged) u.pin_off = stage_at(u.bytes);
+  }
+  for (Down& w : downs) {
+    w.staged = !page_locked(w.dst);
+    if (w.staged) w.pin_off = stage_at(w.bytes);
+  }
+  cudaGetLastError();  // start from a clean error state (see admit)
+  uint8_t* pin = static_cast<uint8_t*>(slot_staging(s, lead.slot, pin_need));
+  if (!pin) return B200D2_ERR_OOM;
+  lead.out_copies.clear();
+  lead.dbuf = slot_device(s, lead.slot, lead.footprint);
+  if (!lead.dbuf) return B200D2_ERR_OOM;
+  uint8_t* d = static_cast<uint8_t*>(lead.dbuf);
+  // the merged orientations: each request's Euler matrices at its columns;
+  // the columns between requests (projected, read by no particle) repeat the
+  // next request's first matrix
+  float* eu = reinterpret_cast<float*>(pin + p_eu);
+  int end = 0;
+  for (int k = 0; k < n; ++k) {
+    const b200d2::MergedRequest& m = L.mr[k];
+    for (int c = end; c < m.col0; ++c) memcpy(eu + (size_t)c * 9, grp[k]->eul.data(), 9 * sizeof(float));
+    memcpy(eu + (size_t)m.col0 * 9, grp[k]->eul.data(), (size_t)m.O * 9 * sizeof(float));
+    end = m.col0 + m.O;
+  }
+  cudaError_t first = cudaSuccess;
+  auto note = [&](cudaError_t e) {
+    if (e != cudaSuccess && first == cudaSuccess) first = e;
+  };
+  note(cudaEventRecord(lead.ev0, st));
+  for (const Up& u : ups) {
+    const void* src = u.src;
+    if (u.staged) {
+      memcpy(pin + u.pin_off, u.src, u.bytes);
+      src = pin + u.pin_off;
+    }
+    note(cudaMemcpyAsync(d + u.dev_off, src, u.bytes, cudaMemcpyHostToDevice, st));
+  }
+  note(cudaMemcpyAsync(d + o_eu, eu, eu_bytes, cudaMemcpyHostToDevice, st));
+  for (int k = 0; k < n; ++k) {
+    const size_t img = up256((size_t)grp[k]->r.P * ref.N_img * sizeof(float));
+    md[k].re = reinterpret_cast<const float*>(d + o_in[k]);
+    md[k].im = reinterpret_cast<const float*>(d + o_in[k] + img);
+    md[k].corr = reinterpret_cast<const float*>(d + o_in[k] + 2 * img);
+    md[k].out = reinterpret_cast<float*>(d + o_out[k]);
+  }
+  int rc = b200d2::merged_enqueue(L.mb, reinterpret_cast<const float*>(d + o_eu), md.data(),
+                                  reinterpret_cast<double*>(d + o_mn), reinterpret_cast<long long*>(d + o_am),
+                                  d + o_mb, pin + p_tab, st);
+  for (const Down& w : downs) {
+    if (w.staged) {
+      note(cudaMemcpyAsync(pin + w.pin_off, d + w.dev_off, w.bytes, cudaMemcpyDeviceToHost, st));
+      lead.out_copies.push_back(HostCopy{w.dst, pin + w.pin_off, w.bytes});
+    } else {
+      note(cudaMemcpyAsync(w.dst, d + w.dev_off, w.bytes, cudaMemcpyDeviceToHost, st));
+    }
+  }
+  note(cudaEventRecord(lead.ev1, st));
+  lead.timed = first == cudaSuccess;
+  if (rc == B200D2_OK && first != cudaSuccess) rc = b200d2::status_from_cuda(first);
+  lead.status = rc;
+  const cudaError_t e = cudaLaunchHostFunc(st, on_done, &lead);
+  if (e != cudaSuccess) return b200d2::status_from_cuda(e);
+  return B200D2_OK;
+}
+
 void sched_loop(b200d2_server* s) {
   cudaSetDevice(s->device);
   std::unique_lock<std::mutex> lk(s->mu);
@@ -306,8 +493,19 @@ void sched_loop(b200d2_server* s) {
         if (q.status == -1) q.status = B200D2_OK;
         s->slot_busy[q.slot] = 0;
         s->st.bytes_in_use -= q.footprint;
+        s->st.stream_s += q.device_s;
         s->st.completed++;
         if (q.status == B200D2_OK) s->st.evals += (long long)q.r.P * q.r.O * q.r.T;
+        // the requests merged into this one's run finish with it
+        for (const std::shared_ptr<Req>& m : q.members) {
+          m->device_s = q.device_s;
+          m->t_done = q.t_done;
+          m->status = q.status;
+          s->st.completed++;
+          if (m->status == B200D2_OK) s->st.evals += (long long)m->r.P * m->r.O * m->r.T;
+          m->finished.store(1);
+        }
+        q.members.clear();
         s->inflight.erase(s->inflight.begin() + i);
         progress = true;
       } else {
@@ -333,6 +531,72 @@ void sched_loop(b200d2_server* s) {
         ++it;
         continue;
       }
+      // merge later queued requests on the same reference into this one's
+      // run while the particle and request limits and the budget allow
+      std::vector<std::shared_ptr<Req>> grp;
+      MergedLayout L;
+      if (s->merge_requests > 1 && b200d2::is_tc_precision(s->prec) && q.r.P < s->merge_particles) {
+        grp.push_back(*it);
+        int P = q.r.P;
+        for (auto jt = std::next(it); jt != s->queue.end() && (int)grp.size() < s->merge_requests; ++jt)
+          if ((*jt)->r.ref == q.r.ref && P + (*jt)->r.P <= s->merge_particles) {
+            grp.push_back(*jt);
+            P += (*jt)->r.P;
+          }
+        while (grp.size() > 1) {
+          if (merged_layout(s, grp, L) == B200D2_OK && s->st.bytes_in_use + L.footprint <= s->budget) break;
+          b200d2::merged_destroy(L.mb);
+          L.mb = nullptr;
+          grp.pop_back();
+        }
+        if (grp.size() < 2) grp.clear();
+      }
+      if (!grp.empty()) {
+        // the slot for the merged footprint, chosen as above
+        int fit2 = -1;
+        for (int k = 0; k < s->slots; ++k)
+          if (!s->slot_busy[k] && s->dev_bytes[k] >= L.footprint && (fit2 < 0 || s->dev_bytes[k] < s->dev_bytes[fit2]))
+            fit2 = k;
+        if (fit2 >= 0) {
+          slot = fit2;
+        } else {
+          for (int k = 0; k < s->slots; ++k)
+            if (!s->slot_busy[k] && s->dev_bytes[k] > s->dev_bytes[slot]) slot = k;
+        }
+        q.slot = slot;
+        q.footprint = L.footprint;
+        s->slot_busy[slot] = 1;
+        s->st.bytes_in_use += q.footprint;
+        s->st.peak_bytes = std::max(s->st.peak_bytes, s->st.bytes_in_use);
+        for (size_t k = 1; k < grp.size(); ++k) {
+          grp[k]->member = true;
+          grp[k]->footprint = 0;
+          q.members.push_back(grp[k]);
+        }
+        const double t_admit = now_s();
+        const int rc = admit_merged(s, q, grp, L);
+        s->st.admit_host_s += now_s() - t_admit;
+        b200d2::merged_destroy(L.mb);
+        if (rc != B200D2_OK && !q.finished.load()) {
+          q.status = rc;
+          q.t_done = now_s();
+          q.finished.store(1);
+        }
+        s->st.merged_admissions++;
+        s->st.merged_requests += (long long)grp.size();
+        s->inflight.push_back(*it);
+        s->queue.erase(std::remove_if(s->queue.begin(), s->queue.end(),
+                                      [&](const std::shared_ptr<Req>& x) {
+                                        return x.get() == &q || x->member;
+                                      }),
+                       s->queue.end());
+        int busy = 0;
+        for (const auto& x : s->inflight) busy += 1 + (int)x->members.size();
+        s->st.max_in_flight = std::max(s->st.max_in_flight, busy);
+        progress = true;
+        it = s->queue.begin();  // the queue changed: scan it again
+        continue;
+      }
       q.slot = slot;
       s->slot_busy[slot] = 1;
       s->st.bytes_in_use += q.footprint;
@@ -348,10 +612,16 @@ void sched_loop(b200d2_server* s) {
       }
       s->inflight.push_back(*it);
       it = s->queue.erase(it);
-      s->st.max_in_flight = std::max(s->st.max_in_flight, (int)s->inflight.size());
+      int busy = 0;
+      for (const auto& x : s->inflight) busy += 1 + (int)x->members.size();
+      s->st.max_in_flight = std::max(s->st.max_in_flight, busy);
       progress = true;
     }
-    s->st.in_flight = (int)s->inflight.size();
+    {
+      int busy = 0;
+      for (const auto& x : s->inflight) busy += 1 + (int)x->members.size();
+      s->st.in_flight = busy;
+    }
     s->st.queued = (int)s->queue.size();
     if (s->stop && s->queue.empty() && s->inflight.empty()) break;
     if (!progress) s->cv_sched.wait_for(lk, std::chrono::microseconds(200));
@@ -415,6 +685,9 @@ extern "C" int b200d2_server_create(int slots, size_t hbm_budget_bytes, int prec
       cudaGetLastError();
     }
   }
+  // load every kernel the requests can launch now: a kernel loaded at its
+  // first launch (lazy module loading) can wait for the slots' running work
+  if (b200d2::is_tc_precision(precision) && b200d2::tc_preload(precision) != B200D2_OK) cudaGetLastError();
   s->sched = std::thread(sched_loop, s);
   *out = s;
   return B200D2_OK;
@@ -530,6 +803,14 @@ extern "C" int b200d2_server_cancel(b200d2_server* s, long long ticket) {
   return B200D2_OK;
 }
 
+extern "C" int b200d2_server_set_merging(b200d2_server* s, int max_requests, int max_particles) {
+  if (!s || max_requests < 1 || max_particles < 1) return B200D2_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->merge_requests = max_requests;
+  s->merge_particles = max_particles;
+  return B200D2_OK;
+}
+
 extern "C" int b200d2_server_get_stats(b200d2_server* s, b200d2_server_stats* st) {
   if (!s || !st) return B200D2_ERR_INVALID;
   std::lock_guard<std::mutex> lk(s->mu);
@@ -551,6 +832,7 @@ extern "C" int b200d2_server_destroy(b200d2_server* s) {
   }
   for (void* p : s->pin)
     if (p) cudaFreeHost(p);
+  for (void* p : s->pin_retired) cudaFreeHost(p);
   for (void* p : s->dev)
     if (p) cudaFree(p);
   if (s->pool) cudaMemPoolDestroy(s->pool);

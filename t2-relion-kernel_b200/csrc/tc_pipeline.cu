@@ -212,6 +212,10 @@ struct UnevenTabs {
   const float2* tab_txy;  // [ntab] translation of each phase table
   int ntab;
   int Mrows;
+  // merged batches (block-diagonal, no plan): per request, host
+  // (first particle, particles, first column, columns); plans have none
+  const int4* h_groups;
+  int ngroups;
 };
 
 // Optional tables of an uneven batch; all null for a uniform batch.
@@ -767,8 +771,10 @@ template <int WM, int WN>
 __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* __restrict__ wcomp, int Kq,
                                                        const double* __restrict__ q, int O, int P,
                                                        const double* __restrict__ normx, double* na,
-                                                       float2* na_hl, int cc) {
-  // Kq: row stride of wcomp and q, a multiple of 16, zero padded; the last
+                                                       float2* na_hl, int cc, long long ld) {
+  // Kq: row stride of wcomp and q, a multiple of 16, zero padded; ld: row
+  // stride of na and na_hl (O, or the merged batch's width for one request's
+  // block of it); the last
   // slab is zero-filled past Kq.  Shared rows padded to 36 doubles (288 B,
   // 16-byte aligned): the fragment loads of a half-warp (rows g, columns t,
   // g, t < 4) fall on distinct bank pairs 4g + t (mod 16).
@@ -842,13 +848,13 @@ __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* _
         if (o < O) {
           if (cc) {
             const double k = -sqrt(2.0 / acc[i][j][h]);
-            na[(size_t)p * O + o] = k;
-            na_hl[(size_t)p * O + o] = make_float2((float)k, 0.f);
+            na[(size_t)p * ld + o] = k;
+            na_hl[(size_t)p * ld + o] = make_float2((float)k, 0.f);
           } else {
             const double v = normx[p] + acc[i][j][h];
-            na[(size_t)p * O + o] = v;
+            na[(size_t)p * ld + o] = v;
             const float hi = (float)v;  // v = hi + lo to 48 bits: the combine's double-float operand
-            na_hl[(size_t)p * O + o] = make_float2(hi, (float)(v - (double)hi));
+            na_hl[(size_t)p * ld + o] = make_float2(hi, (float)(v - (double)hi));
           }
         }
       }
@@ -857,13 +863,13 @@ __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* _
 
 template <int WM, int WN>
 static cudaError_t launch_norma(cudaStream_t s, const double* wcomp, int Kq, const double* q, int O, int P,
-                                const double* normx, double* na, float2* na_hl, int cc) {
+                                const double* normx, double* na, float2* na_hl, int cc, long long ld) {
   static std::atomic<unsigned long long> opted{0};  // above 48 KB of dynamic shared memory
   const cudaError_t e = smem_opt_in(tc_norma_kernel<WM, WN>, (int)norma_smem_bytes<WM, WN>(), opted);
   if (e != cudaSuccess) return e;
   const dim3 grid((O + 16 * WN - 1) / (16 * WN), (P + 16 * WM - 1) / (16 * WM));
   tc_norma_kernel<WM, WN><<<grid, kNormaThreads, norma_smem_bytes<WM, WN>(), s>>>(wcomp, Kq, q, O, P, normx, na,
-                                                                                 na_hl, cc);
+                                                                                 na_hl, cc, ld);
   return cudaSuccess;
 }
 
@@ -2482,20 +2488,39 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       break;
     case 4: {
       // the largest tile (particles x orientations: 64 x 64, 32 x 64, 16 x 64,
-      // 16 x 32, 16 x 16) that still gives every SM a CTA
+      // 16 x 32, 16 x 16) that still gives every SM a CTA.  A merged batch
+      // (block-diagonal) launches once per request: its particles against its
+      // own orientation columns, in place inside the batch-wide nA rows.
       const int sms = num_sms();
       const int cc = b.score == B200D2_SCORE_CC;
-      auto ctas = [&](int cp, int co) { return (long long)((g.O + co - 1) / co) * ((g.P + cp - 1) / cp); };
-      if (ctas(64, 64) >= sms)
-        B200D2_CUDA_TRY((launch_norma<4, 4>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc)));
-      else if (ctas(32, 64) >= sms)
-        B200D2_CUDA_TRY((launch_norma<2, 4>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc)));
-      else if (ctas(16, 64) >= sms)
-        B200D2_CUDA_TRY((launch_norma<1, 4>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc)));
-      else if (ctas(16, 32) >= sms)
-        B200D2_CUDA_TRY((launch_norma<1, 2>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc)));
-      else
-        B200D2_CUDA_TRY((launch_norma<1, 1>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc)));
+      const int nblk = (U && U->ngroups > 0) ? U->ngroups : 1;
+      for (int gi = 0; gi < nblk; ++gi) {
+        int p0 = 0, np = g.P, c0 = 0, no = g.O;
+        if (U && U->ngroups > 0) {
+          const int4 gr = U->h_groups[gi];  // first particle, particles, first column, columns
+          p0 = gr.x;
+          np = gr.y;
+          c0 = gr.z;
+          no = gr.w;
+        }
+        const double* w0 = wcomp + (size_t)p0 * g.Kq;
+        const double* q0 = q + (size_t)c0 * g.Kq;
+        const double* nx0 = normx + p0;
+        double* na0 = na + (size_t)p0 * g.O + c0;
+        float2* nh0 = na_hl + (size_t)p0 * g.O + c0;
+        auto ctas = [&](int cp, int co) { return (long long)((no + co - 1) / co) * ((np + cp - 1) / cp); };
+        if (ctas(64, 64) >= sms)
+          B200D2_CUDA_TRY((launch_norma<4, 4>(s, w0, g.Kq, q0, no, np, nx0, na0, nh0, cc, g.O)));
+        else if (ctas(32, 64) >= sms)
+          B200D2_CUDA_TRY((launch_norma<2, 4>(s, w0, g.Kq, q0, no, np, nx0, na0, nh0, cc, g.O)));
+        else if (ctas(16, 64) >= sms)
+          B200D2_CUDA_TRY((launch_norma<1, 4>(s, w0, g.Kq, q0, no, np, nx0, na0, nh0, cc, g.O)));
+        else if (ctas(16, 32) >= sms)
+          B200D2_CUDA_TRY((launch_norma<1, 2>(s, w0, g.Kq, q0, no, np, nx0, na0, nh0, cc, g.O)));
+        else
+          B200D2_CUDA_TRY((launch_norma<1, 1>(s, w0, g.Kq, q0, no, np, nx0, na0, nh0, cc, g.O)));
+        if (gi + 1 < nblk) count_launch();
+      }
       break;
     }
     case 5: {
@@ -3286,6 +3311,284 @@ extern "C" int b200d2_plan_destroy(b200d2_plan* p) {
   b200d2::plan_free(p);
   return B200D2_OK;
 }
+
+// ------------------------------------------------------------------ merged batches
+// Several requests on one reference in one pipeline run (the serving loop's
+// merged admissions), block-diagonal: request r's particles are scored only
+// against its own orientation columns [col0_r, col0_r + O_r) of the merged
+// orientation set, at its own translations, through the uneven batch
+// kernels (per-particle rows, orientation maps and outputs).  Unlike a plan,
+// nothing is allocated, timed or synchronised: the tables are built on the
+// host when the batch is created, and merged_enqueue copies them from the
+// caller's page-locked staging area into the caller's device memory and
+// launches the stages, all in the order of one stream.  The FP64 norms run
+// once per request (its block of particles x columns), so no request pays
+// for another's orientations there either; the contraction's work list
+// holds the (m tile, n tile) pairs that some row of the m tile needs.
+namespace b200d2 {
+
+struct MergedBatch {
+  b200d2_view view;
+  int prec = 0, N_img = 0, n = 0, P = 0, O = 0;
+  std::vector<MergedRequest> req;
+  std::vector<int> part0;          // first particle of each request
+  std::vector<int4> rows, groups;  // groups: (first particle, particles, first column, columns)
+  std::vector<int> row0;           // first row of each particle
+  std::vector<int2> tiles[3];      // 128 x 256, 128 x 128, 256 x 256 (CTA pairs)
+  std::vector<float2> txy;
+  std::vector<int> inv;            // [n][O]
+  TcGeom g;
+  GemmVariant var;
+  // device layout from the caller's base: the workspace, then the tables
+  // (mirrored byte for byte by the staging area)
+  size_t off_tab = 0, off_parts = 0, off_rows = 0, off_tiles[3] = {0, 0, 0}, off_txy = 0, off_inv = 0, dev_bytes = 0;
+};
+
+MergedBatch* merged_create(const b200d2_view& v, int N_img, int precision, const MergedRequest* r, int n, int O_cols,
+                           int* status) {
+  auto fail = [&](int st) -> MergedBatch* {
+    if (status) *status = st;
+    return nullptr;
+  };
+  if (!r || n <= 0 || N_img <= 0 || O_cols <= 0) return fail(B200D2_ERR_INVALID);
+  if (!is_tc_precision(precision)) return fail(B200D2_ERR_UNSUPPORTED);
+  if (v.mdlZ == 0 || (long long)v.imgX * v.imgY < N_img || v.maxR > 4096) return fail(B200D2_ERR_INVALID);
+  for (int k = 0; k < n; ++k) {
+    const MergedRequest& q = r[k];
+    if (q.P <= 0 || q.O <= 0 || q.T <= 0 || !q.h_tx || !q.h_ty || q.col0 < 0 || q.col0 % 256 != 0 ||
+        (long long)q.col0 + q.O > O_cols || (k > 0 && q.col0 < r[k - 1].col0 + r[k - 1].O))
+      return fail(B200D2_ERR_INVALID);
+    if ((long long)q.O * q.T >= 0xffffffffLL) return fail(B200D2_ERR_UNSUPPORTED);
+  }
+  MergedBatch* m = new MergedBatch();
+  m->view = v;
+  m->prec = precision;
+  m->N_img = N_img;
+  m->n = n;
+  m->O = O_cols;
+  m->req.assign(r, r + n);
+  // translation sets shared between requests share their phase tables
+  std::map<std::vector<std::pair<uint32_t, uint32_t>>, int> sets;
+  std::vector<int> tab0(n), req_of;
+  for (int k = 0; k < n; ++k) {
+    const MergedRequest& q = r[k];
+    std::vector<std::pair<uint32_t, uint32_t>> key(q.T);
+    for (int t = 0; t < q.T; ++t) {
+      uint32_t a, c;
+      memcpy(&a, &q.h_tx[t], 4);
+      memcpy(&c, &q.h_ty[t], 4);
+      key[t] = {a, c};
+    }
+    auto it = sets.find(key);
+    if (it == sets.end()) {
+      it = sets.emplace(key, (int)m->txy.size()).first;
+      for (int t = 0; t < q.T; ++t) m->txy.push_back(make_float2(q.h_tx[t], q.h_ty[t]));
+    }
+    tab0[k] = it->second;
+    m->part0.push_back(m->P);
+    m->groups.push_back(make_int4(m->P, q.P, q.col0, q.O));
+    for (int i = 0; i < q.P; ++i) {
+      m->row0.push_back((int)m->rows.size());
+      req_of.push_back(k);
+      for (int t = 0; t < q.T; ++t) m->rows.push_back(make_int4(m->P + i, t, tab0[k] + t, 0));
+    }
+    m->P += q.P;
+  }
+  const int Mrows = (int)m->rows.size();
+  const int Mtiles = (Mrows + 127) / 128, Ntiles = (O_cols + 255) / 256, Ntiles128 = (O_cols + 127) / 128;
+  // work lists: an m tile's rows belong to a run of consecutive requests;
+  // it needs the 128-column blocks of their column ranges
+  auto blocks_of = [&](int rr0, int rr1, std::vector<char>& un) {
+    std::fill(un.begin(), un.end(), 0);
+    for (int k = req_of[m->rows[rr0].x]; k <= req_of[m->rows[rr1 - 1].x]; ++k)
+      for (int c = r[k].col0 / 128; c <= (r[k].col0 + r[k].O - 1) / 128; ++c) un[c] = 1;
+  };
+  std::vector<char> un(Ntiles128, 0);
+  for (int mt = 0; mt < (Mtiles + 1) / 2; ++mt) {  // 256-row m-tiles of CTA pairs
+    blocks_of(mt * 256, std::min(Mrows, mt * 256 + 256), un);
+    for (int c = 0; c < Ntiles; ++c)
+      if (un[2 * c] || (2 * c + 1 < Ntiles128 && un[2 * c + 1])) m->tiles[2].push_back(make_int2(mt, c));
+  }
+  for (int mt = 0; mt < Mtiles; ++mt) {
+    blocks_of(mt * 128, std::min(Mrows, mt * 128 + 128), un);
+    for (int c = 0; c < Ntiles; ++c)
+      if (un[2 * c] || (2 * c + 1 < Ntiles128 && un[2 * c + 1])) m->tiles[0].push_back(make_int2(mt, c));
+    for (int c = 0; c < Ntiles128; ++c)
+      if (un[c]) m->tiles[1].push_back(make_int2(mt, c));
+  }
+  m->inv.assign((size_t)n * O_cols, -1);
+  for (int k = 0; k < n; ++k)
+    for (int o = 0; o < r[k].O; ++o) m->inv[(size_t)k * O_cols + r[k].col0 + o] = o;
+
+  b200d2_batch b;
+  memset(&b, 0, sizeof(b));
+  b.O = O_cols;
+  b.T = (int)m->txy.size();  // number of phase tables
+  b.P = m->P;
+  b.N_img = N_img;
+  b.img_stride = N_img;
+  m->g = make_geom(v, b, precision, Mrows, false);
+  // CTA pairs while their tiles give every pair of SMs one, else 128-wide
+  // single-CTA tiles (twice the tiles); no k-splits
+  if ((long long)m->tiles[2].size() >= num_sms() / 2) {
+    m->var.row_bytes = 128;
+    m->var.bn = 256;
+    m->var.pair = 1;
+  } else {
+    m->var.row_bytes = gemm_row_bytes();
+    m->var.bn = 128;
+    m->var.pair = 2;
+  }
+  m->var.split = 1;
+  size_t o = align_up(m->g.total, 256);
+  m->off_tab = o;
+  auto take = [&](size_t bytes) {
+    const size_t at = o;
+    o = align_up(o + bytes, 256);
+    return at;
+  };
+  m->off_parts = take(sizeof(PartDev) * (size_t)m->P);
+  m->off_rows = take(sizeof(int4) * m->rows.size());
+  for (int w = 0; w < 3; ++w) m->off_tiles[w] = take(sizeof(int2) * std::max<size_t>(m->tiles[w].size(), 1));
+  m->off_txy = take(sizeof(float2) * m->txy.size());
+  m->off_inv = take(sizeof(int) * m->inv.size());
+  m->dev_bytes = o;
+  if (status) *status = B200D2_OK;
+  return m;
+}
+
+size_t merged_device_bytes(const MergedBatch* m) { return m ? m->dev_bytes : 0; }
+size_t merged_host_bytes(const MergedBatch* m) { return m ? m->dev_bytes - m->off_tab : 0; }
+void merged_destroy(MergedBatch* m) { delete m; }
+
+int merged_enqueue(MergedBatch* m, const float* d_eulers, const MergedDev* d, double* d_min, long long* d_argmin,
+                   void* dmem, void* hstage, cudaStream_t s) {
+  if (!m || !d_eulers || !d || !d_min || !d_argmin || !dmem || !hstage) return B200D2_ERR_INVALID;
+  NvtxRange range("b200d2 merged batch");
+  uint8_t* dev = static_cast<uint8_t*>(dmem);
+  // the staging area mirrors the device tables: host(off) holds dev + off
+  auto host = [&](size_t off) { return static_cast<uint8_t*>(hstage) + (off - m->off_tab); };
+  const int* d_inv = reinterpret_cast<const int*>(dev + m->off_inv);
+  PartDev* hp = reinterpret_cast<PartDev*>(host(m->off_parts));
+  for (int k = 0; k < m->n; ++k) {
+    const MergedRequest& q = m->req[k];
+    if (!d[k].re || !d[k].im || !d[k].corr || !d[k].out) return B200D2_ERR_INVALID;
+    for (int i = 0; i < q.P; ++i) {
+      PartDev& x = hp[m->part0[k] + i];
+      x.re = d[k].re + (size_t)i * m->N_img;
+      x.im = d[k].im + (size_t)i * m->N_img;
+      x.corr = d[k].corr + (size_t)i * m->N_img;
+      x.out = d[k].out + (size_t)i * q.O * q.T;
+      x.inv = d_inv + (size_t)k * m->O;
+      x.T = q.T;
+      x.O = q.O;
+      x.row0 = m->row0[m->part0[k] + i];
+      x.pad = 0;
+    }
+  }
+  memcpy(host(m->off_rows), m->rows.data(), sizeof(int4) * m->rows.size());
+  for (int w = 0; w < 3; ++w) memcpy(host(m->off_tiles[w]), m->tiles[w].data(), sizeof(int2) * m->tiles[w].size());
+  memcpy(host(m->off_txy), m->txy.data(), sizeof(float2) * m->txy.size());
+  memcpy(host(m->off_inv), m->inv.data(), sizeof(int) * m->inv.size());
+  B200D2_CUDA_TRY(cudaMemcpyAsync(dev + m->off_tab, hstage, m->dev_bytes - m->off_tab, cudaMemcpyHostToDevice, s));
+  UnevenTabs U{reinterpret_cast<const PartDev*>(dev + m->off_parts),
+               reinterpret_cast<const int4*>(dev + m->off_rows),
+               {reinterpret_cast<const int2*>(dev + m->off_tiles[0]), reinterpret_cast<const int2*>(dev + m->off_tiles[1]),
+                reinterpret_cast<const int2*>(dev + m->off_tiles[2])},
+               {(int)m->tiles[0].size(), (int)m->tiles[1].size(), (int)m->tiles[2].size()},
+               reinterpret_cast<const float2*>(dev + m->off_txy),
+               (int)m->txy.size(),
+               (int)m->rows.size(),
+               m->groups.data(),
+               m->n};
+  b200d2_batch b;
+  memset(&b, 0, sizeof(b));
+  b.d_eulers = d_eulers;
+  b.O = m->O;
+  b.T = (int)m->txy.size();
+  b.P = m->P;
+  b.N_img = m->N_img;
+  b.d_real = d[0].re;  // unused by the tabled kernels; kept valid
+  b.d_imag = d[0].im;
+  b.d_corr = d[0].corr;
+  b.img_stride = m->N_img;
+  b.d_diff2 = d[0].out;
+  b.d_min = d_min;
+  b.d_argmin = d_argmin;
+  int st = B200D2_OK;
+  for (int i = 0; i < kNumStages && st == B200D2_OK; ++i) st = dispatch_stage(m->view, b, m->prec, m->g, dmem, i, s, &U, m->var);
+  return st;
+}
+
+}  // namespace b200d2
+
+// ------------------------------------------------------------------ kernel preload
+// With CUDA's lazy module loading (the default), a kernel is loaded on its
+// first launch, and loading it can wait for the work already running on the
+// device.  A server whose requests pick tile shapes, norm tiles and
+// contraction variants by size would meet new ones mid-run: one such load
+// stalled every request in flight for about 30 ms at C5.  Loading every
+// kernel a precision's pipeline can launch up front (cudaFuncGetAttributes
+// loads the function) moves that cost to set-up.
+namespace b200d2 {
+
+template <int PREC>
+static cudaError_t preload_prec() {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaSuccess;
+  auto get = [&](const void* f) {
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, f);
+  };
+  get((const void*)tc_project_kernel<PREC>);
+  get((const void*)tc_project_scaled_kernel<PREC>);
+  get((const void*)tc_gen_a_kernel<PREC, false>);
+  get((const void*)tc_gen_a_kernel<PREC, true>);
+  get((const void*)tc_gemm_kernel<PREC, 64, 128, false>);
+  get((const void*)tc_gemm_kernel<PREC, 64, 256, false>);
+  get((const void*)tc_gemm_kernel<PREC, 128, 128, false>);
+  get((const void*)tc_gemm_kernel<PREC, 128, 256, false>);
+  get((const void*)tc_gemm_kernel<PREC, 64, 128, true>);
+  get((const void*)tc_gemm_kernel<PREC, 64, 256, true>);
+  get((const void*)tc_gemm_kernel<PREC, 128, 128, true>);
+  get((const void*)tc_gemm_kernel<PREC, 128, 256, true>);
+  get((const void*)tc_gemm_pair_kernel<PREC, 64, false>);
+  get((const void*)tc_gemm_pair_kernel<PREC, 128, false>);
+  get((const void*)tc_gemm_pair_kernel<PREC, 64, true>);
+  get((const void*)tc_gemm_pair_kernel<PREC, 128, true>);
+  return e;
+}
+
+int tc_preload(int precision) {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaSuccess;
+  auto get = [&](const void* f) {
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, f);
+  };
+  get((const void*)tc_pixel_list_kernel);
+  get((const void*)tc_phase_kernel);
+  get((const void*)tc_phase2d_kernel);
+  get((const void*)tc_phase_compact_kernel);
+  get((const void*)tc_scale_a_kernel);
+  get((const void*)tc_normx_kernel);
+  get((const void*)tc_norma_kernel<4, 4>);
+  get((const void*)tc_norma_kernel<2, 4>);
+  get((const void*)tc_norma_kernel<1, 4>);
+  get((const void*)tc_norma_kernel<1, 2>);
+  get((const void*)tc_norma_kernel<1, 1>);
+  get((const void*)tc_finalize_kernel);
+  if (e != cudaSuccess) return status_from_cuda(e);
+  switch (precision) {
+    case B200D2_PREC_BF16X3: e = preload_prec<B200D2_PREC_BF16X3>(); break;
+    case B200D2_PREC_TF32X3: e = preload_prec<B200D2_PREC_TF32X3>(); break;
+    case B200D2_PREC_TF32: e = preload_prec<B200D2_PREC_TF32>(); break;
+    case B200D2_PREC_FP16X3: e = preload_prec<B200D2_PREC_FP16X3>(); break;
+    case B200D2_PREC_FP16: e = preload_prec<B200D2_PREC_FP16>(); break;
+    default: return B200D2_ERR_UNSUPPORTED;
+  }
+  return status_from_cuda(e);
+}
+
+}  // namespace b200d2
 
 extern "C" int b200d2_workspace_status(const void* d_workspace, void* stream, int* status) {
   if (!d_workspace || !status) return B200D2_ERR_INVALID;

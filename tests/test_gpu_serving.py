@@ -89,6 +89,7 @@ def test_serving_admission_by_budget(pkg, synth, cuda):
     view = proj.view(prob.imgX, prob.imgY, prob.imgMaxR)
     budget = 4 << 20  # 4 MiB: one small request (~2.5 MiB with its workspace) at a time
     srv = pkg.Server(slots=2, hbm_budget=budget, precision=pkg.PREC_TF32)
+    srv.set_merging(1)  # one request per admission: the budget alone bounds what runs together
     ref = srv.add_reference(view, prob.eulers, prob.N_img)
     tx = np.zeros(1, np.float32)
     big = np.arange(prob.O, dtype=np.int32)
@@ -217,3 +218,64 @@ def test_serving_allocation_failure_is_reported(pkg, synth, cuda):
     np.testing.assert_array_equal(mn, mn2)
     fresh.close()
     proj.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("PREC_TF32", 1e-3), ("PREC_BF16X3", 1e-5)])
+def test_serving_merged_requests(pkg, synth, oracle, cuda, precision, tol):
+    """Queued requests on one reference run as one merged, block-diagonal
+    batch (b200d2_server_set_merging): each request's particles against its
+    own orientation subset at its own translations.  One slot, held by a
+    long request on another reference, makes the small requests queue; they
+    are then admitted together.  Each merged result equals the same request
+    run alone with merging off (same kernels, same sums: within 1e-6 and the
+    same argmin), and agrees with the FP64 CUDA-core kernel within the
+    precision's tolerance."""
+    torch = cuda
+    prec = getattr(pkg, precision)
+    rng = np.random.default_rng(29)
+    blk = synth.make_problem("c2", P=64)
+    prob = synth.make_problem("c1", P=8)
+    projs = [pkg.Projector(p.projector, use_texture=1) for p in (blk, prob)]
+    vb, view = (pj.view(p.imgX, p.imgY, p.imgMaxR) for pj, p in zip(projs, (blk, prob)))
+    srv = pkg.Server(slots=1, hbm_budget=8 << 30, precision=prec)
+    rb = srv.add_reference(vb, blk.eulers, blk.N_img)
+    ref = srv.add_reference(view, prob.eulers, prob.N_img)
+    reqs = _requests(synth, rng, prob, ref, 7)
+    reqs[0]["orient"] = np.arange(3, 300, dtype=np.int32)  # 297 columns: a gap to the next request's
+    # the blocker: 64 C2 particles with their 133 MB diff2 copied back through
+    # the staging buffer (tens of ms), so that the small requests queue
+    blk_out = np.zeros((blk.P, blk.O, blk.T), np.float32)
+    t_blk = srv.submit(rb, blk.fimg_re, blk.fimg_im, blk.corr, np.arange(blk.O, dtype=np.int32), blk.trans_x,
+                       blk.trans_y, blk_out, np.zeros(blk.P), np.zeros(blk.P, np.int64))
+    mix = [_submit(srv, rq) for rq in reqs]
+    assert srv.wait(t_blk)[0] == 0
+    for t, *_ in mix:
+        assert srv.wait(t)[0] == 0
+    st = srv.stats()
+    assert st["completed"] == len(reqs) + 1
+    assert st["merged_admissions"] >= 1 and st["merged_requests"] >= 2
+
+    srv.set_merging(1)  # off: every request alone
+    for rq, (_, out_mix, mn_mix, am_mix) in zip(reqs, mix):
+        t, out, mn, am = _submit(srv, rq)
+        assert srv.wait(t)[0] == 0
+        assert oracle.error_stats(out_mix, out)["max_rel"] <= 1e-6
+        np.testing.assert_array_equal(am_mix, am)
+        assert np.all(mn_mix == out_mix.reshape(len(rq["ps"]), -1).min(axis=1))
+    assert srv.stats()["merged_admissions"] == st["merged_admissions"]
+
+    eul_all = prob.eulers.reshape(-1, 9)
+    for rq, (_, out_mix, _, _) in zip(reqs, mix):
+        eul = torch.as_tensor(np.ascontiguousarray(eul_all[rq["orient"]].reshape(-1)), device="cuda")
+        tx, ty = torch.as_tensor(rq["tx"], device="cuda"), torch.as_tensor(rq["ty"], device="cuda")
+        for i in range(len(rq["ps"])):
+            d = torch.zeros(rq["orient"].size * rq["tx"].size, device="cuda", dtype=torch.float64)
+            pkg.run_diff2_kernel_coarse_double(view, tx, ty, torch.as_tensor(rq["corr"][i], device="cuda"),
+                                               torch.as_tensor(rq["real"][i], device="cuda"),
+                                               torch.as_tensor(rq["imag"][i], device="cuda"), eul, d,
+                                               rq["orient"].size, rq["tx"].size, prob.N_img)
+            torch.cuda.synchronize()
+            assert oracle.error_stats(out_mix[i].ravel(), d.cpu().numpy())["max_rel"] <= tol
+    srv.close()
+    for pj in projs:
+        pj.close()
