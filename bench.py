@@ -1418,8 +1418,10 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
 
     def replay(precision, slots, budget, limit_s, burst=False, merge=True):
         srv = pkg.Server(slots=slots, hbm_budget=budget, precision=precision)
-        if not merge:
-            srv.set_merging(1)
+        # the warm-up below grows every slot's buffer with requests submitted
+        # together: one request per admission there, or they would be merged
+        # onto one slot
+        srv.set_merging(1)
         ids = [srv.add_reference(rf["view"], rf["pr"].eulers, rf["pr"].N_img) for rf in refs]
 
         def submit(q):
@@ -1450,6 +1452,8 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
                 heavy = max(mine, key=nbytes)
                 for tk, _ in [submit(heavy) for _ in range(slots)]:
                     srv.wait(tk)
+        if merge:
+            srv.set_merging(8, 512)
         st0 = srv.stats()
         admit0, stream0 = st0["admit_host_s"], st0["stream_s"]
         t0 = time.perf_counter()
@@ -1481,7 +1485,7 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
                 "p99_ms": float(np.percentile(lat_ms, 99)), "mean_ms": float(lat_ms.mean()),
                 "evals": ev, "evals_per_s": ev / span, "span_s": span, "max_in_flight": stats["max_in_flight"],
                 "peak_bytes": stats["peak_bytes"], "admit_host_s_per_s": (stats["admit_host_s"] - admit0) / span,
-                # merged admissions over the whole run (warm-up included) and the requests they carried
+                # merged admissions of the trace (the warm-up has none) and the requests they carried
                 "merged_admissions": stats["merged_admissions"], "merged_requests": stats["merged_requests"],
                 # each admission's stream time (first copy in to last copy out; a merged
                 # admission once) summed, per second of the run

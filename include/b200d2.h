@@ -401,7 +401,9 @@ int b200d2_server_get_stats(b200d2_server* s, b200d2_server_stats* st);
  * queued request that fits together with later queued requests on the same
  * reference (arrival order), up to max_requests requests and max_particles
  * particles in all, as one batch: one copy-in, one pipeline run and one
- * copy-out on one slot, instead of a pipeline per request.  The batch is
+ * copy-out on one slot, instead of a pipeline per request, when the merged
+ * run fits the buffer an idle slot already holds (a merge never grows a
+ * slot's buffer, which maps memory while the queue waits).  The batch is
  * block-diagonal: each request's particles are scored against its own
  * orientations at its own translations only, so no request pays for
  * another's, and each result equals the request's result alone (same

@@ -532,10 +532,16 @@ void sched_loop(b200d2_server* s) {
         continue;
       }
       // merge later queued requests on the same reference into this one's
-      // run while the particle and request limits and the budget allow
+      // run while the particle and request limits and the budget allow, and
+      // while the merged run fits an idle slot's buffer as it is (a merge
+      // never makes a slot grow, which maps memory while the queue waits)
       std::vector<std::shared_ptr<Req>> grp;
       MergedLayout L;
-      if (s->merge_requests > 1 && b200d2::is_tc_precision(s->prec) && q.r.P < s->merge_particles) {
+      size_t idle_max = 0;
+      for (int k = 0; k < s->slots; ++k)
+        if (!s->slot_busy[k]) idle_max = std::max(idle_max, s->dev_bytes[k]);
+      if (s->merge_requests > 1 && b200d2::is_tc_precision(s->prec) && q.r.P < s->merge_particles &&
+          q.footprint < idle_max) {
         grp.push_back(*it);
         int P = q.r.P;
         for (auto jt = std::next(it); jt != s->queue.end() && (int)grp.size() < s->merge_requests; ++jt)
@@ -544,7 +550,9 @@ void sched_loop(b200d2_server* s) {
             P += (*jt)->r.P;
           }
         while (grp.size() > 1) {
-          if (merged_layout(s, grp, L) == B200D2_OK && s->st.bytes_in_use + L.footprint <= s->budget) break;
+          if (merged_layout(s, grp, L) == B200D2_OK && s->st.bytes_in_use + L.footprint <= s->budget &&
+              L.footprint <= idle_max)
+            break;
           b200d2::merged_destroy(L.mb);
           L.mb = nullptr;
           grp.pop_back();

@@ -279,3 +279,64 @@ def test_serving_merged_requests(pkg, synth, oracle, cuda, precision, tol):
     srv.close()
     for pj in projs:
         pj.close()
+
+
+def test_serving_c5_shapes(pkg, synth, oracle, cuda):
+    """The serving workload's own shapes: three resident references at
+    coarse image sizes 48, 64 and 96 (all 4608 orientations), requests of
+    4-24 particles against random 10-100 % orientation subsets at
+    translation radii 2-6 px, TF32 with FP64 norms.  Submitted together on
+    two slots (so that requests queue, overlap and merge), each result equals
+    the request run alone with merging off (1e-6, same argmin), and one
+    particle of every request agrees with the FP64 CUDA-core kernel (1e-3)."""
+    torch = cuda
+    rng = np.random.default_rng(31)
+    probs = [synth.make_problem(n, seed=20251203 + i, P=24) for i, n in enumerate(("c5s", "c5m", "c5l"))]
+    projs = [pkg.Projector(p.projector, use_texture=1) for p in probs]
+    views = [pj.view(p.imgX, p.imgY, p.imgMaxR) for pj, p in zip(projs, probs)]
+    srv = pkg.Server(slots=2, hbm_budget=16 << 30, precision=pkg.PREC_TF32)
+    refs = [srv.add_reference(v, p.eulers, p.N_img) for v, p in zip(views, probs)]
+    reqs = []
+    for k in range(9):
+        r = k % 3
+        prob = probs[r]
+        P = int(rng.integers(4, 25))
+        ps = np.sort(rng.choice(prob.P, P, replace=False))
+        O = max(1, int(round(rng.uniform(0.1, 1.0) * prob.O)))
+        orient = np.sort(rng.choice(prob.O, O, replace=False)).astype(np.int32)
+        rad = int(rng.integers(2, 7))
+        sh = synth.translation_grid(rad * rad)
+        tx = (-2 * np.pi * sh[:, 0] / prob.projector.ori_size).astype(np.float32)
+        ty = (-2 * np.pi * sh[:, 1] / prob.projector.ori_size).astype(np.float32)
+        reqs.append(dict(ref=refs[r], r=r, prob=prob, ps=ps, real=np.ascontiguousarray(prob.fimg_re[ps]),
+                         imag=np.ascontiguousarray(prob.fimg_im[ps]), corr=np.ascontiguousarray(prob.corr[ps]),
+                         orient=orient, tx=tx, ty=ty))
+    mix = [_submit(srv, rq) for rq in reqs]
+    for t, *_ in mix:
+        assert srv.wait(t, timeout=300.0)[0] == 0
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["max_in_flight"] >= 2
+
+    srv.set_merging(1)
+    for rq, (_, out_mix, mn_mix, am_mix) in zip(reqs, mix):
+        t, out, mn, am = _submit(srv, rq)
+        assert srv.wait(t, timeout=300.0)[0] == 0
+        assert oracle.error_stats(out_mix, out)["max_rel"] <= 1e-6
+        np.testing.assert_array_equal(am_mix, am)
+
+    for rq, (_, out_mix, _, _) in zip(reqs, mix):
+        prob = rq["prob"]
+        eul = torch.as_tensor(np.ascontiguousarray(prob.eulers.reshape(-1, 9)[rq["orient"]].reshape(-1)),
+                              device="cuda")
+        tx, ty = torch.as_tensor(rq["tx"], device="cuda"), torch.as_tensor(rq["ty"], device="cuda")
+        i = len(rq["ps"]) // 2
+        d = torch.zeros(rq["orient"].size * rq["tx"].size, device="cuda", dtype=torch.float64)
+        pkg.run_diff2_kernel_coarse_double(views[rq["r"]], tx, ty, torch.as_tensor(rq["corr"][i], device="cuda"),
+                                           torch.as_tensor(rq["real"][i], device="cuda"),
+                                           torch.as_tensor(rq["imag"][i], device="cuda"), eul, d,
+                                           rq["orient"].size, rq["tx"].size, prob.N_img)
+        torch.cuda.synchronize()
+        assert oracle.error_stats(out_mix[i].ravel(), d.cpu().numpy())["max_rel"] <= 1e-3
+    srv.close()
+    for pj in projs:
+        pj.close()
