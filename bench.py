@@ -547,7 +547,13 @@ def ours_arm(args):
                            "tuned_gemm_ms": {f"rb{v[0]}_n{v[1]}_s{v[2]}_p{v[3]}": ms for v, ms in info["tuned"]},
                            "work_tiles_pair": info["tiles_pair"],
                            "work_tiles_n128": info["tiles_n128"],
-                           "work_tiles": info["tiles"], "dense_tiles": info["tiles_dense"], "rows": info["rows"]})
+                           "work_tiles": info["tiles"], "dense_tiles": info["tiles_dense"], "rows": info["rows"],
+                           # FP64 norm stage: needed (particle tile x 64 orientations) blocks per tile
+                           # height, the height chosen, and each height's time
+                           "norm_blocks": dict(zip(("p64", "p32", "p16"), info["norm_tiles"])),
+                           "norm_dense_blocks": {f"p{h}": -(-P // h) * -(-pr.O // 64) for h in (64, 32, 16)},
+                           "norm_tile_p": info["norm_tile_p"],
+                           "norm_tuned_ms": dict(zip(("p64", "p32", "p16"), info["norm_tuned_ms"]))})
     else:
         out = torch.empty(P * O * T, device=dev, dtype=torch.float32)
         mn = torch.empty(P, device=dev, dtype=torch.float64)

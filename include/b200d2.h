@@ -314,6 +314,12 @@ typedef struct b200d2_plan_info {
   int n_tuned;
   int tuned_variant[B200D2_PLAN_MAX_VARIANTS][4];
   double tuned_ms[B200D2_PLAN_MAX_VARIANTS];
+  /* FP64 norm stage: blocks of (particle tile x 64 orientations) that some
+   * particle needs, for particle tiles of 64, 32 and 16 (plan order); the
+   * tile height in use; with B200D2_PLAN_AUTOTUNE each height's time in ms */
+  int norm_tiles[3];
+  int norm_tile_p;
+  double norm_tuned_ms[3];
 } b200d2_plan_info;
 
 typedef struct b200d2_plan b200d2_plan;
@@ -397,9 +403,10 @@ int b200d2_server_submit(b200d2_server* s, const b200d2_request* req,
 int b200d2_server_wait(b200d2_server* s, long long ticket, double timeout_s,
                        double* latency_s, double* device_s);
 int b200d2_server_get_stats(b200d2_server* s, b200d2_server_stats* st);
-/* Merged admissions.  When a slot frees up, the scheduler runs the first
- * queued request that fits together with later queued requests on the same
- * reference (arrival order), up to max_requests requests and max_particles
+/* Merged admissions.  When a slot frees up while more requests are queued
+ * than slots are idle, the scheduler runs the first queued request that fits
+ * together with later queued requests on the same reference (arrival order),
+ * up to max_requests requests and max_particles
  * particles in all, as one batch: one copy-in, one pipeline run and one
  * copy-out on one slot, instead of a pipeline per request, when the merged
  * run fits the buffer an idle slot already holds (a merge never grows a

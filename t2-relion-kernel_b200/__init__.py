@@ -91,7 +91,8 @@ class PlanInfo(C.Structure):
         ("evals", C.c_longlong), ("workspace_bytes", C.c_size_t), ("tile_n", C.c_int), ("split", C.c_int),
         ("pair", C.c_int), ("tiles_n128", C.c_int), ("tiles_pair", C.c_int), ("n_tuned", C.c_int),
         ("tuned_variant", (C.c_int * 4) * PLAN_MAX_VARIANTS),
-        ("tuned_ms", C.c_double * PLAN_MAX_VARIANTS)]
+        ("tuned_ms", C.c_double * PLAN_MAX_VARIANTS), ("norm_tiles", C.c_int * 3), ("norm_tile_p", C.c_int),
+        ("norm_tuned_ms", C.c_double * 3)]
 
 
 class Request(C.Structure):
@@ -394,7 +395,10 @@ class Plan:
     def info(self) -> dict:
         inf = PlanInfo()
         _check(lib().b200d2_plan_get_info(self._h, C.byref(inf)), "plan_get_info")
-        d = {n: getattr(inf, n) for n, _ in PlanInfo._fields_ if n not in ("tuned_ms", "tuned_variant")}
+        d = {n: getattr(inf, n) for n, _ in PlanInfo._fields_
+             if n not in ("tuned_ms", "tuned_variant", "norm_tiles", "norm_tuned_ms")}
+        d["norm_tiles"] = list(inf.norm_tiles)
+        d["norm_tuned_ms"] = list(inf.norm_tuned_ms)
         # autotuner record: ((row_bytes, tile_n, split), ms) per variant timed
         d["tuned"] = [(tuple(inf.tuned_variant[i]), inf.tuned_ms[i]) for i in range(inf.n_tuned)]
         return d

@@ -531,17 +531,24 @@ void sched_loop(b200d2_server* s) {
         ++it;
         continue;
       }
-      // merge later queued requests on the same reference into this one's
-      // run while the particle and request limits and the budget allow, and
-      // while the merged run fits an idle slot's buffer as it is (a merge
-      // never makes a slot grow, which maps memory while the queue waits)
+      // under a backlog (more queued requests than idle slots), merge later
+      // queued requests on the same reference into this one's run while the
+      // particle and request limits and the budget allow, and while the
+      // merged run fits an idle slot's buffer as it is (a merge never makes a
+      // slot grow, which maps memory while the queue waits).  Without a
+      // backlog every request gets a slot of its own: merging then would put
+      // work on one slot that idle slots could run beside it.
       std::vector<std::shared_ptr<Req>> grp;
       MergedLayout L;
       size_t idle_max = 0;
+      int idle = 0;
       for (int k = 0; k < s->slots; ++k)
-        if (!s->slot_busy[k]) idle_max = std::max(idle_max, s->dev_bytes[k]);
+        if (!s->slot_busy[k]) {
+          idle_max = std::max(idle_max, s->dev_bytes[k]);
+          ++idle;
+        }
       if (s->merge_requests > 1 && b200d2::is_tc_precision(s->prec) && q.r.P < s->merge_particles &&
-          q.footprint < idle_max) {
+          q.footprint < idle_max && (int)s->queue.size() > idle) {
         grp.push_back(*it);
         int P = q.r.P;
         for (auto jt = std::next(it); jt != s->queue.end() && (int)grp.size() < s->merge_requests; ++jt)

@@ -212,10 +212,13 @@ struct UnevenTabs {
   const float2* tab_txy;  // [ntab] translation of each phase table
   int ntab;
   int Mrows;
-  // merged batches (block-diagonal, no plan): per request, host
-  // (first particle, particles, first column, columns); plans have none
-  const int4* h_groups;
-  int ngroups;
+  // the norm kernel's work lists (64-, 32- and 16-particle tiles by 64
+  // orientations) over the particle order nperm (null: 0 .. P-1), and the
+  // list in use (-1: the first whose tiles give every SM a CTA)
+  const int2* ntile[3];
+  int nntile[3];
+  const int* nperm;
+  int nsel;
 };
 
 // Optional tables of an uneven batch; all null for a uniform batch.
@@ -771,10 +774,13 @@ template <int WM, int WN>
 __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* __restrict__ wcomp, int Kq,
                                                        const double* __restrict__ q, int O, int P,
                                                        const double* __restrict__ normx, double* na,
-                                                       float2* na_hl, int cc, long long ld) {
+                                                       float2* na_hl, int cc, long long ld,
+                                                       const int2* __restrict__ tiles,
+                                                       const int* __restrict__ pperm) {
   // Kq: row stride of wcomp and q, a multiple of 16, zero padded; ld: row
-  // stride of na and na_hl (O, or the merged batch's width for one request's
-  // block of it); the last
+  // stride of na and na_hl.  Uneven batches pass a work list `tiles` of
+  // (particle tile, orientation tile) pairs that some particle needs, one per
+  // CTA, with particle tiles over the order pperm (null: 0 .. P-1); the last
   // slab is zero-filled past Kq.  Shared rows padded to 36 doubles (288 B,
   // 16-byte aligned): the fragment loads of a half-warp (rows g, columns t,
   // g, t < 4) fall on distinct bank pairs 4g + t (mod 16).
@@ -786,7 +792,16 @@ __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* _
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gid = lane >> 2, tig = lane & 3;
   const int wp0 = (warp >> 1) * 8 * WM, wo0 = (warp & 1) * 8 * WN;
-  const int p0 = blockIdx.y * CP, o0 = blockIdx.x * CO;
+  int p0, o0;
+  if (tiles) {
+    const int2 tl = tiles[blockIdx.x];
+    p0 = tl.x * CP;
+    o0 = tl.y * CO;
+  } else {
+    p0 = blockIdx.y * CP;
+    o0 = blockIdx.x * CO;
+  }
+  auto prow = [&](int pl) { return pperm ? pperm[pl] : pl; };  // pl < P
   double acc[WM][WN][2];
 #pragma unroll
   for (int i = 0; i < WM; ++i)
@@ -799,7 +814,7 @@ __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* _
     for (int e = tid; e < CP * (KC / 2); e += NT) {
       const int pp = e / (KC / 2), k = 2 * (e % (KC / 2));
       const bool ok = p0 + pp < P && k0 + k < Kq;
-      cp_async16(dw + pp * LD + k, ok ? wcomp + (size_t)(p0 + pp) * Kq + k0 + k : wcomp, ok);
+      cp_async16(dw + pp * LD + k, ok ? wcomp + (size_t)prow(p0 + pp) * Kq + k0 + k : wcomp, ok);
     }
     for (int e = tid; e < CO * (KC / 2); e += NT) {
       const int oo = e / (KC / 2), k = 2 * (e % (KC / 2));
@@ -838,8 +853,9 @@ __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* _
   cp_async_wait<0>();
 #pragma unroll
   for (int i = 0; i < WM; ++i) {
-    const int p = p0 + wp0 + 8 * i + gid;
-    if (p >= P) continue;
+    const int pl = p0 + wp0 + 8 * i + gid;
+    if (pl >= P) continue;
+    const int p = prow(pl);
 #pragma unroll
     for (int j = 0; j < WN; ++j)
 #pragma unroll
@@ -863,14 +879,38 @@ __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* _
 
 template <int WM, int WN>
 static cudaError_t launch_norma(cudaStream_t s, const double* wcomp, int Kq, const double* q, int O, int P,
-                                const double* normx, double* na, float2* na_hl, int cc, long long ld) {
+                                const double* normx, double* na, float2* na_hl, int cc, long long ld,
+                                const int2* tiles = nullptr, int ntiles = 0, const int* pperm = nullptr) {
   static std::atomic<unsigned long long> opted{0};  // above 48 KB of dynamic shared memory
   const cudaError_t e = smem_opt_in(tc_norma_kernel<WM, WN>, (int)norma_smem_bytes<WM, WN>(), opted);
   if (e != cudaSuccess) return e;
-  const dim3 grid((O + 16 * WN - 1) / (16 * WN), (P + 16 * WM - 1) / (16 * WM));
+  const dim3 grid = tiles ? dim3(ntiles) : dim3((O + 16 * WN - 1) / (16 * WN), (P + 16 * WM - 1) / (16 * WM));
+  if (tiles && ntiles == 0) return cudaSuccess;
   tc_norma_kernel<WM, WN><<<grid, kNormaThreads, norma_smem_bytes<WM, WN>(), s>>>(wcomp, Kq, q, O, P, normx, na,
-                                                                                 na_hl, cc, ld);
+                                                                                 na_hl, cc, ld, tiles, pperm);
   return cudaSuccess;
+}
+
+// Work lists of the norm kernel for an uneven batch, one per particle-tile
+// height (64, 32, 16 particles; 64 orientations wide): the (particle tile,
+// orientation tile) pairs in which some particle of the tile needs some
+// column of the tile.  need(pl, blk) says whether the pl-th particle of the
+// order needs 128-column block blk.
+template <class Need>
+static void norma_lists(int P, int O, Need need, std::vector<int2> (&lists)[3]) {
+  const int nb = (O + 127) / 128, no = (O + 63) / 64;
+  for (int li = 0; li < 3; ++li) {
+    const int cp = 64 >> li;
+    lists[li].clear();
+    std::vector<char> un(nb);
+    for (int pt = 0; pt < (P + cp - 1) / cp; ++pt) {
+      std::fill(un.begin(), un.end(), 0);
+      for (int pl = pt * cp; pl < std::min(P, pt * cp + cp); ++pl)
+        for (int b = 0; b < nb; ++b) un[b] |= need(pl, b);
+      for (int ot = 0; ot < no; ++ot)
+        if (un[ot / 2]) lists[li].push_back(make_int2(pt, ot));
+    }
+  }
 }
 
 // ------------------------------------------------------------------ stage 5
@@ -2488,39 +2528,33 @@ static int launch_stage(const b200d2_view& v, const b200d2_batch& b, const TcGeo
       break;
     case 4: {
       // the largest tile (particles x orientations: 64 x 64, 32 x 64, 16 x 64,
-      // 16 x 32, 16 x 16) that still gives every SM a CTA.  A merged batch
-      // (block-diagonal) launches once per request: its particles against its
-      // own orientation columns, in place inside the batch-wide nA rows.
+      // 16 x 32, 16 x 16) that still gives every SM a CTA
       const int sms = num_sms();
       const int cc = b.score == B200D2_SCORE_CC;
-      const int nblk = (U && U->ngroups > 0) ? U->ngroups : 1;
-      for (int gi = 0; gi < nblk; ++gi) {
-        int p0 = 0, np = g.P, c0 = 0, no = g.O;
-        if (U && U->ngroups > 0) {
-          const int4 gr = U->h_groups[gi];  // first particle, particles, first column, columns
-          p0 = gr.x;
-          np = gr.y;
-          c0 = gr.z;
-          no = gr.w;
-        }
-        const double* w0 = wcomp + (size_t)p0 * g.Kq;
-        const double* q0 = q + (size_t)c0 * g.Kq;
-        const double* nx0 = normx + p0;
-        double* na0 = na + (size_t)p0 * g.O + c0;
-        float2* nh0 = na_hl + (size_t)p0 * g.O + c0;
-        auto ctas = [&](int cp, int co) { return (long long)((no + co - 1) / co) * ((np + cp - 1) / cp); };
-        if (ctas(64, 64) >= sms)
-          B200D2_CUDA_TRY((launch_norma<4, 4>(s, w0, g.Kq, q0, no, np, nx0, na0, nh0, cc, g.O)));
-        else if (ctas(32, 64) >= sms)
-          B200D2_CUDA_TRY((launch_norma<2, 4>(s, w0, g.Kq, q0, no, np, nx0, na0, nh0, cc, g.O)));
-        else if (ctas(16, 64) >= sms)
-          B200D2_CUDA_TRY((launch_norma<1, 4>(s, w0, g.Kq, q0, no, np, nx0, na0, nh0, cc, g.O)));
-        else if (ctas(16, 32) >= sms)
-          B200D2_CUDA_TRY((launch_norma<1, 2>(s, w0, g.Kq, q0, no, np, nx0, na0, nh0, cc, g.O)));
+      if (U && U->ntile[0]) {  // uneven batch: only the blocks some particle needs
+        const int li = U->nsel >= 0 ? U->nsel : U->nntile[0] >= sms ? 0 : U->nntile[1] >= sms ? 1 : 2;
+        if (li == 0)
+          B200D2_CUDA_TRY((launch_norma<4, 4>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc, g.O, U->ntile[0],
+                                              U->nntile[0], U->nperm)));
+        else if (li == 1)
+          B200D2_CUDA_TRY((launch_norma<2, 4>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc, g.O, U->ntile[1],
+                                              U->nntile[1], U->nperm)));
         else
-          B200D2_CUDA_TRY((launch_norma<1, 1>(s, w0, g.Kq, q0, no, np, nx0, na0, nh0, cc, g.O)));
-        if (gi + 1 < nblk) count_launch();
+          B200D2_CUDA_TRY((launch_norma<1, 4>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc, g.O, U->ntile[2],
+                                              U->nntile[2], U->nperm)));
+        break;
       }
+      auto ctas = [&](int cp, int co) { return (long long)((g.O + co - 1) / co) * ((g.P + cp - 1) / cp); };
+      if (ctas(64, 64) >= sms)
+        B200D2_CUDA_TRY((launch_norma<4, 4>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc, g.O)));
+      else if (ctas(32, 64) >= sms)
+        B200D2_CUDA_TRY((launch_norma<2, 4>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc, g.O)));
+      else if (ctas(16, 64) >= sms)
+        B200D2_CUDA_TRY((launch_norma<1, 4>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc, g.O)));
+      else if (ctas(16, 32) >= sms)
+        B200D2_CUDA_TRY((launch_norma<1, 2>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc, g.O)));
+      else
+        B200D2_CUDA_TRY((launch_norma<1, 1>(s, wcomp, g.Kq, q, g.O, g.P, normx, na, na_hl, cc, g.O)));
       break;
     }
     case 5: {
@@ -2875,6 +2909,8 @@ struct b200d2_plan {
   int2* d_tiles = nullptr;     // work list, 256-wide tiles
   int2* d_tiles128 = nullptr;  // work list, 128-wide tiles
   int2* d_tiles_pair = nullptr;  // work list, 256 x 256 tiles of CTA pairs
+  int2* d_ntile[3] = {nullptr, nullptr, nullptr};  // norm kernel work lists
+  int* d_nperm = nullptr;                         // particle order of their tiles
   float2* d_txy = nullptr;
   int* d_inv = nullptr;
   float* d_eul_perm = nullptr;
@@ -2892,7 +2928,8 @@ static void plan_free(b200d2_plan* p) {
   if (p->graph) cudaGraphDestroy(p->graph);
   if (p->stream) cudaStreamDestroy(p->stream);
   for (void* d : {(void*)p->ws, (void*)p->d_parts, (void*)p->d_rows, (void*)p->d_tiles, (void*)p->d_tiles128,
-                  (void*)p->d_tiles_pair, (void*)p->d_txy, (void*)p->d_inv, (void*)p->d_eul_perm})
+                  (void*)p->d_tiles_pair, (void*)p->d_ntile[0], (void*)p->d_ntile[1], (void*)p->d_ntile[2],
+                  (void*)p->d_nperm, (void*)p->d_txy, (void*)p->d_inv, (void*)p->d_eul_perm})
     if (d) cudaFree(d);
   delete p;
 }
@@ -2903,6 +2940,26 @@ static int plan_pipeline(b200d2_plan* p, cudaStream_t s, GemmVariant var) {
   for (int i = 0; i < kNumStages && st == B200D2_OK; ++i)
     st = dispatch_stage(p->view, p->batch, p->prec, p->g, p->ws, i, s, &p->U, var);
   return st;
+}
+
+// Best of `reps` timed launches of one stage of the plan (its own stream).
+static double time_stage(b200d2_plan* p, int stage, int reps) {
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  double best = 1e30;
+  for (int r = 0; r < reps + 1; ++r) {  // the first launch is not counted
+    cudaEventRecord(a, p->stream);
+    const int st = dispatch_stage(p->view, p->batch, p->prec, p->g, p->ws, stage, p->stream, &p->U, p->var);
+    cudaEventRecord(b, p->stream);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (st == B200D2_OK && r > 0) best = std::min(best, (double)ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return best;
 }
 
 static double time_gemm(b200d2_plan* p, GemmVariant var, int reps) {
@@ -3159,6 +3216,13 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   upload(reinterpret_cast<void**>(&p->d_tiles), tiles.data(), tiles.size() * sizeof(int2));
   upload(reinterpret_cast<void**>(&p->d_tiles128), tiles128.data(), tiles128.size() * sizeof(int2));
   upload(reinterpret_cast<void**>(&p->d_tiles_pair), tiles_pair.data(), tiles_pair.size() * sizeof(int2));
+  // the norm kernel's work lists, particle tiles in plan order (particles
+  // chained by the column blocks they need share tiles)
+  std::vector<int2> nlist[3];
+  norma_lists(P, O_all, [&](int pl, int blk) { return need_n[ord[pl]][blk]; }, nlist);
+  for (int li = 0; li < 3; ++li)
+    upload(reinterpret_cast<void**>(&p->d_ntile[li]), nlist[li].data(), nlist[li].size() * sizeof(int2));
+  upload(reinterpret_cast<void**>(&p->d_nperm), ord.data(), ord.size() * sizeof(int));
   upload(reinterpret_cast<void**>(&p->d_txy), txy.data(), txy.size() * sizeof(float2));
   upload(reinterpret_cast<void**>(&p->d_inv), inv.data(), inv.size() * sizeof(int));
   if (st == B200D2_OK)
@@ -3175,7 +3239,11 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
                     {(int)tiles.size(), (int)tiles128.size(), (int)tiles_pair.size()},
                     p->d_txy,
                     (int)txy.size(),
-                    Mrows};
+                    Mrows,
+                    {p->d_ntile[0], p->d_ntile[1], p->d_ntile[2]},
+                    {(int)nlist[0].size(), (int)nlist[1].size(), (int)nlist[2].size()},
+                    p->d_nperm,
+                    -1};
 
   memset(&p->info, 0, sizeof(p->info));
   p->info.P = P;
@@ -3187,9 +3255,12 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
   p->info.stages = kNumStages;
   p->info.tiles_n128 = (int)tiles128.size();
   p->info.tiles_pair = (int)tiles_pair.size();
+  for (int li = 0; li < 3; ++li) p->info.norm_tiles[li] = (int)nlist[li].size();
   p->info.workspace_bytes = p->g.total + rows.size() * sizeof(int4) +
                             (tiles.size() + tiles128.size() + tiles_pair.size()) * sizeof(int2) +
-                            txy.size() * sizeof(float2) + inv.size() * sizeof(int) + hp.size() * sizeof(PartDev);
+                            txy.size() * sizeof(float2) + inv.size() * sizeof(int) + hp.size() * sizeof(PartDev) +
+                            (nlist[0].size() + nlist[1].size() + nlist[2].size()) * sizeof(int2) +
+                            ord.size() * sizeof(int);
 
   // warm run (also sets kernel attributes outside any capture)
   // without the autotuner a plan takes the process-wide variant
@@ -3261,9 +3332,30 @@ extern "C" int b200d2_plan_create(const b200d2_view* view, const float* d_eulers
       std::lock_guard<std::mutex> lk(g_tune_mu);
       g_tune_cache[key] = p->var;
     }
+    // the norm stage's particle-tile height: smaller tiles skip more blocks
+    // that no particle of the tile needs, larger ones reuse more operands
+    if (st == B200D2_OK) {
+      double best = 1e30;
+      int best_li = -1;
+      for (int li = 0; li < 3 && st == B200D2_OK; ++li) {
+        p->U.nsel = li;
+        const double ms = time_stage(p, 4, 3);
+        p->info.norm_tuned_ms[li] = ms;
+        if (ms < best) {
+          best = ms;
+          best_li = li;
+        }
+      }
+      p->U.nsel = best_li;
+    }
     // leave the outputs as one full run with the chosen variant produces them
     st = plan_pipeline(p, p->stream, p->var);
     if (st == B200D2_OK) st = status_from_cuda(cudaStreamSynchronize(p->stream));
+  }
+  {
+    const int li = p->U.nsel >= 0 ? p->U.nsel
+                   : p->U.nntile[0] >= num_sms() ? 0 : p->U.nntile[1] >= num_sms() ? 1 : 2;
+    p->info.norm_tile_p = 64 >> li;
   }
   p->info.row_bytes = p->var.row_bytes;
   p->info.tile_n = p->var.bn;
@@ -3321,10 +3413,10 @@ extern "C" int b200d2_plan_destroy(b200d2_plan* p) {
 // nothing is allocated, timed or synchronised: the tables are built on the
 // host when the batch is created, and merged_enqueue copies them from the
 // caller's page-locked staging area into the caller's device memory and
-// launches the stages, all in the order of one stream.  The FP64 norms run
-// once per request (its block of particles x columns), so no request pays
-// for another's orientations there either; the contraction's work list
-// holds the (m tile, n tile) pairs that some row of the m tile needs.
+// launches the stages, all in the order of one stream.  The FP64 norms and
+// the contraction run over work lists of the blocks some particle needs
+// (particle tile x orientation tile, m tile x n tile), so no request pays
+// for another's orientations there either.
 namespace b200d2 {
 
 struct MergedBatch {
@@ -3332,16 +3424,18 @@ struct MergedBatch {
   int prec = 0, N_img = 0, n = 0, P = 0, O = 0;
   std::vector<MergedRequest> req;
   std::vector<int> part0;          // first particle of each request
-  std::vector<int4> rows, groups;  // groups: (first particle, particles, first column, columns)
+  std::vector<int4> rows;
   std::vector<int> row0;           // first row of each particle
   std::vector<int2> tiles[3];      // 128 x 256, 128 x 128, 256 x 256 (CTA pairs)
+  std::vector<int2> ntile[3];      // norm kernel work lists (64-, 32-, 16-particle tiles)
   std::vector<float2> txy;
   std::vector<int> inv;            // [n][O]
   TcGeom g;
   GemmVariant var;
   // device layout from the caller's base: the workspace, then the tables
   // (mirrored byte for byte by the staging area)
-  size_t off_tab = 0, off_parts = 0, off_rows = 0, off_tiles[3] = {0, 0, 0}, off_txy = 0, off_inv = 0, dev_bytes = 0;
+  size_t off_tab = 0, off_parts = 0, off_rows = 0, off_tiles[3] = {0, 0, 0}, off_ntile[3] = {0, 0, 0}, off_txy = 0,
+         off_inv = 0, dev_bytes = 0;
 };
 
 MergedBatch* merged_create(const b200d2_view& v, int N_img, int precision, const MergedRequest* r, int n, int O_cols,
@@ -3386,7 +3480,6 @@ MergedBatch* merged_create(const b200d2_view& v, int N_img, int precision, const
     }
     tab0[k] = it->second;
     m->part0.push_back(m->P);
-    m->groups.push_back(make_int4(m->P, q.P, q.col0, q.O));
     for (int i = 0; i < q.P; ++i) {
       m->row0.push_back((int)m->rows.size());
       req_of.push_back(k);
@@ -3416,6 +3509,13 @@ MergedBatch* merged_create(const b200d2_view& v, int N_img, int precision, const
     for (int c = 0; c < Ntiles128; ++c)
       if (un[c]) m->tiles[1].push_back(make_int2(mt, c));
   }
+  // the norm kernel's blocks: a particle tile needs its requests' columns
+  norma_lists(m->P, O_cols,
+              [&](int pl, int blk) {
+                const MergedRequest& q = r[req_of[pl]];
+                return blk >= q.col0 / 128 && blk <= (q.col0 + q.O - 1) / 128;
+              },
+              m->ntile);
   m->inv.assign((size_t)n * O_cols, -1);
   for (int k = 0; k < n; ++k)
     for (int o = 0; o < r[k].O; ++o) m->inv[(size_t)k * O_cols + r[k].col0 + o] = o;
@@ -3450,6 +3550,7 @@ MergedBatch* merged_create(const b200d2_view& v, int N_img, int precision, const
   m->off_parts = take(sizeof(PartDev) * (size_t)m->P);
   m->off_rows = take(sizeof(int4) * m->rows.size());
   for (int w = 0; w < 3; ++w) m->off_tiles[w] = take(sizeof(int2) * std::max<size_t>(m->tiles[w].size(), 1));
+  for (int w = 0; w < 3; ++w) m->off_ntile[w] = take(sizeof(int2) * std::max<size_t>(m->ntile[w].size(), 1));
   m->off_txy = take(sizeof(float2) * m->txy.size());
   m->off_inv = take(sizeof(int) * m->inv.size());
   m->dev_bytes = o;
@@ -3488,6 +3589,7 @@ int merged_enqueue(MergedBatch* m, const float* d_eulers, const MergedDev* d, do
   }
   memcpy(host(m->off_rows), m->rows.data(), sizeof(int4) * m->rows.size());
   for (int w = 0; w < 3; ++w) memcpy(host(m->off_tiles[w]), m->tiles[w].data(), sizeof(int2) * m->tiles[w].size());
+  for (int w = 0; w < 3; ++w) memcpy(host(m->off_ntile[w]), m->ntile[w].data(), sizeof(int2) * m->ntile[w].size());
   memcpy(host(m->off_txy), m->txy.data(), sizeof(float2) * m->txy.size());
   memcpy(host(m->off_inv), m->inv.data(), sizeof(int) * m->inv.size());
   B200D2_CUDA_TRY(cudaMemcpyAsync(dev + m->off_tab, hstage, m->dev_bytes - m->off_tab, cudaMemcpyHostToDevice, s));
@@ -3499,8 +3601,11 @@ int merged_enqueue(MergedBatch* m, const float* d_eulers, const MergedDev* d, do
                reinterpret_cast<const float2*>(dev + m->off_txy),
                (int)m->txy.size(),
                (int)m->rows.size(),
-               m->groups.data(),
-               m->n};
+               {reinterpret_cast<const int2*>(dev + m->off_ntile[0]), reinterpret_cast<const int2*>(dev + m->off_ntile[1]),
+                reinterpret_cast<const int2*>(dev + m->off_ntile[2])},
+               {(int)m->ntile[0].size(), (int)m->ntile[1].size(), (int)m->ntile[2].size()},
+               nullptr,
+               -1};
   b200d2_batch b;
   memset(&b, 0, sizeof(b));
   b.d_eulers = d_eulers;
