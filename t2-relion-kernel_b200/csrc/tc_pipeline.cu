@@ -770,7 +770,7 @@ constexpr size_t norma_smem_bytes() {
 }
 
 constexpr int kNormaThreads = 128;
-template <int WM, int WN>
+template <int WM, int WN, bool LIST>
 __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* __restrict__ wcomp, int Kq,
                                                        const double* __restrict__ q, int O, int P,
                                                        const double* __restrict__ normx, double* na,
@@ -793,7 +793,7 @@ __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* _
   const int gid = lane >> 2, tig = lane & 3;
   const int wp0 = (warp >> 1) * 8 * WM, wo0 = (warp & 1) * 8 * WN;
   int p0, o0;
-  if (tiles) {
+  if (LIST) {
     const int2 tl = tiles[blockIdx.x];
     p0 = tl.x * CP;
     o0 = tl.y * CO;
@@ -801,7 +801,7 @@ __global__ void __launch_bounds__(kNormaThreads) tc_norma_kernel(const double* _
     p0 = blockIdx.y * CP;
     o0 = blockIdx.x * CO;
   }
-  auto prow = [&](int pl) { return pperm ? pperm[pl] : pl; };  // pl < P
+  auto prow = [&](int pl) { return (LIST && pperm) ? pperm[pl] : pl; };  // pl < P
   double acc[WM][WN][2];
 #pragma unroll
   for (int i = 0; i < WM; ++i)
@@ -881,13 +881,21 @@ template <int WM, int WN>
 static cudaError_t launch_norma(cudaStream_t s, const double* wcomp, int Kq, const double* q, int O, int P,
                                 const double* normx, double* na, float2* na_hl, int cc, long long ld,
                                 const int2* tiles = nullptr, int ntiles = 0, const int* pperm = nullptr) {
-  static std::atomic<unsigned long long> opted{0};  // above 48 KB of dynamic shared memory
-  const cudaError_t e = smem_opt_in(tc_norma_kernel<WM, WN>, (int)norma_smem_bytes<WM, WN>(), opted);
+  // above 48 KB of dynamic shared memory, per device
+  static std::atomic<unsigned long long> opted{0}, opted_list{0};
+  if (tiles) {
+    const cudaError_t e = smem_opt_in(tc_norma_kernel<WM, WN, true>, (int)norma_smem_bytes<WM, WN>(), opted_list);
+    if (e != cudaSuccess) return e;
+    if (ntiles == 0) return cudaSuccess;
+    tc_norma_kernel<WM, WN, true><<<ntiles, kNormaThreads, norma_smem_bytes<WM, WN>(), s>>>(
+        wcomp, Kq, q, O, P, normx, na, na_hl, cc, ld, tiles, pperm);
+    return cudaSuccess;
+  }
+  const cudaError_t e = smem_opt_in(tc_norma_kernel<WM, WN, false>, (int)norma_smem_bytes<WM, WN>(), opted);
   if (e != cudaSuccess) return e;
-  const dim3 grid = tiles ? dim3(ntiles) : dim3((O + 16 * WN - 1) / (16 * WN), (P + 16 * WM - 1) / (16 * WM));
-  if (tiles && ntiles == 0) return cudaSuccess;
-  tc_norma_kernel<WM, WN><<<grid, kNormaThreads, norma_smem_bytes<WM, WN>(), s>>>(wcomp, Kq, q, O, P, normx, na,
-                                                                                 na_hl, cc, ld, tiles, pperm);
+  const dim3 grid((O + 16 * WN - 1) / (16 * WN), (P + 16 * WM - 1) / (16 * WM));
+  tc_norma_kernel<WM, WN, false><<<grid, kNormaThreads, norma_smem_bytes<WM, WN>(), s>>>(
+      wcomp, Kq, q, O, P, normx, na, na_hl, cc, ld, nullptr, nullptr);
   return cudaSuccess;
 }
 
@@ -3675,11 +3683,14 @@ int tc_preload(int precision) {
   get((const void*)tc_phase_compact_kernel);
   get((const void*)tc_scale_a_kernel);
   get((const void*)tc_normx_kernel);
-  get((const void*)tc_norma_kernel<4, 4>);
-  get((const void*)tc_norma_kernel<2, 4>);
-  get((const void*)tc_norma_kernel<1, 4>);
-  get((const void*)tc_norma_kernel<1, 2>);
-  get((const void*)tc_norma_kernel<1, 1>);
+  get((const void*)tc_norma_kernel<4, 4, false>);
+  get((const void*)tc_norma_kernel<2, 4, false>);
+  get((const void*)tc_norma_kernel<1, 4, false>);
+  get((const void*)tc_norma_kernel<1, 2, false>);
+  get((const void*)tc_norma_kernel<1, 1, false>);
+  get((const void*)tc_norma_kernel<4, 4, true>);
+  get((const void*)tc_norma_kernel<2, 4, true>);
+  get((const void*)tc_norma_kernel<1, 4, true>);
   get((const void*)tc_finalize_kernel);
   if (e != cudaSuccess) return status_from_cuda(e);
   switch (precision) {
