@@ -1459,7 +1459,7 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
                 for tk, _ in [submit(heavy) for _ in range(slots)]:
                     srv.wait(tk)
         if merge:
-            srv.set_merging(8, 512)
+            srv.set_merging(8, 512, 128)
         st0 = srv.stats()
         admit0, stream0 = st0["admit_host_s"], st0["stream_s"]
         t0 = time.perf_counter()
@@ -1493,6 +1493,8 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
                 "peak_bytes": stats["peak_bytes"], "admit_host_s_per_s": (stats["admit_host_s"] - admit0) / span,
                 # merged admissions of the trace (the warm-up has none) and the requests they carried
                 "merged_admissions": stats["merged_admissions"], "merged_requests": stats["merged_requests"],
+                # longest scheduler-thread time of one admission over the whole run, warm-up included
+                "admit_host_max_ms": stats["admit_host_max_s"] * 1e3,
                 # each admission's stream time (first copy in to last copy out; a merged
                 # admission once) summed, per second of the run
                 "device_s_per_s": (stats["stream_s"] - stream0) / span,

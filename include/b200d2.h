@@ -377,6 +377,7 @@ typedef struct b200d2_server_stats {
   long long merged_admissions, merged_requests;
   double stream_s; /* slot-stream time of the completed admissions (first copy in to
                       last copy out; a merged admission counted once) */
+  double admit_host_max_s; /* longest scheduler-thread time of one admission */
 } b200d2_server_stats;
 
 /* slots: concurrent streams; hbm_budget_bytes: device bytes the in-flight
@@ -406,7 +407,8 @@ int b200d2_server_get_stats(b200d2_server* s, b200d2_server_stats* st);
 /* Merged admissions.  When a slot frees up while more requests are queued
  * than slots are idle, the scheduler runs the first queued request that fits
  * together with later queued requests on the same reference (arrival order),
- * up to max_requests requests and max_particles
+ * each of at most max_request_particles particles (a larger request fills
+ * the GPU on its own), up to max_requests requests and max_particles
  * particles in all, as one batch: one copy-in, one pipeline run and one
  * copy-out on one slot, instead of a pipeline per request, when the merged
  * run fits the buffer an idle slot already holds (a merge never grows a
@@ -416,8 +418,9 @@ int b200d2_server_get_stats(b200d2_server* s, b200d2_server_stats* st);
  * another's, and each result equals the request's result alone (same
  * kernels, same sums).  The merged requests complete together.  Tensor-core
  * servers only; max_requests = 1 turns merging off.  Default: 8 requests,
- * 512 particles. */
-int b200d2_server_set_merging(b200d2_server* s, int max_requests, int max_particles);
+ * 512 particles, 128 particles per request. */
+int b200d2_server_set_merging(b200d2_server* s, int max_requests, int max_particles,
+                              int max_request_particles);
 /* Cancel a queued request: it will not run, and b200d2_server_wait returns
  * B200D2_ERR_CANCELLED for it.  B200D2_ERR_UNSUPPORTED when the request has
  * been admitted already (work on the GPU is not interrupted; wait for it),

@@ -109,7 +109,7 @@ class ServerStats(C.Structure):
                 ("evals", C.c_longlong), ("in_flight", C.c_int), ("queued", C.c_int), ("max_in_flight", C.c_int),
                 ("bytes_in_use", C.c_size_t), ("peak_bytes", C.c_size_t), ("admit_host_s", C.c_double),
                 ("cancelled", C.c_longlong), ("merged_admissions", C.c_longlong), ("merged_requests", C.c_longlong),
-                ("stream_s", C.c_double)]
+                ("stream_s", C.c_double), ("admit_host_max_s", C.c_double)]
 
 
 # status codes (b200d2_status)
@@ -165,7 +165,7 @@ def _declare(L):
         "b200d2_server_wait": [P, C.c_longlong, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)],
         "b200d2_server_get_stats": [P, C.POINTER(ServerStats)],
         "b200d2_server_cancel": [P, C.c_longlong],
-        "b200d2_server_set_merging": [P, I, I],
+        "b200d2_server_set_merging": [P, I, I, I],
         "b200d2_server_destroy": [P],
         "b200d2_coarse_weights": [P, I, I, I, P, P, P, I, P, P, P, Z, P],
         "b200d2_significance": [P, I, C.c_longlong, P, C.c_double, C.c_longlong, P, P, P, P, Z, P],
@@ -467,10 +467,11 @@ class Server:
         self._keep.pop(ticket, None)
         return st, lat.value, dev.value
 
-    def set_merging(self, max_requests: int = 8, max_particles: int = 512):
+    def set_merging(self, max_requests: int = 8, max_particles: int = 512, max_request_particles: int = 128):
         """Merged admissions (b200d2_server_set_merging): queued requests on one
         reference run as one block-diagonal batch; max_requests=1 turns it off."""
-        _check(lib().b200d2_server_set_merging(self._h, max_requests, max_particles), "server_set_merging")
+        _check(lib().b200d2_server_set_merging(self._h, max_requests, max_particles, max_request_particles),
+               "server_set_merging")
 
     def cancel(self, ticket: int) -> int:
         """Cancel a queued request (b200d2_server_cancel): 0, or the status code

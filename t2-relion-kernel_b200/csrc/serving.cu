@@ -103,6 +103,7 @@ struct b200d2_server {
   // merged admissions (b200d2_server_set_merging): queued requests on one
   // reference run as one batch, at most this many requests and particles
   int merge_requests = 8, merge_particles = 512;
+  int merge_request_particles = 128;  // only requests this small are merged
 };
 
 namespace {
@@ -538,6 +539,7 @@ void sched_loop(b200d2_server* s) {
       // slot grow, which maps memory while the queue waits).  Without a
       // backlog every request gets a slot of its own: merging then would put
       // work on one slot that idle slots could run beside it.
+      const double t_merge = now_s();  // the merge decision counts as admission time
       std::vector<std::shared_ptr<Req>> grp;
       MergedLayout L;
       size_t idle_max = 0;
@@ -547,22 +549,26 @@ void sched_loop(b200d2_server* s) {
           idle_max = std::max(idle_max, s->dev_bytes[k]);
           ++idle;
         }
-      if (s->merge_requests > 1 && b200d2::is_tc_precision(s->prec) && q.r.P < s->merge_particles &&
+      // Only small requests are merged: a large one fills the GPU with its
+      // own pipeline, and bundling it would hold the others until it ends.
+      const int small = std::min(s->merge_request_particles, s->merge_particles);
+      if (s->merge_requests > 1 && b200d2::is_tc_precision(s->prec) && q.r.P <= small &&
           q.footprint < idle_max && (int)s->queue.size() > idle) {
         grp.push_back(*it);
         int P = q.r.P;
         for (auto jt = std::next(it); jt != s->queue.end() && (int)grp.size() < s->merge_requests; ++jt)
-          if ((*jt)->r.ref == q.r.ref && P + (*jt)->r.P <= s->merge_particles) {
+          if ((*jt)->r.ref == q.r.ref && (*jt)->r.P <= small && P + (*jt)->r.P <= s->merge_particles) {
             grp.push_back(*jt);
             P += (*jt)->r.P;
           }
+        // a group that does not fit is halved (its tables are built once per try)
         while (grp.size() > 1) {
           if (merged_layout(s, grp, L) == B200D2_OK && s->st.bytes_in_use + L.footprint <= s->budget &&
               L.footprint <= idle_max)
             break;
           b200d2::merged_destroy(L.mb);
           L.mb = nullptr;
-          grp.pop_back();
+          grp.resize(grp.size() / 2);
         }
         if (grp.size() < 2) grp.clear();
       }
@@ -591,6 +597,7 @@ void sched_loop(b200d2_server* s) {
         const double t_admit = now_s();
         const int rc = admit_merged(s, q, grp, L);
         s->st.admit_host_s += now_s() - t_admit;
+        s->st.admit_host_max_s = std::max(s->st.admit_host_max_s, now_s() - t_merge);
         b200d2::merged_destroy(L.mb);
         if (rc != B200D2_OK && !q.finished.load()) {
           q.status = rc;
@@ -619,6 +626,7 @@ void sched_loop(b200d2_server* s) {
       const double t_admit = now_s();
       const int rc = admit(s, q);
       s->st.admit_host_s += now_s() - t_admit;
+      s->st.admit_host_max_s = std::max(s->st.admit_host_max_s, now_s() - t_admit);
       if (rc != B200D2_OK && !q.finished.load()) {
         // nothing was left on the stream that would signal completion
         q.status = rc;
@@ -703,6 +711,10 @@ extern "C" int b200d2_server_create(int slots, size_t hbm_budget_bytes, int prec
   // load every kernel the requests can launch now: a kernel loaded at its
   // first launch (lazy module loading) can wait for the slots' running work
   if (b200d2::is_tc_precision(precision) && b200d2::tc_preload(precision) != B200D2_OK) cudaGetLastError();
+  // page-locked staging buffers of a first size, so that small requests and
+  // merged tables do not pin memory while the queue waits
+  for (int k = 0; k < slots; ++k) slot_staging(s, k, (size_t)8 << 20);
+  cudaGetLastError();
   s->sched = std::thread(sched_loop, s);
   *out = s;
   return B200D2_OK;
@@ -818,11 +830,13 @@ extern "C" int b200d2_server_cancel(b200d2_server* s, long long ticket) {
   return B200D2_OK;
 }
 
-extern "C" int b200d2_server_set_merging(b200d2_server* s, int max_requests, int max_particles) {
-  if (!s || max_requests < 1 || max_particles < 1) return B200D2_ERR_INVALID;
+extern "C" int b200d2_server_set_merging(b200d2_server* s, int max_requests, int max_particles,
+                                         int max_request_particles) {
+  if (!s || max_requests < 1 || max_particles < 1 || max_request_particles < 1) return B200D2_ERR_INVALID;
   std::lock_guard<std::mutex> lk(s->mu);
   s->merge_requests = max_requests;
   s->merge_particles = max_particles;
+  s->merge_request_particles = max_request_particles;
   return B200D2_OK;
 }
 
