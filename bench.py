@@ -243,6 +243,7 @@ def parse():
     ap.add_argument("--serve-seconds-default", type=float, default=2.0,
                     help="length of the serving trace run beside the default bench line")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving trace of the default line")
+    ap.add_argument("--serve-slots", type=int, default=4, help="c5: stream slots of the server")
     ap.add_argument("--serve-fp32-seconds", type=float, default=0.5,
                     help="c5: part of the trace replayed through the FP32 baseline")
     ap.add_argument("--operand-gen", type=int, default=0, choices=[0, 1],
@@ -936,7 +937,7 @@ def ours_arm(args):
 
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
-        serving = serving_trace(pkg, synth, args.serve_seconds_default, args.serve_fp32_seconds)
+        serving = serving_trace(pkg, synth, args.serve_seconds_default, args.serve_fp32_seconds, args.serve_slots)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1384,7 +1385,7 @@ def cc_study(args):
 C5_REFS = ("c5s", "c5m", "c5l")
 
 
-def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
+def serving_trace(pkg, synth, horizon: float, fp32_seconds: float, slots: int = 4) -> dict:
     """Serving loop (config c5): Poisson arrivals at 200 requests/s over three
     resident references (coarse sizes 48 / 64 / 96); each request scores a
     contiguous run of 16-512 particles (log-uniform) from the reference's
@@ -1493,8 +1494,11 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
                 "peak_bytes": stats["peak_bytes"], "admit_host_s_per_s": (stats["admit_host_s"] - admit0) / span,
                 # merged admissions of the trace (the warm-up has none) and the requests they carried
                 "merged_admissions": stats["merged_admissions"], "merged_requests": stats["merged_requests"],
-                # longest scheduler-thread time of one admission over the whole run, warm-up included
+                # longest scheduler-thread time of one admission during the trace (the maxima
+                # restart at the stats read after the warm-up), and of its buffer and launch phases
                 "admit_host_max_ms": stats["admit_host_max_s"] * 1e3,
+                "admit_grow_max_ms": stats["admit_grow_max_s"] * 1e3,
+                "admit_launch_max_ms": stats["admit_launch_max_s"] * 1e3,
                 # each admission's stream time (first copy in to last copy out; a merged
                 # admission once) summed, per second of the run
                 "device_s_per_s": (stats["stream_s"] - stream0) / span,
@@ -1502,13 +1506,13 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
                              "P": p_, "O": o_, "T": t_} for a, b, c, r, p_, o_, t_ in sorted(slow)[-5:]]}
 
     try:
-        tc = replay(pkg.PREC_TF32, 4, 48 << 30, horizon)
+        tc = replay(pkg.PREC_TF32, slots, 48 << 30, horizon)
         # capacity: the same requests submitted back to back, so that the
         # queue never empties and evals/s measures the server, not the offered
         # load (latencies then include the queueing of the whole burst)
-        sat = replay(pkg.PREC_TF32, 4, 48 << 30, horizon, burst=True)
+        sat = replay(pkg.PREC_TF32, slots, 48 << 30, horizon, burst=True)
         # the same burst with one request per admission (merging off)
-        sat1 = replay(pkg.PREC_TF32, 4, 48 << 30, horizon, burst=True, merge=False)
+        sat1 = replay(pkg.PREC_TF32, slots, 48 << 30, horizon, burst=True, merge=False)
         # the FP32 baseline cannot keep up with 200 requests/s; replay the
         # first part of the same trace so the run stays bounded
         fp32 = replay(pkg.PREC_FP32, 1, 48 << 30, min(horizon, fp32_seconds))
@@ -1519,7 +1523,7 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float) -> dict:
                         f"3 resident references (image 48/64/96, 4608 orientations), 16-512 "
                         f"particles per request, 10-100 % orientation subsets, translation radius "
                         f"2-6 px, outputs: per-particle min/argmin",
-            "slots": 4, "hbm_budget_gib": 48, "trace_evals": evals,
+            "slots": slots, "hbm_budget_gib": 48, "trace_evals": evals,
             "tensor_core_tf32": tc, "tensor_core_tf32_saturated": sat,
             "tensor_core_tf32_saturated_unmerged": sat1, "fp32_cuda_core_per_request": fp32,
             "evals_per_s_ratio": tc["evals_per_s"] / fp32["evals_per_s"]}
@@ -1531,7 +1535,7 @@ def serving_arm(args):
     pkg = load_package()
     synth = load_synth()
     torch.cuda.set_device(0)
-    r = serving_trace(pkg, synth, args.serve_seconds, args.serve_fp32_seconds)
+    r = serving_trace(pkg, synth, args.serve_seconds, args.serve_fp32_seconds, args.serve_slots)
     tc = r["tensor_core_tf32"]
     line = {"metric": "p99 request latency (coarse-pass serving)", "value": tc["p99_ms"], "unit": "ms",
             "n_gpus": 1, "higher_is_better": False, "dtype": "tf32", "data": "synthetic",

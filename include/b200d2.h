@@ -377,7 +377,11 @@ typedef struct b200d2_server_stats {
   long long merged_admissions, merged_requests;
   double stream_s; /* slot-stream time of the completed admissions (first copy in to
                       last copy out; a merged admission counted once) */
-  double admit_host_max_s; /* longest scheduler-thread time of one admission */
+  /* longest scheduler-thread time of one admission, and of two of its
+   * phases: the slot's device buffer (growth maps memory) and the launch of
+   * the request's work; each covers the time since the previous
+   * b200d2_server_get_stats, which resets them */
+  double admit_host_max_s, admit_grow_max_s, admit_launch_max_s;
 } b200d2_server_stats;
 
 /* slots: concurrent streams; hbm_budget_bytes: device bytes the in-flight

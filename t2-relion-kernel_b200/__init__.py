@@ -109,7 +109,8 @@ class ServerStats(C.Structure):
                 ("evals", C.c_longlong), ("in_flight", C.c_int), ("queued", C.c_int), ("max_in_flight", C.c_int),
                 ("bytes_in_use", C.c_size_t), ("peak_bytes", C.c_size_t), ("admit_host_s", C.c_double),
                 ("cancelled", C.c_longlong), ("merged_admissions", C.c_longlong), ("merged_requests", C.c_longlong),
-                ("stream_s", C.c_double), ("admit_host_max_s", C.c_double)]
+                ("stream_s", C.c_double), ("admit_host_max_s", C.c_double), ("admit_grow_max_s", C.c_double),
+                ("admit_launch_max_s", C.c_double)]
 
 
 # status codes (b200d2_status)

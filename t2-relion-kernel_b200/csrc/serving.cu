@@ -248,7 +248,9 @@ int admit(b200d2_server* s, Req& q) {
   uint8_t* pin = static_cast<uint8_t*>(slot_staging(s, q.slot, pin_need));
   if (pin_need && !pin) return B200D2_ERR_OOM;
   q.out_copies.clear();
+  const double t_grow = now_s();
   q.dbuf = slot_device(s, q.slot, q.footprint);
+  s->st.admit_grow_max_s = std::max(s->st.admit_grow_max_s, now_s() - t_grow);
   if (!q.dbuf) return B200D2_ERR_OOM;
   uint8_t* d = static_cast<uint8_t*>(q.dbuf);
   // the first failure among the copies and event records; the request still
@@ -283,7 +285,9 @@ int admit(b200d2_server* s, Req& q) {
   b.accumulate = 0;
   b.d_min = reinterpret_cast<double*>(d + o_mn);
   b.d_argmin = reinterpret_cast<long long*>(d + o_am);
+  const double t_run = now_s();
   int rc = b200d2_diff2_coarse_batch(&ref.view, &b, s->prec, q.ws_bytes ? d + o_ws : nullptr, q.ws_bytes, st);
+  s->st.admit_launch_max_s = std::max(s->st.admit_launch_max_s, now_s() - t_run);
   for (const Down& w : downs) {
     if (!w.dst) continue;
     if (w.staged) {
@@ -423,7 +427,9 @@ int admit_merged(b200d2_server* s, Req& lead, const std::vector<std::shared_ptr<
   uint8_t* pin = static_cast<uint8_t*>(slot_staging(s, lead.slot, pin_need));
   if (!pin) return B200D2_ERR_OOM;
   lead.out_copies.clear();
+  const double t_grow = now_s();
   lead.dbuf = slot_device(s, lead.slot, lead.footprint);
+  s->st.admit_grow_max_s = std::max(s->st.admit_grow_max_s, now_s() - t_grow);
   if (!lead.dbuf) return B200D2_ERR_OOM;
   uint8_t* d = static_cast<uint8_t*>(lead.dbuf);
   // the merged orientations: each request's Euler matrices at its columns;
@@ -458,9 +464,11 @@ int admit_merged(b200d2_server* s, Req& lead, const std::vector<std::shared_ptr<
     md[k].corr = reinterpret_cast<const float*>(d + o_in[k] + 2 * img);
     md[k].out = reinterpret_cast<float*>(d + o_out[k]);
   }
+  const double t_run = now_s();
   int rc = b200d2::merged_enqueue(L.mb, reinterpret_cast<const float*>(d + o_eu), md.data(),
                                   reinterpret_cast<double*>(d + o_mn), reinterpret_cast<long long*>(d + o_am),
                                   d + o_mb, pin + p_tab, st);
+  s->st.admit_launch_max_s = std::max(s->st.admit_launch_max_s, now_s() - t_run);
   for (const Down& w : downs) {
     if (w.staged) {
       note(cudaMemcpyAsync(pin + w.pin_off, d + w.dev_off, w.bytes, cudaMemcpyDeviceToHost, st));
@@ -844,6 +852,8 @@ extern "C" int b200d2_server_get_stats(b200d2_server* s, b200d2_server_stats* st
   if (!s || !st) return B200D2_ERR_INVALID;
   std::lock_guard<std::mutex> lk(s->mu);
   *st = s->st;
+  // the maxima cover the time since the previous read
+  s->st.admit_host_max_s = s->st.admit_grow_max_s = s->st.admit_launch_max_s = 0.0;
   return B200D2_OK;
 }
 
