@@ -1499,6 +1499,10 @@ def serving_trace(pkg, synth, horizon: float, fp32_seconds: float, slots: int = 
                 "admit_host_max_ms": stats["admit_host_max_s"] * 1e3,
                 "admit_grow_max_ms": stats["admit_grow_max_s"] * 1e3,
                 "admit_launch_max_ms": stats["admit_launch_max_s"] * 1e3,
+                # where the slowest latencies went: longest wait for admission, and
+                # longest time from admission to completion beyond the stream time
+                "queue_wait_max_ms": stats["queue_wait_max_s"] * 1e3,
+                "done_lag_max_ms": stats["done_lag_max_s"] * 1e3,
                 # each admission's stream time (first copy in to last copy out; a merged
                 # admission once) summed, per second of the run
                 "device_s_per_s": (stats["stream_s"] - stream0) / span,

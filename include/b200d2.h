@@ -382,6 +382,10 @@ typedef struct b200d2_server_stats {
    * the request's work; each covers the time since the previous
    * b200d2_server_get_stats, which resets them */
   double admit_host_max_s, admit_grow_max_s, admit_launch_max_s;
+  /* since the previous read as well: the longest wait of a request from
+   * submission to admission, and the longest time from an admission to its
+   * completion callback beyond its stream time */
+  double queue_wait_max_s, done_lag_max_s;
 } b200d2_server_stats;
 
 /* slots: concurrent streams; hbm_budget_bytes: device bytes the in-flight

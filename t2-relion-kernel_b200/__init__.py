@@ -110,7 +110,7 @@ class ServerStats(C.Structure):
                 ("bytes_in_use", C.c_size_t), ("peak_bytes", C.c_size_t), ("admit_host_s", C.c_double),
                 ("cancelled", C.c_longlong), ("merged_admissions", C.c_longlong), ("merged_requests", C.c_longlong),
                 ("stream_s", C.c_double), ("admit_host_max_s", C.c_double), ("admit_grow_max_s", C.c_double),
-                ("admit_launch_max_s", C.c_double)]
+                ("admit_launch_max_s", C.c_double), ("queue_wait_max_s", C.c_double), ("done_lag_max_s", C.c_double)]
 
 
 # status codes (b200d2_status)

@@ -61,7 +61,7 @@ struct Req {
   std::vector<HostCopy> out_copies;
   size_t ws_bytes = 0, footprint = 0;
   int status = -1;  // -1 pending, else a b200d2_status
-  double t_submit = 0, t_done = 0, device_s = 0;
+  double t_submit = 0, t_done = 0, device_s = 0, t_admit = 0;
   int slot = -1;
   void* dbuf = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -500,6 +500,14 @@ void sched_loop(b200d2_server* s) {
         if (q.timed && cudaEventElapsedTime(&ms, q.ev0, q.ev1) == cudaSuccess) q.device_s = ms / 1e3;
         cudaGetLastError();
         if (q.status == -1) q.status = B200D2_OK;
+        if (q.timed) {
+          // where a request's latency went: waiting for admission, and the
+          // time from admission to its completion callback beyond its stream time
+          s->st.queue_wait_max_s = std::max(s->st.queue_wait_max_s, q.t_admit - q.t_submit);
+          s->st.done_lag_max_s = std::max(s->st.done_lag_max_s, q.t_done - q.t_admit - q.device_s);
+          for (const std::shared_ptr<Req>& m : q.members)
+            s->st.queue_wait_max_s = std::max(s->st.queue_wait_max_s, q.t_admit - m->t_submit);
+        }
         s->slot_busy[q.slot] = 0;
         s->st.bytes_in_use -= q.footprint;
         s->st.stream_s += q.device_s;
@@ -603,6 +611,7 @@ void sched_loop(b200d2_server* s) {
           q.members.push_back(grp[k]);
         }
         const double t_admit = now_s();
+        q.t_admit = t_admit;
         const int rc = admit_merged(s, q, grp, L);
         s->st.admit_host_s += now_s() - t_admit;
         s->st.admit_host_max_s = std::max(s->st.admit_host_max_s, now_s() - t_merge);
@@ -632,6 +641,7 @@ void sched_loop(b200d2_server* s) {
       s->st.bytes_in_use += q.footprint;
       s->st.peak_bytes = std::max(s->st.peak_bytes, s->st.bytes_in_use);
       const double t_admit = now_s();
+      q.t_admit = t_admit;
       const int rc = admit(s, q);
       s->st.admit_host_s += now_s() - t_admit;
       s->st.admit_host_max_s = std::max(s->st.admit_host_max_s, now_s() - t_admit);
@@ -854,6 +864,7 @@ extern "C" int b200d2_server_get_stats(b200d2_server* s, b200d2_server_stats* st
   *st = s->st;
   // the maxima cover the time since the previous read
   s->st.admit_host_max_s = s->st.admit_grow_max_s = s->st.admit_launch_max_s = 0.0;
+  s->st.queue_wait_max_s = s->st.done_lag_max_s = 0.0;
   return B200D2_OK;
 }
 
